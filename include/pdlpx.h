@@ -1,0 +1,277 @@
+/*
+ * pdlpx.h -- C ABI of the B200-native PDLP engine (drop-in for mipx's PDLP path).
+ *
+ * Every entry point is plain C: opaque handles, plain pointers and sizes, int32
+ * error codes (PDLPX_OK == 0), no exceptions and no torch types.  Caller buffers
+ * are copied on entry (the same ownership rule as mipx::PdlpSolver::load, which
+ * copies the LpProblem, src/lp/pdlp.cpp:445-455); outputs are written into
+ * caller-provided host buffers.
+ *
+ * Reference interface each group replaces (paths inside spoorendonk/mipx):
+ *   pdlpx_options            <- mipx::PdlpOptions            include/mipx/pdlp.h:19-87
+ *   pdlpx_result             <- mipx::LpResult               include/mipx/lp_solver.h:11-16
+ *   status codes             <- mipx::Status                 include/mipx/core.h:11-19
+ *   pdlpx_create/destroy     <- PdlpSolver ctor/dtor          include/mipx/pdlp.h:89-92
+ *   pdlpx_set_options        <- PdlpSolver::setOptions        include/mipx/pdlp.h:122
+ *   pdlpx_load_csr           <- PdlpSolver::load(LpProblem)   include/mipx/pdlp.h:94, src/lp/pdlp.cpp:445-455
+ *   pdlpx_solve              <- PdlpSolver::solve             include/mipx/pdlp.h:95, src/lp/pdlp.cpp:801-1720
+ *   pdlpx_get_primal/dual    <- getPrimalValues/getDualValues include/mipx/pdlp.h:100-101, src/lp/pdlp.cpp:2800-2806
+ *   pdlpx_get_reduced_costs  <- getReducedCosts               src/lp/pdlp.cpp:2808-2819
+ *   pdlpx_set_warm_start     <- setWarmStart/clearWarmStart   include/mipx/pdlp.h:114-120
+ *   pdlpx_set_stop_flag      <- PdlpOptions::stop_flag        include/mipx/pdlp.h:86
+ *   pdlpx_add_rows ...       <- addRows/removeRows/setColBounds/setObjective  src/lp/pdlp.cpp:2833-2907
+ *   pdlpx_used_gpu           <- PdlpSolver::usedGpu           include/mipx/pdlp.h:124
+ */
+#ifndef PDLPX_H
+#define PDLPX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status of a solve: same values and order as mipx::Status (core.h:11-19) ---- */
+enum {
+    PDLPX_STATUS_OPTIMAL = 0,
+    PDLPX_STATUS_INFEASIBLE = 1,
+    PDLPX_STATUS_UNBOUNDED = 2,
+    PDLPX_STATUS_ITER_LIMIT = 3,
+    PDLPX_STATUS_TIME_LIMIT = 4,
+    PDLPX_STATUS_NODE_LIMIT = 5,
+    PDLPX_STATUS_ERROR = 6
+};
+
+/* ---- error codes returned by every call ---- */
+enum {
+    PDLPX_OK = 0,
+    PDLPX_E_INVALID = 1,     /* bad argument (null pointer, size mismatch, bad CSR) */
+    PDLPX_E_NOT_LOADED = 2,  /* solve/get before load */
+    PDLPX_E_CUDA = 3,        /* a CUDA runtime call failed; see pdlpx_last_error */
+    PDLPX_E_NOMEM = 4,       /* device allocation failed */
+    PDLPX_E_NO_DEVICE = 5,   /* no CUDA device visible */
+    PDLPX_E_TIMEOUT = 6,     /* a bounded device wait ran out */
+    PDLPX_E_BUSY = 7,        /* server queue full / over HBM budget */
+    PDLPX_E_UNKNOWN_TICKET = 8
+};
+
+enum { PDLPX_NORM_L2 = 0, PDLPX_NORM_LINF = 1 };
+enum { PDLPX_MINIMIZE = 0, PDLPX_MAXIMIZE = 1 };
+
+/* Precision modes of the engine (no counterpart in the reference, which is FP64 only). */
+enum {
+    PDLPX_PREC_MIXED = 0, /* FP32 matrix/iterates/SpMV, FP64 checks, PI, objective, FP64 polish */
+    PDLPX_PREC_FP64 = 1   /* FP64 throughout ("plain FP64 GPU" mode) */
+};
+
+/* Field-for-field image of mipx::PdlpOptions (include/mipx/pdlp.h:19-87) plus engine knobs.
+ * Booleans are int32 (0/1).  Call pdlpx_options_default() to get the reference defaults. */
+typedef struct pdlpx_options {
+    int32_t max_iter;                 /* 4000000 */
+    double optimality_tol;            /* 5e-5 (relative gap) */
+    double primal_tol;                /* 5e-5 */
+    double dual_tol;                  /* 5e-5 */
+    double max_solve_seconds;         /* -1 = no limit */
+    int32_t optimality_norm;          /* PDLPX_NORM_L2 */
+    int32_t sv_max_iter;              /* 5000 power iterations */
+    double sv_tol;                    /* 1e-4 */
+    int32_t adaptive_step;            /* 0 */
+    double adaptive_step_down;        /* 0.7 */
+    double adaptive_step_up;          /* 1.0 */
+    double adaptive_step_min;         /* 1e-6 */
+    double adaptive_step_max;         /* 1e3 */
+    double primal_weight;             /* 1.0 */
+    int32_t update_primal_weight;     /* 1 */
+    double pid_kp;                    /* 0.99 */
+    double pid_ki;                    /* 0.01 */
+    double pid_kd;                    /* 0.0 */
+    double pid_i_smooth;              /* 0.3 */
+    double restart_sufficient_decay;  /* 0.2 */
+    double restart_necessary_decay;   /* 0.5 */
+    double restart_artificial_fraction; /* 0.36 */
+    int32_t termination_eval_frequency; /* 200 */
+    double matrix_zero_tol;           /* 0 = off */
+    int32_t enable_polishing;         /* 1 */
+    double polish_primal_tol;         /* 1e-6 */
+    double polish_dual_tol;           /* 1e-6 */
+    int32_t polish_max_iter;          /* 500000 */
+    int32_t do_ruiz_scaling;          /* 1 */
+    int32_t ruiz_iterations;          /* 10 */
+    int32_t do_pock_chambolle_scaling;/* 1 */
+    int32_t do_bound_obj_rescaling;   /* 1 */
+    int32_t preconditioner_refresh;   /* 0 */
+    double preconditioner_refresh_ratio; /* 10 */
+    int32_t anderson_acceleration;    /* 0 */
+    int32_t anderson_window_size;     /* 5 */
+    double anderson_regularization;   /* 1e-10 */
+    int32_t use_gpu;                  /* 1 */
+    int32_t gpu_min_rows;             /* 512 (the engine always runs on the GPU; kept for parity of the struct) */
+    int32_t gpu_min_nnz;              /* 10000 */
+    int32_t verbose;                  /* 1 in the reference; the engine prints the same progress lines */
+    /* ---- engine knobs (no counterpart in the reference) ---- */
+    int32_t precision;                /* PDLPX_PREC_MIXED */
+    int32_t device;                   /* CUDA device ordinal, default 0 */
+    int32_t fp64_switch;              /* mixed mode: FP32 phase hands over to FP64 when its KKT stalls (1) */
+    int32_t spmv_group_a;             /* 0 = autotune; else threads per row of A (1,2,4,8,16,32) */
+    int32_t spmv_group_at;            /* 0 = autotune; else threads per row of A^T */
+    int32_t reserved[8];
+} pdlpx_options;
+
+/* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */
+typedef struct pdlpx_result {
+    int32_t status;           /* PDLPX_STATUS_* */
+    double objective;         /* original space; 0 unless optimal (pdlp.cpp:1705-1709) */
+    int32_t iterations;       /* PDHG iterations including polish */
+    double work_units;        /* iterations * (4 nnz + 2 (m+n)), deterministic (pdlp.cpp:1716-1719) */
+    /* ---- diagnostics ---- */
+    double rel_primal_resid;  /* last check, reference definition (L2 or Linf per options) */
+    double rel_dual_resid;
+    double rel_gap;
+    double primal_objective;  /* last check, original space */
+    double dual_objective;
+    int32_t fp64_iterations;  /* iterations run in the FP64 phase (mixed mode) */
+    int32_t restarts;
+    double step_size;
+    double primal_weight;
+    double solve_seconds;     /* wall time of pdlpx_solve */
+    double device_seconds;    /* device time of the iteration loop (CUDA events) */
+    int32_t used_gpu;
+    int32_t kernel_launches;  /* engine kernel launches issued by this solve */
+} pdlpx_result;
+
+typedef struct pdlpx_solver pdlpx_solver; /* opaque */
+
+/* ---- options / errors ---- */
+void pdlpx_options_default(pdlpx_options* opts);
+const char* pdlpx_error_string(int32_t code);
+/* Last error message recorded on this handle (never NULL). */
+const char* pdlpx_last_error(const pdlpx_solver* h);
+/* Number of visible CUDA devices (0 on a host without a GPU; never fails). */
+int32_t pdlpx_device_count(void);
+/* Library version string. */
+const char* pdlpx_version(void);
+
+/* ---- single-LP solver (PdlpSolver : LpSolver) ---- */
+int32_t pdlpx_create(const pdlpx_options* opts, pdlpx_solver** out);
+int32_t pdlpx_destroy(pdlpx_solver* h);
+int32_t pdlpx_set_options(pdlpx_solver* h, const pdlpx_options* opts);
+int32_t pdlpx_get_options(const pdlpx_solver* h, pdlpx_options* out);
+/* Load an LP in ranged form row_lb <= A x <= row_ub, col_lb <= x <= col_ub.
+ * A is CSR (m rows, n cols); column indices need not be sorted; +-INFINITY (or
+ * |v| >= 1e30 is NOT special-cased: pass IEEE infinities) marks absent bounds.
+ * sense: PDLPX_MINIMIZE / PDLPX_MAXIMIZE.  Clears any warm start (pdlp.h:117). */
+int32_t pdlpx_load_csr(pdlpx_solver* h, int32_t m, int32_t n, int32_t nnz,
+                       const int32_t* row_ptr, const int32_t* col_idx, const double* val,
+                       const double* obj, const double* col_lb, const double* col_ub,
+                       const double* row_lb, const double* row_ub,
+                       int32_t sense, double obj_offset);
+/* Warm start in original space; silently ignored at solve time when the sizes
+ * do not match the loaded problem (pdlp.cpp:918-919). */
+int32_t pdlpx_set_warm_start(pdlpx_solver* h, const double* x, int32_t nx,
+                             const double* y, int32_t ny);
+int32_t pdlpx_clear_warm_start(pdlpx_solver* h);
+/* Cooperative cancel: *flag != 0 makes the solve return ITER_LIMIT at the next
+ * batch boundary (pdlp.cpp:972-976).  NULL clears.  Read with an atomic load. */
+int32_t pdlpx_set_stop_flag(pdlpx_solver* h, const int32_t* flag);
+int32_t pdlpx_solve(pdlpx_solver* h, pdlpx_result* out);
+int32_t pdlpx_get_status(const pdlpx_solver* h, int32_t* status);
+int32_t pdlpx_get_objective(const pdlpx_solver* h, double* objective);
+/* Copy the last solution (original space) into x[0..n) / y[0..m). */
+int32_t pdlpx_get_primal(const pdlpx_solver* h, double* x, int32_t n);
+int32_t pdlpx_get_dual(const pdlpx_solver* h, double* y, int32_t m);
+int32_t pdlpx_get_reduced_costs(const pdlpx_solver* h, double* rc, int32_t n);
+int32_t pdlpx_used_gpu(const pdlpx_solver* h, int32_t* used);
+int32_t pdlpx_get_dims(const pdlpx_solver* h, int32_t* m, int32_t* n, int32_t* nnz);
+/* Incremental edits; each re-runs the scaling pipeline like the reference.
+ * Invalid input is ignored silently (pdlp.cpp:2841-2853). */
+int32_t pdlpx_add_rows(pdlpx_solver* h, int32_t rows, const int32_t* starts,
+                       const int32_t* indices, const double* values, int32_t nvals,
+                       const double* lower, const double* upper);
+int32_t pdlpx_remove_rows(pdlpx_solver* h, const int32_t* rows, int32_t count);
+int32_t pdlpx_set_col_bounds(pdlpx_solver* h, int32_t col, double lower, double upper);
+int32_t pdlpx_set_objective(pdlpx_solver* h, const double* obj, int32_t n);
+
+/* Scaled problem as the engine prepared it (for parity of the scaling pipeline
+ * with pdlp.cpp:469-669).  Any output pointer may be NULL.  Sizes: n, n, n, m, m, m, n, m, n. */
+int32_t pdlpx_get_scaling(const pdlpx_solver* h, double* col_scale, double* cscaled,
+                          double* col_lb_scaled, double* row_scale, double* row_lb_scaled,
+                          double* row_ub_scaled, double* tau_base, double* sigma_base,
+                          double* col_ub_scaled, double* objective_scale,
+                          double* constraint_scale);
+
+/* Average device time in milliseconds of one launch of the fused primal step,
+ * the fused dual step and the FP64 check pass (both kernels) on the loaded
+ * problem, each launched `reps` times back to back on the engine's stream
+ * between CUDA events.  Needs a completed pdlpx_solve on this handle; leaves
+ * the returned solution untouched.  Any output pointer may be NULL. */
+int32_t pdlpx_time_kernels(pdlpx_solver* h, int32_t reps, double* ms_primal, double* ms_dual,
+                           double* ms_check);
+/* Threads per row chosen for A (dual step) and A^T (primal step), and the grid
+ * sizes of the two step kernels. */
+int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t* group_at,
+                                int32_t* blocks_primal, int32_t* blocks_dual);
+
+/* ---- batched solve: many independent LPs in one persistent launch ---- */
+typedef struct pdlpx_lp {
+    int32_t m, n, nnz;
+    const int32_t* row_ptr;
+    const int32_t* col_idx;
+    const double* val;
+    const double* obj;
+    const double* col_lb;
+    const double* col_ub;
+    const double* row_lb;
+    const double* row_ub;
+    int32_t sense;
+    double obj_offset;
+    const double* warm_x; /* optional (NULL) */
+    const double* warm_y; /* optional (NULL) */
+} pdlpx_lp;
+
+/* Solve count LPs with one option set.  results[count]; x_out[k] / y_out[k] may be
+ * NULL or point to n_k / m_k doubles. */
+int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts,
+                          pdlpx_result* results, double* const* x_out, double* const* y_out);
+
+/* ---- device kernels exposed for parity tests (host buffers in and out) ---- */
+/* y = A x with the engine's SpMV kernel.  precision: PDLPX_PREC_MIXED (FP32 values,
+ * FP32 x, FP32 accumulation) or PDLPX_PREC_FP64.  group: threads per row (0 = auto). */
+int32_t pdlpx_csr_spmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* row_ptr,
+                       const int32_t* col_idx, const double* val, const double* x, double* y,
+                       int32_t precision, int32_t group);
+
+/* ---- seeded synthetic LP generators (configs of the benchmark suite) ----
+ * Output arrays are allocated by the library and released with pdlpx_free_lp. */
+typedef struct pdlpx_gen_lp {
+    int32_t m, n, nnz;
+    int32_t* row_ptr;
+    int32_t* col_idx;
+    double* val;
+    double* obj;
+    double* col_lb;
+    double* col_ub;
+    double* row_lb;
+    double* row_ub;
+    double* x0;        /* feasible point used by the construction (length n) */
+    int32_t* is_int;   /* integrality marks (length n) or NULL */
+} pdlpx_gen_lp;
+
+/* Random sparse LP: columns with U{nnz_lo..nnz_hi} nonzeros at uniform rows,
+ * values N(0,1) (duplicates summed), x0~U[0,10], rows alternate '=' and '<='
+ * with b = A x0 (+U[0,1] slack on '<='), 0<=x<=10, c~N(0,1). */
+int32_t pdlpx_gen_random(int32_t m, int32_t n, int32_t nnz_lo, int32_t nnz_hi, uint64_t seed,
+                         pdlpx_gen_lp* out);
+/* Transportation LP: s supplies x d demands, costs U[1,100], supplies U[50,150],
+ * demands U[50,150] rescaled to total 0.95 * total supply. */
+int32_t pdlpx_gen_transport(int32_t s, int32_t d, uint64_t seed, pdlpx_gen_lp* out);
+/* Large LP: power-law column counts (min 2, max kmax, mean kmean), values N(0,1),
+ * a fraction big_frac of rows scaled by big_scale, random-LP feasibility construction. */
+int32_t pdlpx_gen_powerlaw(int32_t m, int32_t n, int32_t kmin, int32_t kmax, double kmean,
+                           double big_frac, double big_scale, uint64_t seed, pdlpx_gen_lp* out);
+void pdlpx_free_lp(pdlpx_gen_lp* lp);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDLPX_H */

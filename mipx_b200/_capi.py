@@ -1,0 +1,151 @@
+"""ctypes binding of ``include/pdlpx.h`` (the engine's C ABI).
+
+The structure layouts below mirror the header field for field; ``check_layout``
+compares their sizes with what the library reports through its own calls.
+Loading fails loudly when the library is missing: there is no Python or CPU
+stand-in for the device engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+from . import build as _build
+
+i32 = C.c_int32
+f64 = C.c_double
+P_i32 = C.POINTER(C.c_int32)
+P_f64 = C.POINTER(C.c_double)
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("max_iter", i32), ("optimality_tol", f64), ("primal_tol", f64), ("dual_tol", f64),
+        ("max_solve_seconds", f64), ("optimality_norm", i32), ("sv_max_iter", i32), ("sv_tol", f64),
+        ("adaptive_step", i32), ("adaptive_step_down", f64), ("adaptive_step_up", f64),
+        ("adaptive_step_min", f64), ("adaptive_step_max", f64), ("primal_weight", f64),
+        ("update_primal_weight", i32), ("pid_kp", f64), ("pid_ki", f64), ("pid_kd", f64),
+        ("pid_i_smooth", f64), ("restart_sufficient_decay", f64), ("restart_necessary_decay", f64),
+        ("restart_artificial_fraction", f64), ("termination_eval_frequency", i32),
+        ("matrix_zero_tol", f64), ("enable_polishing", i32), ("polish_primal_tol", f64),
+        ("polish_dual_tol", f64), ("polish_max_iter", i32), ("do_ruiz_scaling", i32),
+        ("ruiz_iterations", i32), ("do_pock_chambolle_scaling", i32), ("do_bound_obj_rescaling", i32),
+        ("preconditioner_refresh", i32), ("preconditioner_refresh_ratio", f64),
+        ("anderson_acceleration", i32), ("anderson_window_size", i32), ("anderson_regularization", f64),
+        ("use_gpu", i32), ("gpu_min_rows", i32), ("gpu_min_nnz", i32), ("verbose", i32),
+        ("precision", i32), ("device", i32), ("fp64_switch", i32), ("spmv_group_a", i32),
+        ("spmv_group_at", i32), ("reserved", i32 * 8),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("status", i32), ("objective", f64), ("iterations", i32), ("work_units", f64),
+        ("rel_primal_resid", f64), ("rel_dual_resid", f64), ("rel_gap", f64),
+        ("primal_objective", f64), ("dual_objective", f64), ("fp64_iterations", i32),
+        ("restarts", i32), ("step_size", f64), ("primal_weight", f64), ("solve_seconds", f64),
+        ("device_seconds", f64), ("used_gpu", i32), ("kernel_launches", i32),
+    ]
+
+
+class Lp(C.Structure):
+    _fields_ = [
+        ("m", i32), ("n", i32), ("nnz", i32), ("row_ptr", P_i32), ("col_idx", P_i32), ("val", P_f64),
+        ("obj", P_f64), ("col_lb", P_f64), ("col_ub", P_f64), ("row_lb", P_f64), ("row_ub", P_f64),
+        ("sense", i32), ("obj_offset", f64), ("warm_x", P_f64), ("warm_y", P_f64),
+    ]
+
+
+class GenLp(C.Structure):
+    _fields_ = [
+        ("m", i32), ("n", i32), ("nnz", i32), ("row_ptr", P_i32), ("col_idx", P_i32), ("val", P_f64),
+        ("obj", P_f64), ("col_lb", P_f64), ("col_ub", P_f64), ("row_lb", P_f64), ("row_ub", P_f64),
+        ("x0", P_f64), ("is_int", P_i32),
+    ]
+
+
+# (name, restype, argtypes) of every entry point declared in include/pdlpx.h
+SIGNATURES = [
+    ("pdlpx_options_default", None, [C.POINTER(Options)]),
+    ("pdlpx_error_string", C.c_char_p, [i32]),
+    ("pdlpx_last_error", C.c_char_p, [C.c_void_p]),
+    ("pdlpx_device_count", i32, []),
+    ("pdlpx_version", C.c_char_p, []),
+    ("pdlpx_create", i32, [C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    ("pdlpx_destroy", i32, [C.c_void_p]),
+    ("pdlpx_set_options", i32, [C.c_void_p, C.POINTER(Options)]),
+    ("pdlpx_get_options", i32, [C.c_void_p, C.POINTER(Options)]),
+    ("pdlpx_load_csr", i32, [C.c_void_p, i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, P_f64, P_f64,
+                             P_f64, i32, f64]),
+    ("pdlpx_set_warm_start", i32, [C.c_void_p, P_f64, i32, P_f64, i32]),
+    ("pdlpx_clear_warm_start", i32, [C.c_void_p]),
+    ("pdlpx_set_stop_flag", i32, [C.c_void_p, P_i32]),
+    ("pdlpx_solve", i32, [C.c_void_p, C.POINTER(Result)]),
+    ("pdlpx_get_status", i32, [C.c_void_p, P_i32]),
+    ("pdlpx_get_objective", i32, [C.c_void_p, P_f64]),
+    ("pdlpx_get_primal", i32, [C.c_void_p, P_f64, i32]),
+    ("pdlpx_get_dual", i32, [C.c_void_p, P_f64, i32]),
+    ("pdlpx_get_reduced_costs", i32, [C.c_void_p, P_f64, i32]),
+    ("pdlpx_used_gpu", i32, [C.c_void_p, P_i32]),
+    ("pdlpx_get_dims", i32, [C.c_void_p, P_i32, P_i32, P_i32]),
+    ("pdlpx_add_rows", i32, [C.c_void_p, i32, P_i32, P_i32, P_f64, i32, P_f64, P_f64]),
+    ("pdlpx_remove_rows", i32, [C.c_void_p, P_i32, i32]),
+    ("pdlpx_set_col_bounds", i32, [C.c_void_p, i32, f64, f64]),
+    ("pdlpx_set_objective", i32, [C.c_void_p, P_f64, i32]),
+    ("pdlpx_get_scaling", i32, [C.c_void_p] + [P_f64] * 11),
+    ("pdlpx_time_kernels", i32, [C.c_void_p, i32, P_f64, P_f64, P_f64]),
+    ("pdlpx_get_launch_config", i32, [C.c_void_p, P_i32, P_i32, P_i32, P_i32]),
+    ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),
+                                C.POINTER(P_f64), C.POINTER(P_f64)]),
+    ("pdlpx_csr_spmv", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, i32, i32]),
+    ("pdlpx_gen_random", i32, [i32, i32, i32, i32, C.c_uint64, C.POINTER(GenLp)]),
+    ("pdlpx_gen_transport", i32, [i32, i32, C.c_uint64, C.POINTER(GenLp)]),
+    ("pdlpx_gen_powerlaw", i32, [i32, i32, i32, i32, f64, f64, f64, C.c_uint64, C.POINTER(GenLp)]),
+    ("pdlpx_free_lp", None, [C.POINTER(GenLp)]),
+]
+
+_lib = None
+
+
+def lib_path() -> Path:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Load libpdlpx.so (building it first when it is absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not path.exists():
+        if not build_if_missing:
+            raise RuntimeError(f"engine library missing: {path}")
+        _build.build()
+    lib = C.CDLL(str(path), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def default_options() -> Options:
+    o = Options()
+    load().pdlpx_options_default(C.byref(o))
+    return o
+
+
+class PdlpxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pdlpx error {code}: {msg}")
+        self.code = code
+
+
+def check(code: int, handle=None) -> None:
+    if code != 0:
+        lib = load()
+        detail = lib.pdlpx_last_error(handle).decode() if handle is not None else ""
+        base = lib.pdlpx_error_string(code).decode()
+        raise PdlpxError(code, f"{base}: {detail}" if detail else base)

@@ -1,0 +1,1420 @@
+// Host orchestration of the PDLP engine and the non-template kernels.
+//
+// Solve flow (PdlpSolver::solve / solveGpu, pdlp.cpp:801-869, 1739-2792):
+//   1. trivial cases on the host exactly as the reference (n == 0, m == 0);
+//   2. device image of the scaled LP (FP32 and FP64 matrix values, packed
+//      per-row / per-column constants, iterates) in one arena;
+//   3. power iteration for the step size, device-resident, graph chunks;
+//   4. restart cycles: one CUDA graph = N fused iterations + FP64 check +
+//      controller + conditional restart copy (+ FP32->FP64 hand-over);
+//      the host only reads the 200-byte state after each cycle to stop;
+//   5. unscale on the host (pdlp.cpp:2678-2712).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <random>
+
+#include "engine.hpp"
+#include "kernels.cuh"
+
+namespace pdlpx {
+
+#define PDLPX_CK(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);             \
+            return e_ == cudaErrorMemoryAllocation ? PDLPX_E_NOMEM : PDLPX_E_CUDA;       \
+        }                                                                                \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Non-template kernels
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kBlock) promoteIterates(PromoteArgs a) {
+    const DevState* st = a.st;
+    if (st->done || st->prec != 0 || !st->promote) return;
+    const int total = a.n > a.m ? a.n : a.m;
+    for (int k = blockIdx.x * kBlock + threadIdx.x; k < total; k += gridDim.x * kBlock) {
+        if (k < a.n) {
+            a.xc64[k] = a.xc[k];
+            a.xi64[k] = a.xi[k];
+            a.xh64[k] = a.xh[k];
+        }
+        if (k < a.m) {
+            a.yc64[k] = a.yc[k];
+            a.yi64[k] = a.yi[k];
+            a.yh64[k] = a.yh[k];
+        }
+    }
+}
+
+__global__ void finishPromote(DevState* st) {
+    if (!st->done && st->prec == 0 && st->promote) st->prec = 1;
+}
+
+// Reduce [nb][NS] partials in fixed order into out[NS] (block of kBlock threads).
+template <int NS>
+__device__ void reducePartials(const double* part, int nb, const int (&ops)[NS], double* out) {
+    double acc[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc[s] = slotInit(ops[s]);
+    for (int b = threadIdx.x; b < nb; b += kBlock) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const double v = part[static_cast<size_t>(b) * NS + s];
+            acc[s] = ops[s] == OP_SUM ? acc[s] + v : (ops[s] == OP_MIN ? fmin(acc[s], v) : fmax(acc[s], v));
+        }
+    }
+    blockReduceSlots<NS>(acc, ops, out);
+}
+
+// Restart / primal weight / polish / termination logic of one check
+// (pdlp.cpp:2228-2469 main loop, 2592-2666 polish), FP64, one thread.
+__device__ void controlStep(DevState& s, const DevConst& c, const double* rows, const double* cols) {
+    const int cur = s.phase == 0 ? s.total : s.polish_count;
+    const int lim = s.phase == 0 ? c.max_iter : c.polish_max_iter;
+    const int batch = min(c.N, lim - cur);
+    s.total += batch;
+    s.inner += batch;
+    if (s.phase == 1) s.polish_count += batch;
+    s.checks += 1;
+
+    const double dx2 = cols[C_PDIST], dy2 = rows[R_DDIST];
+    const double movement = dx2 * s.pw + dy2 / s.pw;
+    const double interaction = cols[C_INTER] * (2.0 * s.step);
+    const double fpe = sqrt(fmax(movement + interaction, 0.0));
+    if (s.fpe0 < 0.0) s.fpe0 = fpe;
+
+    const double rel_p = sqrt(rows[R_PRES_SQ]) / (1.0 + c.b_norm);
+    const double rel_pi = rows[R_PRES_MAX] / (1.0 + c.b_norm);
+    const double rel_d = sqrt(cols[C_DRES_SQ]) / (1.0 + c.c_norm);
+    const double rel_di = cols[C_DRES_MAX] / (1.0 + c.c_norm);
+    const double pterm = c.linf ? rel_pi : rel_p;
+    const double dterm = c.linf ? rel_di : rel_d;
+    const double unsc = 1.0 / (c.obj_scale * c.con_scale);
+    const double pobj = c.offset + c.obj_sign * cols[C_POBJ] * unsc;
+    const double dobj = c.offset + c.obj_sign * (cols[C_DOBJ_COL] + rows[R_DOBJ_ROW]) * unsc;
+    const double gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    s.rel_p = rel_p;
+    s.rel_d = rel_d;
+    s.rel_pi = rel_pi;
+    s.rel_di = rel_di;
+    s.pterm = pterm;
+    s.dterm = dterm;
+    s.gap = gap;
+    s.pobj = pobj;
+    s.dobj = dobj;
+    s.fpe = fpe;
+    s.restart = 0;
+    s.promote = 0;
+
+    auto piUpdate = [&](double rp, double rd, bool track_best) {
+        const double pd = sqrt(dx2), dd = sqrt(dy2);
+        const double ratio = rp > 1e-15 ? rd / rp : 0.0;
+        if (pd > 1e-16 && dd > 1e-16 && pd < 1e12 && dd < 1e12 && ratio > 1e-8 && ratio < 1e8) {
+            const double e = log(dd) - log(pd) - log(s.pw);
+            s.esum = c.ismooth * s.esum + e;
+            const double de = e - s.elast;
+            s.pw *= exp(c.kp * e + c.ki * s.esum + c.kd * de);
+            s.pw = fmin(fmax(s.pw, 1e-4), 1e8);
+            s.elast = e;
+            if (track_best) {
+                const double score = fabs(log10(fmax(rd, 1e-15)) - log10(fmax(rp, 1e-15)));
+                if (score < s.best_score) {
+                    s.best_score = score;
+                    s.best_pw = s.pw;
+                }
+            }
+        } else if (track_best) {
+            s.pw = s.best_pw;
+            s.esum = 0.0;
+            s.elast = 0.0;
+        }
+    };
+    auto resetCycle = [&]() {
+        s.restart = 1;
+        s.restarts += 1;
+        s.inner = 0;
+        s.fpe0 = -1.0;
+        s.last_fpe = CUDART_INF;
+        s.have_prev = 0;
+    };
+
+    if (s.phase == 0) {
+        if (pterm <= c.primal_tol && dterm <= c.dual_tol && gap <= c.opt_tol) {
+            s.converged = 1;
+            if (c.enable_polish && (pterm > c.polish_ptol || dterm > c.polish_dtol)) {
+                s.phase = 1;  // polish: restart from pdhg iterates (pdlp.cpp:2524-2529)
+                s.polish_count = 0;
+                s.restart = 1;
+                s.inner = 0;
+                s.fpe0 = -1.0;
+                s.last_fpe = CUDART_INF;
+            } else {
+                s.done = 1;
+                s.status = PDLPX_STATUS_OPTIMAL;
+            }
+        } else {
+            if (c.adaptive) {  // GPU variant of the adaptive step (pdlp.cpp:2274-2307)
+                if (s.have_prev) {
+                    const double ad = rows[R_ADAPT], xd = cols[C_ADAPT];
+                    if (xd > 1e-30) {
+                        const double lip2 = ad / xd;
+                        const double ls = 0.998 / sqrt(fmax(lip2, 1e-30));
+                        const double ns = s.step > ls ? s.step * c.step_down : s.step * c.step_up;
+                        s.step = fmin(fmax(ns, c.step_lb), c.step_ub);
+                    }
+                }
+                s.have_prev = 1;
+            }
+            if (s.total >= 10 * c.N && s.total % (10 * c.N) == 0) {
+                // Farkas dual ray (pdlp.cpp:119-211) from scaled-space reductions.
+                const double yq = sqrt(rows[R_YNORM]);
+                if (c.m > 0 && yq / c.obj_scale >= 1e-15) {
+                    const double thr = 1e-6 * yq;
+                    const bool signs = !(rows[R_MIN_LE] < -thr) && !(rows[R_MAX_GE] > thr) &&
+                                       !(cols[C_MIN_GLB] < -thr) && !(cols[C_MAX_GUB] > thr);
+                    if (signs) {
+                        const double farkas = (rows[R_FARKAS_ROW] - cols[C_COLSUP]) / (c.con_scale * yq);
+                        if (farkas < -1e-6) {
+                            s.done = 1;
+                            s.status = PDLPX_STATUS_INFEASIBLE;
+                            s.cert_hit = 1;
+                        }
+                    }
+                }
+                // Primal ray (pdlp.cpp:220-284).
+                const double xq = sqrt(cols[C_XNORM]);
+                if (!s.done && c.n > 0 && xq / c.con_scale >= 1e-15) {
+                    const double thr = 1e-6 * xq;
+                    const bool ok = !(cols[C_MIN_XLB] < -thr) && !(cols[C_MAX_XUB] > thr) &&
+                                    !(rows[R_UB_TWO] > thr) && !(rows[R_UB_LE] > thr) &&
+                                    !(rows[R_UB_GE] < -thr);
+                    if (ok && cols[C_POBJ] / (c.obj_scale * xq) < -1e-6) {
+                        s.done = 1;
+                        s.status = PDLPX_STATUS_UNBOUNDED;
+                        s.cert_hit = 2;
+                    }
+                }
+            }
+            if (!s.done) {
+                bool rs = false;
+                if (s.total == c.N)
+                    rs = true;
+                else if (s.fpe0 > 0.0 && fpe <= c.suff * s.fpe0)
+                    rs = true;
+                else if (s.fpe0 > 0.0 && fpe <= c.nec * s.fpe0 && fpe > s.last_fpe)
+                    rs = true;
+                else if (s.inner >= static_cast<int>(c.art * static_cast<double>(s.total)))
+                    rs = true;
+                s.last_fpe = fpe;
+                if (rs) {
+                    if (c.update_pw) piUpdate(rel_p, rel_d, true);
+                    // Preconditioner refresh recomputes sigma/tau from the unchanged scaled
+                    // matrix (pdlp.cpp:713-742), which reproduces the same values; only the
+                    // reference weight moves.
+                    if (c.precond_refresh && s.precond_pw > 0.0) {
+                        const double drift = s.pw / s.precond_pw;
+                        if (drift > c.precond_ratio || drift < 1.0 / c.precond_ratio) s.precond_pw = s.pw;
+                    }
+                    resetCycle();
+                }
+                if (s.total >= c.max_iter) {
+                    s.done = 1;
+                    s.status = PDLPX_STATUS_ITER_LIMIT;
+                }
+            }
+        }
+    } else {
+        if (pterm <= c.polish_ptol && dterm <= c.polish_dtol) {
+            s.done = 1;
+            s.status = PDLPX_STATUS_OPTIMAL;
+        } else {
+            bool rs = false;
+            if (s.polish_count == batch)
+                rs = true;
+            else if (s.fpe0 > 0.0 && fpe <= c.suff * s.fpe0)
+                rs = true;
+            else if (s.fpe0 > 0.0 && fpe <= c.nec * s.fpe0 && fpe > s.last_fpe)
+                rs = true;
+            else if (s.inner >= static_cast<int>(c.art * static_cast<double>(s.polish_count)))
+                rs = true;
+            s.last_fpe = fpe;
+            if (rs) {
+                if (c.update_pw) piUpdate(rel_p, rel_d, false);
+                resetCycle();
+            }
+            if (s.polish_count >= c.polish_max_iter) {
+                s.done = 1;
+                s.status = PDLPX_STATUS_OPTIMAL;
+            }
+        }
+    }
+
+    // Mixed precision: hand the iterates to FP64 when the FP32 phase stops improving.
+    if (c.mixed && c.fp64_switch && s.prec == 0 && !s.done) {
+        const double pt = s.phase == 0 ? c.primal_tol : c.polish_ptol;
+        const double dt = s.phase == 0 ? c.dual_tol : c.polish_dtol;
+        double score = fmax(pterm / pt, dterm / dt);
+        if (s.phase == 0) score = fmax(score, gap / c.opt_tol);
+        if (score < 0.7 * s.best_kkt) {
+            s.best_kkt = score;
+            s.stall = 0;
+        } else {
+            s.stall += 1;
+        }
+        if (s.stall >= c.stall_limit || (c.switch_score > 0.0 && score <= c.switch_score)) s.promote = 1;
+    }
+    s.tau_fac = static_cast<float>(s.step / s.pw);
+    s.sig_fac = static_cast<float>(s.step * s.pw);
+}
+
+__global__ void __launch_bounds__(kBlock) controller(DevState* st, const DevConst* dc, const double* part_rows,
+                                                    const double* part_cols, int prec) {
+    if (st->done || st->prec != prec) return;
+    __shared__ double rows[kRowSlots];
+    __shared__ double cols[kColSlots];
+    int rops[kRowSlots], cops[kColSlots];
+#pragma unroll
+    for (int s = 0; s < kRowSlots; ++s) rops[s] = rowSlotOp(s);
+#pragma unroll
+    for (int s = 0; s < kColSlots; ++s) cops[s] = colSlotOp(s);
+    reducePartials<kRowSlots>(part_rows, dc->nb_rows, rops, rows);
+    __syncthreads();
+    reducePartials<kColSlots>(part_cols, dc->nb_cols, cops, cols);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DevState s = *st;
+        controlStep(s, *dc, rows, cols);
+        *st = s;
+    }
+}
+
+// ---- power iteration -------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) powerFinish1(PowerArgs a) {
+    if (a.ps->done) return;
+    __shared__ double out[2];
+    const int ops[2] = {OP_SUM, OP_SUM};
+    reducePartials<2>(a.part, a.nb, ops, out);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a.ps->s2 = out[0];
+        a.ps->nrm = sqrt(out[1]);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) powerNormalize(PowerArgs a) {
+    if (a.ps->done) return;
+    const double s2 = a.ps->s2, nrm = a.ps->nrm;
+    double acc[1] = {0.0};
+    for (int j = blockIdx.x * kBlock + threadIdx.x; j < a.n; j += gridDim.x * kBlock) {
+        const double xn = a.xn[j];
+        const double d = xn - s2 * a.x[j];
+        acc[0] += d * d;
+        if (nrm >= 1e-15) a.x[j] = xn / nrm;
+    }
+    const int ops[1] = {OP_SUM};
+    blockReduceSlots<1>(acc, ops, a.part + static_cast<size_t>(blockIdx.x) * 2);
+}
+
+__global__ void __launch_bounds__(kBlock) powerFinish2(PowerArgs a) {
+    if (a.ps->done) return;
+    __shared__ double out[1];
+    double acc[1] = {0.0};
+    for (int b = threadIdx.x; b < a.nb; b += kBlock) acc[0] += a.part[static_cast<size_t>(b) * 2];
+    const int ops[1] = {OP_SUM};
+    blockReduceSlots<1>(acc, ops, out);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        PowerState& p = *a.ps;
+        p.resid = sqrt(out[0]);
+        p.iter += 1;
+        if (p.nrm < 1e-15 || p.resid < a.tol * fabs(p.s2) || p.iter >= a.max_iter) p.done = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers (G dispatch)
+// ---------------------------------------------------------------------------
+#define PDLPX_G_SWITCH(G, CALL)                   \
+    switch (G) {                                  \
+        case 1: { constexpr int GG = 1; CALL; } break;     \
+        case 2: { constexpr int GG = 2; CALL; } break;     \
+        case 4: { constexpr int GG = 4; CALL; } break;     \
+        case 8: { constexpr int GG = 8; CALL; } break;     \
+        case 16: { constexpr int GG = 16; CALL; } break;   \
+        case 32: { constexpr int GG = 32; CALL; } break;   \
+        case 64: { constexpr int GG = 64; CALL; } break;   \
+        case 128: { constexpr int GG = 128; CALL; } break; \
+        default: { constexpr int GG = 256; CALL; } break;  \
+    }
+
+static int gridFor(int64_t rows, int G) {
+    const int64_t threads = rows * G;
+    return static_cast<int>(std::max<int64_t>(1, (threads + kBlock - 1) / kBlock));
+}
+
+int32_t pickGroup(int64_t nnz, int32_t rows) {
+    if (rows <= 0) return 1;
+    const double mean = static_cast<double>(nnz) / rows;
+    if (mean <= 3) return 1;
+    if (mean <= 6) return 2;
+    if (mean <= 12) return 4;
+    if (mean <= 24) return 8;
+    if (mean <= 48) return 16;
+    if (mean <= 128) return 32;
+    if (mean <= 384) return 64;
+    if (mean <= 768) return 128;
+    return 256;
+}
+
+// ---------------------------------------------------------------------------
+// Device image
+// ---------------------------------------------------------------------------
+struct DeviceLp {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    int m = 0, n = 0, nnz = 0;
+    bool mixed = true;
+    int gA = 1, gAT = 1;
+    int nb_rows = 1, nb_cols = 1, nb_pi = 1;
+
+    int *a_ptr = nullptr, *a_idx = nullptr, *at_ptr = nullptr, *at_idx = nullptr;
+    float *a_v32 = nullptr, *at_v32 = nullptr;
+    double *a_v64 = nullptr, *at_v64 = nullptr;
+    ColPack<float>* cp32 = nullptr;
+    RowPack<float>* rp32 = nullptr;
+    ColPack<double>* cp64 = nullptr;
+    RowPack<double>* rp64 = nullptr;
+    double *c64 = nullptr, *lb64 = nullptr, *ub64 = nullptr, *cs64 = nullptr, *tau64 = nullptr;
+    double *rl64 = nullptr, *ru64 = nullptr, *rs64 = nullptr, *sig64 = nullptr;
+    float *xc32 = nullptr, *xi32 = nullptr, *xr32 = nullptr, *xh32 = nullptr;
+    float *yc32 = nullptr, *yi32 = nullptr, *yh32 = nullptr;
+    double *xc64 = nullptr, *xi64 = nullptr, *xr64 = nullptr, *xh64 = nullptr;
+    double *yc64 = nullptr, *yi64 = nullptr, *yh64 = nullptr;
+    double *prev_ax = nullptr, *prev_xh = nullptr;
+    double *pi_x = nullptr, *pi_y = nullptr, *pi_xn = nullptr, *pi_part = nullptr;
+    double *part_rows = nullptr, *part_cols = nullptr;
+    DevState* st = nullptr;
+    DevConst* dc = nullptr;
+    PowerState* ps = nullptr;
+    DevState* h_st = nullptr;    // pinned mirror
+    PowerState* h_ps = nullptr;  // pinned mirror
+
+    cudaGraphExec_t cycle[2] = {nullptr, nullptr};
+    int cycle_N[2] = {0, 0};
+    cudaGraphExec_t power = nullptr;
+    int launches_cycle[2] = {0, 0};
+    int launches_power = 0;
+    static constexpr int kPowerChunk = 8;
+
+    ~DeviceLp() {
+        for (auto& g : cycle)
+            if (g) cudaGraphExecDestroy(g);
+        if (power) cudaGraphExecDestroy(power);
+        if (arena) cudaFree(arena);
+        if (h_st) cudaFreeHost(h_st);
+        if (h_ps) cudaFreeHost(h_ps);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    IterArgs<float> iter32(const pdlpx_options& o) const {
+        IterArgs<float> a{};
+        a.at_ptr = at_ptr;
+        a.at_idx = at_idx;
+        a.at_val = at_v32;
+        a.a_ptr = a_ptr;
+        a.a_idx = a_idx;
+        a.a_val = a_v32;
+        a.cp = cp32;
+        a.rp = rp32;
+        a.xc = xc32;
+        a.xi = xi32;
+        a.xr = xr32;
+        a.xh = xh32;
+        a.yc = yc32;
+        a.yi = yi32;
+        a.yh = yh32;
+        a.st = st;
+        a.m = m;
+        a.n = n;
+        a.max_iter = o.max_iter;
+        a.polish_max_iter = o.polish_max_iter;
+        a.N = o.termination_eval_frequency;
+        return a;
+    }
+    IterArgs<double> iter64(const pdlpx_options& o) const {
+        IterArgs<double> a{};
+        a.at_ptr = at_ptr;
+        a.at_idx = at_idx;
+        a.at_val = at_v64;
+        a.a_ptr = a_ptr;
+        a.a_idx = a_idx;
+        a.a_val = a_v64;
+        a.cp = cp64;
+        a.rp = rp64;
+        a.xc = xc64;
+        a.xi = xi64;
+        a.xr = xr64;
+        a.xh = xh64;
+        a.yc = yc64;
+        a.yi = yi64;
+        a.yh = yh64;
+        a.st = st;
+        a.m = m;
+        a.n = n;
+        a.max_iter = o.max_iter;
+        a.polish_max_iter = o.polish_max_iter;
+        a.N = o.termination_eval_frequency;
+        return a;
+    }
+    template <class T>
+    CheckArgs<T> check(const T* xh, const T* xi, const T* yh, const T* yi) const {
+        CheckArgs<T> c{};
+        c.a_ptr = a_ptr;
+        c.a_idx = a_idx;
+        c.a_val = a_v64;
+        c.at_ptr = at_ptr;
+        c.at_idx = at_idx;
+        c.at_val = at_v64;
+        c.xh = xh;
+        c.xi = xi;
+        c.yh = yh;
+        c.yi = yi;
+        c.c64 = c64;
+        c.lb64 = lb64;
+        c.ub64 = ub64;
+        c.cs64 = cs64;
+        c.tau64 = tau64;
+        c.rl64 = rl64;
+        c.ru64 = ru64;
+        c.rs64 = rs64;
+        c.sig64 = sig64;
+        c.prev_ax = prev_ax;
+        c.prev_xh = prev_xh;
+        c.part_rows = part_rows;
+        c.part_cols = part_cols;
+        c.dc = dc;
+        c.st = st;
+        c.m = m;
+        c.n = n;
+        return c;
+    }
+};
+
+namespace {
+
+template <class T>
+IterArgs<T> iterArgs(const DeviceLp& d, const pdlpx_options& o);
+template <>
+IterArgs<float> iterArgs<float>(const DeviceLp& d, const pdlpx_options& o) {
+    return d.iter32(o);
+}
+template <>
+IterArgs<double> iterArgs<double>(const DeviceLp& d, const pdlpx_options& o) {
+    return d.iter64(o);
+}
+
+// One restart cycle: N fused iterations, check, controller, restart copy.
+template <class T>
+int launchCycle(DeviceLp& d, const pdlpx_options& o) {
+    const IterArgs<T> ia = iterArgs<T>(d, o);
+    const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
+    cudaStream_t s = d.stream;
+    const int gp = gridFor(d.n, d.gAT), gd = gridFor(d.m, d.gA);
+    int launches = 0;
+    for (int k = 1; k <= o.termination_eval_frequency; ++k) {
+        PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, k)));
+        PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, k)));
+        launches += 2;
+    }
+    PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
+    PDLPX_G_SWITCH(d.gAT, (checkCols<GG, T><<<d.nb_cols, kBlock, 0, s>>>(ca)));
+    controller<<<1, kBlock, 0, s>>>(d.st, d.dc, d.part_rows, d.part_cols, sizeof(T) == 8 ? 1 : 0);
+    const int nb = std::max(1, std::min(gridFor(std::max(d.m, d.n), 1), 8 * d.sms));
+    restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc);
+    launches += 4;
+    if (sizeof(T) == 4 && d.mixed) {
+        PromoteArgs pa{d.xc32, d.xi32, d.xh32, d.yc32, d.yi32, d.yh32, d.xc64, d.xi64,
+                       d.xh64, d.yc64, d.yi64, d.yh64, d.st,   d.n,    d.m};
+        promoteIterates<<<nb, kBlock, 0, s>>>(pa);
+        finishPromote<<<1, 1, 0, s>>>(d.st);
+        launches += 2;
+    }
+    return launches;
+}
+
+template <class V>
+int launchPowerChunk(DeviceLp& d, const PowerArgs& pa, const PowerMat<V>& mt, int chunk) {
+    cudaStream_t s = d.stream;
+    int launches = 0;
+    for (int it = 0; it < chunk; ++it) {
+        PDLPX_G_SWITCH(d.gA, (powerA<GG, V><<<gridFor(d.m, d.gA), kBlock, 0, s>>>(pa, mt)));
+        PDLPX_G_SWITCH(d.gAT, (powerAt<GG, V><<<d.nb_pi, kBlock, 0, s>>>(pa, mt)));
+        powerFinish1<<<1, kBlock, 0, s>>>(pa);
+        powerNormalize<<<d.nb_pi, kBlock, 0, s>>>(pa);
+        powerFinish2<<<1, kBlock, 0, s>>>(pa);
+        launches += 5;
+    }
+    return launches;
+}
+
+template <class T>
+void packCols(const ScaledLp& sc, std::vector<ColPack<T>>& out) {
+    out.resize(sc.c.size());
+    for (size_t j = 0; j < sc.c.size(); ++j)
+        out[j] = ColPack<T>{static_cast<T>(sc.c[j]), static_cast<T>(sc.cl[j]), static_cast<T>(sc.cu[j]),
+                            static_cast<T>(sc.tau[j])};
+}
+template <class T>
+void packRows(const ScaledLp& sc, std::vector<RowPack<T>>& out) {
+    out.resize(sc.rl.size());
+    for (size_t i = 0; i < sc.rl.size(); ++i)
+        out[i] = RowPack<T>{static_cast<T>(sc.sigma[i]), static_cast<T>(sc.rl[i]), static_cast<T>(sc.ru[i]),
+                            static_cast<T>(sc.row_type[i])};
+}
+
+bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
+    if (lim < 0.0) return false;
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= lim;
+}
+
+}  // namespace
+
+// Build (or rebuild) the device image of the scaled LP.
+static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, const pdlpx_options& o,
+                           std::string& err) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        err = "no CUDA device visible";
+        return PDLPX_E_NO_DEVICE;
+    }
+    const int dev = (o.device >= 0 && o.device < count) ? o.device : 0;
+    PDLPX_CK(cudaSetDevice(dev));
+    dp.reset(new DeviceLp());
+    DeviceLp& d = *dp;
+    d.device = dev;
+    PDLPX_CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    PDLPX_CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    d.m = sc.a.rows;
+    d.n = sc.a.cols;
+    d.nnz = sc.a.nnz();
+    d.mixed = o.precision != PDLPX_PREC_FP64;
+    const int64_t m = d.m, n = d.n, nnz = d.nnz;
+    d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz, d.m);
+    d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz, d.n);
+    const int cap = 4 * d.sms;
+    d.nb_rows = std::max(1, std::min(gridFor(m, d.gA), cap));
+    d.nb_cols = std::max(1, std::min(gridFor(n, d.gAT), cap));
+    d.nb_pi = d.nb_cols;
+
+    // Arena layout.
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 255) & ~static_cast<size_t>(255);
+        return at;
+    };
+    const bool mixed = d.mixed;
+    const size_t o_a_ptr = take(4 * (m + 1)), o_a_idx = take(4 * nnz), o_at_ptr = take(4 * (n + 1)),
+                 o_at_idx = take(4 * nnz);
+    const size_t o_a_v64 = take(8 * nnz), o_at_v64 = take(8 * nnz);
+    const size_t o_a_v32 = mixed ? take(4 * nnz) : 0, o_at_v32 = mixed ? take(4 * nnz) : 0;
+    const size_t o_cp32 = mixed ? take(16 * n) : 0, o_rp32 = mixed ? take(16 * m) : 0;
+    const size_t o_cp64 = take(32 * n), o_rp64 = take(32 * m);
+    const size_t o_c64 = take(8 * n), o_lb64 = take(8 * n), o_ub64 = take(8 * n), o_cs64 = take(8 * n),
+                 o_tau64 = take(8 * n);
+    const size_t o_rl64 = take(8 * m), o_ru64 = take(8 * m), o_rs64 = take(8 * m), o_sig64 = take(8 * m);
+    size_t o_x32[4] = {0, 0, 0, 0}, o_y32[3] = {0, 0, 0};
+    if (mixed) {
+        for (auto& v : o_x32) v = take(4 * n);
+        for (auto& v : o_y32) v = take(4 * m);
+    }
+    size_t o_x64[4], o_y64[3];
+    for (auto& v : o_x64) v = take(8 * n);
+    for (auto& v : o_y64) v = take(8 * m);
+    const bool adaptive = o.adaptive_step != 0;
+    const size_t o_prev_ax = adaptive ? take(8 * m) : 0, o_prev_xh = adaptive ? take(8 * n) : 0;
+    const size_t o_pi_x = take(8 * n), o_pi_y = take(8 * m), o_pi_xn = take(8 * n),
+                 o_pi_part = take(8 * 2 * d.nb_pi);
+    const size_t o_prow = take(8 * kRowSlots * d.nb_rows), o_pcol = take(8 * kColSlots * d.nb_cols);
+    const size_t o_st = take(sizeof(DevState)), o_dc = take(sizeof(DevConst)), o_ps = take(sizeof(PowerState));
+    d.arena_bytes = off;
+    PDLPX_CK(cudaMalloc(reinterpret_cast<void**>(&d.arena), d.arena_bytes));
+    PDLPX_CK(cudaMallocHost(reinterpret_cast<void**>(&d.h_st), sizeof(DevState)));
+    PDLPX_CK(cudaMallocHost(reinterpret_cast<void**>(&d.h_ps), sizeof(PowerState)));
+    char* b = d.arena;
+    d.a_ptr = reinterpret_cast<int*>(b + o_a_ptr);
+    d.a_idx = reinterpret_cast<int*>(b + o_a_idx);
+    d.at_ptr = reinterpret_cast<int*>(b + o_at_ptr);
+    d.at_idx = reinterpret_cast<int*>(b + o_at_idx);
+    d.a_v64 = reinterpret_cast<double*>(b + o_a_v64);
+    d.at_v64 = reinterpret_cast<double*>(b + o_at_v64);
+    if (mixed) {
+        d.a_v32 = reinterpret_cast<float*>(b + o_a_v32);
+        d.at_v32 = reinterpret_cast<float*>(b + o_at_v32);
+        d.cp32 = reinterpret_cast<ColPack<float>*>(b + o_cp32);
+        d.rp32 = reinterpret_cast<RowPack<float>*>(b + o_rp32);
+        d.xc32 = reinterpret_cast<float*>(b + o_x32[0]);
+        d.xi32 = reinterpret_cast<float*>(b + o_x32[1]);
+        d.xr32 = reinterpret_cast<float*>(b + o_x32[2]);
+        d.xh32 = reinterpret_cast<float*>(b + o_x32[3]);
+        d.yc32 = reinterpret_cast<float*>(b + o_y32[0]);
+        d.yi32 = reinterpret_cast<float*>(b + o_y32[1]);
+        d.yh32 = reinterpret_cast<float*>(b + o_y32[2]);
+    }
+    d.cp64 = reinterpret_cast<ColPack<double>*>(b + o_cp64);
+    d.rp64 = reinterpret_cast<RowPack<double>*>(b + o_rp64);
+    d.c64 = reinterpret_cast<double*>(b + o_c64);
+    d.lb64 = reinterpret_cast<double*>(b + o_lb64);
+    d.ub64 = reinterpret_cast<double*>(b + o_ub64);
+    d.cs64 = reinterpret_cast<double*>(b + o_cs64);
+    d.tau64 = reinterpret_cast<double*>(b + o_tau64);
+    d.rl64 = reinterpret_cast<double*>(b + o_rl64);
+    d.ru64 = reinterpret_cast<double*>(b + o_ru64);
+    d.rs64 = reinterpret_cast<double*>(b + o_rs64);
+    d.sig64 = reinterpret_cast<double*>(b + o_sig64);
+    d.xc64 = reinterpret_cast<double*>(b + o_x64[0]);
+    d.xi64 = reinterpret_cast<double*>(b + o_x64[1]);
+    d.xr64 = reinterpret_cast<double*>(b + o_x64[2]);
+    d.xh64 = reinterpret_cast<double*>(b + o_x64[3]);
+    d.yc64 = reinterpret_cast<double*>(b + o_y64[0]);
+    d.yi64 = reinterpret_cast<double*>(b + o_y64[1]);
+    d.yh64 = reinterpret_cast<double*>(b + o_y64[2]);
+    if (adaptive) {
+        d.prev_ax = reinterpret_cast<double*>(b + o_prev_ax);
+        d.prev_xh = reinterpret_cast<double*>(b + o_prev_xh);
+    }
+    d.pi_x = reinterpret_cast<double*>(b + o_pi_x);
+    d.pi_y = reinterpret_cast<double*>(b + o_pi_y);
+    d.pi_xn = reinterpret_cast<double*>(b + o_pi_xn);
+    d.pi_part = reinterpret_cast<double*>(b + o_pi_part);
+    d.part_rows = reinterpret_cast<double*>(b + o_prow);
+    d.part_cols = reinterpret_cast<double*>(b + o_pcol);
+    d.st = reinterpret_cast<DevState*>(b + o_st);
+    d.dc = reinterpret_cast<DevConst*>(b + o_dc);
+    d.ps = reinterpret_cast<PowerState*>(b + o_ps);
+
+    // Upload.
+    cudaStream_t s = d.stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return bytes == 0 ? cudaSuccess : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    PDLPX_CK(up(d.a_ptr, sc.a.ptr.data(), 4 * (m + 1)));
+    PDLPX_CK(up(d.a_idx, sc.a.idx.data(), 4 * nnz));
+    PDLPX_CK(up(d.at_ptr, sc.at.ptr.data(), 4 * (n + 1)));
+    PDLPX_CK(up(d.at_idx, sc.at.idx.data(), 4 * nnz));
+    PDLPX_CK(up(d.a_v64, sc.a.val.data(), 8 * nnz));
+    PDLPX_CK(up(d.at_v64, sc.at.val.data(), 8 * nnz));
+    std::vector<float> f32;
+    if (mixed) {
+        f32.assign(sc.a.val.begin(), sc.a.val.end());
+        PDLPX_CK(up(d.a_v32, f32.data(), 4 * nnz));
+        PDLPX_CK(cudaStreamSynchronize(s));
+        f32.assign(sc.at.val.begin(), sc.at.val.end());
+        PDLPX_CK(up(d.at_v32, f32.data(), 4 * nnz));
+        std::vector<ColPack<float>> cp;
+        std::vector<RowPack<float>> rp;
+        packCols(sc, cp);
+        packRows(sc, rp);
+        PDLPX_CK(up(d.cp32, cp.data(), 16 * n));
+        PDLPX_CK(up(d.rp32, rp.data(), 16 * m));
+        PDLPX_CK(cudaStreamSynchronize(s));
+    }
+    {
+        std::vector<ColPack<double>> cp;
+        std::vector<RowPack<double>> rp;
+        packCols(sc, cp);
+        packRows(sc, rp);
+        PDLPX_CK(up(d.cp64, cp.data(), 32 * n));
+        PDLPX_CK(up(d.rp64, rp.data(), 32 * m));
+        PDLPX_CK(up(d.c64, sc.c.data(), 8 * n));
+        PDLPX_CK(up(d.lb64, sc.cl.data(), 8 * n));
+        PDLPX_CK(up(d.ub64, sc.cu.data(), 8 * n));
+        PDLPX_CK(up(d.cs64, sc.col_scale.data(), 8 * n));
+        PDLPX_CK(up(d.tau64, sc.tau.data(), 8 * n));
+        PDLPX_CK(up(d.rl64, sc.rl.data(), 8 * m));
+        PDLPX_CK(up(d.ru64, sc.ru.data(), 8 * m));
+        PDLPX_CK(up(d.rs64, sc.row_scale.data(), 8 * m));
+        PDLPX_CK(up(d.sig64, sc.sigma.data(), 8 * m));
+        PDLPX_CK(cudaStreamSynchronize(s));
+    }
+    return PDLPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine() { pdlpx_options_default(&opt_); }
+Engine::~Engine() = default;
+
+int32_t Engine::load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const int32_t* ci,
+                     const double* v, const double* obj, const double* cl, const double* cu,
+                     const double* rl, const double* ru, int32_t sense, double offset) {
+    if (m < 0 || n < 0 || nnz < 0) {
+        last_error = "negative dimension";
+        return PDLPX_E_INVALID;
+    }
+    if ((n > 0 && (obj == nullptr || cl == nullptr || cu == nullptr)) ||
+        (m > 0 && (rl == nullptr || ru == nullptr))) {
+        last_error = "null bound / objective array";
+        return PDLPX_E_INVALID;
+    }
+    HostLp lp;
+    lp.m = m;
+    lp.n = n;
+    lp.maximize = sense == PDLPX_MAXIMIZE;
+    if (!canonicalCsr(m, n, nnz, rp, ci, v, lp.a)) {
+        last_error = "invalid CSR matrix";
+        return PDLPX_E_INVALID;
+    }
+    lp.obj.assign(obj, obj + n);
+    lp.cl.assign(cl, cl + n);
+    lp.cu.assign(cu, cu + n);
+    lp.rl.assign(rl, rl + m);
+    lp.ru.assign(ru, ru + m);
+    lp.offset = offset;
+    lp_ = std::move(lp);
+    loaded_ = true;
+    status_ = PDLPX_STATUS_ERROR;
+    objective_ = 0.0;
+    iterations_ = 0;
+    has_warm_ = false;
+    warm_x_.clear();
+    warm_y_.clear();
+    x_orig_.assign(static_cast<size_t>(n), 0.0);
+    y_orig_.assign(static_cast<size_t>(m), 0.0);
+    rescale();
+    return PDLPX_OK;
+}
+
+void Engine::rescale() {
+    buildScaled(lp_, opt_, sc_);
+    dev_.reset();
+}
+
+void Engine::setWarmStart(const double* x, int32_t nx, const double* y, int32_t ny) {
+    warm_x_.assign(x, x + std::max(0, nx));
+    warm_y_.assign(y, y + std::max(0, ny));
+    has_warm_ = true;
+}
+
+void Engine::clearWarmStart() {
+    warm_x_.clear();
+    warm_y_.clear();
+    has_warm_ = false;
+}
+
+void Engine::reducedCosts(std::vector<double>& rc) const {
+    rc.assign(static_cast<size_t>(lp_.n), 0.0);
+    if (!loaded_ || y_orig_.empty()) return;
+    std::vector<double> aty(static_cast<size_t>(lp_.n), 0.0);
+    csrMultiplyTranspose(lp_.a, y_orig_.data(), aty.data());
+    for (int32_t j = 0; j < lp_.n; ++j) rc[j] = lp_.obj[j] + aty[j];
+}
+
+void Engine::addRows(int32_t rows, const int32_t* starts, const int32_t* idx, const double* vals,
+                     int32_t nvals, const double* lo, const double* up) {
+    if (!loaded_ || rows <= 0 || starts == nullptr) return;
+    for (int32_t r = 0; r < rows; ++r) {
+        const int32_t s = starts[r], e = starts[r + 1];
+        if (s < 0 || e < s || e > nvals) return;
+    }
+    for (int32_t r = 0; r < rows; ++r) {
+        std::vector<std::pair<int32_t, double>> ent;
+        for (int32_t k = starts[r]; k < starts[r + 1]; ++k) ent.emplace_back(idx[k], vals[k]);
+        std::stable_sort(ent.begin(), ent.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (const auto& [c, v] : ent) {  // SparseMatrix::addRow keeps entries as given (sorted)
+            lp_.a.idx.push_back(c);
+            lp_.a.val.push_back(v);
+        }
+        lp_.a.ptr.push_back(static_cast<int32_t>(lp_.a.idx.size()));
+        lp_.rl.push_back(lo[r]);
+        lp_.ru.push_back(up[r]);
+    }
+    lp_.m += rows;
+    lp_.a.rows = lp_.m;
+    y_orig_.resize(static_cast<size_t>(lp_.m), 0.0);
+    rescale();
+}
+
+void Engine::removeRows(const int32_t* rows, int32_t count) {
+    if (!loaded_ || count <= 0 || rows == nullptr) return;
+    std::vector<int32_t> s(rows, rows + count);
+    std::sort(s.begin(), s.end());
+    s.erase(std::unique(s.begin(), s.end()), s.end());
+    std::vector<char> drop(static_cast<size_t>(lp_.m), 0);
+    for (int32_t r : s)
+        if (r >= 0 && r < lp_.m) drop[r] = 1;
+    Csr a;
+    a.cols = lp_.n;
+    std::vector<double> rl, ru;
+    for (int32_t i = 0; i < lp_.m; ++i) {
+        if (drop[i]) continue;
+        for (int32_t k = lp_.a.ptr[i]; k < lp_.a.ptr[i + 1]; ++k) {
+            a.idx.push_back(lp_.a.idx[k]);
+            a.val.push_back(lp_.a.val[k]);
+        }
+        a.ptr.push_back(static_cast<int32_t>(a.idx.size()));
+        rl.push_back(lp_.rl[i]);
+        ru.push_back(lp_.ru[i]);
+    }
+    a.rows = static_cast<int32_t>(rl.size());
+    lp_.a = std::move(a);
+    lp_.rl = std::move(rl);
+    lp_.ru = std::move(ru);
+    lp_.m = lp_.a.rows;
+    y_orig_.assign(static_cast<size_t>(lp_.m), 0.0);
+    rescale();
+}
+
+void Engine::setColBounds(int32_t col, double lo, double up) {
+    if (!loaded_ || col < 0 || col >= lp_.n) return;
+    lp_.cl[col] = lo;
+    lp_.cu[col] = up;
+    rescale();
+}
+
+void Engine::setObjective(const double* obj, int32_t n) {
+    if (!loaded_ || obj == nullptr || n != lp_.n) return;
+    lp_.obj.assign(obj, obj + n);
+    rescale();
+}
+
+int32_t Engine::solveTrivial(pdlpx_result* out) {
+    const int32_t m = lp_.m, n = lp_.n;
+    if (n == 0) {  // pdlp.cpp:813-820
+        status_ = PDLPX_STATUS_OPTIMAL;
+        objective_ = lp_.offset;
+        iterations_ = 0;
+        x_orig_.clear();
+        y_orig_.assign(static_cast<size_t>(m), 0.0);
+    } else {  // m == 0: bounds-only LP, pdlp.cpp:823-860
+        x_orig_.resize(static_cast<size_t>(n));
+        double ov = lp_.offset;
+        bool unbounded = false;
+        for (int32_t j = 0; j < n; ++j) {
+            const double c = sc_.c[j], lb = sc_.cl[j], ub = sc_.cu[j];
+            double xj;
+            if (c > 0.0) {
+                if (!std::isfinite(lb)) {
+                    unbounded = true;
+                    break;
+                }
+                xj = lb;
+            } else if (c < 0.0) {
+                if (!std::isfinite(ub)) {
+                    unbounded = true;
+                    break;
+                }
+                xj = ub;
+            } else {
+                xj = std::isfinite(lb) ? lb : (std::isfinite(ub) ? ub : 0.0);
+            }
+            x_orig_[j] = xj * sc_.col_scale[j] / sc_.con_scale;
+            ov += lp_.obj[j] * x_orig_[j];
+        }
+        iterations_ = 0;
+        if (unbounded) {
+            status_ = PDLPX_STATUS_UNBOUNDED;
+            objective_ = 0.0;
+        } else {
+            y_orig_.assign(static_cast<size_t>(m), 0.0);
+            objective_ = ov;
+            status_ = PDLPX_STATUS_OPTIMAL;
+        }
+    }
+    used_gpu_ = false;
+    std::memset(out, 0, sizeof(*out));
+    out->status = status_;
+    out->objective = objective_;
+    return PDLPX_OK;
+}
+
+int32_t Engine::solve(pdlpx_result* out) {
+    if (out == nullptr) {
+        last_error = "null result";
+        return PDLPX_E_INVALID;
+    }
+    if (!loaded_) {  // pdlp.cpp:802-805
+        status_ = PDLPX_STATUS_ERROR;
+        std::memset(out, 0, sizeof(*out));
+        out->status = status_;
+        last_error = "solve before load";
+        return PDLPX_E_NOT_LOADED;
+    }
+    if (opt_.anderson_acceleration && opt_.anderson_window_size >= 2) {
+        last_error = "anderson_acceleration is not available in the device engine";
+        return PDLPX_E_INVALID;
+    }
+    if (opt_.termination_eval_frequency <= 0) {
+        last_error = "termination_eval_frequency must be positive";
+        return PDLPX_E_INVALID;
+    }
+    if (lp_.n == 0 || lp_.m == 0) return solveTrivial(out);
+    const int32_t rc = solveDevice(out);
+    if (rc != PDLPX_OK) {
+        status_ = PDLPX_STATUS_ERROR;
+        objective_ = 0.0;
+        out->status = status_;
+    }
+    return rc;
+}
+
+int32_t Engine::solveDevice(pdlpx_result* out) {
+    std::string& err = last_error;
+    const auto t0 = std::chrono::steady_clock::now();
+    std::memset(out, 0, sizeof(*out));
+    used_gpu_ = false;
+    const bool want_mixed = opt_.precision != PDLPX_PREC_FP64;
+    if (!dev_ || dev_->mixed != want_mixed || (opt_.adaptive_step != 0) != (dev_->prev_ax != nullptr)) {
+        const int32_t rc = buildDevice(dev_, sc_, opt_, err);
+        if (rc != PDLPX_OK) {
+            dev_.reset();
+            return rc;
+        }
+    }
+    DeviceLp& d = *dev_;
+    PDLPX_CK(cudaSetDevice(d.device));
+    cudaStream_t s = d.stream;
+    const int32_t m = lp_.m, n = lp_.n;
+    const int N = opt_.termination_eval_frequency;
+    int launches = 0;
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PDLPX_CK(cudaEventCreate(&ev0));
+    PDLPX_CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev_guard{ev0, ev1};
+    PDLPX_CK(cudaEventRecord(ev0, s));
+
+    // ---- power iteration (start vector: mt19937(42) normals, pdlp.cpp:1990-2001)
+    double step = 1.0;
+    {
+        std::mt19937 rng(42);
+        std::normal_distribution<double> dist(0.0, 1.0);
+        std::vector<double> x0(static_cast<size_t>(n));
+        for (auto& v : x0) v = dist(rng);
+        double xn = 0.0;
+        for (double v : x0) xn += v * v;
+        xn = std::sqrt(xn);
+        if (xn < 1e-15) xn = 1.0;
+        for (auto& v : x0) v /= xn;
+        PDLPX_CK(cudaMemcpyAsync(d.pi_x, x0.data(), 8 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        PowerState ps0{1.0, 0.0, 0.0, 0, opt_.sv_max_iter <= 0 ? 1 : 0};
+        *d.h_ps = ps0;
+        PDLPX_CK(cudaMemcpyAsync(d.ps, d.h_ps, sizeof(PowerState), cudaMemcpyHostToDevice, s));
+        PowerArgs pa{};
+        pa.x = d.pi_x;
+        pa.y = d.pi_y;
+        pa.xn = d.pi_xn;
+        pa.part = d.pi_part;
+        pa.ps = d.ps;
+        pa.m = m;
+        pa.n = n;
+        pa.max_iter = opt_.sv_max_iter;
+        pa.nb = d.nb_pi;
+        pa.tol = opt_.sv_tol;
+        if (!d.power) {
+            // FP32 matrix values in mixed mode, FP64 in FP64 mode; vectors and sums FP64.
+            cudaGraph_t g = nullptr;
+            PDLPX_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            if (d.mixed) {
+                const PowerMat<float> mt{d.a_ptr, d.a_idx, d.a_v32, d.at_ptr, d.at_idx, d.at_v32};
+                d.launches_power = launchPowerChunk(d, pa, mt, DeviceLp::kPowerChunk);
+            } else {
+                const PowerMat<double> mt{d.a_ptr, d.a_idx, d.a_v64, d.at_ptr, d.at_idx, d.at_v64};
+                d.launches_power = launchPowerChunk(d, pa, mt, DeviceLp::kPowerChunk);
+            }
+            PDLPX_CK(cudaStreamEndCapture(s, &g));
+            const cudaError_t ie = cudaGraphInstantiate(&d.power, g, 0);
+            cudaGraphDestroy(g);
+            PDLPX_CK(ie);
+        }
+        for (int guard = 0; guard < 1 + opt_.sv_max_iter / DeviceLp::kPowerChunk + 1; ++guard) {
+            if (d.h_ps->done) break;
+            PDLPX_CK(cudaGraphLaunch(d.power, s));
+            launches += d.launches_power;
+            PDLPX_CK(cudaMemcpyAsync(d.h_ps, d.ps, sizeof(PowerState), cudaMemcpyDeviceToHost, s));
+            PDLPX_CK(cudaStreamSynchronize(s));
+        }
+        const double spectral = std::sqrt(std::max(d.h_ps->s2, 1e-12));
+        step = 0.998 / spectral;
+    }
+
+    // ---- constants and initial state
+    DevConst dc{};
+    dc.m = m;
+    dc.n = n;
+    dc.N = N;
+    dc.max_iter = opt_.max_iter;
+    dc.polish_max_iter = opt_.polish_max_iter;
+    dc.linf = opt_.optimality_norm == PDLPX_NORM_LINF;
+    dc.update_pw = opt_.update_primal_weight != 0;
+    dc.enable_polish = opt_.enable_polishing != 0;
+    dc.mixed = d.mixed;
+    dc.fp64_switch = opt_.fp64_switch != 0;
+    dc.adaptive = opt_.adaptive_step != 0;
+    dc.precond_refresh = opt_.preconditioner_refresh != 0;
+    dc.nb_rows = d.nb_rows;
+    dc.nb_cols = d.nb_cols;
+    dc.stall_limit = 30;
+    dc.primal_tol = opt_.primal_tol;
+    dc.dual_tol = opt_.dual_tol;
+    dc.opt_tol = opt_.optimality_tol;
+    dc.polish_ptol = opt_.polish_primal_tol;
+    dc.polish_dtol = opt_.polish_dual_tol;
+    dc.kp = opt_.pid_kp;
+    dc.ki = opt_.pid_ki;
+    dc.kd = opt_.pid_kd;
+    dc.ismooth = opt_.pid_i_smooth;
+    dc.suff = opt_.restart_sufficient_decay;
+    dc.nec = opt_.restart_necessary_decay;
+    dc.art = opt_.restart_artificial_fraction;
+    terminationNorms(lp_, opt_.optimality_norm, dc.c_norm, dc.b_norm);
+    dc.obj_sign = sc_.obj_sign;
+    dc.obj_scale = sc_.obj_scale;
+    dc.con_scale = sc_.con_scale;
+    dc.offset = lp_.offset;
+    dc.step_lb = step * opt_.adaptive_step_min;
+    dc.step_ub = step * opt_.adaptive_step_max;
+    dc.step_down = opt_.adaptive_step_down;
+    dc.step_up = opt_.adaptive_step_up;
+    dc.precond_ratio = opt_.preconditioner_refresh_ratio;
+    dc.switch_score = 0.0;
+    PDLPX_CK(cudaMemcpyAsync(d.dc, &dc, sizeof(DevConst), cudaMemcpyHostToDevice, s));
+
+    DevState st0{};
+    st0.step = step;
+    st0.pw = opt_.primal_weight;
+    st0.tau_fac = static_cast<float>(step / st0.pw);
+    st0.sig_fac = static_cast<float>(step * st0.pw);
+    st0.prec = d.mixed ? 0 : 1;
+    st0.fpe0 = -1.0;
+    st0.last_fpe = std::numeric_limits<double>::infinity();
+    st0.best_pw = st0.pw;
+    st0.best_score = std::numeric_limits<double>::infinity();
+    st0.best_kkt = std::numeric_limits<double>::infinity();
+    st0.precond_pw = sc_.precond_pw;
+    *d.h_st = st0;
+    PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+
+    // ---- initial iterates (zero or warm start, pdlp.cpp:1812-1827)
+    const bool warm = has_warm_ && static_cast<int32_t>(warm_x_.size()) == n &&
+                      static_cast<int32_t>(warm_y_.size()) == m;
+    std::vector<double> wx, wy;
+    if (warm) {
+        wx.resize(n);
+        wy.resize(m);
+        for (int32_t j = 0; j < n; ++j) wx[j] = warm_x_[j] / sc_.col_scale[j] * sc_.con_scale;
+        for (int32_t i = 0; i < m; ++i) wy[i] = warm_y_[i] * sc_.obj_scale / (sc_.obj_sign * sc_.row_scale[i]);
+    }
+    if (d.mixed) {
+        std::vector<float> fx(n, 0.0f), fy(m, 0.0f);
+        if (warm) {
+            for (int32_t j = 0; j < n; ++j) fx[j] = static_cast<float>(wx[j]);
+            for (int32_t i = 0; i < m; ++i) fy[i] = static_cast<float>(wy[i]);
+        }
+        for (float* p : {d.xc32, d.xi32, d.xh32, d.xr32})
+            PDLPX_CK(cudaMemcpyAsync(p, fx.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        for (float* p : {d.yc32, d.yi32, d.yh32})
+            PDLPX_CK(cudaMemcpyAsync(p, fy.data(), 4 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
+        PDLPX_CK(cudaStreamSynchronize(s));
+    } else {
+        if (!warm) {
+            wx.assign(n, 0.0);
+            wy.assign(m, 0.0);
+        }
+        for (double* p : {d.xc64, d.xi64, d.xh64, d.xr64})
+            PDLPX_CK(cudaMemcpyAsync(p, wx.data(), 8 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        for (double* p : {d.yc64, d.yi64, d.yh64})
+            PDLPX_CK(cudaMemcpyAsync(p, wy.data(), 8 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
+        PDLPX_CK(cudaStreamSynchronize(s));
+    }
+    if (d.prev_ax) {
+        PDLPX_CK(cudaMemsetAsync(d.prev_ax, 0, 8 * static_cast<size_t>(m), s));
+        PDLPX_CK(cudaMemsetAsync(d.prev_xh, 0, 8 * static_cast<size_t>(n), s));
+    }
+
+    // ---- capture the restart-cycle graphs lazily
+    auto ensureCycle = [&](int prec) -> int32_t {
+        if (d.cycle[prec] && d.cycle_N[prec] == N) return PDLPX_OK;
+        if (d.cycle[prec]) {
+            cudaGraphExecDestroy(d.cycle[prec]);
+            d.cycle[prec] = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        PDLPX_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        d.launches_cycle[prec] = prec == 0 ? launchCycle<float>(d, opt_) : launchCycle<double>(d, opt_);
+        PDLPX_CK(cudaStreamEndCapture(s, &g));
+        const cudaError_t ie = cudaGraphInstantiate(&d.cycle[prec], g, 0);
+        cudaGraphDestroy(g);
+        PDLPX_CK(ie);
+        d.cycle_N[prec] = N;
+        return PDLPX_OK;
+    };
+
+    used_gpu_ = true;
+    bool stopped = false, timed_out = false;
+    int switch_total = -1;
+    int prec = d.mixed ? 0 : 1;
+    while (true) {
+        if (timeUp(t0, opt_.max_solve_seconds)) {
+            timed_out = true;
+            break;
+        }
+        if (stop_flag_ != nullptr && __atomic_load_n(stop_flag_, __ATOMIC_RELAXED) != 0) {
+            stopped = true;
+            break;
+        }
+        const int32_t rc = ensureCycle(prec);
+        if (rc != PDLPX_OK) return rc;
+        PDLPX_CK(cudaGraphLaunch(d.cycle[prec], s));
+        launches += d.launches_cycle[prec];
+        PDLPX_CK(cudaMemcpyAsync(d.h_st, d.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        PDLPX_CK(cudaStreamSynchronize(s));
+        const DevState& h = *d.h_st;
+        if (opt_.verbose && (h.total <= N || h.total % (10 * N) == 0)) {
+            std::printf("PDLP %7d  pobj=% .8e  pinf=% .2e  dinf=% .2e  gap=% .2e  fpe=% .2e  pw=% .2e  step=% .2e  [B200%s]\n",
+                        h.total, h.pobj, h.pterm, h.dterm, h.gap, h.fpe, h.pw, h.step,
+                        h.prec == 0 ? " fp32" : " fp64");
+            std::fflush(stdout);
+        }
+        if (h.done) break;
+        if (h.prec != prec) {
+            prec = h.prec;
+            switch_total = h.total;
+        }
+    }
+    PDLPX_CK(cudaEventRecord(ev1, s));
+    PDLPX_CK(cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+
+    const DevState fin = *d.h_st;
+    int32_t status;
+    if (fin.done) {
+        status = fin.status;
+        if (status == PDLPX_STATUS_ITER_LIMIT && timeUp(t0, opt_.max_solve_seconds)) status = PDLPX_STATUS_TIME_LIMIT;
+    } else if (fin.converged) {
+        status = PDLPX_STATUS_OPTIMAL;  // polish interrupted (pdlp.cpp:2546-2550)
+    } else {
+        status = stopped ? PDLPX_STATUS_ITER_LIMIT : PDLPX_STATUS_TIME_LIMIT;
+    }
+    (void)timed_out;
+
+    // ---- results (pdlp.cpp:2678-2712)
+    const int fprec = fin.prec;
+    std::vector<double> xh(n), yh(m);
+    if (status == PDLPX_STATUS_OPTIMAL || status == PDLPX_STATUS_INFEASIBLE || status == PDLPX_STATUS_UNBOUNDED) {
+        if (fprec == 0) {
+            std::vector<float> fx(n), fy(m);
+            PDLPX_CK(cudaMemcpyAsync(fx.data(), d.xh32, 4 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, s));
+            PDLPX_CK(cudaMemcpyAsync(fy.data(), d.yh32, 4 * static_cast<size_t>(m), cudaMemcpyDeviceToHost, s));
+            PDLPX_CK(cudaStreamSynchronize(s));
+            for (int32_t j = 0; j < n; ++j) xh[j] = fx[j];
+            for (int32_t i = 0; i < m; ++i) yh[i] = fy[i];
+        } else {
+            PDLPX_CK(cudaMemcpyAsync(xh.data(), d.xh64, 8 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, s));
+            PDLPX_CK(cudaMemcpyAsync(yh.data(), d.yh64, 8 * static_cast<size_t>(m), cudaMemcpyDeviceToHost, s));
+            PDLPX_CK(cudaStreamSynchronize(s));
+        }
+    }
+    objective_ = 0.0;
+    if (status == PDLPX_STATUS_OPTIMAL) {
+        x_orig_.resize(n);
+        const double ic = 1.0 / sc_.con_scale;
+        for (int32_t j = 0; j < n; ++j) {
+            double xj = xh[j] * sc_.col_scale[j] * ic;
+            if (std::isfinite(lp_.cl[j])) xj = std::max(xj, lp_.cl[j]);
+            if (std::isfinite(lp_.cu[j])) xj = std::min(xj, lp_.cu[j]);
+            x_orig_[j] = xj;
+        }
+        y_orig_.resize(m);
+        const double io = 1.0 / sc_.obj_scale;
+        for (int32_t i = 0; i < m; ++i) y_orig_[i] = sc_.obj_sign * yh[i] * sc_.row_scale[i] * io;
+        double ov = lp_.offset;
+        for (int32_t j = 0; j < n; ++j) ov += lp_.obj[j] * x_orig_[j];
+        objective_ = ov;
+    } else if (status == PDLPX_STATUS_INFEASIBLE) {
+        y_orig_.resize(m);
+        const double io = 1.0 / sc_.obj_scale;
+        for (int32_t i = 0; i < m; ++i) y_orig_[i] = sc_.obj_sign * yh[i] * sc_.row_scale[i] * io;
+    } else if (status == PDLPX_STATUS_UNBOUNDED) {
+        x_orig_.resize(n);
+        const double ic = 1.0 / sc_.con_scale;
+        for (int32_t j = 0; j < n; ++j) x_orig_[j] = xh[j] * sc_.col_scale[j] * ic;
+    }
+    status_ = status;
+    iterations_ = fin.total;
+
+    out->status = status;
+    out->objective = objective_;
+    out->iterations = fin.total;
+    out->work_units = static_cast<double>(fin.total) *
+                      (4.0 * static_cast<double>(sc_.a.nnz()) + 2.0 * static_cast<double>(m + n));
+    out->rel_primal_resid = fin.pterm;
+    out->rel_dual_resid = fin.dterm;
+    out->rel_gap = fin.gap;
+    out->primal_objective = fin.pobj;
+    out->dual_objective = fin.dobj;
+    out->fp64_iterations = d.mixed ? (switch_total >= 0 ? fin.total - switch_total : 0) : fin.total;
+    out->restarts = fin.restarts;
+    out->step_size = fin.step;
+    out->primal_weight = fin.pw;
+    out->solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    out->device_seconds = ms * 1e-3;
+    out->used_gpu = 1;
+    out->kernel_launches = launches;
+    return PDLPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel timing (roofline numerator): eager launches between CUDA events on the
+// engine's stream, on a scratch copy of the solver state so that the step
+// kernels are active; the saved state is restored afterwards.
+// ---------------------------------------------------------------------------
+namespace {
+template <class T>
+int32_t timeStepKernels(DeviceLp& d, const pdlpx_options& o, int reps, float ms[3], std::string& err) {
+    const IterArgs<T> ia = iterArgs<T>(d, o);
+    const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
+    cudaStream_t s = d.stream;
+    const int gp = gridFor(d.n, d.gAT), gd = gridFor(d.m, d.gA);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) PDLPX_CK(cudaEventCreate(&e));
+    // warm-up launch of each
+    PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_CK(cudaEventRecord(ev[0], s));
+    for (int r = 0; r < reps; ++r) PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_CK(cudaEventRecord(ev[1], s));
+    for (int r = 0; r < reps; ++r) PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_CK(cudaEventRecord(ev[2], s));
+    for (int r = 0; r < reps; ++r) {
+        PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
+        PDLPX_G_SWITCH(d.gAT, (checkCols<GG, T><<<d.nb_cols, kBlock, 0, s>>>(ca)));
+    }
+    PDLPX_CK(cudaEventRecord(ev[3], s));
+    PDLPX_CK(cudaGetLastError());
+    PDLPX_CK(cudaEventSynchronize(ev[3]));
+    for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    return PDLPX_OK;
+}
+}  // namespace
+
+int32_t Engine::timeKernels(int32_t reps, double* ms_primal, double* ms_dual, double* ms_check) {
+    std::string& err = last_error;
+    if (!dev_ || !used_gpu_) {
+        err = "time_kernels needs a completed device solve";
+        return PDLPX_E_NOT_LOADED;
+    }
+    if (reps <= 0) reps = 1;
+    DeviceLp& d = *dev_;
+    PDLPX_CK(cudaSetDevice(d.device));
+    cudaStream_t s = d.stream;
+    DevState saved{};
+    PDLPX_CK(cudaMemcpyAsync(&saved, d.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    PDLPX_CK(cudaStreamSynchronize(s));
+    DevState t = saved;
+    t.done = 0;
+    t.phase = 0;
+    t.total = 0;
+    t.inner = 0;
+    *d.h_st = t;
+    PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+    float ms[3] = {0, 0, 0};
+    const int32_t rc = t.prec == 0 ? timeStepKernels<float>(d, opt_, reps, ms, err)
+                                   : timeStepKernels<double>(d, opt_, reps, ms, err);
+    *d.h_st = saved;
+    PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+    PDLPX_CK(cudaStreamSynchronize(s));
+    if (rc != PDLPX_OK) return rc;
+    if (ms_primal) *ms_primal = ms[0] / reps;
+    if (ms_dual) *ms_dual = ms[1] / reps;
+    if (ms_check) *ms_check = ms[2] / reps;
+    return PDLPX_OK;
+}
+
+int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const {
+    if (!dev_) return PDLPX_E_NOT_LOADED;
+    if (ga) *ga = dev_->gA;
+    if (gat) *gat = dev_->gAT;
+    if (bp) *bp = gridFor(dev_->n, dev_->gAT);
+    if (bd) *bd = gridFor(dev_->m, dev_->gA);
+    return PDLPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Parity entry point: one SpMV with the engine's kernel.
+// ---------------------------------------------------------------------------
+int32_t deviceSpmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* rp, const int32_t* ci,
+                   const double* val, const double* x, double* y, int32_t precision, int32_t group,
+                   std::string& err) {
+    if (rows < 0 || cols < 0 || nnz < 0 || (rows > 0 && (rp == nullptr || y == nullptr)) ||
+        (nnz > 0 && (ci == nullptr || val == nullptr)) || (cols > 0 && x == nullptr)) {
+        err = "invalid argument";
+        return PDLPX_E_INVALID;
+    }
+    if (rows == 0) return PDLPX_OK;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        err = "no CUDA device visible";
+        return PDLPX_E_NO_DEVICE;
+    }
+    const int G = group > 0 ? group : pickGroup(nnz, rows);
+    const bool f64 = precision == PDLPX_PREC_FP64;
+    const size_t vb = f64 ? 8 : 4;
+    char* buf = nullptr;
+    const size_t o_rp = 0, o_ci = o_rp + ((4 * (static_cast<size_t>(rows) + 1) + 255) & ~size_t(255)),
+                 o_v = o_ci + ((4 * static_cast<size_t>(nnz) + 255) & ~size_t(255)),
+                 o_x = o_v + ((vb * nnz + 255) & ~size_t(255)), o_y = o_x + ((vb * cols + 255) & ~size_t(255)),
+                 total = o_y + vb * rows;
+    PDLPX_CK(cudaMalloc(reinterpret_cast<void**>(&buf), total));
+    struct Free {
+        char* p;
+        ~Free() { cudaFree(p); }
+    } guard{buf};
+    PDLPX_CK(cudaMemcpy(buf + o_rp, rp, 4 * (static_cast<size_t>(rows) + 1), cudaMemcpyHostToDevice));
+    if (nnz > 0) PDLPX_CK(cudaMemcpy(buf + o_ci, ci, 4 * static_cast<size_t>(nnz), cudaMemcpyHostToDevice));
+    const int grid = gridFor(rows, G);
+    if (f64) {
+        if (nnz > 0) PDLPX_CK(cudaMemcpy(buf + o_v, val, 8 * static_cast<size_t>(nnz), cudaMemcpyHostToDevice));
+        if (cols > 0) PDLPX_CK(cudaMemcpy(buf + o_x, x, 8 * static_cast<size_t>(cols), cudaMemcpyHostToDevice));
+        PDLPX_G_SWITCH(G, (spmvKernel<GG, double><<<grid, kBlock>>>(
+                              rows, reinterpret_cast<int*>(buf + o_rp), reinterpret_cast<int*>(buf + o_ci),
+                              reinterpret_cast<double*>(buf + o_v), reinterpret_cast<double*>(buf + o_x),
+                              reinterpret_cast<double*>(buf + o_y))));
+        PDLPX_CK(cudaGetLastError());
+        PDLPX_CK(cudaMemcpy(y, buf + o_y, 8 * static_cast<size_t>(rows), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> fv(val, val + nnz), fx(x, x + cols), fy(rows);
+        if (nnz > 0) PDLPX_CK(cudaMemcpy(buf + o_v, fv.data(), 4 * static_cast<size_t>(nnz), cudaMemcpyHostToDevice));
+        if (cols > 0) PDLPX_CK(cudaMemcpy(buf + o_x, fx.data(), 4 * static_cast<size_t>(cols), cudaMemcpyHostToDevice));
+        PDLPX_G_SWITCH(G, (spmvKernel<GG, float><<<grid, kBlock>>>(
+                              rows, reinterpret_cast<int*>(buf + o_rp), reinterpret_cast<int*>(buf + o_ci),
+                              reinterpret_cast<float*>(buf + o_v), reinterpret_cast<float*>(buf + o_x),
+                              reinterpret_cast<float*>(buf + o_y))));
+        PDLPX_CK(cudaGetLastError());
+        PDLPX_CK(cudaMemcpy(fy.data(), buf + o_y, 4 * static_cast<size_t>(rows), cudaMemcpyDeviceToHost));
+        for (int32_t i = 0; i < rows; ++i) y[i] = fy[i];
+    }
+    return PDLPX_OK;
+}
+
+}  // namespace pdlpx

@@ -1,0 +1,91 @@
+// Engine: one LP, its scaled copy, its device image and the solve loop.
+// This is the C++ host side behind the C ABI (pdlpx.h); its public methods
+// mirror mipx::PdlpSolver (include/mipx/pdlp.h:89-174).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pdlpx.h"
+#include "problem.hpp"
+
+namespace pdlpx {
+
+struct DeviceLp;  // device buffers, graphs (engine.cu)
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    void setOptions(const pdlpx_options& o) { opt_ = o; }
+    const pdlpx_options& options() const { return opt_; }
+
+    // Copies the problem (PdlpSolver::load, pdlp.cpp:445-455).  Returns PDLPX_*.
+    int32_t load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const int32_t* ci,
+                 const double* v, const double* obj, const double* cl, const double* cu,
+                 const double* rl, const double* ru, int32_t sense, double offset);
+    int32_t solve(pdlpx_result* out);
+
+    void setWarmStart(const double* x, int32_t nx, const double* y, int32_t ny);
+    void clearWarmStart();
+    void setStopFlag(const int32_t* f) { stop_flag_ = f; }
+
+    bool loaded() const { return loaded_; }
+    int32_t status() const { return status_; }
+    double objective() const { return objective_; }
+    bool usedGpu() const { return used_gpu_; }
+    const std::vector<double>& primal() const { return x_orig_; }
+    const std::vector<double>& dual() const { return y_orig_; }
+    void reducedCosts(std::vector<double>& rc) const;
+    const HostLp& problem() const { return lp_; }
+    const ScaledLp& scaled() const { return sc_; }
+
+    // Incremental edits (pdlp.cpp:2833-2907): edit the original, rescale.
+    void addRows(int32_t rows, const int32_t* starts, const int32_t* idx, const double* vals,
+                 int32_t nvals, const double* lo, const double* up);
+    void removeRows(const int32_t* rows, int32_t count);
+    void setColBounds(int32_t col, double lo, double up);
+    void setObjective(const double* obj, int32_t n);
+
+    // Kernel timing for the roofline report (pdlpx_time_kernels).
+    int32_t timeKernels(int32_t reps, double* ms_primal, double* ms_dual, double* ms_check);
+    int32_t launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const;
+
+    std::string last_error;
+
+private:
+    void rescale();
+    int32_t solveTrivial(pdlpx_result* out);
+    int32_t solveDevice(pdlpx_result* out);
+
+    pdlpx_options opt_{};
+    HostLp lp_;
+    ScaledLp sc_;
+    bool loaded_ = false;
+    std::vector<double> warm_x_, warm_y_;
+    bool has_warm_ = false;
+    const int32_t* stop_flag_ = nullptr;
+
+    int32_t status_ = PDLPX_STATUS_ERROR;
+    double objective_ = 0.0;
+    int32_t iterations_ = 0;
+    bool used_gpu_ = false;
+    std::vector<double> x_orig_, y_orig_;
+
+    std::unique_ptr<DeviceLp> dev_;
+};
+
+// Threads per row for the CSR kernels, from the mean row length.
+int32_t pickGroup(int64_t nnz, int32_t rows);
+
+// Device SpMV used by pdlpx_csr_spmv (host buffers in/out).
+int32_t deviceSpmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* rp, const int32_t* ci,
+                   const double* val, const double* x, double* y, int32_t precision, int32_t group,
+                   std::string& err);
+
+}  // namespace pdlpx

