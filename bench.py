@@ -49,13 +49,15 @@ TOL = 1e-6
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=2)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--supplies", type=int, default=1000)
     p.add_argument("--demands", type=int, default=1000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--verbose", action="store_true")
+    p.add_argument("--profile", type=int, default=0, metavar="ITERS",
+                   help="profiling run: one solve of the workload capped at ITERS iterations, no JSON line")
     return p.parse_args()
 
 
@@ -234,6 +236,15 @@ def main():
     lp, _ = G.transport_lp(args.supplies, args.demands, 7)
     m, n, nnz = lp.num_rows, lp.num_cols, lp.matrix.numNonzeros()
     opts = PdlpOptions(verbose=args.verbose, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local)
+    if args.profile:
+        opts.max_iter = args.profile
+        s = PdlpSolver()
+        s.setOptions(opts)
+        s.load(lp)
+        r = s.solve()
+        print(f"profile run: status={int(r.status)} iterations={r.iterations} launches={r.kernel_launches} "
+              f"config={s.launchConfig()}", flush=True)
+        return
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     solver = PdlpSolver()

@@ -114,7 +114,9 @@ typedef struct pdlpx_options {
     int32_t fp64_switch;              /* mixed mode: FP32 phase hands over to FP64 when its KKT stalls (1) */
     int32_t spmv_group_a;             /* 0 = autotune; else threads per row of A (1,2,4,8,16,32) */
     int32_t spmv_group_at;            /* 0 = autotune; else threads per row of A^T */
-    int32_t reserved[8];
+    int32_t autotune;                 /* 1: time the step kernels' launch shapes on LPs with >= 100k
+                                         nonzeros and keep the fastest; 0: row-length heuristic */
+    int32_t reserved[7];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

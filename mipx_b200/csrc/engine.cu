@@ -42,12 +42,10 @@ __global__ void __launch_bounds__(kBlock) promoteIterates(PromoteArgs a) {
     const int total = a.n > a.m ? a.n : a.m;
     for (int k = blockIdx.x * kBlock + threadIdx.x; k < total; k += gridDim.x * kBlock) {
         if (k < a.n) {
-            a.xc64[k] = a.xc[k];
             a.xi64[k] = a.xi[k];
             a.xh64[k] = a.xh[k];
         }
         if (k < a.m) {
-            a.yc64[k] = a.yc[k];
             a.yi64[k] = a.yi[k];
             a.yh64[k] = a.yh[k];
         }
@@ -257,19 +255,24 @@ __device__ void controlStep(DevState& s, const DevConst& c, const double* rows, 
         }
     }
 
-    // Mixed precision: hand the iterates to FP64 when the FP32 phase stops improving.
+    // Mixed precision: hand the iterates to FP64 when the FP32 phase stalls close
+    // to the tolerance (score = worst KKT term / its tolerance <= switch_score).
+    // Far from the tolerance FP32 rounding is not what limits progress, so long
+    // PDHG plateaus there stay in FP32.
     if (c.mixed && c.fp64_switch && s.prec == 0 && !s.done) {
         const double pt = s.phase == 0 ? c.primal_tol : c.polish_ptol;
         const double dt = s.phase == 0 ? c.dual_tol : c.polish_dtol;
         double score = fmax(pterm / pt, dterm / dt);
         if (s.phase == 0) score = fmax(score, gap / c.opt_tol);
-        if (score < 0.7 * s.best_kkt) {
-            s.best_kkt = score;
-            s.stall = 0;
-        } else {
-            s.stall += 1;
+        if (score <= c.switch_score) {
+            if (score < 0.7 * s.best_kkt) {
+                s.best_kkt = score;
+                s.stall = 0;
+            } else {
+                s.stall += 1;
+            }
+            if (s.stall >= c.stall_limit) s.promote = 1;
         }
-        if (s.stall >= c.stall_limit || (c.switch_score > 0.0 && score <= c.switch_score)) s.promote = 1;
     }
     s.tau_fac = static_cast<float>(s.step / s.pw);
     s.sig_fac = static_cast<float>(s.step * s.pw);
@@ -355,6 +358,50 @@ __global__ void __launch_bounds__(kBlock) powerFinish2(PowerArgs a) {
         default: { constexpr int GG = 256; CALL; } break;  \
     }
 
+#define PDLPX_SHAPE_CASE(I, CALL)                                                         \
+    case I: {                                                                             \
+        constexpr int GG = kShapes[I].G, RR = kShapes[I].R, UU = kShapes[I].U;            \
+        CALL;                                                                             \
+    } break;
+#define PDLPX_SHAPE_SWITCH(S, CALL)                                                                        \
+    switch (S) {                                                                                           \
+        PDLPX_SHAPE_CASE(0, CALL) PDLPX_SHAPE_CASE(1, CALL) PDLPX_SHAPE_CASE(2, CALL)                      \
+        PDLPX_SHAPE_CASE(3, CALL) PDLPX_SHAPE_CASE(4, CALL) PDLPX_SHAPE_CASE(5, CALL)                      \
+        PDLPX_SHAPE_CASE(6, CALL) PDLPX_SHAPE_CASE(7, CALL) PDLPX_SHAPE_CASE(8, CALL)                      \
+        PDLPX_SHAPE_CASE(9, CALL) PDLPX_SHAPE_CASE(10, CALL) PDLPX_SHAPE_CASE(11, CALL)                    \
+        PDLPX_SHAPE_CASE(12, CALL) PDLPX_SHAPE_CASE(13, CALL) PDLPX_SHAPE_CASE(14, CALL)                   \
+        default: {                                                                                         \
+            constexpr int GG = kShapes[15].G, RR = kShapes[15].R, UU = kShapes[15].U;                      \
+            CALL;                                                                                          \
+        } break;                                                                                           \
+    }
+static_assert(kNumShapes == 16, "shape switch covers 16 shapes");
+
+static int gridForShape(int64_t rows, int shape) {
+    const int64_t per_block = static_cast<int64_t>(kBlock / kShapes[shape].G) * kShapes[shape].R;
+    return static_cast<int>(std::max<int64_t>(1, (rows + per_block - 1) / per_block));
+}
+
+// Default launch shape from the mean row length (the autotuner's starting point).
+static int defaultShape(int64_t nnz, int32_t rows) {
+    const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
+    if (mean <= 3) return 2;    // G=1, R=4
+    if (mean <= 6) return 4;    // G=2, R=2
+    if (mean <= 12) return 5;   // G=4
+    if (mean <= 24) return 7;   // G=8
+    if (mean <= 48) return 8;   // G=16
+    if (mean <= 128) return 9;  // G=32
+    if (mean <= 384) return 12; // G=64, U=8
+    if (mean <= 768) return 13; // G=128, U=8
+    return 15;                  // G=256, U=8
+}
+
+static int shapeForGroup(int G) {
+    for (int i = 0; i < kNumShapes; ++i)
+        if (kShapes[i].G == G && kShapes[i].R == 1) return i;
+    return -1;
+}
+
 static int gridFor(int64_t rows, int G) {
     const int64_t threads = rows * G;
     return static_cast<int>(std::max<int64_t>(1, (threads + kBlock - 1) / kBlock));
@@ -385,7 +432,9 @@ struct DeviceLp {
     size_t arena_bytes = 0;
     int m = 0, n = 0, nnz = 0;
     bool mixed = true;
-    int gA = 1, gAT = 1;
+    int gA = 1, gAT = 1;        // lanes per row of the check / power kernels
+    int shapeP = 0, shapeD = 0;  // step kernel shapes (kShapes index): primal (A^T), dual (A)
+    bool tuned = false;
     int nb_rows = 1, nb_cols = 1, nb_pi = 1;
 
     int *a_ptr = nullptr, *a_idx = nullptr, *at_ptr = nullptr, *at_idx = nullptr;
@@ -397,8 +446,8 @@ struct DeviceLp {
     RowPack<double>* rp64 = nullptr;
     double *c64 = nullptr, *lb64 = nullptr, *ub64 = nullptr, *cs64 = nullptr, *tau64 = nullptr;
     double *rl64 = nullptr, *ru64 = nullptr, *rs64 = nullptr, *sig64 = nullptr;
-    float *xc32 = nullptr, *xi32 = nullptr, *xr32 = nullptr, *xh32 = nullptr;
-    float *yc32 = nullptr, *yi32 = nullptr, *yh32 = nullptr;
+    float *xi32 = nullptr, *xr32 = nullptr, *xh32 = nullptr;  // current x / y are always FP64
+    float *yi32 = nullptr, *yh32 = nullptr;
     double *xc64 = nullptr, *xi64 = nullptr, *xr64 = nullptr, *xh64 = nullptr;
     double *yc64 = nullptr, *yi64 = nullptr, *yh64 = nullptr;
     double *prev_ax = nullptr, *prev_xh = nullptr;
@@ -437,11 +486,11 @@ struct DeviceLp {
         a.a_val = a_v32;
         a.cp = cp32;
         a.rp = rp32;
-        a.xc = xc32;
+        a.xc = xc64;
         a.xi = xi32;
         a.xr = xr32;
         a.xh = xh32;
-        a.yc = yc32;
+        a.yc = yc64;
         a.yi = yi32;
         a.yh = yh32;
         a.st = st;
@@ -530,11 +579,11 @@ int launchCycle(DeviceLp& d, const pdlpx_options& o) {
     const IterArgs<T> ia = iterArgs<T>(d, o);
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
-    const int gp = gridFor(d.n, d.gAT), gd = gridFor(d.m, d.gA);
+    const int gp = gridForShape(d.n, d.shapeP), gd = gridForShape(d.m, d.shapeD);
     int launches = 0;
     for (int k = 1; k <= o.termination_eval_frequency; ++k) {
-        PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, k)));
-        PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, k)));
+        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, k)));
+        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, k)));
         launches += 2;
     }
     PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
@@ -544,8 +593,7 @@ int launchCycle(DeviceLp& d, const pdlpx_options& o) {
     restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc);
     launches += 4;
     if (sizeof(T) == 4 && d.mixed) {
-        PromoteArgs pa{d.xc32, d.xi32, d.xh32, d.yc32, d.yi32, d.yh32, d.xc64, d.xi64,
-                       d.xh64, d.yc64, d.yi64, d.yh64, d.st,   d.n,    d.m};
+        PromoteArgs pa{d.xi32, d.xh32, d.yi32, d.yh32, d.xi64, d.xh64, d.yi64, d.yh64, d.st, d.n, d.m};
         promoteIterates<<<nb, kBlock, 0, s>>>(pa);
         finishPromote<<<1, 1, 0, s>>>(d.st);
         launches += 2;
@@ -612,6 +660,10 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
     const int64_t m = d.m, n = d.n, nnz = d.nnz;
     d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz, d.m);
     d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz, d.n);
+    d.shapeD = o.spmv_group_a > 0 && shapeForGroup(o.spmv_group_a) >= 0 ? shapeForGroup(o.spmv_group_a)
+                                                                         : defaultShape(nnz, d.m);
+    d.shapeP = o.spmv_group_at > 0 && shapeForGroup(o.spmv_group_at) >= 0 ? shapeForGroup(o.spmv_group_at)
+                                                                           : defaultShape(nnz, d.n);
     const int cap = 4 * d.sms;
     d.nb_rows = std::max(1, std::min(gridFor(m, d.gA), cap));
     d.nb_cols = std::max(1, std::min(gridFor(n, d.gAT), cap));
@@ -634,7 +686,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
     const size_t o_c64 = take(8 * n), o_lb64 = take(8 * n), o_ub64 = take(8 * n), o_cs64 = take(8 * n),
                  o_tau64 = take(8 * n);
     const size_t o_rl64 = take(8 * m), o_ru64 = take(8 * m), o_rs64 = take(8 * m), o_sig64 = take(8 * m);
-    size_t o_x32[4] = {0, 0, 0, 0}, o_y32[3] = {0, 0, 0};
+    size_t o_x32[3] = {0, 0, 0}, o_y32[2] = {0, 0};
     if (mixed) {
         for (auto& v : o_x32) v = take(4 * n);
         for (auto& v : o_y32) v = take(4 * m);
@@ -664,13 +716,11 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
         d.at_v32 = reinterpret_cast<float*>(b + o_at_v32);
         d.cp32 = reinterpret_cast<ColPack<float>*>(b + o_cp32);
         d.rp32 = reinterpret_cast<RowPack<float>*>(b + o_rp32);
-        d.xc32 = reinterpret_cast<float*>(b + o_x32[0]);
-        d.xi32 = reinterpret_cast<float*>(b + o_x32[1]);
-        d.xr32 = reinterpret_cast<float*>(b + o_x32[2]);
-        d.xh32 = reinterpret_cast<float*>(b + o_x32[3]);
-        d.yc32 = reinterpret_cast<float*>(b + o_y32[0]);
-        d.yi32 = reinterpret_cast<float*>(b + o_y32[1]);
-        d.yh32 = reinterpret_cast<float*>(b + o_y32[2]);
+        d.xi32 = reinterpret_cast<float*>(b + o_x32[0]);
+        d.xr32 = reinterpret_cast<float*>(b + o_x32[1]);
+        d.xh32 = reinterpret_cast<float*>(b + o_x32[2]);
+        d.yi32 = reinterpret_cast<float*>(b + o_y32[0]);
+        d.yh32 = reinterpret_cast<float*>(b + o_y32[1]);
     }
     d.cp64 = reinterpret_cast<ColPack<double>*>(b + o_cp64);
     d.rp64 = reinterpret_cast<RowPack<double>*>(b + o_rp64);
@@ -748,6 +798,82 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
         PDLPX_CK(up(d.sig64, sc.sigma.data(), 8 * m));
         PDLPX_CK(cudaStreamSynchronize(s));
     }
+    return PDLPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: time the candidate launch shapes of each step kernel on the loaded
+// LP (eager launches between CUDA events on the engine's stream, on a scratch
+// solver state) and keep the fastest.  A candidate must beat the current pick
+// by 3% to replace it, so near-ties keep the default shape.  The step kernels
+// accumulate in FP64, so the pick changes results at most in the last bit of
+// an FP32-stored value.  The iterates written here are overwritten by the
+// solve's initialisation.
+// ---------------------------------------------------------------------------
+template <class T>
+static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, bool tune_d, std::string& err) {
+    cudaStream_t s = d.stream;
+    DevState t{};
+    t.step = 1e-3;
+    t.pw = 1.0;
+    t.prec = precTag<T>();
+    t.fpe0 = -1.0;
+    *d.h_st = t;
+    PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
+    const IterArgs<T> ia = iterArgs<T>(d, o);
+    T* const xs[3] = {ia.xi, ia.xr, ia.xh};
+    T* const ys[2] = {ia.yi, ia.yh};
+    for (int k = 0; k < 3; ++k) PDLPX_CK(cudaMemsetAsync(xs[k], 0, sizeof(T) * static_cast<size_t>(d.n), s));
+    for (int k = 0; k < 2; ++k) PDLPX_CK(cudaMemsetAsync(ys[k], 0, sizeof(T) * static_cast<size_t>(d.m), s));
+    PDLPX_CK(cudaMemsetAsync(ia.xc, 0, 8 * static_cast<size_t>(d.n), s));
+    PDLPX_CK(cudaMemsetAsync(ia.yc, 0, 8 * static_cast<size_t>(d.m), s));
+    cudaEvent_t e0, e1;
+    PDLPX_CK(cudaEventCreate(&e0));
+    PDLPX_CK(cudaEventCreate(&e1));
+    struct G2 {
+        cudaEvent_t a, b;
+        ~G2() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } guard{e0, e1};
+    auto timeShape = [&](bool primal, int shape, float& ms) -> int32_t {
+        const int grid = primal ? gridForShape(d.n, shape) : gridForShape(d.m, shape);
+        constexpr int reps = 5;
+        for (int r = 0; r <= reps; ++r) {
+            if (r == 1) PDLPX_CK(cudaEventRecord(e0, s));
+            if (primal) {
+                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1)));
+            } else {
+                PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1)));
+            }
+        }
+        PDLPX_CK(cudaEventRecord(e1, s));
+        PDLPX_CK(cudaGetLastError());
+        PDLPX_CK(cudaEventSynchronize(e1));
+        PDLPX_CK(cudaEventElapsedTime(&ms, e0, e1));
+        return PDLPX_OK;
+    };
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool primal = pass == 0;
+        if ((primal && !tune_p) || (!primal && !tune_d)) continue;
+        int& pick = primal ? d.shapeP : d.shapeD;
+        const int g0 = kShapes[pick].G;
+        float best = 0.0f;
+        int32_t rc = timeShape(primal, pick, best);
+        if (rc != PDLPX_OK) return rc;
+        for (int c = 0; c < kNumShapes; ++c) {
+            if (c == pick || kShapes[c].G * 4 < g0 || kShapes[c].G > g0 * 4) continue;
+            float ms = 0.0f;
+            rc = timeShape(primal, c, ms);
+            if (rc != PDLPX_OK) return rc;
+            if (ms < 0.97f * best) {
+                best = ms;
+                pick = c;
+            }
+        }
+    }
+    d.tuned = true;
     return PDLPX_OK;
 }
 
@@ -986,6 +1112,12 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     DeviceLp& d = *dev_;
     PDLPX_CK(cudaSetDevice(d.device));
     cudaStream_t s = d.stream;
+    if (opt_.autotune && !d.tuned && d.nnz >= 100000) {
+        const bool tp = opt_.spmv_group_at <= 0, td = opt_.spmv_group_a <= 0;
+        const int32_t rc = d.mixed ? autotuneShapes<float>(d, opt_, tp, td, err)
+                                   : autotuneShapes<double>(d, opt_, tp, td, err);
+        if (rc != PDLPX_OK) return rc;
+    }
     const int32_t m = lp_.m, n = lp_.n;
     const int N = opt_.termination_eval_frequency;
     int launches = 0;
@@ -1072,7 +1204,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     dc.precond_refresh = opt_.preconditioner_refresh != 0;
     dc.nb_rows = d.nb_rows;
     dc.nb_cols = d.nb_cols;
-    dc.stall_limit = 30;
+    dc.stall_limit = 10;
     dc.primal_tol = opt_.primal_tol;
     dc.dual_tol = opt_.dual_tol;
     dc.opt_tol = opt_.optimality_tol;
@@ -1095,7 +1227,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     dc.step_down = opt_.adaptive_step_down;
     dc.step_up = opt_.adaptive_step_up;
     dc.precond_ratio = opt_.preconditioner_refresh_ratio;
-    dc.switch_score = 0.0;
+    dc.switch_score = 30.0;
     PDLPX_CK(cudaMemcpyAsync(d.dc, &dc, sizeof(DevConst), cudaMemcpyHostToDevice, s));
 
     DevState st0{};
@@ -1129,10 +1261,14 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
             for (int32_t j = 0; j < n; ++j) fx[j] = static_cast<float>(wx[j]);
             for (int32_t i = 0; i < m; ++i) fy[i] = static_cast<float>(wy[i]);
         }
-        for (float* p : {d.xc32, d.xi32, d.xh32, d.xr32})
+        for (float* p : {d.xi32, d.xh32, d.xr32})
             PDLPX_CK(cudaMemcpyAsync(p, fx.data(), 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
-        for (float* p : {d.yc32, d.yi32, d.yh32})
+        for (float* p : {d.yi32, d.yh32})
             PDLPX_CK(cudaMemcpyAsync(p, fy.data(), 4 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
+        // current iterates (FP64) start equal to the FP32 anchors
+        std::vector<double> dx(fx.begin(), fx.end()), dy(fy.begin(), fy.end());
+        PDLPX_CK(cudaMemcpyAsync(d.xc64, dx.data(), 8 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
+        PDLPX_CK(cudaMemcpyAsync(d.yc64, dy.data(), 8 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
         PDLPX_CK(cudaStreamSynchronize(s));
     } else {
         if (!warm) {
@@ -1169,14 +1305,11 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     };
 
     used_gpu_ = true;
-    bool stopped = false, timed_out = false;
+    bool stopped = false;
     int switch_total = -1;
     int prec = d.mixed ? 0 : 1;
     while (true) {
-        if (timeUp(t0, opt_.max_solve_seconds)) {
-            timed_out = true;
-            break;
-        }
+        if (timeUp(t0, opt_.max_solve_seconds)) break;
         if (stop_flag_ != nullptr && __atomic_load_n(stop_flag_, __ATOMIC_RELAXED) != 0) {
             stopped = true;
             break;
@@ -1215,7 +1348,6 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     } else {
         status = stopped ? PDLPX_STATUS_ITER_LIMIT : PDLPX_STATUS_TIME_LIMIT;
     }
-    (void)timed_out;
 
     // ---- results (pdlp.cpp:2678-2712)
     const int fprec = fin.prec;
@@ -1294,16 +1426,18 @@ int32_t timeStepKernels(DeviceLp& d, const pdlpx_options& o, int reps, float ms[
     const IterArgs<T> ia = iterArgs<T>(d, o);
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
-    const int gp = gridFor(d.n, d.gAT), gd = gridFor(d.m, d.gA);
+    const int gp = gridForShape(d.n, d.shapeP), gd = gridForShape(d.m, d.shapeD);
     cudaEvent_t ev[4];
     for (auto& e : ev) PDLPX_CK(cudaEventCreate(&e));
     // warm-up launch of each
-    PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, 1)));
-    PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, 1)));
+    PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, 1)));
     PDLPX_CK(cudaEventRecord(ev[0], s));
-    for (int r = 0; r < reps; ++r) PDLPX_G_SWITCH(d.gAT, (primalStep<GG, T><<<gp, kBlock, 0, s>>>(ia, 1)));
+    for (int r = 0; r < reps; ++r)
+        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, 1)));
     PDLPX_CK(cudaEventRecord(ev[1], s));
-    for (int r = 0; r < reps; ++r) PDLPX_G_SWITCH(d.gA, (dualStep<GG, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    for (int r = 0; r < reps; ++r)
+        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, 1)));
     PDLPX_CK(cudaEventRecord(ev[2], s));
     for (int r = 0; r < reps; ++r) {
         PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
@@ -1353,10 +1487,10 @@ int32_t Engine::timeKernels(int32_t reps, double* ms_primal, double* ms_dual, do
 
 int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const {
     if (!dev_) return PDLPX_E_NOT_LOADED;
-    if (ga) *ga = dev_->gA;
-    if (gat) *gat = dev_->gAT;
-    if (bp) *bp = gridFor(dev_->n, dev_->gAT);
-    if (bd) *bd = gridFor(dev_->m, dev_->gA);
+    if (ga) *ga = kShapes[dev_->shapeD].G;
+    if (gat) *gat = kShapes[dev_->shapeP].G;
+    if (bp) *bp = gridForShape(dev_->n, dev_->shapeP);
+    if (bd) *bd = gridForShape(dev_->m, dev_->shapeD);
     return PDLPX_OK;
 }
 

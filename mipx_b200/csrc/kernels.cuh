@@ -105,11 +105,15 @@ struct IterArgs {
     const T* __restrict__ a_val;
     const ColPack<T>* __restrict__ cp;
     const RowPack<T>* __restrict__ rp;
-    T* xc;  // current x
-    T* xi;  // initial (anchor) x
-    T* xr;  // reflected x
-    T* xh;  // pdhg x (written on the last iteration of a batch)
-    T* yc;
+    // The current iterates carry the Halpern state from one iteration to the
+    // next and stay FP64 in every mode: rounding them to FP32 on each store is
+    // a random walk of ~sqrt(K) * 6e-8 over K iterations, which stalled a
+    // 1M-variable transportation LP at 1e-4 relative primal residual.
+    double* xc;  // current x
+    T* xi;       // initial (anchor) x
+    T* xr;       // reflected x (gathered by the dual SpMV)
+    T* xh;       // pdhg x (written on the last iteration of a batch)
+    double* yc;  // current y (gathered by the primal SpMV)
     T* yi;
     T* yh;
     DevState* st;
@@ -220,25 +224,41 @@ __device__ __forceinline__ T groupSum(T s) {
     }
 }
 
-// Partial dot product of one CSR row against a gathered vector, lane-strided
-// with four independent accumulators (memory-level parallelism).
+// Partial dot product of one CSR row against a gathered vector.  Lane-strided;
+// every round issues U index/value loads per lane together (predicated, so a
+// row whose length is not a multiple of U*G has no sequential tail), then the U
+// gathers.  A masked slot gathers x[0], which exists whenever the row is
+// non-empty.  FP32 data accumulate in FP64: a float*float product is exact in
+// double, so the only rounding left is that of the stored operands.
+template <int G, int U, class Acc, class V, class X>
+__device__ __forceinline__ Acc rowDotU(int b, int e, int lane, const int* __restrict__ idx,
+                                       const V* __restrict__ val, const X* __restrict__ x) {
+    Acc s[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) s[u] = Acc(0);
+    for (int k0 = b + lane; k0 < e; k0 += U * G) {
+        int c[U];
+        V v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u * G;
+            const bool ok = k < e;
+            c[u] = ok ? __ldg(idx + k) : 0;
+            v[u] = ok ? __ldg(val + k) : V(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) s[u] += static_cast<Acc>(v[u]) * static_cast<Acc>(__ldg(x + c[u]));
+    }
+    Acc t = s[0];
+#pragma unroll
+    for (int u = 1; u < U; ++u) t += s[u];
+    return t;
+}
+
 template <int G, class Acc, class V, class X>
 __device__ __forceinline__ Acc rowDot(int b, int e, int lane, const int* __restrict__ idx,
                                       const V* __restrict__ val, const X* __restrict__ x) {
-    Acc s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    int k = b + lane;
-    for (; k + 3 * G < e; k += 4 * G) {
-        const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G), c2 = __ldg(idx + k + 2 * G),
-                  c3 = __ldg(idx + k + 3 * G);
-        const V v0 = __ldg(val + k), v1 = __ldg(val + k + G), v2 = __ldg(val + k + 2 * G),
-                v3 = __ldg(val + k + 3 * G);
-        s0 += static_cast<Acc>(v0) * static_cast<Acc>(__ldg(x + c0));
-        s1 += static_cast<Acc>(v1) * static_cast<Acc>(__ldg(x + c1));
-        s2 += static_cast<Acc>(v2) * static_cast<Acc>(__ldg(x + c2));
-        s3 += static_cast<Acc>(v3) * static_cast<Acc>(__ldg(x + c3));
-    }
-    for (; k < e; k += G) s0 += static_cast<Acc>(__ldg(val + k)) * static_cast<Acc>(__ldg(x + __ldg(idx + k)));
-    return (s0 + s1) + (s2 + s3);
+    return rowDotU<G, 4, Acc>(b, e, lane, idx, val, x);
 }
 
 // Two dot products of one row (A^T y and A^T (y - y0)) in one pass.
@@ -302,96 +322,157 @@ __device__ __forceinline__ bool active(const DevState* st, int prec, int koff, i
 }
 
 template <class T>
-__device__ __forceinline__ T primalTau(const DevState* st, T tb);
-template <>
-__device__ __forceinline__ float primalTau<float>(const DevState* st, float tb) {
-    return st->tau_fac * tb;
-}
-template <>
-__device__ __forceinline__ double primalTau<double>(const DevState* st, double tb) {
-    return st->step * tb / st->pw;  // same association as pdlp_kernels.cu:62
-}
-template <class T>
-__device__ __forceinline__ T dualSigma(const DevState* st, T sb);
-template <>
-__device__ __forceinline__ float dualSigma<float>(const DevState* st, float sb) {
-    return st->sig_fac * sb;
-}
-template <>
-__device__ __forceinline__ double dualSigma<double>(const DevState* st, double sb) {
-    return st->step * sb * st->pw;  // pdlp_kernels.cu:111
-}
-
-template <class T>
 __host__ __device__ constexpr int precTag() {
     return sizeof(T) == 8 ? 1 : 0;
 }
 
-// Fused A^T y_cur + Halpern primal step.  One G-lane group per column j.
-template <int G, class T>
+// Launch shapes of the step kernels: G lanes per row, R rows per group (rows
+// r*slab apart so every load instruction is coalesced across the block), U
+// loads per lane per round.  The table is the autotuner's search space.
+struct StepShape {
+    int G, R, U;
+};
+constexpr StepShape kShapes[] = {
+    {1, 1, 2}, {1, 2, 2}, {1, 4, 2}, {2, 1, 2}, {2, 2, 2}, {4, 1, 4}, {4, 2, 4}, {8, 1, 4},
+    {16, 1, 4}, {32, 1, 4}, {32, 1, 8}, {64, 1, 4}, {64, 1, 8}, {128, 1, 8}, {256, 1, 4}, {256, 1, 8},
+};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+// Fused A^T y_cur + Halpern primal step (pdlp_kernels.cu:46-88 around a fused
+// SpMV).  All loads of the R columns -- row pointers, packed constants,
+// current / anchor x, then the A^T row entries and the y gathers -- are issued
+// before the solver state is consulted, so their latencies overlap.  The step
+// arithmetic is FP64 whatever the storage type (same association as the
+// reference: tau = step * tau_base / omega), results are rounded once on store.
+template <int G, int R, int U, class T>
 __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
+    constexpr int slab = kBlock / G;
+    const int lane = threadIdx.x % G;
+    const int j0 = blockIdx.x * (slab * R) + threadIdx.x / G;
+    const int* __restrict__ ptr = p.at_ptr;
+    const ColPack<T>* __restrict__ cp = p.cp;
+    const double* __restrict__ xcp = p.xc;
+    const T* __restrict__ xip = p.xi;
+    int b[R], e[R];
+    ColPack<T> q[R];
+    double xc[R];
+    T xi[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + r * slab;
+        b[r] = 0;
+        e[r] = 0;
+        q[r] = ColPack<T>{T(0), T(0), T(0), T(0)};
+        xc[r] = 0.0;
+        xi[r] = T(0);
+        if (j < p.n) {
+            b[r] = ptr[j];
+            e[r] = ptr[j + 1];
+            if (lane == 0) {
+                q[r] = cp[j];
+                xc[r] = xcp[j];
+                xi[r] = xip[j];
+            }
+        }
+    }
+    double s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = rowDotU<G, U, double>(b[r], e[r], lane, p.at_idx, p.at_val, p.yc);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
-    const int t = blockIdx.x * kBlock + threadIdx.x;
-    const int j = t / G, lane = t % G;
-    const bool valid = j < p.n;
-    T s = 0;
-    if (valid) s = rowDot<G, T>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yc);
-    s = groupSum<G>(s);
-    if (valid && lane == 0) {
-        const int k = p.st->inner + koff;
-        const T lam = static_cast<T>(static_cast<double>(k) / static_cast<double>(k + 1));
-        const ColPack<T> q = p.cp[j];
-        const T xc = p.xc[j], xi = p.xi[j];
-        const T tau = primalTau<T>(p.st, q.tau);
-        T xh = xc - tau * (q.c + s);
-        if (xh < q.lb) xh = q.lb;
-        if (xh > q.ub) xh = q.ub;
-        const T xr = T(2) * xh - xc;
-        p.xr[j] = xr;
-        p.xc[j] = lam * xr + (T(1) - lam) * xi;
-        if (last) p.xh[j] = xh;
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = groupSum<G>(s[r]);
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + r * slab;
+        if (lane != 0 || j >= p.n) continue;
+        const double xcd = xc[r], xid = xi[r];
+        const double tau = step * static_cast<double>(q[r].tau) / pw;
+        double xh = xcd - tau * (static_cast<double>(q[r].c) + s[r]);
+        const double lb = q[r].lb, ub = q[r].ub;
+        if (xh < lb) xh = lb;
+        if (xh > ub) xh = ub;
+        const double xr = 2.0 * xh - xcd;
+        p.xr[j] = static_cast<T>(xr);
+        p.xc[j] = lam * xr + (1.0 - lam) * xid;
+        if (last) p.xh[j] = static_cast<T>(xh);
     }
 }
 
-// Fused A x_refl + dual proximal step.  One G-lane group per row i.
-template <int G, class T>
+// Fused A x_refl + dual proximal step (pdlp_kernels.cu:94-157), same structure.
+template <int G, int R, int U, class T>
 __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
+    constexpr int slab = kBlock / G;
+    const int lane = threadIdx.x % G;
+    const int i0 = blockIdx.x * (slab * R) + threadIdx.x / G;
+    const int* __restrict__ ptr = p.a_ptr;
+    const RowPack<T>* __restrict__ rp = p.rp;
+    const double* __restrict__ ycp = p.yc;
+    const T* __restrict__ yip = p.yi;
+    int b[R], e[R];
+    RowPack<T> q[R];
+    double yc[R];
+    T yi[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = i0 + r * slab;
+        b[r] = 0;
+        e[r] = 0;
+        q[r] = RowPack<T>{T(0), T(0), T(0), T(0)};
+        yc[r] = 0.0;
+        yi[r] = T(0);
+        if (i < p.m) {
+            b[r] = ptr[i];
+            e[r] = ptr[i + 1];
+            if (lane == 0) {
+                q[r] = rp[i];
+                yc[r] = ycp[i];
+                yi[r] = yip[i];
+            }
+        }
+    }
+    double s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = rowDotU<G, U, double>(b[r], e[r], lane, p.a_idx, p.a_val, p.xr);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
-    const int t = blockIdx.x * kBlock + threadIdx.x;
-    const int i = t / G, lane = t % G;
-    const bool valid = i < p.m;
-    T s = 0;
-    if (valid) s = rowDot<G, T>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xr);
-    s = groupSum<G>(s);
-    if (valid && lane == 0) {
-        const int k = p.st->inner + koff;
-        const T lam = static_cast<T>(static_cast<double>(k) / static_cast<double>(k + 1));
-        const RowPack<T> q = p.rp[i];
-        const T yc = p.yc[i], yi = p.yi[i];
-        const T sig = dualSigma<T>(p.st, q.sigma);
-        const T v = yc + sig * s;
-        T py;
-        if (q.type == T(0)) {
-            py = v - sig * q.rl;
-        } else if (q.type == T(1)) {
-            py = v - sig * q.ru;
-            if (py < T(0)) py = T(0);
-        } else if (q.type == T(2)) {
-            py = v - sig * q.rl;
-            if (py > T(0)) py = T(0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = groupSum<G>(s[r]);
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = i0 + r * slab;
+        if (lane != 0 || i >= p.m) continue;
+        const double ycd = yc[r], yid = yi[r];
+        const double sig = step * static_cast<double>(q[r].sigma) * pw;
+        const double v = ycd + sig * s[r];
+        const double rl = q[r].rl, ru = q[r].ru;
+        const int type = static_cast<int>(q[r].type);
+        double py;
+        if (type == 0) {
+            py = v - sig * rl;
+        } else if (type == 1) {
+            py = v - sig * ru;
+            if (py < 0.0) py = 0.0;
+        } else if (type == 2) {
+            py = v - sig * rl;
+            if (py > 0.0) py = 0.0;
         } else {
-            if (v >= sig * q.ru)
-                py = v - sig * q.ru;
-            else if (v <= sig * q.rl)
-                py = v - sig * q.rl;
+            if (v >= sig * ru)
+                py = v - sig * ru;
+            else if (v <= sig * rl)
+                py = v - sig * rl;
             else
-                py = T(0);
+                py = 0.0;
         }
-        const T yr = T(2) * py - yc;
-        p.yc[i] = lam * yr + (T(1) - lam) * yi;
-        if (last) p.yh[i] = py;
+        const double yr = 2.0 * py - ycd;
+        p.yc[i] = lam * yr + (1.0 - lam) * yid;
+        if (last) p.yh[i] = static_cast<T>(py);
     }
 }
 
@@ -523,10 +604,15 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
             const bool hl = isfinite(lb), hu = isfinite(ub);
             acc[C_POBJ] += c * xh;
             const double g = c + aty;
+            // Bound activity is judged against the bounds the iterate precision
+            // clamped to (FP32-rounded in mixed mode): an FP32 x_hat sitting on
+            // float(ub) < ub is at its bound, not interior.
+            const double lbT = static_cast<double>(static_cast<T>(lb));
+            const double ubT = static_cast<double>(static_cast<T>(ub));
             double dr;
-            if (xh <= lb + 1e-12 && hl)
+            if (xh <= lbT + 1e-12 && hl)
                 dr = fmin(g, 0.0);
-            else if (xh >= ub - 1e-12 && hu)
+            else if (xh >= ubT - 1e-12 && hu)
                 dr = fmax(g, 0.0);
             else
                 dr = g;
@@ -568,7 +654,7 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
 // executed only when the controller decided to restart.
 template <class T>
 __global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n, int m, const T* xh,
-                                                     const T* yh, T* xi, T* yi, T* xc, T* yc) {
+                                                     const T* yh, T* xi, T* yi, double* xc, double* yc) {
     if (st->done || st->prec != precTag<T>() || !st->restart) return;
     for (int k = blockIdx.x * kBlock + threadIdx.x; k < (n > m ? n : m); k += gridDim.x * kBlock) {
         if (k < n) {
@@ -585,9 +671,9 @@ __global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n,
 }
 
 // FP32 -> FP64 hand-over of the iterate set (mixed precision mode).
-struct PromoteArgs {
-    const float *xc, *xi, *xh, *yc, *yi, *yh;
-    double *xc64, *xi64, *xh64, *yc64, *yi64, *yh64;
+struct PromoteArgs {  // the current iterates are FP64 in both modes and need no copy
+    const float *xi, *xh, *yi, *yh;
+    double *xi64, *xh64, *yi64, *yh64;
     DevState* st;
     int n, m;
 };
@@ -658,17 +744,17 @@ __global__ void powerFinish1(PowerArgs a);
 __global__ void __launch_bounds__(kBlock) powerNormalize(PowerArgs a);
 __global__ void powerFinish2(PowerArgs a);
 
-// Plain SpMV for the parity entry point pdlpx_csr_spmv.
+// Plain SpMV for the parity entry point pdlpx_csr_spmv (FP64 accumulation, like the step kernels).
 template <int G, class T>
 __global__ void __launch_bounds__(kBlock) spmvKernel(int rows, const int* ptr, const int* idx, const T* val,
                                                     const T* x, T* y) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
     const int i = t / G, lane = t % G;
     const bool valid = i < rows;
-    T s = 0;
-    if (valid) s = rowDot<G, T>(ptr[i], ptr[i + 1], lane, idx, val, x);
+    double s = 0;
+    if (valid) s = rowDot<G, double>(ptr[i], ptr[i + 1], lane, idx, val, x);
     s = groupSum<G>(s);
-    if (valid && lane == 0) y[i] = s;
+    if (valid && lane == 0) y[i] = static_cast<T>(s);
 }
 
 }  // namespace pdlpx

@@ -125,6 +125,7 @@ class PdlpOptions:
     fp64_switch: bool = True
     spmv_group_a: int = 0
     spmv_group_at: int = 0
+    autotune: bool = True
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
