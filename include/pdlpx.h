@@ -115,8 +115,11 @@ typedef struct pdlpx_options {
     int32_t spmv_group_a;             /* 0 = autotune; else threads per row of A (1,2,4,8,16,32) */
     int32_t spmv_group_at;            /* 0 = autotune; else threads per row of A^T */
     int32_t autotune;                 /* 1: time the step kernels' launch shapes on LPs with >= 100k
-                                         nonzeros and keep the fastest; 0: row-length heuristic */
-    int32_t reserved[7];
+                                         nonzeros and keep the fastest; 0 (default): row-length table,
+                                         deterministic */
+    int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step */
+    int32_t shape_dual;               /* 0 = automatic; k > 0 pins launch shape k-1 of the dual step */
+    int32_t reserved[5];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */
@@ -241,6 +244,16 @@ int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_option
 int32_t pdlpx_csr_spmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* row_ptr,
                        const int32_t* col_idx, const double* val, const double* x, double* y,
                        int32_t precision, int32_t group);
+
+/* Row violation of a point x against ranged rows, FP64 on the device (host
+ * buffers in and out): v_i = (A x)_i - clamp((A x)_i, row_lb_i, row_ub_i),
+ * *sum_sq = sum_i v_i^2, *max_abs = max_i |v_i|.  This is the primal-residual
+ * reduction of the convergence check (pdlp.cpp:1106-1117) exposed on its own;
+ * the reduction order is fixed, so repeated calls return identical values. */
+int32_t pdlpx_row_violation(int32_t m, int32_t n, int32_t nnz, const int32_t* row_ptr,
+                            const int32_t* col_idx, const double* val, const double* x,
+                            const double* row_lb, const double* row_ub, double* sum_sq,
+                            double* max_abs);
 
 /* ---- seeded synthetic LP generators (configs of the benchmark suite) ----
  * Output arrays are allocated by the library and released with pdlpx_free_lp. */

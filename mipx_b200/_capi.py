@@ -35,7 +35,8 @@ class Options(C.Structure):
         ("anderson_acceleration", i32), ("anderson_window_size", i32), ("anderson_regularization", f64),
         ("use_gpu", i32), ("gpu_min_rows", i32), ("gpu_min_nnz", i32), ("verbose", i32),
         ("precision", i32), ("device", i32), ("fp64_switch", i32), ("spmv_group_a", i32),
-        ("spmv_group_at", i32), ("autotune", i32), ("reserved", i32 * 7),
+        ("spmv_group_at", i32), ("autotune", i32), ("shape_primal", i32), ("shape_dual", i32),
+        ("reserved", i32 * 5),
     ]
 
 
@@ -99,6 +100,7 @@ SIGNATURES = [
     ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),
                                 C.POINTER(P_f64), C.POINTER(P_f64)]),
     ("pdlpx_csr_spmv", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, i32, i32]),
+    ("pdlpx_row_violation", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, P_f64, P_f64, P_f64]),
     ("pdlpx_gen_random", i32, [i32, i32, i32, i32, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_gen_transport", i32, [i32, i32, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_gen_powerlaw", i32, [i32, i32, i32, i32, f64, f64, f64, C.c_uint64, C.POINTER(GenLp)]),

@@ -89,7 +89,9 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->fp64_switch = 1;
     o->spmv_group_a = 0;
     o->spmv_group_at = 0;
-    o->autotune = 1;
+    o->autotune = 0;
+    o->shape_primal = 0;
+    o->shape_dual = 0;
 }
 
 const char* pdlpx_error_string(int32_t code) {

@@ -382,18 +382,19 @@ static int gridForShape(int64_t rows, int shape) {
     return static_cast<int>(std::max<int64_t>(1, (rows + per_block - 1) / per_block));
 }
 
-// Default launch shape from the mean row length (the autotuner's starting point).
+// Default launch shape from the mean row length (deterministic; the
+// autotuner's starting point).  Picks measured on B200 with FP32 storage: mean
+// 2 (1M x 2 transportation A^T) -> G=1; mean 8 -> G=2..4; mean 20 -> G=8;
+// mean 1000 (2000 x 1000 transportation A) -> G=64.
 static int defaultShape(int64_t nnz, int32_t rows) {
     const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
-    if (mean <= 3) return 2;    // G=1, R=4
-    if (mean <= 6) return 4;    // G=2, R=2
-    if (mean <= 12) return 5;   // G=4
-    if (mean <= 24) return 7;   // G=8
-    if (mean <= 48) return 8;   // G=16
-    if (mean <= 128) return 9;  // G=32
-    if (mean <= 384) return 12; // G=64, U=8
-    if (mean <= 768) return 13; // G=128, U=8
-    return 15;                  // G=256, U=8
+    if (mean <= 3) return 0;     // G=1
+    if (mean <= 6) return 3;     // G=2
+    if (mean <= 12) return 5;    // G=4
+    if (mean <= 24) return 7;    // G=8
+    if (mean <= 48) return 8;    // G=16
+    if (mean <= 128) return 9;   // G=32
+    return 11;                   // G=64
 }
 
 static int shapeForGroup(int G) {
@@ -664,6 +665,8 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
                                                                          : defaultShape(nnz, d.m);
     d.shapeP = o.spmv_group_at > 0 && shapeForGroup(o.spmv_group_at) >= 0 ? shapeForGroup(o.spmv_group_at)
                                                                            : defaultShape(nnz, d.n);
+    if (o.shape_dual > 0 && o.shape_dual <= kNumShapes) d.shapeD = o.shape_dual - 1;
+    if (o.shape_primal > 0 && o.shape_primal <= kNumShapes) d.shapeP = o.shape_primal - 1;
     const int cap = 4 * d.sms;
     d.nb_rows = std::max(1, std::min(gridFor(m, d.gA), cap));
     d.nb_cols = std::max(1, std::min(gridFor(n, d.gAT), cap));
@@ -1113,7 +1116,8 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     PDLPX_CK(cudaSetDevice(d.device));
     cudaStream_t s = d.stream;
     if (opt_.autotune && !d.tuned && d.nnz >= 100000) {
-        const bool tp = opt_.spmv_group_at <= 0, td = opt_.spmv_group_a <= 0;
+        const bool tp = opt_.spmv_group_at <= 0 && opt_.shape_primal <= 0;
+        const bool td = opt_.spmv_group_a <= 0 && opt_.shape_dual <= 0;
         const int32_t rc = d.mixed ? autotuneShapes<float>(d, opt_, tp, td, err)
                                    : autotuneShapes<double>(d, opt_, tp, td, err);
         if (rc != PDLPX_OK) return rc;

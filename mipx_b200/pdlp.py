@@ -125,7 +125,9 @@ class PdlpOptions:
     fp64_switch: bool = True
     spmv_group_a: int = 0
     spmv_group_at: int = 0
-    autotune: bool = True
+    autotune: bool = False
+    shape_primal: int = 0
+    shape_dual: int = 0
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -451,3 +453,18 @@ def csr_spmv(matrix: SparseMatrix, x, precision: Precision = Precision.Mixed, gr
     _capi.check(lib.pdlpx_csr_spmv(matrix.rows, matrix.cols, int(v.size), _pi(rp), _pi(ci), _pd(v), _pd(xa),
                                    _pd(y), int(precision), int(group)))
     return y
+
+
+def row_violation(matrix: SparseMatrix, x, row_lower, row_upper) -> tuple[float, float]:
+    """(sum_i v_i^2, max_i |v_i|) with v = A x - clamp(A x, row_lower, row_upper), FP64 on the device."""
+    lib = _capi.load()
+    xa = np.ascontiguousarray(x, dtype=np.float64)
+    rl = np.ascontiguousarray(row_lower, dtype=np.float64)
+    ru = np.ascontiguousarray(row_upper, dtype=np.float64)
+    rp = np.ascontiguousarray(matrix.row_starts, dtype=np.int32)
+    ci = np.ascontiguousarray(matrix.col_indices, dtype=np.int32)
+    v = np.ascontiguousarray(matrix.values, dtype=np.float64)
+    s, mx = C.c_double(), C.c_double()
+    _capi.check(lib.pdlpx_row_violation(matrix.rows, matrix.cols, int(v.size), _pi(rp), _pi(ci), _pd(v), _pd(xa),
+                                        _pd(rl), _pd(ru), C.byref(s), C.byref(mx)))
+    return s.value, mx.value

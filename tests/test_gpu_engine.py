@@ -318,3 +318,26 @@ def test_fp32_only_reaches_tight_tolerance():
                  GC.options("rand_2000x5000", precision=Precision.Mixed, fp64_switch=False))
     assert r.status == Status.Optimal and r.fp64_iterations == 0
     assert abs(r.objective - e["objective"]) <= 1e-6 * (1 + abs(e["objective"]))
+
+
+def _violation_ref(A, x, rl, ru):
+    ax = O.oracle_spmv(A, x)
+    v = ax - np.clip(ax, rl, ru)
+    return float(np.sum(v * v)), float(np.max(np.abs(v))) if v.size else 0.0
+
+
+@pytest.mark.parametrize("name,rows,cols,lens_fn", SPMV_SHAPES[:4])
+def test_row_violation_matches_numpy(name, rows, cols, lens_fn):
+    """pdlpx_row_violation (FP64, fixed-order reduction) against an FP64 numpy sum:
+    relative 1e-12 on the sum of squares, exact max."""
+    from mipx_b200.pdlp import row_violation
+    A = _rand_csr(rows, cols, lens_fn(np.random.default_rng(7)), 8)
+    x = np.random.default_rng(9).standard_normal(cols)
+    ax = O.oracle_spmv(A, x)
+    rl = np.where(np.arange(rows) % 3 == 0, -np.inf, ax - 0.5)
+    ru = np.where(np.arange(rows) % 3 == 1, np.inf, ax - 1.0 + (np.arange(rows) % 2))
+    s, mx = row_violation(A, x, rl, ru)
+    s_ref, mx_ref = _violation_ref(A, x, rl, ru)
+    assert abs(s - s_ref) <= 1e-12 * (1.0 + s_ref)
+    assert abs(mx - mx_ref) <= 1e-12 * (1.0 + mx_ref)
+    assert row_violation(A, x, rl, ru) == (s, mx)  # deterministic
