@@ -255,6 +255,25 @@ int32_t pdlpx_row_violation(int32_t m, int32_t n, int32_t nnz, const int32_t* ro
                             const double* row_lb, const double* row_ub, double* sum_sq,
                             double* max_abs);
 
+/* Same reduction for callers that cannot allocate device memory (code running
+ * inside another framework's memory pool or under an allocation-free policy).
+ * No counterpart in the reference.  All pointers are DEVICE pointers; the result
+ * (sum_sq, max_abs) is written to d_out[0..1] on `stream` (a cudaStream_t, NULL =
+ * the legacy default stream); synchronise before reading it.  The call allocates
+ * nothing: the per-block partials live in a fixed 64 KiB device array that every
+ * GPU loading the library holds until exit.  Limit: at most 4096 blocks of 256
+ * threads, i.e. m * G <= 1048576 where G is the threads per row chosen from the
+ * mean row length nnz/m (1 up to 3, 2 up to 6, 4 up to 12, 8 up to 24, 16 up to
+ * 48, 32 up to 128, 64 up to 384, 128 up to 768, else 256); larger inputs return
+ * PDLPX_E_INVALID with the reason in pdlpx_last_error(NULL).  The first call on
+ * each device resolves the array's device address with that device current;
+ * make that first call before any stream capture.  Calls share the array and
+ * race if they overlap on the GPU. */
+int32_t pdlpx_row_violation_noalloc(int32_t m, int32_t n, int32_t nnz, const int32_t* d_row_ptr,
+                                    const int32_t* d_col_idx, const double* d_val,
+                                    const double* d_x, const double* d_row_lb,
+                                    const double* d_row_ub, double* d_out, void* stream);
+
 /* ---- seeded synthetic LP generators (configs of the benchmark suite) ----
  * Output arrays are allocated by the library and released with pdlpx_free_lp. */
 typedef struct pdlpx_gen_lp {

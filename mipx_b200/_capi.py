@@ -101,6 +101,7 @@ SIGNATURES = [
                                 C.POINTER(P_f64), C.POINTER(P_f64)]),
     ("pdlpx_csr_spmv", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, i32, i32]),
     ("pdlpx_row_violation", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, P_f64, P_f64, P_f64]),
+    ("pdlpx_row_violation_noalloc", i32, [i32, i32, i32] + [C.c_void_p] * 8),
     ("pdlpx_gen_random", i32, [i32, i32, i32, i32, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_gen_transport", i32, [i32, i32, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_gen_powerlaw", i32, [i32, i32, i32, i32, f64, f64, f64, C.c_uint64, C.POINTER(GenLp)]),

@@ -20,6 +20,12 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+void pdlpx::setGlobalError(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
 template <class F>
 int32_t guarded(pdlpx_solver* h, F&& f) {
     try {

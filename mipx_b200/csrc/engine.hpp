@@ -83,6 +83,9 @@ private:
 // Threads per row for the CSR kernels, from the mean row length.
 int32_t pickGroup(int64_t nnz, int32_t rows);
 
+// Message returned by pdlpx_last_error(NULL) on this thread (calls without a handle).
+void setGlobalError(const std::string& msg);
+
 // Device SpMV used by pdlpx_csr_spmv (host buffers in/out).
 int32_t deviceSpmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* rp, const int32_t* ci,
                    const double* val, const double* x, double* y, int32_t precision, int32_t group,

@@ -7,6 +7,7 @@
 // the partials in fixed order, so the result is deterministic.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -80,6 +81,25 @@ static cudaError_t launchRowViolation(int m, int G, const int* ptr, const int* i
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot call cudaMalloc: code running
+// inside another framework's memory pool, or under a graph or allocator policy
+// that forbids new device allocations.  For them the per-block partials of the
+// row kernel live in this fixed device array instead of a cudaMalloc'd buffer.
+// Every GPU that loads this library holds the array (64 KiB) until the process
+// exits.  All calls on a device share it and it keeps the last call's contents;
+// every block writes its own partial before the final pass reads it, so nothing
+// needs clearing, but calls that overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocBlocks = 4096;  // at most 4096 row blocks of 256 threads per call
+static __device__ __align__(256) double g_row_violation_scratch[2 * kNoAllocBlocks];
+
+namespace {
+std::mutex g_scratch_mutex;
+constexpr int kMaxDevices = 256;
+double* g_scratch_address[kMaxDevices] = {};  // device address of the array, per device
+}  // namespace
+
 }  // namespace pdlpx
 
 using namespace pdlpx;
@@ -133,6 +153,58 @@ int32_t pdlpx_row_violation(int32_t m, int32_t n, int32_t nnz, const int32_t* ro
     if (cudaMemcpy(out, buf + o_out, 16, cudaMemcpyDeviceToHost) != cudaSuccess) return PDLPX_E_CUDA;
     *sum_sq = out[0];
     *max_abs = out[1];
+    return PDLPX_OK;
+}
+
+int32_t pdlpx_row_violation_noalloc(int32_t m, int32_t n, int32_t nnz, const int32_t* d_row_ptr,
+                                    const int32_t* d_col_idx, const double* d_val, const double* d_x,
+                                    const double* d_row_lb, const double* d_row_ub, double* d_out, void* stream) {
+    if (m < 0 || n < 0 || nnz < 0 || d_out == nullptr ||
+        (m > 0 && (d_row_ptr == nullptr || d_row_lb == nullptr || d_row_ub == nullptr)) ||
+        (nnz > 0 && (d_col_idx == nullptr || d_val == nullptr)) || (n > 0 && d_x == nullptr)) {
+        setGlobalError("pdlpx_row_violation_noalloc: invalid argument");
+        return PDLPX_E_INVALID;
+    }
+    const int G = pickGroup(nnz, m);
+    const int nb = rowViolationBlocks(m, G);
+    if (nb > kNoAllocBlocks) {
+        setGlobalError("pdlpx_row_violation_noalloc: " + std::to_string(m) + " rows at " + std::to_string(G) +
+                       " threads per row need " + std::to_string(nb) + " blocks; the fixed scratch holds " +
+                       std::to_string(kNoAllocBlocks) + " (m * G <= 1048576)");
+        return PDLPX_E_INVALID;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        setGlobalError("pdlpx_row_violation_noalloc: no current CUDA device");
+        return PDLPX_E_NO_DEVICE;
+    }
+    double* scratch = nullptr;
+    {
+        // One-time set-up per device, with that device current: resolve the
+        // array's device address (host code cannot use the symbol itself).
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        if (g_scratch_address[dev] == nullptr) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_row_violation_scratch);
+            if (e != cudaSuccess || p == nullptr) {
+                setGlobalError(std::string("pdlpx_row_violation_noalloc: cudaGetSymbolAddress failed: ") +
+                               cudaGetErrorString(e));
+                return PDLPX_E_CUDA;
+            }
+            g_scratch_address[dev] = static_cast<double*>(p);
+        }
+        scratch = g_scratch_address[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (m == 0) {
+        return cudaMemsetAsync(d_out, 0, 2 * sizeof(double), s) == cudaSuccess ? PDLPX_OK : PDLPX_E_CUDA;
+    }
+    const cudaError_t e =
+        launchRowViolation(m, G, d_row_ptr, d_col_idx, d_val, d_x, d_row_lb, d_row_ub, scratch, d_out, s);
+    if (e != cudaSuccess) {
+        setGlobalError(std::string("pdlpx_row_violation_noalloc: launch failed: ") + cudaGetErrorString(e));
+        return PDLPX_E_CUDA;
+    }
     return PDLPX_OK;
 }
 
