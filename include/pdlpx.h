@@ -119,7 +119,12 @@ typedef struct pdlpx_options {
                                          deterministic */
     int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step */
     int32_t shape_dual;               /* 0 = automatic; k > 0 pins launch shape k-1 of the dual step */
-    int32_t reserved[5];
+    int32_t batch_cluster;            /* pdlpx_batch_solve: CTAs per LP (thread-block cluster size,
+                                         1..8; 0 = 4) */
+    int32_t batch_resident;           /* pdlpx_batch_solve, mixed precision: 1 (default) runs an LP's FP32
+                                         phase from the cluster's shared memory when its slices fit;
+                                         0 keeps every phase in global memory */
+    int32_t reserved[3];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

@@ -98,6 +98,8 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->autotune = 0;
     o->shape_primal = 0;
     o->shape_dual = 0;
+    o->batch_cluster = 0;
+    o->batch_resident = 1;
 }
 
 const char* pdlpx_error_string(int32_t code) {
@@ -323,32 +325,21 @@ int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t
 int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts, pdlpx_result* results,
                           double* const* x_out, double* const* y_out) {
     if (count < 0 || (count > 0 && (lps == nullptr || results == nullptr))) return PDLPX_E_INVALID;
-    // Sequential device solves, one engine per LP (the persistent batched
-    // kernel replaces this loop; results are identical by construction).
-    for (int32_t k = 0; k < count; ++k) {
-        pdlpx_solver h;
-        if (opts) h.engine.setOptions(*opts);
-        const pdlpx_lp& lp = lps[k];
-        int32_t rc = guarded(&h, [&] {
-            return h.engine.load(lp.m, lp.n, lp.nnz, lp.row_ptr, lp.col_idx, lp.val, lp.obj, lp.col_lb, lp.col_ub,
-                                 lp.row_lb, lp.row_ub, lp.sense, lp.obj_offset);
-        });
-        if (rc != PDLPX_OK) {
-            g_last_error = h.engine.last_error;
-            return rc;
-        }
-        if (lp.warm_x && lp.warm_y) h.engine.setWarmStart(lp.warm_x, lp.n, lp.warm_y, lp.m);
-        rc = guarded(&h, [&] { return h.engine.solve(&results[k]); });
-        if (rc != PDLPX_OK) {
-            g_last_error = h.engine.last_error;
-            return rc;
-        }
-        if (x_out && x_out[k] && !h.engine.primal().empty())
-            std::memcpy(x_out[k], h.engine.primal().data(), sizeof(double) * h.engine.primal().size());
-        if (y_out && y_out[k] && !h.engine.dual().empty())
-            std::memcpy(y_out[k], h.engine.dual().data(), sizeof(double) * h.engine.dual().size());
+    if (count == 0) return PDLPX_OK;
+    pdlpx_options o;
+    if (opts)
+        o = *opts;
+    else
+        pdlpx_options_default(&o);
+    try {
+        return pdlpx::batchSolve(count, lps, o, results, x_out, y_out, g_last_error);
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return PDLPX_E_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return PDLPX_E_INVALID;
     }
-    return PDLPX_OK;
 }
 
 int32_t pdlpx_csr_spmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx,

@@ -83,6 +83,10 @@ private:
 // Threads per row for the CSR kernels, from the mean row length.
 int32_t pickGroup(int64_t nnz, int32_t rows);
 
+// Batched solve of independent LPs in one persistent cluster launch (batch.cu).
+int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
+                   double* const* x_out, double* const* y_out, std::string& err);
+
 // Message returned by pdlpx_last_error(NULL) on this thread (calls without a handle).
 void setGlobalError(const std::string& msg);
 

@@ -48,7 +48,7 @@ struct DevState {
     int stall;      // checks since the best KKT score improved (mixed mode)
     int have_prev;  // adaptive step: previous check stored
     int cert_hit;   // 1 infeasible certificate, 2 unbounded certificate
-    int pad0;
+    int switch_total;  // iteration count at the FP32 -> FP64 hand-over (-1: none)
     double fpe0, last_fpe;   // restart bookkeeping (initial_fpe / last_trial_fpe)
     double esum, elast;      // PI controller integral / last error
     double best_pw, best_score;
@@ -504,6 +504,95 @@ __device__ __forceinline__ double slotInit(int op) {
     return op == OP_SUM ? 0.0 : (op == OP_MIN ? CUDART_INF : -CUDART_INF);
 }
 
+// Row terms of the check for one row with (A x_hat)_i = ax: primal residual
+// (pdlp.cpp:1106-1117), dual-objective row term (pdlp.cpp:1185-1199), dual
+// movement, and the Farkas / primal-ray certificate terms of pdlp.cpp:119-284
+// in scaled space.
+__device__ __forceinline__ void accRowMetrics(double (&acc)[kRowSlots], const DevConst& dc, double ax, double rl,
+                                              double ru, double r, double y, double yi) {
+    const double cl = ax < rl ? rl : (ru < ax ? ru : ax);
+    const double v = (ax - cl) / (dc.con_scale * r);
+    acc[R_PRES_SQ] += v * v;
+    acc[R_PRES_MAX] = fmax(acc[R_PRES_MAX], fabs(v));
+    const double dy = y - yi;
+    const bool hl = isfinite(rl), hu = isfinite(ru);
+    double yp = y;
+    if (!hu) yp = fmin(yp, 0.0);
+    if (!hl) yp = fmax(yp, 0.0);
+    if (yp > 0.0 && hu)
+        acc[R_DOBJ_ROW] -= yp * ru;
+    else if (yp < 0.0 && hl)
+        acc[R_DOBJ_ROW] -= yp * rl;
+    acc[R_DDIST] += dy * dy;
+    const double yo = y * r;
+    acc[R_YNORM] += yo * yo;
+    const double yq = dc.obj_sign * yo;
+    if (hu && !hl) acc[R_MIN_LE] = fmin(acc[R_MIN_LE], yq);
+    if (hl && !hu) acc[R_MAX_GE] = fmax(acc[R_MAX_GE], yq);
+    const double ys = dc.obj_sign * y;
+    if (rl == ru)
+        acc[R_FARKAS_ROW] += ys * rl;
+    else if (ys > 0.0 && hu)
+        acc[R_FARKAS_ROW] += ys * ru;
+    else if (ys < 0.0 && hl)
+        acc[R_FARKAS_ROW] += ys * rl;
+    const double axr = ax / r;
+    if (hl && hu)
+        acc[R_UB_TWO] = fmax(acc[R_UB_TWO], fabs(axr));
+    else if (hu)
+        acc[R_UB_LE] = fmax(acc[R_UB_LE], axr);
+    else if (hl)
+        acc[R_UB_GE] = fmin(acc[R_UB_GE], axr);
+}
+
+// Column terms of the check for one column with (A^T y_hat)_j = aty and
+// (A^T (y_hat - y_init))_j = atdy: primal objective, projected dual residual
+// (pdlp.cpp:1123-1145), dual-objective column term (pdlp.cpp:1170-1184), primal
+// movement and interaction, certificate terms.  Bound activity is judged
+// against the bounds the iterate precision T clamped to: an FP32 x_hat sitting
+// on float(ub) < ub is at its bound, not interior.
+template <class T>
+__device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const DevConst& dc, double xh, double xi,
+                                              double c, double lb, double ub, double cs, double aty, double atdy) {
+    const double dx = xh - xi;
+    const bool hl = isfinite(lb), hu = isfinite(ub);
+    acc[C_POBJ] += c * xh;
+    const double g = c + aty;
+    const double lbT = static_cast<double>(static_cast<T>(lb));
+    const double ubT = static_cast<double>(static_cast<T>(ub));
+    double dr;
+    if (xh <= lbT + 1e-12 && hl)
+        dr = fmin(g, 0.0);
+    else if (xh >= ubT - 1e-12 && hu)
+        dr = fmax(g, 0.0);
+    else
+        dr = g;
+    const double d = dr / (dc.obj_scale * cs);
+    acc[C_DRES_SQ] += d * d;
+    acc[C_DRES_MAX] = fmax(acc[C_DRES_MAX], fabs(d));
+    double gp = g;
+    if (!hl) gp = fmin(gp, 0.0);
+    if (!hu) gp = fmax(gp, 0.0);
+    if (gp > 0.0 && hl)
+        acc[C_DOBJ_COL] += gp * lb;
+    else if (gp < 0.0 && hu)
+        acc[C_DOBJ_COL] += gp * ub;
+    acc[C_PDIST] += dx * dx;
+    acc[C_INTER] += atdy * dx;
+    const double xo = xh * cs;
+    acc[C_XNORM] += xo * xo;
+    if (hl) acc[C_MIN_XLB] = fmin(acc[C_MIN_XLB], xo);
+    if (hu) acc[C_MAX_XUB] = fmax(acc[C_MAX_XUB], xo);
+    const double g2 = dc.obj_sign * aty;
+    const double gq = g2 / cs;
+    if (hl) acc[C_MIN_GLB] = fmin(acc[C_MIN_GLB], gq);
+    if (hu) acc[C_MAX_GUB] = fmax(acc[C_MAX_GUB], gq);
+    if (g2 > 0.0 && hl)
+        acc[C_COLSUP] += g2 * lb;
+    else if (g2 < 0.0 && hu)
+        acc[C_COLSUP] += g2 * ub;
+}
+
 // FP64 row pass of the check: A x_hat and all row metrics (pdlp_kernels.cu:280-371,
 // pdlp.cpp:1106-1120, 1185-1199, certificates pdlp.cpp:119-284).
 template <int G, class T>
@@ -528,41 +617,8 @@ __global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
         if (valid) ax = rowDot<G, double>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh);
         ax = groupSum<G>(ax);
         if (valid && lane == 0) {
-            const double rl = p.rl64[i], ru = p.ru64[i], r = p.rs64[i];
-            const double cl = ax < rl ? rl : (ru < ax ? ru : ax);
-            const double v = (ax - cl) / (dc.con_scale * r);
-            acc[R_PRES_SQ] += v * v;
-            acc[R_PRES_MAX] = fmax(acc[R_PRES_MAX], fabs(v));
-            const double y = static_cast<double>(p.yh[i]);
-            const double dy = y - static_cast<double>(p.yi[i]);
-            const bool hl = isfinite(rl), hu = isfinite(ru);
-            double yp = y;
-            if (!hu) yp = fmin(yp, 0.0);
-            if (!hl) yp = fmax(yp, 0.0);
-            if (yp > 0.0 && hu)
-                acc[R_DOBJ_ROW] -= yp * ru;
-            else if (yp < 0.0 && hl)
-                acc[R_DOBJ_ROW] -= yp * rl;
-            acc[R_DDIST] += dy * dy;
-            const double yo = y * r;
-            acc[R_YNORM] += yo * yo;
-            const double yq = dc.obj_sign * yo;
-            if (hu && !hl) acc[R_MIN_LE] = fmin(acc[R_MIN_LE], yq);
-            if (hl && !hu) acc[R_MAX_GE] = fmax(acc[R_MAX_GE], yq);
-            const double ys = dc.obj_sign * y;
-            if (rl == ru)
-                acc[R_FARKAS_ROW] += ys * rl;
-            else if (ys > 0.0 && hu)
-                acc[R_FARKAS_ROW] += ys * ru;
-            else if (ys < 0.0 && hl)
-                acc[R_FARKAS_ROW] += ys * rl;
-            const double axr = ax / r;
-            if (hl && hu)
-                acc[R_UB_TWO] = fmax(acc[R_UB_TWO], fabs(axr));
-            else if (hu)
-                acc[R_UB_LE] = fmax(acc[R_UB_LE], axr);
-            else if (hl)
-                acc[R_UB_GE] = fmin(acc[R_UB_GE], axr);
+            accRowMetrics(acc, dc, ax, p.rl64[i], p.ru64[i], p.rs64[i], static_cast<double>(p.yh[i]),
+                          static_cast<double>(p.yi[i]));
             if (adapt) {
                 const double d = ax - p.prev_ax[i];
                 acc[R_ADAPT] += p.sig64[i] * d * d;
@@ -599,47 +655,8 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
         atdy = groupSum<G>(atdy);
         if (valid && lane == 0) {
             const double xh = static_cast<double>(p.xh[j]);
-            const double dx = xh - static_cast<double>(p.xi[j]);
-            const double c = p.c64[j], lb = p.lb64[j], ub = p.ub64[j], cs = p.cs64[j];
-            const bool hl = isfinite(lb), hu = isfinite(ub);
-            acc[C_POBJ] += c * xh;
-            const double g = c + aty;
-            // Bound activity is judged against the bounds the iterate precision
-            // clamped to (FP32-rounded in mixed mode): an FP32 x_hat sitting on
-            // float(ub) < ub is at its bound, not interior.
-            const double lbT = static_cast<double>(static_cast<T>(lb));
-            const double ubT = static_cast<double>(static_cast<T>(ub));
-            double dr;
-            if (xh <= lbT + 1e-12 && hl)
-                dr = fmin(g, 0.0);
-            else if (xh >= ubT - 1e-12 && hu)
-                dr = fmax(g, 0.0);
-            else
-                dr = g;
-            const double d = dr / (dc.obj_scale * cs);
-            acc[C_DRES_SQ] += d * d;
-            acc[C_DRES_MAX] = fmax(acc[C_DRES_MAX], fabs(d));
-            double gp = g;
-            if (!hl) gp = fmin(gp, 0.0);
-            if (!hu) gp = fmax(gp, 0.0);
-            if (gp > 0.0 && hl)
-                acc[C_DOBJ_COL] += gp * lb;
-            else if (gp < 0.0 && hu)
-                acc[C_DOBJ_COL] += gp * ub;
-            acc[C_PDIST] += dx * dx;
-            acc[C_INTER] += atdy * dx;
-            const double xo = xh * cs;
-            acc[C_XNORM] += xo * xo;
-            if (hl) acc[C_MIN_XLB] = fmin(acc[C_MIN_XLB], xo);
-            if (hu) acc[C_MAX_XUB] = fmax(acc[C_MAX_XUB], xo);
-            const double g2 = dc.obj_sign * aty;
-            const double gq = g2 / cs;
-            if (hl) acc[C_MIN_GLB] = fmin(acc[C_MIN_GLB], gq);
-            if (hu) acc[C_MAX_GUB] = fmax(acc[C_MAX_GUB], gq);
-            if (g2 > 0.0 && hl)
-                acc[C_COLSUP] += g2 * lb;
-            else if (g2 < 0.0 && hu)
-                acc[C_COLSUP] += g2 * ub;
+            accColMetrics<T>(acc, dc, xh, static_cast<double>(p.xi[j]), p.c64[j], p.lb64[j], p.ub64[j], p.cs64[j],
+                             aty, atdy);
             if (adapt) {
                 const double dd = xh - p.prev_xh[j];
                 acc[C_ADAPT] += dd * dd / p.tau64[j];

@@ -1,0 +1,104 @@
+"""Batched solve (pdlpx_batch_solve: one persistent cluster launch for many LPs).
+
+* parity: a mixed batch of the reference's golden cases (optimal, infeasible,
+  unbounded, trivial) reproduces the reference's statuses, and objectives within
+  2 * tol * (1 + |obj|) for LPs solved to relative KKT tol (two points that each
+  meet the gap test), within the mipx GPU-vs-CPU bounds otherwise;
+* batch invariance: an LP's result is bit-identical when solved alone and inside
+  a batch of other LPs (one cluster per LP, fixed reduction order);
+* cluster sizes 1, 2 and 8 and the FP64 mode all solve the same LPs.
+"""
+import numpy as np
+import pytest
+
+import golden_cases as GC
+from mipx_b200 import generators as G
+from mipx_b200.pdlp import PdlpOptions, Precision, Status, batch_solve
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
+
+
+def _check_against_golden(name, r):
+    e = GC.INDEX[name]
+    assert int(r.status) == e["status"], (name, r.status)
+    if e["status"] != Status.Optimal:
+        return
+    ref = e["objective"]
+    tol = e["options"]["optimality_tol"]
+    if e["options"]["primal_tol"] <= 1e-6:
+        assert abs(r.objective - ref) <= 2 * tol * (1 + abs(ref)), (name, r.objective, ref)
+    else:
+        bound = 1e-4 if name in ("medium", "simple") else 1e-3 * max(1.0, abs(ref))
+        assert abs(r.objective - ref) <= max(bound, 2e-4 * abs(ref)), (name, r.objective, ref)
+
+
+# golden cases that share one option set can go into one batch
+DEFAULT_CASES = ["simple", "col_bound_binding", "maximize", "medium", "bounds_only", "empty",
+                 "unbounded_bounds_only"]
+TIGHT_CASES = ["medium_tight", "ranged", "rand_60x150", "rand_200x500", "rand_500x1250", "rand_2000x5000"]
+
+
+@pytest.mark.parametrize("precision", [Precision.Mixed, Precision.FP64])
+def test_batch_golden_tight(precision):
+    probs = [GC.problem(k) for k in TIGHT_CASES]
+    o = PdlpOptions(verbose=False, max_iter=500000, precision=precision, **TIGHT)
+    out = batch_solve(probs, o)
+    for name, (r, x, y) in zip(TIGHT_CASES, out):
+        _check_against_golden(name, r)
+        assert r.used_gpu and r.kernel_launches == 1
+
+
+def test_batch_golden_default_options_with_trivial_lps():
+    probs = [GC.problem(k) for k in DEFAULT_CASES]
+    o = PdlpOptions(verbose=False, max_iter=500000)
+    out = batch_solve(probs, o)
+    for name, (r, x, y) in zip(DEFAULT_CASES, out):
+        _check_against_golden(name, r)
+
+
+def test_batch_statuses():
+    names = ["infeasible", "infeasible_eq", "unbounded_constrained"]
+    out = batch_solve([GC.problem(k) for k in names], PdlpOptions(verbose=False, max_iter=100000))
+    for name, (r, _, _) in zip(names, out):
+        assert int(r.status) == GC.INDEX[name]["status"], name
+
+
+def test_batch_invariance_alone_and_in_mix():
+    target, _ = G.random_lp(700, 1750, 4, 12, 77)
+    others = [G.random_lp(m, int(2.5 * m), 4, 12, 500 + k)[0] for k, m in enumerate(
+        [200, 3000, 450, 1200, 900, 2500, 300, 1600] * 5)]
+    o = PdlpOptions(verbose=False, **TIGHT)
+    alone = batch_solve([target], o)[0]
+    mix = batch_solve(others[:20] + [target] + others[20:], o)[20]
+    assert alone[0].status == Status.Optimal
+    assert alone[0].iterations == mix[0].iterations
+    assert alone[0].objective == mix[0].objective
+    np.testing.assert_array_equal(alone[1], mix[1])
+    np.testing.assert_array_equal(alone[2], mix[2])
+
+
+@pytest.mark.parametrize("cluster", [2, 4])
+def test_batch_shared_memory_phase_matches_global_phase(cluster):
+    """The FP32 phase run from the cluster's shared memory (slices resident, gathers
+    over distributed shared memory) and the same phase over global memory reach
+    the same tolerance-level answers on LPs that fit and LPs that do not."""
+    lps = [G.random_lp(m, int(2.5 * m), 4, 12, 1300 + k)[0] for k, m in enumerate((150, 700, 1600, 3000, 9000))]
+    base = dict(verbose=False, batch_cluster=cluster, **TIGHT)
+    res = batch_solve(lps, PdlpOptions(batch_resident=True, **base))
+    glob = batch_solve(lps, PdlpOptions(batch_resident=False, **base))
+    for (r, x, _), (q, _, _) in zip(res, glob):
+        assert r.status == q.status == Status.Optimal
+        assert abs(r.objective - q.objective) <= 2e-6 * (1 + abs(q.objective))
+
+
+@pytest.mark.parametrize("cluster", [1, 2, 8])
+def test_batch_cluster_sizes(cluster):
+    lps = [G.random_lp(m, int(2.5 * m), 4, 12, 900 + k)[0] for k, m in enumerate((300, 1000, 2200))]
+    o = PdlpOptions(verbose=False, batch_cluster=cluster, **TIGHT)
+    ref = batch_solve(lps, PdlpOptions(verbose=False, **TIGHT))
+    out = batch_solve(lps, o)
+    for (r, _, _), (q, _, _) in zip(out, ref):
+        assert r.status == q.status == Status.Optimal
+        assert abs(r.objective - q.objective) <= 2e-6 * (1 + abs(q.objective))
