@@ -119,11 +119,11 @@ typedef struct pdlpx_options {
                                          deterministic */
     int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step */
     int32_t shape_dual;               /* 0 = automatic; k > 0 pins launch shape k-1 of the dual step */
-    int32_t batch_cluster;            /* pdlpx_batch_solve: CTAs per LP (thread-block cluster size,
-                                         1..8; 0 = 4) */
-    int32_t batch_resident;           /* pdlpx_batch_solve, mixed precision: 1 (default) runs an LP's FP32
-                                         phase from the cluster's shared memory when its slices fit;
-                                         0 keeps every phase in global memory */
+    int32_t batch_pack_mb;            /* pdlpx_batch_solve: device megabytes per pack of LPs solved
+                                         together (0 = 85% of free device memory); larger batches are
+                                         split into packs solved one after another */
+    int32_t batch_compact;            /* pdlpx_batch_solve: 1 (default) drops finished LPs from the
+                                         launches once they idle enough tiles; 0 never */
     int32_t reserved[3];
 } pdlpx_options;
 

@@ -1,32 +1,32 @@
-// Batched PDLP: many independent LPs in one persistent launch of thread-block
-// clusters (pdlpx_batch_solve).
+// Packed batched PDLP (pdlpx_batch_solve).
 //
-// Each cluster of K CTAs pulls LPs from an atomic queue (largest first) and
-// solves one LP completely before taking the next: the LP's columns and rows
-// are split across the K CTAs, the primal and dual phases of every PDHG
-// iteration are separated by hardware cluster barriers, and the power
-// iteration, FP64 check pass, controller (restart / primal weight / polish /
-// termination, the same controlStep as the single-LP graph) and FP32 -> FP64
-// hand-over all run inside the kernel.  Every CTA of a cluster reads the same
-// partials after a barrier and runs the controller on its own copy of the
-// solver state, so all control decisions -- and therefore the barrier
-// sequence -- are identical across the cluster by construction; there are no
-// spin waits.  Vectors written by other CTAs during the kernel are read with
-// L2-coherent loads (ld.global.cg); the matrix and per-row / per-column
-// constants are read-only for the whole launch.
+// The LPs of a pack share one device image with global numbering: LP l owns
+// rows [r0_l, r0_l + m_l) and columns [c0_l, c0_l + n_l) of a block-diagonal
+// A and A^T, so the gathers of the step kernels are those of the single-LP
+// kernels.  Rows and columns are cut into tiles that never straddle two LPs;
+// a tile is as tall as one block of the LP's launch shape covers.  One launch
+// of a step kernel covers every tile of every LP with that shape: the block
+// reads its tile and the tile's LP state, then runs the single-LP row bodies
+// (primalRows / dualRows) in the LP's current precision with the LP's own step
+// size, primal weight and Halpern count.  LPs restart, switch precision,
+// polish and finish independently: per-LP DevState / DevConst, and the
+// single-LP controlStep run by one warp per LP over the LP's tile partials in
+// fixed order.  A restart cycle of the whole pack -- N iterations, the FP64
+// check, the controllers, restart copies and FP32 -> FP64 hand-overs -- is one
+// CUDA graph launch.  When finished LPs leave enough tiles idle, the host drops
+// them from the tile lists and captures a smaller graph.
 //
-// An LP is solved by one cluster with the same code and reduction order
-// whatever else is in the batch, so its result is bit-identical alone and in
-// any mix (batch invariance).
-#include <cooperative_groups.h>
-
+// An LP's tiles, launch shape and reduction order depend on that LP alone, so
+// its result is bit-identical alone and in any mix (batch invariance).  A batch
+// larger than the device budget is split into packs solved one after another.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
-#include <numeric>
+#include <memory>
 #include <random>
 #include <thread>
 #include <vector>
@@ -34,842 +34,314 @@
 #include "control.cuh"
 #include "engine.hpp"
 #include "kernels.cuh"
-
-namespace cg = cooperative_groups;
+#include "shapes.cuh"
 
 namespace pdlpx {
 namespace {
 
-constexpr int kMaxCluster = 8;
-constexpr int kSlots = kRowSlots + kColSlots;
-constexpr int kPartStride = kSlots + 3;  // per CTA rank: check slots + 3 power-iteration slots
-
-struct BatchLp {
-    IterArgs<float> it32;
+struct PackArgs {
+    IterArgs<float> it32;  // global arrays of the pack (st is set per tile)
     IterArgs<double> it64;
     CheckArgs<float> ck32;
     CheckArgs<double> ck64;
-    const float* a_v32;
-    const float* at_v32;
-    double* pi_x;
+    const int4* ctiles;  // column tiles: (LP, first column, end column, 0)
+    const int4* rtiles;  // row tiles
+    const int4* lpt;     // per LP: first column tile, column tiles, first row tile, row tiles
+    DevState* st;
+    const DevConst* dc;
+    PowerState* ps;
+    int* flags;           // per LP after each cycle: 1 done, 2 FP64 iterates
+    int* counters;        // [0] LPs whose power iteration has finished
+    double* part_cols;    // [column tile][kColSlots]
+    double* part_rows;    // [row tile][kRowSlots]
+    double* pi_x;         // power iteration vectors (global numbering)
     double* pi_y;
     double* pi_xn;
-    double* part;  // [kMaxCluster][kPartStride]
-    DevState* st;  // initial state in, final state out
-    const DevConst* dc;
-    int m, n, gA, gAT, mixed, sv_max_iter;
+    double* pi_part;      // [column tile][2]
+    int L, mixed, sv_max_iter;
     double sv_tol;
-    // Slices: rank r owns rows [r*pr, (r+1)*pr) and columns [r*pc, (r+1)*pc) (clipped).
-    int pr, pc;
-    // Shared-memory residency: 1 when the FP32 phase runs from the cluster's
-    // shared memory; capA / capAT = largest per-rank nonzero count of A / A^T.
-    int smem, capA, capAT;
 };
 
-// Shared-memory image of one CTA's slice (identical offsets on every rank, so a
-// remote address is the local address mapped to the owner's rank).
-struct SLayout {
-    int o_cp, o_rp, o_xc, o_yc, o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_xi, o_xh, o_xr, o_yi, o_yh;
-    int bytes;
-};
+constexpr int kCtlWarps = 4;  // LPs per block of the per-LP kernels
 
-__host__ __device__ inline int sAlign(int b) { return (b + 15) & ~15; }
-
-__host__ __device__ inline SLayout smemLayout(int pr, int pc, int capA, int capAT) {
-    SLayout L{};
-    int o = 0;
-    L.o_cp = o;
-    o += sAlign(16 * pc);
-    L.o_rp = o;
-    o += sAlign(16 * pr);
-    L.o_xc = o;
-    o += sAlign(8 * pc);
-    L.o_yc = o;
-    o += sAlign(8 * pr);
-    L.o_aptr = o;
-    o += sAlign(4 * (pr + 1));
-    L.o_aidx = o;
-    o += sAlign(4 * capA);
-    L.o_aval = o;
-    o += sAlign(4 * capA);
-    L.o_atptr = o;
-    o += sAlign(4 * (pc + 1));
-    L.o_atidx = o;
-    o += sAlign(4 * capAT);
-    L.o_atval = o;
-    o += sAlign(4 * capAT);
-    L.o_xi = o;
-    o += sAlign(4 * pc);
-    L.o_xh = o;
-    o += sAlign(4 * pc);
-    L.o_xr = o;
-    o += sAlign(4 * pc);
-    L.o_yi = o;
-    o += sAlign(4 * pr);
-    L.o_yh = o;
-    o += sAlign(4 * pr);
-    L.bytes = o;
-    return L;
+__device__ __forceinline__ double combine(int op, double a, double b) {
+    return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
 }
 
-// Dynamic shared memory requested per CTA when some LP of the batch is resident.
-constexpr int kSmemBudget = 220 * 1024;
-
-template <class X>
-__device__ __forceinline__ double ldc(const X* p) {
-    return static_cast<double>(__ldcg(p));
-}
-
-// Row dot product with the gathered vector read through L2 (coherent across
-// the cluster's SMs); matrix entries through the read-only path.
-template <int G, int U, class V, class X>
-__device__ __forceinline__ double rowDotC(int b, int e, int lane, const int* __restrict__ idx,
-                                          const V* __restrict__ val, const X* x) {
-    double s[U];
+// Reduce the [tile][NS] partials of `count` tiles starting at `first` across
+// one warp, in an order fixed by the tile count alone; lane 0 holds the result.
+template <int NS>
+__device__ __forceinline__ void warpTiles(const double* part, int first, int count, int lane, const int (&ops)[NS],
+                                          double (&out)[NS]) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) s[u] = 0.0;
-    for (int k0 = b + lane; k0 < e; k0 += U * G) {
-        int c[U];
-        V v[U];
+    for (int s = 0; s < NS; ++s) out[s] = slotInit(ops[s]);
+    for (int t = lane; t < count; t += 32) {
+        const double* p = part + static_cast<size_t>(first + t) * NS;
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int k = k0 + u * G;
-            const bool ok = k < e;
-            c[u] = ok ? __ldg(idx + k) : 0;
-            v[u] = ok ? __ldg(val + k) : V(0);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) s[u] += static_cast<double>(v[u]) * ldc(x + c[u]);
-    }
-    double t = s[0];
-#pragma unroll
-    for (int u = 1; u < U; ++u) t += s[u];
-    return t;
-}
-
-// ---- PDHG phases over a slice [lo, hi) of columns / rows -------------------
-// Trip counts are block-uniform (all threads step `base` together), so the
-// width-G shuffles of groupSum always see their whole warp.
-template <int G, class T>
-__device__ void slicePrimal(const IterArgs<T>& p, int lo, int hi, double step, double pw, double lam, bool last) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int j = base + threadIdx.x / G;
-        const bool valid = j < hi;
-        double s = 0.0;
-        if (valid) s = rowDotC<G, 4>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yc);
-        s = groupSum<G>(s);
-        if (valid && lane == 0) {
-            const ColPack<T> q = p.cp[j];
-            const double xcd = p.xc[j], xid = p.xi[j];
-            const double tau = step * static_cast<double>(q.tau) / pw;
-            double xh = xcd - tau * (static_cast<double>(q.c) + s);
-            const double lb = q.lb, ub = q.ub;
-            if (xh < lb) xh = lb;
-            if (xh > ub) xh = ub;
-            const double xr = 2.0 * xh - xcd;
-            p.xr[j] = static_cast<T>(xr);
-            p.xc[j] = lam * xr + (1.0 - lam) * xid;
-            if (last) p.xh[j] = static_cast<T>(xh);
-        }
-    }
-}
-
-template <int G, class T>
-__device__ void sliceDual(const IterArgs<T>& p, int lo, int hi, double step, double pw, double lam, bool last) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int i = base + threadIdx.x / G;
-        const bool valid = i < hi;
-        double s = 0.0;
-        if (valid) s = rowDotC<G, 4>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xr);
-        s = groupSum<G>(s);
-        if (valid && lane == 0) {
-            const RowPack<T> q = p.rp[i];
-            const double ycd = p.yc[i], yid = p.yi[i];
-            const double sig = step * static_cast<double>(q.sigma) * pw;
-            const double v = ycd + sig * s;
-            const double rl = q.rl, ru = q.ru;
-            const int type = static_cast<int>(q.type);
-            double py;
-            if (type == 0) {
-                py = v - sig * rl;
-            } else if (type == 1) {
-                py = v - sig * ru;
-                if (py < 0.0) py = 0.0;
-            } else if (type == 2) {
-                py = v - sig * rl;
-                if (py > 0.0) py = 0.0;
-            } else {
-                if (v >= sig * ru)
-                    py = v - sig * ru;
-                else if (v <= sig * rl)
-                    py = v - sig * rl;
-                else
-                    py = 0.0;
-            }
-            const double yr = 2.0 * py - ycd;
-            p.yc[i] = lam * yr + (1.0 - lam) * yid;
-            if (last) p.yh[i] = static_cast<T>(py);
-        }
-    }
-}
-
-// ---- FP64 check pass over a slice (same per-row / per-column terms as checkRows / checkCols)
-template <int G, class T>
-__device__ void sliceCheckRows(const CheckArgs<T>& p, const DevConst& dc, int lo, int hi, double (&acc)[kRowSlots]) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int i = base + threadIdx.x / G;
-        const bool valid = i < hi;
-        double ax = 0.0;
-        if (valid) ax = rowDotC<G, 4>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh);
-        ax = groupSum<G>(ax);
-        if (valid && lane == 0)
-            accRowMetrics(acc, dc, ax, p.rl64[i], p.ru64[i], p.rs64[i], static_cast<double>(p.yh[i]),
-                          static_cast<double>(p.yi[i]));
-    }
-}
-
-template <int G, class T>
-__device__ void sliceCheckCols(const CheckArgs<T>& p, const DevConst& dc, int lo, int hi, double (&acc)[kColSlots]) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int j = base + threadIdx.x / G;
-        const bool valid = j < hi;
-        double aty = 0.0, atdy = 0.0;
-        if (valid) {
-            for (int k = p.at_ptr[j] + lane; k < p.at_ptr[j + 1]; k += G) {
-                const int c = __ldg(p.at_idx + k);
-                const double v = __ldg(p.at_val + k);
-                const double yv = ldc(p.yh + c);
-                aty += v * yv;
-                atdy += v * (yv - ldc(p.yi + c));
-            }
-        }
-        aty = groupSum<G>(aty);
-        atdy = groupSum<G>(atdy);
-        if (valid && lane == 0)
-            accColMetrics<T>(acc, dc, static_cast<double>(p.xh[j]), static_cast<double>(p.xi[j]), p.c64[j], p.lb64[j],
-                             p.ub64[j], p.cs64[j], aty, atdy);
-    }
-}
-
-// ---- power iteration phases ------------------------------------------------
-template <int G, class V>
-__device__ void slicePowerRows(const int* ptr, const int* idx, const V* val, const double* x, double* y, int lo,
-                               int hi) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int i = base + threadIdx.x / G;
-        const bool valid = i < hi;
-        double s = 0.0;
-        if (valid) s = rowDotC<G, 4>(ptr[i], ptr[i + 1], lane, idx, val, x);
-        s = groupSum<G>(s);
-        if (valid && lane == 0) y[i] = s;
-    }
-}
-
-template <int G, class V>
-__device__ void slicePowerCols(const int* ptr, const int* idx, const V* val, const double* y, const double* x,
-                               double* xn, int lo, int hi, double (&acc)[2]) {
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = lo; base < hi; base += per) {
-        const int j = base + threadIdx.x / G;
-        const bool valid = j < hi;
-        double s = 0.0;
-        if (valid) s = rowDotC<G, 4>(ptr[j], ptr[j + 1], lane, idx, val, y);
-        s = groupSum<G>(s);
-        if (valid && lane == 0) {
-            xn[j] = s;
-            acc[0] += x[j] * s;
-            acc[1] += s * s;
-        }
-    }
-}
-
-#define PDLPX_BATCH_G(GV, CALL)                       \
-    switch (GV) {                                     \
-        case 1: { constexpr int GG = 1; CALL; } break;   \
-        case 2: { constexpr int GG = 2; CALL; } break;   \
-        case 4: { constexpr int GG = 4; CALL; } break;   \
-        case 8: { constexpr int GG = 8; CALL; } break;   \
-        case 16: { constexpr int GG = 16; CALL; } break; \
-        default: { constexpr int GG = 32; CALL; } break; \
-    }
-
-__device__ inline int batchGroup(int g) { return g > 32 ? 32 : g; }
-
-// Spectral-norm estimate of one LP by the cluster (pdlp.cpp:748-795, FP64 vectors).
-template <class V>
-__device__ double clusterPower(const BatchLp& d, const int* a_ptr, const int* a_idx, const V* a_val,
-                               const int* at_ptr, const int* at_idx, const V* at_val, int rank, int K,
-                               cg::cluster_group& cl, int r0, int r1, int c0, int c1, double* sred) {
-    const int gA = batchGroup(d.gA), gAT = batchGroup(d.gAT);
-    double s2 = 1.0;
-    for (int it = 0; it < d.sv_max_iter; ++it) {
-        PDLPX_BATCH_G(gA, (slicePowerRows<GG, V>(a_ptr, a_idx, a_val, d.pi_x, d.pi_y, r0, r1)));
-        cl.sync();
-        double acc[2] = {0.0, 0.0};
-        PDLPX_BATCH_G(gAT, (slicePowerCols<GG, V>(at_ptr, at_idx, at_val, d.pi_y, d.pi_x, d.pi_xn, c0, c1, acc)));
-        const int ops2[2] = {OP_SUM, OP_SUM};
-        blockReduceSlots<2>(acc, ops2, d.part + rank * kPartStride + kSlots);
-        cl.sync();
-        if (threadIdx.x == 0) {
-            double a = 0.0, b = 0.0;
-            for (int r = 0; r < K; ++r) {
-                a += ldc(d.part + r * kPartStride + kSlots);
-                b += ldc(d.part + r * kPartStride + kSlots + 1);
-            }
-            sred[0] = a;
-            sred[1] = sqrt(b);
-        }
-        __syncthreads();
-        s2 = sred[0];
-        const double nrm = sred[1];
-        double acc1[1] = {0.0};
-        for (int j = c0 + threadIdx.x; j < c1; j += kBlock) {
-            const double xn = d.pi_xn[j];
-            const double dd = xn - s2 * d.pi_x[j];
-            acc1[0] += dd * dd;
-            if (nrm >= 1e-15) d.pi_x[j] = xn / nrm;
-        }
-        const int ops1[1] = {OP_SUM};
-        blockReduceSlots<1>(acc1, ops1, d.part + rank * kPartStride + kSlots + 2);
-        cl.sync();
-        if (threadIdx.x == 0) {
-            double rr = 0.0;
-            for (int r = 0; r < K; ++r) rr += ldc(d.part + r * kPartStride + kSlots + 2);
-            sred[2] = sqrt(rr);
-        }
-        __syncthreads();
-        const double resid = sred[2];
-        __syncthreads();
-        if (nrm < 1e-15 || resid < d.sv_tol * fabs(s2)) break;
-    }
-    return s2;
-}
-
-// One restart cycle of one LP: N iterations, check, controller, restart copy, hand-over.
-template <class T>
-__device__ void clusterCycle(const BatchLp& d, const IterArgs<T>& it, const CheckArgs<T>& ck, int rank, int K,
-                             cg::cluster_group& cl, DevState& sst, const DevConst& sdc, int r0, int r1, int c0,
-                             int c1) {
-    const int gA = batchGroup(d.gA), gAT = batchGroup(d.gAT);
-    const int cur = sst.phase == 0 ? sst.total : sst.polish_count;
-    const int lim = sst.phase == 0 ? sdc.max_iter : sdc.polish_max_iter;
-    const int batch = min(sdc.N, lim - cur);
-    const double step = sst.step, pw = sst.pw;
-    const int inner = sst.inner;
-    for (int k = 1; k <= batch; ++k) {
-        const double lam = static_cast<double>(inner + k) / static_cast<double>(inner + k + 1);
-        const bool last = k == batch;
-        PDLPX_BATCH_G(gAT, (slicePrimal<GG, T>(it, c0, c1, step, pw, lam, last)));
-        cl.sync();
-        PDLPX_BATCH_G(gA, (sliceDual<GG, T>(it, r0, r1, step, pw, lam, last)));
-        cl.sync();
-    }
-    int rops[kRowSlots], cops[kColSlots];
-    double racc[kRowSlots], cacc[kColSlots];
-#pragma unroll
-    for (int s = 0; s < kRowSlots; ++s) {
-        rops[s] = rowSlotOp(s);
-        racc[s] = slotInit(rops[s]);
+        for (int s = 0; s < NS; ++s) out[s] = combine(ops[s], out[s], p[s]);
     }
 #pragma unroll
-    for (int s = 0; s < kColSlots; ++s) {
-        cops[s] = colSlotOp(s);
-        cacc[s] = slotInit(cops[s]);
-    }
-    PDLPX_BATCH_G(gA, (sliceCheckRows<GG, T>(ck, sdc, r0, r1, racc)));
-    PDLPX_BATCH_G(gAT, (sliceCheckCols<GG, T>(ck, sdc, c0, c1, cacc)));
-    blockReduceSlots<kRowSlots>(racc, rops, d.part + rank * kPartStride);
-    blockReduceSlots<kColSlots>(cacc, cops, d.part + rank * kPartStride + kRowSlots);
-    cl.sync();
-    if (threadIdx.x == 0) {
-        double rows[kRowSlots], cols[kColSlots];
-        for (int s = 0; s < kRowSlots; ++s) {
-            double v = slotInit(rops[s]);
-            for (int r = 0; r < K; ++r) {
-                const double w = ldc(d.part + r * kPartStride + s);
-                v = rops[s] == OP_SUM ? v + w : (rops[s] == OP_MIN ? fmin(v, w) : fmax(v, w));
-            }
-            rows[s] = v;
-        }
-        for (int s = 0; s < kColSlots; ++s) {
-            double v = slotInit(cops[s]);
-            for (int r = 0; r < K; ++r) {
-                const double w = ldc(d.part + r * kPartStride + kRowSlots + s);
-                v = cops[s] == OP_SUM ? v + w : (cops[s] == OP_MIN ? fmin(v, w) : fmax(v, w));
-            }
-            cols[s] = v;
-        }
-        controlStep(sst, sdc, rows, cols);
-    }
-    __syncthreads();
-    if (sst.restart) {
-        for (int j = c0 + threadIdx.x; j < c1; j += kBlock) {
-            const T v = it.xh[j];
-            it.xi[j] = v;
-            it.xc[j] = static_cast<double>(v);
-        }
-        for (int i = r0 + threadIdx.x; i < r1; i += kBlock) {
-            const T v = it.yh[i];
-            it.yi[i] = v;
-            it.yc[i] = static_cast<double>(v);
-        }
-    }
-    if (sizeof(T) == 4 && sst.promote && sst.prec == 0 && !sst.done) {
-        for (int j = c0 + threadIdx.x; j < c1; j += kBlock) {
-            d.it64.xi[j] = d.it32.xi[j];
-            d.it64.xh[j] = d.it32.xh[j];
-        }
-        for (int i = r0 + threadIdx.x; i < r1; i += kBlock) {
-            d.it64.yi[i] = d.it32.yi[i];
-            d.it64.yh[i] = d.it32.yh[i];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            sst.prec = 1;
-            sst.switch_total = sst.total;
-        }
-    }
-    __syncthreads();
-    cl.sync();  // restart / hand-over writes visible before the next cycle's gathers
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) out[s] = combine(ops[s], out[s], __shfl_xor_sync(0xffffffffu, out[s], off));
 }
 
-// ---------------------------------------------------------------------------
-// Shared-memory-resident FP32 phase.  The CTA's slice of A (its rows) and A^T
-// (its columns) with FP32 values, its packed constants and its iterates live
-// in its shared memory for the whole FP32 phase; an entry of A / A^T stores its
-// column / row as (owner rank << 24 | index within the owner's slice), so the
-// gathers of x_refl and y_cur read the owner's shared memory directly through
-// distributed shared memory.  HBM is touched only by the FP64 check pass.
-// ---------------------------------------------------------------------------
-__device__ inline unsigned encodeOwner(int g, int per) {
-    const int o = g / per;
-    return (static_cast<unsigned>(o) << 24) | static_cast<unsigned>(g - o * per);
-}
-
-__device__ void smemLoad(const BatchLp& d, char* sm, const SLayout& L, int r0, int nr, int c0, int nc, int& a_off,
-                         int& at_off) {
-    const IterArgs<float>& it = d.it32;
-    a_off = nr > 0 ? __ldg(it.a_ptr + r0) : 0;
-    at_off = nc > 0 ? __ldg(it.at_ptr + c0) : 0;
-    const int a_len = nr > 0 ? __ldg(it.a_ptr + r0 + nr) - a_off : 0;
-    const int at_len = nc > 0 ? __ldg(it.at_ptr + c0 + nc) - at_off : 0;
-    int* aptr = reinterpret_cast<int*>(sm + L.o_aptr);
-    unsigned* aidx = reinterpret_cast<unsigned*>(sm + L.o_aidx);
-    float* aval = reinterpret_cast<float*>(sm + L.o_aval);
-    int* atptr = reinterpret_cast<int*>(sm + L.o_atptr);
-    unsigned* atidx = reinterpret_cast<unsigned*>(sm + L.o_atidx);
-    float* atval = reinterpret_cast<float*>(sm + L.o_atval);
-    for (int i = threadIdx.x; i <= nr; i += kBlock) aptr[i] = nr > 0 ? __ldg(it.a_ptr + r0 + i) - a_off : 0;
-    for (int j = threadIdx.x; j <= nc; j += kBlock) atptr[j] = nc > 0 ? __ldg(it.at_ptr + c0 + j) - at_off : 0;
-    for (int k = threadIdx.x; k < a_len; k += kBlock) {
-        aidx[k] = encodeOwner(__ldg(it.a_idx + a_off + k), d.pc);
-        aval[k] = __ldg(d.a_v32 + a_off + k);
-    }
-    for (int k = threadIdx.x; k < at_len; k += kBlock) {
-        atidx[k] = encodeOwner(__ldg(it.at_idx + at_off + k), d.pr);
-        atval[k] = __ldg(d.at_v32 + at_off + k);
-    }
-    float4* cp = reinterpret_cast<float4*>(sm + L.o_cp);
-    float4* rp = reinterpret_cast<float4*>(sm + L.o_rp);
-    double* xc = reinterpret_cast<double*>(sm + L.o_xc);
-    double* yc = reinterpret_cast<double*>(sm + L.o_yc);
-    float* xi = reinterpret_cast<float*>(sm + L.o_xi);
-    float* xh = reinterpret_cast<float*>(sm + L.o_xh);
-    float* yi = reinterpret_cast<float*>(sm + L.o_yi);
-    float* yh = reinterpret_cast<float*>(sm + L.o_yh);
-    const float4* gcp = reinterpret_cast<const float4*>(it.cp);
-    const float4* grp = reinterpret_cast<const float4*>(it.rp);
-    // Iterates through L2 only: this SM must not keep L1 copies of lines that
-    // other SMs write later in the solve.
-    for (int j = threadIdx.x; j < nc; j += kBlock) {
-        cp[j] = __ldg(gcp + c0 + j);
-        xc[j] = __ldcg(it.xc + c0 + j);
-        xi[j] = __ldcg(it.xi + c0 + j);
-        xh[j] = __ldcg(it.xh + c0 + j);
-    }
-    for (int i = threadIdx.x; i < nr; i += kBlock) {
-        rp[i] = __ldg(grp + r0 + i);
-        yc[i] = __ldcg(it.yc + r0 + i);
-        yi[i] = __ldcg(it.yi + r0 + i);
-        yh[i] = __ldcg(it.yh + r0 + i);
+// ---- PDHG step over one tile ------------------------------------------------
+template <int G, int R, int U>
+__global__ void __launch_bounds__(kBlock) packPrimal(PackArgs a, int tile0, int koff) {
+    const int4 t = a.ctiles[tile0 + blockIdx.x];
+    DevState* st = a.st + t.x;
+    if (st->done) return;
+    const int j0 = t.y + threadIdx.x / G;
+    if (st->prec == 0) {
+        IterArgs<float> p = a.it32;
+        p.st = st;
+        primalRows<G, R, U, float>(p, j0, t.z, koff);
+    } else {
+        IterArgs<double> p = a.it64;
+        p.st = st;
+        primalRows<G, R, U, double>(p, j0, t.z, koff);
     }
 }
 
-// Write the slice's iterates back to the global FP32 / FP64 arrays.
-__device__ void smemStore(const BatchLp& d, char* sm, const SLayout& L, int r0, int nr, int c0, int nc) {
-    const IterArgs<float>& it = d.it32;
-    const double* xc = reinterpret_cast<const double*>(sm + L.o_xc);
-    const double* yc = reinterpret_cast<const double*>(sm + L.o_yc);
-    const float* xi = reinterpret_cast<const float*>(sm + L.o_xi);
-    const float* xh = reinterpret_cast<const float*>(sm + L.o_xh);
-    const float* yi = reinterpret_cast<const float*>(sm + L.o_yi);
-    const float* yh = reinterpret_cast<const float*>(sm + L.o_yh);
-    for (int j = threadIdx.x; j < nc; j += kBlock) {
-        it.xc[c0 + j] = xc[j];
-        it.xi[c0 + j] = xi[j];
-        it.xh[c0 + j] = xh[j];
+template <int G, int R, int U>
+__global__ void __launch_bounds__(kBlock) packDual(PackArgs a, int tile0, int koff) {
+    const int4 t = a.rtiles[tile0 + blockIdx.x];
+    DevState* st = a.st + t.x;
+    if (st->done) return;
+    const int i0 = t.y + threadIdx.x / G;
+    if (st->prec == 0) {
+        IterArgs<float> p = a.it32;
+        p.st = st;
+        dualRows<G, R, U, float>(p, i0, t.z, koff);
+    } else {
+        IterArgs<double> p = a.it64;
+        p.st = st;
+        dualRows<G, R, U, double>(p, i0, t.z, koff);
     }
-    for (int i = threadIdx.x; i < nr; i += kBlock) {
-        it.yc[r0 + i] = yc[i];
-        it.yi[r0 + i] = yi[i];
-        it.yh[r0 + i] = yh[i];
-    }
+}
+
+// ---- FP64 check pass, one partial per tile -----------------------------------
+template <int G>
+__global__ void __launch_bounds__(kBlock) packCheckRows(PackArgs a, int tile0) {
+    const int tile = tile0 + blockIdx.x;
+    const int4 t = a.rtiles[tile];
+    const DevState* st = a.st + t.x;
+    if (st->done) return;
+    double* out = a.part_rows + static_cast<size_t>(tile) * kRowSlots;
+    constexpr int per = kBlock / G;
+    if (st->prec == 0)
+        checkRowsRange<G, float>(a.ck32, a.dc[t.x], t.y, t.z, per, out);
+    else
+        checkRowsRange<G, double>(a.ck64, a.dc[t.x], t.y, t.z, per, out);
 }
 
 template <int G>
-__device__ void smemPrimal(char* sm, const SLayout& L, cg::cluster_group& cl, int nc, double step, double pw,
-                           double lam, bool last) {
-    const int* ptr = reinterpret_cast<const int*>(sm + L.o_atptr);
-    const unsigned* idx = reinterpret_cast<const unsigned*>(sm + L.o_atidx);
-    const float* val = reinterpret_cast<const float*>(sm + L.o_atval);
-    const float4* cp = reinterpret_cast<const float4*>(sm + L.o_cp);
-    double* xc = reinterpret_cast<double*>(sm + L.o_xc);
-    const float* xi = reinterpret_cast<const float*>(sm + L.o_xi);
-    float* xh = reinterpret_cast<float*>(sm + L.o_xh);
-    float* xr = reinterpret_cast<float*>(sm + L.o_xr);
-    double* yc_local = reinterpret_cast<double*>(sm + L.o_yc);
-    const int lane = threadIdx.x % G;
+__global__ void __launch_bounds__(kBlock) packCheckCols(PackArgs a, int tile0) {
+    const int tile = tile0 + blockIdx.x;
+    const int4 t = a.ctiles[tile];
+    const DevState* st = a.st + t.x;
+    if (st->done) return;
+    double* out = a.part_cols + static_cast<size_t>(tile) * kColSlots;
     constexpr int per = kBlock / G;
-    for (int base = 0; base < nc; base += per) {
-        const int jl = base + threadIdx.x / G;
-        const bool valid = jl < nc;
-        double s0 = 0.0, s1 = 0.0;
-        if (valid) {
-            const int e = ptr[jl + 1];
-            int k = ptr[jl] + lane;
-            for (; k + G < e; k += 2 * G) {
-                const unsigned w0 = idx[k], w1 = idx[k + G];
-                const double v0 = cl.map_shared_rank(yc_local, w0 >> 24)[w0 & 0xFFFFFFu];
-                const double v1 = cl.map_shared_rank(yc_local, w1 >> 24)[w1 & 0xFFFFFFu];
-                s0 += static_cast<double>(val[k]) * v0;
-                s1 += static_cast<double>(val[k + G]) * v1;
-            }
-            if (k < e) {
-                const unsigned w = idx[k];
-                s0 += static_cast<double>(val[k]) * cl.map_shared_rank(yc_local, w >> 24)[w & 0xFFFFFFu];
-            }
-        }
-        double s = groupSum<G>(s0 + s1);
-        if (valid && lane == 0) {
-            const float4 q = cp[jl];  // c, lb, ub, tau_base
-            const double xcd = xc[jl], xid = xi[jl];
-            const double tau = step * static_cast<double>(q.w) / pw;
-            double xv = xcd - tau * (static_cast<double>(q.x) + s);
-            const double lb = q.y, ub = q.z;
-            if (xv < lb) xv = lb;
-            if (xv > ub) xv = ub;
-            const double xrv = 2.0 * xv - xcd;
-            xr[jl] = static_cast<float>(xrv);
-            xc[jl] = lam * xrv + (1.0 - lam) * xid;
-            if (last) xh[jl] = static_cast<float>(xv);
-        }
-    }
+    if (st->prec == 0)
+        checkColsRange<G, float>(a.ck32, a.dc[t.x], t.y, t.z, per, out);
+    else
+        checkColsRange<G, double>(a.ck64, a.dc[t.x], t.y, t.z, per, out);
 }
 
-template <int G>
-__device__ void smemDual(char* sm, const SLayout& L, cg::cluster_group& cl, int nr, double step, double pw,
-                         double lam, bool last) {
-    const int* ptr = reinterpret_cast<const int*>(sm + L.o_aptr);
-    const unsigned* idx = reinterpret_cast<const unsigned*>(sm + L.o_aidx);
-    const float* val = reinterpret_cast<const float*>(sm + L.o_aval);
-    const float4* rp = reinterpret_cast<const float4*>(sm + L.o_rp);
-    double* yc = reinterpret_cast<double*>(sm + L.o_yc);
-    const float* yi = reinterpret_cast<const float*>(sm + L.o_yi);
-    float* yh = reinterpret_cast<float*>(sm + L.o_yh);
-    float* xr_local = reinterpret_cast<float*>(sm + L.o_xr);
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = 0; base < nr; base += per) {
-        const int il = base + threadIdx.x / G;
-        const bool valid = il < nr;
-        double s0 = 0.0, s1 = 0.0;
-        if (valid) {
-            const int e = ptr[il + 1];
-            int k = ptr[il] + lane;
-            for (; k + G < e; k += 2 * G) {
-                const unsigned w0 = idx[k], w1 = idx[k + G];
-                const float v0 = cl.map_shared_rank(xr_local, w0 >> 24)[w0 & 0xFFFFFFu];
-                const float v1 = cl.map_shared_rank(xr_local, w1 >> 24)[w1 & 0xFFFFFFu];
-                s0 += static_cast<double>(val[k]) * static_cast<double>(v0);
-                s1 += static_cast<double>(val[k + G]) * static_cast<double>(v1);
-            }
-            if (k < e) {
-                const unsigned w = idx[k];
-                s0 += static_cast<double>(val[k]) *
-                      static_cast<double>(cl.map_shared_rank(xr_local, w >> 24)[w & 0xFFFFFFu]);
-            }
-        }
-        double s = groupSum<G>(s0 + s1);
-        if (valid && lane == 0) {
-            const float4 q = rp[il];  // sigma_base, rl, ru, type
-            const double ycd = yc[il], yid = yi[il];
-            const double sig = step * static_cast<double>(q.x) * pw;
-            const double v = ycd + sig * s;
-            const double rl = q.y, ru = q.z;
-            const int type = static_cast<int>(q.w);
-            double py;
-            if (type == 0) {
-                py = v - sig * rl;
-            } else if (type == 1) {
-                py = v - sig * ru;
-                if (py < 0.0) py = 0.0;
-            } else if (type == 2) {
-                py = v - sig * rl;
-                if (py > 0.0) py = 0.0;
-            } else {
-                if (v >= sig * ru)
-                    py = v - sig * ru;
-                else if (v <= sig * rl)
-                    py = v - sig * rl;
-                else
-                    py = 0.0;
-            }
-            const double yr = 2.0 * py - ycd;
-            yc[il] = lam * yr + (1.0 - lam) * yid;
-            if (last) yh[il] = static_cast<float>(py);
-        }
-    }
-}
-
-template <int G>
-__device__ void smemCheckRows(const BatchLp& d, char* sm, const SLayout& L, cg::cluster_group& cl, const DevConst& dc,
-                              int r0, int nr, int a_off, double (&acc)[kRowSlots]) {
-    const int* ptr = reinterpret_cast<const int*>(sm + L.o_aptr);
-    const unsigned* idx = reinterpret_cast<const unsigned*>(sm + L.o_aidx);
-    const float* xh_local = reinterpret_cast<const float*>(sm + L.o_xh);
-    const float* yh = reinterpret_cast<const float*>(sm + L.o_yh);
-    const float* yi = reinterpret_cast<const float*>(sm + L.o_yi);
-    const double* val64 = d.ck32.a_val + a_off;
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = 0; base < nr; base += per) {
-        const int il = base + threadIdx.x / G;
-        const bool valid = il < nr;
-        double ax = 0.0;
-        if (valid) {
-            for (int k = ptr[il] + lane; k < ptr[il + 1]; k += G) {
-                const unsigned w = idx[k];
-                ax += __ldg(val64 + k) * static_cast<double>(cl.map_shared_rank(xh_local, w >> 24)[w & 0xFFFFFFu]);
-            }
-        }
-        ax = groupSum<G>(ax);
-        if (valid && lane == 0) {
-            const int i = r0 + il;
-            accRowMetrics(acc, dc, ax, d.ck32.rl64[i], d.ck32.ru64[i], d.ck32.rs64[i], static_cast<double>(yh[il]),
-                          static_cast<double>(yi[il]));
-        }
-    }
-}
-
-template <int G>
-__device__ void smemCheckCols(const BatchLp& d, char* sm, const SLayout& L, cg::cluster_group& cl, const DevConst& dc,
-                              int c0, int nc, int at_off, double (&acc)[kColSlots]) {
-    const int* ptr = reinterpret_cast<const int*>(sm + L.o_atptr);
-    const unsigned* idx = reinterpret_cast<const unsigned*>(sm + L.o_atidx);
-    const float* yh_local = reinterpret_cast<const float*>(sm + L.o_yh);
-    const float* yi_local = reinterpret_cast<const float*>(sm + L.o_yi);
-    const float* xh = reinterpret_cast<const float*>(sm + L.o_xh);
-    const float* xi = reinterpret_cast<const float*>(sm + L.o_xi);
-    const double* val64 = d.ck32.at_val + at_off;
-    const int lane = threadIdx.x % G;
-    constexpr int per = kBlock / G;
-    for (int base = 0; base < nc; base += per) {
-        const int jl = base + threadIdx.x / G;
-        const bool valid = jl < nc;
-        double aty = 0.0, atdy = 0.0;
-        if (valid) {
-            for (int k = ptr[jl] + lane; k < ptr[jl + 1]; k += G) {
-                const unsigned w = idx[k];
-                const double v = __ldg(val64 + k);
-                const double yv = cl.map_shared_rank(yh_local, w >> 24)[w & 0xFFFFFFu];
-                const double y0 = cl.map_shared_rank(yi_local, w >> 24)[w & 0xFFFFFFu];
-                aty += v * yv;
-                atdy += v * (yv - y0);
-            }
-        }
-        aty = groupSum<G>(aty);
-        atdy = groupSum<G>(atdy);
-        if (valid && lane == 0) {
-            const int j = c0 + jl;
-            accColMetrics<float>(acc, dc, static_cast<double>(xh[jl]), static_cast<double>(xi[jl]), d.ck32.c64[j],
-                                 d.ck32.lb64[j], d.ck32.ub64[j], d.ck32.cs64[j], aty, atdy);
-        }
-    }
-}
-
-// Combine the K ranks' partials (fixed order) and run the controller; every
-// CTA does this on its own copy of the state and reaches the same result.
-__device__ void clusterControl(const BatchLp& d, int K, DevState& sst, const DevConst& sdc) {
-    if (threadIdx.x != 0) return;
-    double rows[kRowSlots], cols[kColSlots];
-    for (int s = 0; s < kRowSlots; ++s) {
-        const int op = rowSlotOp(s);
-        double v = slotInit(op);
-        for (int r = 0; r < K; ++r) {
-            const double w = ldc(d.part + r * kPartStride + s);
-            v = op == OP_SUM ? v + w : (op == OP_MIN ? fmin(v, w) : fmax(v, w));
-        }
-        rows[s] = v;
-    }
-    for (int s = 0; s < kColSlots; ++s) {
-        const int op = colSlotOp(s);
-        double v = slotInit(op);
-        for (int r = 0; r < K; ++r) {
-            const double w = ldc(d.part + r * kPartStride + kRowSlots + s);
-            v = op == OP_SUM ? v + w : (op == OP_MIN ? fmin(v, w) : fmax(v, w));
-        }
-        cols[s] = v;
-    }
-    controlStep(sst, sdc, rows, cols);
-}
-
-// FP32 phase of one LP from shared memory; returns when the LP is done or
-// handed over to the FP64 (global memory) path.
-__device__ void smemRun(const BatchLp& d, int rank, int K, cg::cluster_group& cl, DevState& sst, const DevConst& sdc,
-                        char* sm, int r0, int nr, int c0, int nc) {
-    const SLayout L = smemLayout(d.pr, d.pc, d.capA, d.capAT);
-    const int gA = batchGroup(d.gA), gAT = batchGroup(d.gAT);
-    int a_off = 0, at_off = 0;
-    smemLoad(d, sm, L, r0, nr, c0, nc, a_off, at_off);
-    __syncthreads();
-    cl.sync();  // every slice resident before the first remote gather
+// ---- per-LP controller: one warp per LP ---------------------------------------
+__global__ void __launch_bounds__(32 * kCtlWarps) packController(PackArgs a) {
+    const int l = blockIdx.x * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L) return;
+    DevState* st = a.st + l;
+    if (st->done) return;
+    const int4 t = a.lpt[l];
     int rops[kRowSlots], cops[kColSlots];
 #pragma unroll
     for (int s = 0; s < kRowSlots; ++s) rops[s] = rowSlotOp(s);
 #pragma unroll
     for (int s = 0; s < kColSlots; ++s) cops[s] = colSlotOp(s);
-    while (!sst.done && sst.prec == 0) {
-        const int cur = sst.phase == 0 ? sst.total : sst.polish_count;
-        const int lim = sst.phase == 0 ? sdc.max_iter : sdc.polish_max_iter;
-        const int batch = min(sdc.N, lim - cur);
-        const double step = sst.step, pw = sst.pw;
-        const int inner = sst.inner;
-        for (int k = 1; k <= batch; ++k) {
-            const double lam = static_cast<double>(inner + k) / static_cast<double>(inner + k + 1);
-            const bool last = k == batch;
-            PDLPX_BATCH_G(gAT, (smemPrimal<GG>(sm, L, cl, nc, step, pw, lam, last)));
-            cl.sync();
-            PDLPX_BATCH_G(gA, (smemDual<GG>(sm, L, cl, nr, step, pw, lam, last)));
-            cl.sync();
-        }
-        double racc[kRowSlots], cacc[kColSlots];
-#pragma unroll
-        for (int s = 0; s < kRowSlots; ++s) racc[s] = slotInit(rops[s]);
-#pragma unroll
-        for (int s = 0; s < kColSlots; ++s) cacc[s] = slotInit(cops[s]);
-        PDLPX_BATCH_G(gA, (smemCheckRows<GG>(d, sm, L, cl, sdc, r0, nr, a_off, racc)));
-        PDLPX_BATCH_G(gAT, (smemCheckCols<GG>(d, sm, L, cl, sdc, c0, nc, at_off, cacc)));
-        blockReduceSlots<kRowSlots>(racc, rops, d.part + rank * kPartStride);
-        blockReduceSlots<kColSlots>(cacc, cops, d.part + rank * kPartStride + kRowSlots);
-        cl.sync();
-        clusterControl(d, K, sst, sdc);
-        __syncthreads();
-        if (sst.restart) {
-            double* xc = reinterpret_cast<double*>(sm + L.o_xc);
-            double* yc = reinterpret_cast<double*>(sm + L.o_yc);
-            float* xi = reinterpret_cast<float*>(sm + L.o_xi);
-            const float* xh = reinterpret_cast<const float*>(sm + L.o_xh);
-            float* yi = reinterpret_cast<float*>(sm + L.o_yi);
-            const float* yh = reinterpret_cast<const float*>(sm + L.o_yh);
-            for (int j = threadIdx.x; j < nc; j += kBlock) {
-                xi[j] = xh[j];
-                xc[j] = static_cast<double>(xh[j]);
-            }
-            for (int i = threadIdx.x; i < nr; i += kBlock) {
-                yi[i] = yh[i];
-                yc[i] = static_cast<double>(yh[i]);
-            }
-        }
-        __syncthreads();
-        if (sst.promote && !sst.done) {
-            // hand-over: slice back to global memory, then FP32 -> FP64 copies
-            smemStore(d, sm, L, r0, nr, c0, nc);
-            __syncthreads();
-            for (int j = c0 + threadIdx.x; j < c0 + nc; j += kBlock) {
-                d.it64.xi[j] = d.it32.xi[j];
-                d.it64.xh[j] = d.it32.xh[j];
-            }
-            for (int i = r0 + threadIdx.x; i < r0 + nr; i += kBlock) {
-                d.it64.yi[i] = d.it32.yi[i];
-                d.it64.yh[i] = d.it32.yh[i];
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                sst.prec = 1;
-                sst.switch_total = sst.total;
-            }
-        }
-        __syncthreads();
-        cl.sync();
+    double rows[kRowSlots], cols[kColSlots];
+    warpTiles<kRowSlots>(a.part_rows, t.z, t.w, lane, rops, rows);
+    warpTiles<kColSlots>(a.part_cols, t.x, t.y, lane, cops, cols);
+    if (lane == 0) {
+        DevState s = *st;
+        controlStep(s, a.dc[l], rows, cols);
+        *st = s;
     }
-    if (sst.done) smemStore(d, sm, L, r0, nr, c0, nc);
-    __syncthreads();
-    cl.sync();  // global copies complete before any later global-path gather
 }
 
-__device__ void clusterSolve(const BatchLp& d, int rank, int K, cg::cluster_group& cl, DevState& sst,
-                             DevConst& sdc, double* sred, char* sm) {
-    if (threadIdx.x == 0) {
-        sst = *d.st;
-        sdc = *d.dc;
+// Restart copy (pdlp_kernels.cu:377-405) and FP32 -> FP64 hand-over per tile:
+// blocks [0, nct) take column tiles, the rest row tiles.
+__global__ void __launch_bounds__(kBlock) packRestart(PackArgs a, int nct) {
+    const bool col = static_cast<int>(blockIdx.x) < nct;
+    const int4 t = col ? a.ctiles[blockIdx.x] : a.rtiles[blockIdx.x - nct];
+    const DevState* st = a.st + t.x;
+    if (st->done) return;
+    const int prec = st->prec;
+    const bool restart = st->restart != 0;
+    const bool promote = prec == 0 && st->promote != 0;
+    if (!restart && !promote) return;
+    for (int k = t.y + threadIdx.x; k < t.z; k += kBlock) {
+        if (col) {
+            if (prec == 0) {
+                if (restart) {
+                    const float v = a.it32.xh[k];
+                    a.it32.xi[k] = v;
+                    a.it32.xc[k] = v;
+                }
+                if (promote) {
+                    a.it64.xi[k] = a.it32.xi[k];
+                    a.it64.xh[k] = a.it32.xh[k];
+                }
+            } else {
+                const double v = a.it64.xh[k];
+                a.it64.xi[k] = v;
+                a.it64.xc[k] = v;
+            }
+        } else {
+            if (prec == 0) {
+                if (restart) {
+                    const float v = a.it32.yh[k];
+                    a.it32.yi[k] = v;
+                    a.it32.yc[k] = v;
+                }
+                if (promote) {
+                    a.it64.yi[k] = a.it32.yi[k];
+                    a.it64.yh[k] = a.it32.yh[k];
+                }
+            } else {
+                const double v = a.it64.yh[k];
+                a.it64.yi[k] = v;
+                a.it64.yc[k] = v;
+            }
+        }
     }
-    __syncthreads();
-    const int r0 = min(d.m, rank * d.pr), r1 = min(d.m, (rank + 1) * d.pr);
-    const int c0 = min(d.n, rank * d.pc), c1 = min(d.n, (rank + 1) * d.pc);
-    double s2 = 1.0;
-    if (d.sv_max_iter > 0) {
-        if (d.mixed)
-            s2 = clusterPower<float>(d, d.it32.a_ptr, d.it32.a_idx, d.a_v32, d.it32.at_ptr, d.it32.at_idx, d.at_v32,
-                                     rank, K, cl, r0, r1, c0, c1, sred);
-        else
-            s2 = clusterPower<double>(d, d.it64.a_ptr, d.it64.a_idx, d.it64.a_val, d.it64.at_ptr, d.it64.at_idx,
-                                      d.it64.at_val, rank, K, cl, r0, r1, c0, c1, sred);
-    }
-    if (threadIdx.x == 0) {
-        sst.step = 0.998 / sqrt(fmax(s2, 1e-12));
-        sst.best_pw = sst.pw;
-    }
-    __syncthreads();
-    cl.sync();
-    if (d.smem && sst.prec == 0 && !sst.done) smemRun(d, rank, K, cl, sst, sdc, sm, r0, r1 - r0, c0, c1 - c0);
-    while (!sst.done) {
-        if (sst.prec == 0)
-            clusterCycle<float>(d, d.it32, d.ck32, rank, K, cl, sst, sdc, r0, r1, c0, c1);
-        else
-            clusterCycle<double>(d, d.it64, d.ck64, rank, K, cl, sst, sdc, r0, r1, c0, c1);
-    }
-    if (rank == 0 && threadIdx.x == 0) *d.st = sst;
 }
 
-__global__ void __launch_bounds__(kBlock) batchSolveKernel(const BatchLp* lps, const int* order, int count,
-                                                          int* queue) {
-    cg::cluster_group cl = cg::this_cluster();
-    const int K = static_cast<int>(cl.num_blocks());
-    const int rank = static_cast<int>(cl.block_rank());
-    extern __shared__ __align__(16) char s_dyn[];
-    __shared__ int s_next;
-    __shared__ DevState sst;
-    __shared__ DevConst sdc;
-    __shared__ double sred[4];
-    while (true) {
-        if (rank == 0 && threadIdx.x == 0) s_next = atomicAdd(queue, 1);
-        cl.sync();
-        const int q = *cl.map_shared_rank(&s_next, 0);
-        cl.sync();  // every CTA has read the index before rank 0 takes the next one
-        if (q >= count) break;
-        clusterSolve(lps[order[q]], rank, K, cl, sst, sdc, sred, s_dyn);
+// Hand-over bookkeeping and the per-LP flags the host reads after a cycle.
+__global__ void packFinish(PackArgs a) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= a.L) return;
+    DevState* st = a.st + l;
+    if (!st->done && st->prec == 0 && st->promote) {
+        st->prec = 1;
+        st->switch_total = st->total;
     }
+    a.flags[l] = (st->done ? 1 : 0) | (st->prec ? 2 : 0);
+}
+
+// ---- power iteration on A^T A per LP (pdlp.cpp:748-795, 1985-2041) ---------------
+template <int G>
+__global__ void __launch_bounds__(kBlock) packPowerA(PackArgs a, int tile0) {
+    const int4 t = a.rtiles[tile0 + blockIdx.x];
+    if (a.ps[t.x].done) return;
+    constexpr int per = kBlock / G;
+    const int lane = threadIdx.x % G;
+    for (int base = t.y; base < t.z; base += per) {
+        const int i = base + threadIdx.x / G;
+        const bool valid = i < t.z;
+        double s = 0.0;
+        if (valid) {
+            const int b = a.it64.a_ptr[i], e = a.it64.a_ptr[i + 1];
+            s = a.mixed ? rowDot<G, double>(b, e, lane, a.it32.a_idx, a.it32.a_val, a.pi_x)
+                        : rowDot<G, double>(b, e, lane, a.it64.a_idx, a.it64.a_val, a.pi_x);
+        }
+        s = groupSum<G>(s);
+        if (valid && lane == 0) a.pi_y[i] = s;
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) packPowerAt(PackArgs a, int tile0) {
+    const int tile = tile0 + blockIdx.x;
+    const int4 t = a.ctiles[tile];
+    if (a.ps[t.x].done) return;
+    constexpr int per = kBlock / G;
+    const int lane = threadIdx.x % G;
+    double acc[2] = {0.0, 0.0};
+    for (int base = t.y; base < t.z; base += per) {
+        const int j = base + threadIdx.x / G;
+        const bool valid = j < t.z;
+        double s = 0.0;
+        if (valid) {
+            const int b = a.it64.at_ptr[j], e = a.it64.at_ptr[j + 1];
+            s = a.mixed ? rowDot<G, double>(b, e, lane, a.it32.at_idx, a.it32.at_val, a.pi_y)
+                        : rowDot<G, double>(b, e, lane, a.it64.at_idx, a.it64.at_val, a.pi_y);
+        }
+        s = groupSum<G>(s);
+        if (valid && lane == 0) {
+            a.pi_xn[j] = s;
+            acc[0] += a.pi_x[j] * s;
+            acc[1] += s * s;
+        }
+    }
+    const int ops[2] = {OP_SUM, OP_SUM};
+    blockReduceSlots<2>(acc, ops, a.pi_part + static_cast<size_t>(tile) * 2);
+}
+
+__global__ void __launch_bounds__(32 * kCtlWarps) packPowerFinish1(PackArgs a) {
+    const int l = blockIdx.x * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L || a.ps[l].done) return;
+    const int4 t = a.lpt[l];
+    const int ops[2] = {OP_SUM, OP_SUM};
+    double out[2];
+    warpTiles<2>(a.pi_part, t.x, t.y, lane, ops, out);
+    if (lane == 0) {
+        a.ps[l].s2 = out[0];
+        a.ps[l].nrm = sqrt(out[1]);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) packPowerNormalize(PackArgs a) {
+    const int tile = blockIdx.x;
+    const int4 t = a.ctiles[tile];
+    const PowerState& ps = a.ps[t.x];
+    if (ps.done) return;
+    const double s2 = ps.s2, nrm = ps.nrm;
+    double acc[1] = {0.0};
+    for (int j = t.y + threadIdx.x; j < t.z; j += kBlock) {
+        const double xn = a.pi_xn[j];
+        const double d = xn - s2 * a.pi_x[j];
+        acc[0] += d * d;
+        if (nrm >= 1e-15) a.pi_x[j] = xn / nrm;
+    }
+    const int ops[1] = {OP_SUM};
+    blockReduceSlots<1>(acc, ops, a.pi_part + static_cast<size_t>(tile) * 2);
+}
+
+__global__ void __launch_bounds__(32 * kCtlWarps) packPowerFinish2(PackArgs a) {
+    const int l = blockIdx.x * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L || a.ps[l].done) return;
+    const int4 t = a.lpt[l];
+    double acc = 0.0;
+    for (int k = lane; k < t.y; k += 32) acc += a.pi_part[static_cast<size_t>(t.x + k) * 2];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) {
+        PowerState& p = a.ps[l];
+        p.resid = sqrt(acc);
+        p.iter += 1;
+        if (p.nrm < 1e-15 || p.resid < a.sv_tol * fabs(p.s2) || p.iter >= a.sv_max_iter) {
+            p.done = 1;
+            atomicAdd(a.counters, 1);
+        }
+    }
+}
+
+// Step size from the spectral-norm estimate (0.998 / ||A||_2, pdlp.cpp:796-800).
+__global__ void packInitStep(PackArgs a) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= a.L) return;
+    DevState& s = a.st[l];
+    const double step = 0.998 / sqrt(fmax(a.ps[l].s2, 1e-12));
+    s.step = step;
+    s.tau_fac = static_cast<float>(step / s.pw);
+    s.sig_fac = static_cast<float>(step * s.pw);
 }
 
 // ---------------------------------------------------------------------------
@@ -880,149 +352,393 @@ struct Item {
     HostLp lp;
     ScaledLp sc;
     bool trivial = false;
-    int gA = 1, gAT = 1;
-    int pr = 1, pc = 1, capA = 0, capAT = 0, smem = 0, sbytes = 0;
-    size_t off = 0, bytes = 0;
-    // offsets within the item's region
-    size_t o_aptr, o_aidx, o_atptr, o_atidx, o_av64, o_atv64, o_av32, o_atv32, o_cp32, o_rp32, o_cp64, o_rp64;
-    size_t o_c, o_lb, o_ub, o_cs, o_tau, o_rl, o_ru, o_rs, o_sig;
-    size_t o_x32[3], o_y32[2], o_x64[4], o_y64[3], o_pix, o_piy, o_pixn, o_part, o_st, o_dc;
+    int shapeP = 0, shapeD = 0;
+    int nct = 0, nrt = 0;  // tiles
+    size_t bytes = 0;      // share of a pack's device image
+    // position within its pack
+    int64_t r0 = 0, c0 = 0, z0 = 0;
+    int l = 0;
 };
 
 size_t al256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
 
-void layoutItem(Item& it, bool mixed) {
-    const size_t m = it.lp.m, n = it.lp.n, nnz = it.sc.a.nnz();
-    size_t o = 0;
-    auto take = [&](size_t b) {
-        const size_t at = o;
-        o += al256(b);
-        return at;
-    };
-    it.o_aptr = take(4 * (m + 1));
-    it.o_aidx = take(4 * nnz);
-    it.o_atptr = take(4 * (n + 1));
-    it.o_atidx = take(4 * nnz);
-    it.o_av64 = take(8 * nnz);
-    it.o_atv64 = take(8 * nnz);
-    it.o_av32 = mixed ? take(4 * nnz) : 0;
-    it.o_atv32 = mixed ? take(4 * nnz) : 0;
-    it.o_cp32 = mixed ? take(16 * n) : 0;
-    it.o_rp32 = mixed ? take(16 * m) : 0;
-    it.o_cp64 = take(32 * n);
-    it.o_rp64 = take(32 * m);
-    it.o_c = take(8 * n);
-    it.o_lb = take(8 * n);
-    it.o_ub = take(8 * n);
-    it.o_cs = take(8 * n);
-    it.o_tau = take(8 * n);
-    it.o_rl = take(8 * m);
-    it.o_ru = take(8 * m);
-    it.o_rs = take(8 * m);
-    it.o_sig = take(8 * m);
-    for (auto& v : it.o_x32) v = mixed ? take(4 * n) : 0;
-    for (auto& v : it.o_y32) v = mixed ? take(4 * m) : 0;
-    for (auto& v : it.o_x64) v = take(8 * n);
-    for (auto& v : it.o_y64) v = take(8 * m);
-    it.o_pix = take(8 * n);
-    it.o_piy = take(8 * m);
-    it.o_pixn = take(8 * n);
-    it.o_part = take(8 * kMaxCluster * kPartStride);
-    it.o_st = take(sizeof(DevState));
-    it.o_dc = take(sizeof(DevConst));
-    it.bytes = o;
+// Device bytes an LP adds to a pack (image + scratch), for the pack split.
+size_t itemBytes(const Item& it, bool mixed) {
+    const size_t m = it.lp.m, n = it.lp.n, z = it.sc.a.nnz();
+    size_t b = 4 * (m + n) + z * (8 + 16 + (mixed ? 8 : 0));           // pointers, indices, values
+    b += n * (32 + 40 + 8 + 24 + 24) + m * (32 + 32 + 8 + 16 + 8);     // packs, checks, FP64 iterates, power
+    if (mixed) b += n * (16 + 12) + m * (16 + 8);
+    b += static_cast<size_t>(it.nct) * (16 + 8 * kColSlots + 16) + static_cast<size_t>(it.nrt) * (16 + 8 * kRowSlots);
+    b += sizeof(DevState) + sizeof(DevConst) + sizeof(PowerState) + 32;
+    return b;
 }
 
-// Uniform slices of K ranks and whether the FP32 phase fits the cluster's
-// shared memory (largest rank's slice image within the per-CTA budget).
-void residency(Item& it, int K, bool mixed, bool allow) {
-    const int m = it.lp.m, n = it.lp.n;
-    it.pr = (m + K - 1) / K;
-    it.pc = (n + K - 1) / K;
-    const auto& ap = it.sc.a.ptr;
-    const auto& atp = it.sc.at.ptr;
-    it.capA = it.capAT = 0;
-    for (int r = 0; r < K; ++r) {
-        const int r0 = std::min(m, r * it.pr), r1 = std::min(m, (r + 1) * it.pr);
-        const int c0 = std::min(n, r * it.pc), c1 = std::min(n, (r + 1) * it.pc);
-        it.capA = std::max(it.capA, ap[r1] - ap[r0]);
-        it.capAT = std::max(it.capAT, atp[c1] - atp[c0]);
+template <class F>
+void parallelFor(int count, F&& f) {
+    const int hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const int nt = std::min(hw, std::max(1, count));
+    if (nt <= 1) {
+        for (int k = 0; k < count; ++k) f(k);
+        return;
     }
-    const SLayout L = smemLayout(it.pr, it.pc, it.capA, it.capAT);
-    it.sbytes = L.bytes;
-    it.smem = allow && mixed && L.bytes <= kSmemBudget && it.pr < (1 << 24) && it.pc < (1 << 24) ? 1 : 0;
+    std::vector<std::thread> ts;
+    std::atomic<int> next{0};
+    for (int t = 0; t < nt; ++t)
+        ts.emplace_back([&] {
+            for (int k = next++; k < count; k = next++) f(k);
+        });
+    for (auto& t : ts) t.join();
 }
 
-template <class T>
-void putv(char* base, size_t off, const std::vector<T>& v) {
-    if (!v.empty()) std::memcpy(base + off, v.data(), v.size() * sizeof(T));
-}
+#define PDLPX_BCK(call)                                                              \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);         \
+            return e_ == cudaErrorMemoryAllocation ? PDLPX_E_NOMEM : PDLPX_E_CUDA;   \
+        }                                                                            \
+    } while (0)
 
-// Fill an item's region of the host staging image (everything the kernel reads).
-void stageItem(const Item& it, const pdlpx_options& o, bool mixed, char* img) {
-    char* b = img + it.off;
+// One launch of a step/check kernel class: tiles [begin, begin + count) of one shape.
+struct Launch {
+    int shape, begin, count;
+};
+
+// Device image and graphs of one pack.
+struct Pack {
+    std::vector<Item*> items;
+    bool mixed = true;
+    int L = 0;
+    int64_t M = 0, Nc = 0, Z = 0;
+    int nct = 0, nrt = 0;  // all tiles
+    // arena layout
+    size_t o_aptr, o_aidx, o_atptr, o_atidx, o_av32, o_atv32, o_av64, o_atv64, o_cp32, o_rp32, o_cp64, o_rp64;
+    size_t o_c, o_lb, o_ub, o_cs, o_tau, o_rl, o_ru, o_rs, o_sig;
+    size_t o_st, o_dc, o_ps, o_ctiles, o_rtiles, o_lpt;
+    size_t image_end;  // [0, image_end) is uploaded from the host image
+    size_t o_xc, o_xi32, o_xr32, o_xh32, o_xi64, o_xr64, o_xh64, o_yc, o_yi32, o_yh32, o_yi64, o_yh64;
+    size_t iter_end;   // [image_end, iter_end): iterates (zero or warm start)
+    size_t o_pix, o_piy, o_pixn, o_pipart, o_pcols, o_prows, o_flags, o_counters;
+    size_t total;
+    char* d = nullptr;
+    cudaStream_t s = nullptr;
+    cudaGraphExec_t cycle = nullptr, power = nullptr;
+    int cycle_launches = 0, power_launches = 0;
+    int active_tiles = 0;  // tiles in the captured cycle graph
+    std::vector<Launch> lc, lr;  // launches of the current tile lists
+    int act_ct = 0, act_rt = 0;  // current (compacted) tile counts
+    PackArgs args{};
+
+    ~Pack() {
+        if (cycle) cudaGraphExecDestroy(cycle);
+        if (power) cudaGraphExecDestroy(power);
+        if (d) cudaFree(d);
+        if (s) cudaStreamDestroy(s);
+    }
+
+    void layout() {
+        size_t o = 0;
+        auto take = [&](size_t b) {
+            const size_t at = o;
+            o += al256(b);
+            return at;
+        };
+        const size_t m = M, n = Nc, z = Z;
+        o_aptr = take(4 * (m + 1));
+        o_aidx = take(4 * z);
+        o_atptr = take(4 * (n + 1));
+        o_atidx = take(4 * z);
+        o_av32 = mixed ? take(4 * z) : 0;
+        o_atv32 = mixed ? take(4 * z) : 0;
+        o_av64 = take(8 * z);
+        o_atv64 = take(8 * z);
+        o_cp32 = mixed ? take(16 * n) : 0;
+        o_rp32 = mixed ? take(16 * m) : 0;
+        o_cp64 = take(32 * n);
+        o_rp64 = take(32 * m);
+        o_c = take(8 * n);
+        o_lb = take(8 * n);
+        o_ub = take(8 * n);
+        o_cs = take(8 * n);
+        o_tau = take(8 * n);
+        o_rl = take(8 * m);
+        o_ru = take(8 * m);
+        o_rs = take(8 * m);
+        o_sig = take(8 * m);
+        o_st = take(sizeof(DevState) * L);
+        o_dc = take(sizeof(DevConst) * L);
+        o_ps = take(sizeof(PowerState) * L);
+        o_ctiles = take(sizeof(int4) * nct);
+        o_rtiles = take(sizeof(int4) * nrt);
+        o_lpt = take(sizeof(int4) * L);
+        o_pix = take(8 * n);
+        image_end = o;
+        o_xc = take(8 * n);
+        o_xi32 = mixed ? take(4 * n) : 0;
+        o_xr32 = mixed ? take(4 * n) : 0;
+        o_xh32 = mixed ? take(4 * n) : 0;
+        o_xi64 = take(8 * n);
+        o_xr64 = take(8 * n);
+        o_xh64 = take(8 * n);
+        o_yc = take(8 * m);
+        o_yi32 = mixed ? take(4 * m) : 0;
+        o_yh32 = mixed ? take(4 * m) : 0;
+        o_yi64 = take(8 * m);
+        o_yh64 = take(8 * m);
+        iter_end = o;
+        o_piy = take(8 * m);
+        o_pixn = take(8 * n);
+        o_pipart = take(16 * static_cast<size_t>(nct));
+        o_pcols = take(8 * kColSlots * static_cast<size_t>(nct));
+        o_prows = take(8 * kRowSlots * static_cast<size_t>(nrt));
+        o_flags = take(4 * static_cast<size_t>(L));
+        o_counters = take(64);
+        total = o;
+    }
+
+    template <class T>
+    T* P(size_t off) const {
+        return reinterpret_cast<T*>(d + off);
+    }
+
+    void makeArgs(const pdlpx_options& o) {
+        PackArgs& a = args;
+        auto fillIter = [&](auto& it, auto* av, auto* atv, auto* cp, auto* rp, auto* xi, auto* xr, auto* xh, auto* yi,
+                            auto* yh) {
+            it.at_ptr = P<int>(o_atptr);
+            it.at_idx = P<int>(o_atidx);
+            it.at_val = atv;
+            it.a_ptr = P<int>(o_aptr);
+            it.a_idx = P<int>(o_aidx);
+            it.a_val = av;
+            it.cp = cp;
+            it.rp = rp;
+            it.xc = P<double>(o_xc);
+            it.xi = xi;
+            it.xr = xr;
+            it.xh = xh;
+            it.yc = P<double>(o_yc);
+            it.yi = yi;
+            it.yh = yh;
+            it.st = nullptr;
+            it.m = static_cast<int>(M);
+            it.n = static_cast<int>(Nc);
+            it.max_iter = o.max_iter;
+            it.polish_max_iter = o.polish_max_iter;
+            it.N = o.termination_eval_frequency;
+        };
+        fillIter(a.it64, P<double>(o_av64), P<double>(o_atv64), P<ColPack<double>>(o_cp64), P<RowPack<double>>(o_rp64),
+                 P<double>(o_xi64), P<double>(o_xr64), P<double>(o_xh64), P<double>(o_yi64), P<double>(o_yh64));
+        if (mixed)
+            fillIter(a.it32, P<float>(o_av32), P<float>(o_atv32), P<ColPack<float>>(o_cp32), P<RowPack<float>>(o_rp32),
+                     P<float>(o_xi32), P<float>(o_xr32), P<float>(o_xh32), P<float>(o_yi32), P<float>(o_yh32));
+        auto fillCheck = [&](auto& c, const auto& it) {
+            c.a_ptr = P<int>(o_aptr);
+            c.a_idx = P<int>(o_aidx);
+            c.a_val = P<double>(o_av64);
+            c.at_ptr = P<int>(o_atptr);
+            c.at_idx = P<int>(o_atidx);
+            c.at_val = P<double>(o_atv64);
+            c.xh = it.xh;
+            c.xi = it.xi;
+            c.yh = it.yh;
+            c.yi = it.yi;
+            c.c64 = P<double>(o_c);
+            c.lb64 = P<double>(o_lb);
+            c.ub64 = P<double>(o_ub);
+            c.cs64 = P<double>(o_cs);
+            c.tau64 = P<double>(o_tau);
+            c.rl64 = P<double>(o_rl);
+            c.ru64 = P<double>(o_ru);
+            c.rs64 = P<double>(o_rs);
+            c.sig64 = P<double>(o_sig);
+            c.prev_ax = nullptr;
+            c.prev_xh = nullptr;
+            c.part_rows = P<double>(o_prows);
+            c.part_cols = P<double>(o_pcols);
+            c.dc = nullptr;
+            c.st = nullptr;
+            c.m = static_cast<int>(M);
+            c.n = static_cast<int>(Nc);
+        };
+        fillCheck(a.ck64, a.it64);
+        if (mixed) fillCheck(a.ck32, a.it32);
+        a.ctiles = P<int4>(o_ctiles);
+        a.rtiles = P<int4>(o_rtiles);
+        a.lpt = P<int4>(o_lpt);
+        a.st = P<DevState>(o_st);
+        a.dc = P<DevConst>(o_dc);
+        a.ps = P<PowerState>(o_ps);
+        a.flags = P<int>(o_flags);
+        a.counters = P<int>(o_counters);
+        a.part_cols = P<double>(o_pcols);
+        a.part_rows = P<double>(o_prows);
+        a.pi_x = P<double>(o_pix);
+        a.pi_y = P<double>(o_piy);
+        a.pi_xn = P<double>(o_pixn);
+        a.pi_part = P<double>(o_pipart);
+        a.L = L;
+        a.mixed = mixed ? 1 : 0;
+        a.sv_max_iter = o.sv_max_iter;
+        a.sv_tol = o.sv_tol;
+    }
+
+    // Tile lists of the LPs with keep[l] set, grouped by launch shape (LP order
+    // within a shape), and the per-LP tile ranges.
+    void tileLists(const std::vector<char>& keep, std::vector<int4>& ct, std::vector<int4>& rt,
+                   std::vector<int4>& lpt) {
+        ct.clear();
+        rt.clear();
+        lpt.assign(L, make_int4(0, 0, 0, 0));
+        lc.clear();
+        lr.clear();
+        for (int side = 0; side < 2; ++side) {
+            std::vector<int4>& out = side == 0 ? ct : rt;
+            std::vector<Launch>& ls = side == 0 ? lc : lr;
+            for (int shape = 0; shape < kNumShapes; ++shape) {
+                const int begin = static_cast<int>(out.size());
+                for (int l = 0; l < L; ++l) {
+                    const Item& it = *items[l];
+                    if (!keep[l] || (side == 0 ? it.shapeP : it.shapeD) != shape) continue;
+                    const int per = rowsPerBlock(shape);
+                    const int64_t lo = side == 0 ? it.c0 : it.r0;
+                    const int64_t cnt = side == 0 ? it.lp.n : it.lp.m;
+                    const int first = static_cast<int>(out.size());
+                    for (int64_t b = 0; b < cnt; b += per)
+                        out.push_back(make_int4(l, static_cast<int>(lo + b), static_cast<int>(lo + std::min(cnt, b + per)), 0));
+                    const int count = static_cast<int>(out.size()) - first;
+                    if (side == 0) {
+                        lpt[l].x = first;
+                        lpt[l].y = count;
+                    } else {
+                        lpt[l].z = first;
+                        lpt[l].w = count;
+                    }
+                }
+                const int count = static_cast<int>(out.size()) - begin;
+                if (count > 0) ls.push_back(Launch{shape, begin, count});
+            }
+        }
+        act_ct = static_cast<int>(ct.size());
+        act_rt = static_cast<int>(rt.size());
+    }
+
+    int launchCycle(int N) {
+        int n = 0;
+        const PackArgs& a = args;
+        for (int k = 1; k <= N; ++k) {
+            for (const Launch& c : lc) {
+                PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU><<<c.count, kBlock, 0, s>>>(a, c.begin, k)));
+                ++n;
+            }
+            for (const Launch& c : lr) {
+                PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU><<<c.count, kBlock, 0, s>>>(a, c.begin, k)));
+                ++n;
+            }
+        }
+        for (const Launch& c : lr) {
+            PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            ++n;
+        }
+        for (const Launch& c : lc) {
+            PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            ++n;
+        }
+        packController<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
+        if (act_ct + act_rt > 0) packRestart<<<act_ct + act_rt, kBlock, 0, s>>>(a, act_ct);
+        packFinish<<<(L + 127) / 128, 128, 0, s>>>(a);
+        return n + 3;
+    }
+
+    int launchPower(int chunk) {
+        int n = 0;
+        const PackArgs& a = args;
+        for (int it = 0; it < chunk; ++it) {
+            for (const Launch& c : lr) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerA<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+                ++n;
+            }
+            for (const Launch& c : lc) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerAt<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+                ++n;
+            }
+            packPowerFinish1<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
+            if (act_ct > 0) packPowerNormalize<<<act_ct, kBlock, 0, s>>>(a);
+            packPowerFinish2<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
+            n += 3;
+        }
+        return n;
+    }
+};
+
+// Host image of one LP's share of the pack.
+void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img, char* iters) {
     const ScaledLp& sc = it.sc;
-    const int32_t m = it.lp.m, n = it.lp.n;
-    putv(b, it.o_aptr, sc.a.ptr);
-    putv(b, it.o_aidx, sc.a.idx);
-    putv(b, it.o_atptr, sc.at.ptr);
-    putv(b, it.o_atidx, sc.at.idx);
-    putv(b, it.o_av64, sc.a.val);
-    putv(b, it.o_atv64, sc.at.val);
-    if (mixed) {
-        putv(b, it.o_av32, std::vector<float>(sc.a.val.begin(), sc.a.val.end()));
-        putv(b, it.o_atv32, std::vector<float>(sc.at.val.begin(), sc.at.val.end()));
-        auto* cp = reinterpret_cast<ColPack<float>*>(b + it.o_cp32);
+    const int32_t m = it.lp.m, n = it.lp.n, z = sc.a.nnz();
+    const int64_t r0 = it.r0, c0 = it.c0, z0 = it.z0;
+    auto I = [&](size_t off) { return reinterpret_cast<int32_t*>(img + off); };
+    auto F = [&](size_t off) { return reinterpret_cast<float*>(img + off); };
+    auto D = [&](size_t off) { return reinterpret_cast<double*>(img + off); };
+    int32_t* aptr = I(pk.o_aptr) + r0;
+    for (int32_t i = 0; i < m; ++i) aptr[i] = static_cast<int32_t>(z0 + sc.a.ptr[i]);
+    int32_t* atptr = I(pk.o_atptr) + c0;
+    for (int32_t j = 0; j < n; ++j) atptr[j] = static_cast<int32_t>(z0 + sc.at.ptr[j]);
+    int32_t* aidx = I(pk.o_aidx) + z0;
+    int32_t* atidx = I(pk.o_atidx) + z0;
+    for (int32_t k = 0; k < z; ++k) {
+        aidx[k] = static_cast<int32_t>(c0 + sc.a.idx[k]);
+        atidx[k] = static_cast<int32_t>(r0 + sc.at.idx[k]);
+    }
+    std::memcpy(D(pk.o_av64) + z0, sc.a.val.data(), 8 * static_cast<size_t>(z));
+    std::memcpy(D(pk.o_atv64) + z0, sc.at.val.data(), 8 * static_cast<size_t>(z));
+    if (pk.mixed) {
+        float* av = F(pk.o_av32) + z0;
+        float* atv = F(pk.o_atv32) + z0;
+        for (int32_t k = 0; k < z; ++k) {
+            av[k] = static_cast<float>(sc.a.val[k]);
+            atv[k] = static_cast<float>(sc.at.val[k]);
+        }
+        auto* cp = reinterpret_cast<ColPack<float>*>(img + pk.o_cp32) + c0;
         for (int32_t j = 0; j < n; ++j)
             cp[j] = ColPack<float>{static_cast<float>(sc.c[j]), static_cast<float>(sc.cl[j]),
                                    static_cast<float>(sc.cu[j]), static_cast<float>(sc.tau[j])};
-        auto* rp = reinterpret_cast<RowPack<float>*>(b + it.o_rp32);
+        auto* rp = reinterpret_cast<RowPack<float>*>(img + pk.o_rp32) + r0;
         for (int32_t i = 0; i < m; ++i)
             rp[i] = RowPack<float>{static_cast<float>(sc.sigma[i]), static_cast<float>(sc.rl[i]),
                                    static_cast<float>(sc.ru[i]), static_cast<float>(sc.row_type[i])};
     }
-    auto* cp64 = reinterpret_cast<ColPack<double>*>(b + it.o_cp64);
+    auto* cp64 = reinterpret_cast<ColPack<double>*>(img + pk.o_cp64) + c0;
     for (int32_t j = 0; j < n; ++j) cp64[j] = ColPack<double>{sc.c[j], sc.cl[j], sc.cu[j], sc.tau[j]};
-    auto* rp64 = reinterpret_cast<RowPack<double>*>(b + it.o_rp64);
+    auto* rp64 = reinterpret_cast<RowPack<double>*>(img + pk.o_rp64) + r0;
     for (int32_t i = 0; i < m; ++i)
         rp64[i] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
-    putv(b, it.o_c, sc.c);
-    putv(b, it.o_lb, sc.cl);
-    putv(b, it.o_ub, sc.cu);
-    putv(b, it.o_cs, sc.col_scale);
-    putv(b, it.o_tau, sc.tau);
-    putv(b, it.o_rl, sc.rl);
-    putv(b, it.o_ru, sc.ru);
-    putv(b, it.o_rs, sc.row_scale);
-    putv(b, it.o_sig, sc.sigma);
-    // initial iterates: zero or the warm start scaled like pdlp.cpp:915-930
-    std::vector<double> wx(n, 0.0), wy(m, 0.0);
-    if (it.in->warm_x != nullptr && it.in->warm_y != nullptr) {
-        for (int32_t j = 0; j < n; ++j) wx[j] = it.in->warm_x[j] / sc.col_scale[j] * sc.con_scale;
-        for (int32_t i = 0; i < m; ++i) wy[i] = it.in->warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+    auto put = [&](size_t off, int64_t at, const std::vector<double>& v) {
+        if (!v.empty()) std::memcpy(D(off) + at, v.data(), 8 * v.size());
+    };
+    put(pk.o_c, c0, sc.c);
+    put(pk.o_lb, c0, sc.cl);
+    put(pk.o_ub, c0, sc.cu);
+    put(pk.o_cs, c0, sc.col_scale);
+    put(pk.o_tau, c0, sc.tau);
+    put(pk.o_rl, r0, sc.rl);
+    put(pk.o_ru, r0, sc.ru);
+    put(pk.o_rs, r0, sc.row_scale);
+    put(pk.o_sig, r0, sc.sigma);
+    // power-iteration start vector: mt19937(42) normals, normalised (pdlp.cpp:1990-2001)
+    {
+        double* x0 = D(pk.o_pix) + c0;
+        std::mt19937 rng(42);
+        std::normal_distribution<double> dist(0.0, 1.0);
+        double xn = 0.0;
+        for (int32_t j = 0; j < n; ++j) {
+            x0[j] = dist(rng);
+            xn += x0[j] * x0[j];
+        }
+        xn = std::sqrt(xn);
+        if (xn < 1e-15) xn = 1.0;
+        for (int32_t j = 0; j < n; ++j) x0[j] /= xn;
     }
-    if (mixed) {
-        std::vector<float> fx(wx.begin(), wx.end()), fy(wy.begin(), wy.end());
-        for (int k = 0; k < 3; ++k) putv(b, it.o_x32[k], fx);
-        for (int k = 0; k < 2; ++k) putv(b, it.o_y32[k], fy);
-        putv(b, it.o_x64[0], std::vector<double>(fx.begin(), fx.end()));
-        putv(b, it.o_y64[0], std::vector<double>(fy.begin(), fy.end()));
-    } else {
-        for (int k = 0; k < 4; ++k) putv(b, it.o_x64[k], wx);
-        for (int k = 0; k < 3; ++k) putv(b, it.o_y64[k], wy);
-    }
-    // power-iteration start vector: mt19937(42) normals, normalised (pdlp.cpp:754-764)
-    std::mt19937 rng(42);
-    std::normal_distribution<double> dist(0.0, 1.0);
-    std::vector<double> x0(n);
-    for (auto& v : x0) v = dist(rng);
-    double xn = 0.0;
-    for (double v : x0) xn += v * v;
-    xn = std::sqrt(xn);
-    if (xn < 1e-15) xn = 1.0;
-    for (auto& v : x0) v /= xn;
-    putv(b, it.o_pix, x0);
-    // state and constants
+    // controller constants and initial state (as the single-LP solve)
     DevConst dc{};
     dc.m = m;
     dc.n = n;
@@ -1032,10 +748,12 @@ void stageItem(const Item& it, const pdlpx_options& o, bool mixed, char* img) {
     dc.linf = o.optimality_norm == PDLPX_NORM_LINF;
     dc.update_pw = o.update_primal_weight != 0;
     dc.enable_polish = o.enable_polishing != 0;
-    dc.mixed = mixed;
+    dc.mixed = pk.mixed;
     dc.fp64_switch = o.fp64_switch != 0;
     dc.adaptive = 0;
     dc.precond_refresh = o.preconditioner_refresh != 0;
+    dc.nb_rows = it.nrt;
+    dc.nb_cols = it.nct;
     dc.stall_limit = 10;
     dc.primal_tol = o.primal_tol;
     dc.dual_tol = o.dual_tol;
@@ -1056,10 +774,11 @@ void stageItem(const Item& it, const pdlpx_options& o, bool mixed, char* img) {
     dc.offset = it.lp.offset;
     dc.precond_ratio = o.preconditioner_refresh_ratio;
     dc.switch_score = 30.0;
-    std::memcpy(b + it.o_dc, &dc, sizeof(dc));
+    reinterpret_cast<DevConst*>(img + pk.o_dc)[it.l] = dc;
     DevState st{};
+    st.step = 1.0;
     st.pw = o.primal_weight;
-    st.prec = mixed ? 0 : 1;
+    st.prec = pk.mixed ? 0 : 1;
     st.fpe0 = -1.0;
     st.last_fpe = std::numeric_limits<double>::infinity();
     st.best_pw = st.pw;
@@ -1067,117 +786,263 @@ void stageItem(const Item& it, const pdlpx_options& o, bool mixed, char* img) {
     st.best_kkt = std::numeric_limits<double>::infinity();
     st.precond_pw = sc.precond_pw;
     st.switch_total = -1;
-    std::memcpy(b + it.o_st, &st, sizeof(st));
+    reinterpret_cast<DevState*>(img + pk.o_st)[it.l] = st;
+    reinterpret_cast<PowerState*>(img + pk.o_ps)[it.l] = PowerState{1.0, 0.0, 0.0, 0, o.sv_max_iter <= 0 ? 1 : 0};
+    // warm start, scaled like pdlp.cpp:1812-1827 (iters is null when no LP of the pack has one)
+    if (iters == nullptr) return;
+    // iterate arrays start at image_end in the arena and at 0 in `iters`
+    auto IF = [&](size_t off) { return reinterpret_cast<float*>(iters + (off - pk.image_end)); };
+    auto ID = [&](size_t off) { return reinterpret_cast<double*>(iters + (off - pk.image_end)); };
+    const bool warm = it.in->warm_x != nullptr && it.in->warm_y != nullptr;
+    std::vector<double> wx(n, 0.0), wy(m, 0.0);
+    if (warm) {
+        for (int32_t j = 0; j < n; ++j) wx[j] = it.in->warm_x[j] / sc.col_scale[j] * sc.con_scale;
+        for (int32_t i = 0; i < m; ++i) wy[i] = it.in->warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+    }
+    if (pk.mixed) {
+        for (int32_t j = 0; j < n; ++j) {
+            const float f = static_cast<float>(wx[j]);
+            IF(pk.o_xi32)[c0 + j] = f;
+            IF(pk.o_xr32)[c0 + j] = f;
+            IF(pk.o_xh32)[c0 + j] = f;
+            ID(pk.o_xc)[c0 + j] = f;
+        }
+        for (int32_t i = 0; i < m; ++i) {
+            const float f = static_cast<float>(wy[i]);
+            IF(pk.o_yi32)[r0 + i] = f;
+            IF(pk.o_yh32)[r0 + i] = f;
+            ID(pk.o_yc)[r0 + i] = f;
+        }
+    } else {
+        const size_t xs[4] = {pk.o_xc, pk.o_xi64, pk.o_xr64, pk.o_xh64};
+        const size_t ys[3] = {pk.o_yc, pk.o_yi64, pk.o_yh64};
+        for (size_t off : xs) std::memcpy(ID(off) + c0, wx.data(), 8 * static_cast<size_t>(n));
+        for (size_t off : ys) std::memcpy(ID(off) + r0, wy.data(), 8 * static_cast<size_t>(m));
+    }
 }
 
-BatchLp descriptor(const Item& it, char* dbase, const pdlpx_options& o, bool mixed) {
-    char* b = dbase + it.off;
-    auto I = [&](size_t off) { return reinterpret_cast<int*>(b + off); };
-    auto F = [&](size_t off) { return reinterpret_cast<float*>(b + off); };
-    auto D = [&](size_t off) { return reinterpret_cast<double*>(b + off); };
-    BatchLp d{};
-    d.m = it.lp.m;
-    d.n = it.lp.n;
-    d.gA = it.gA;
-    d.gAT = it.gAT;
-    d.mixed = mixed;
-    d.sv_max_iter = o.sv_max_iter;
-    d.sv_tol = o.sv_tol;
-    d.pr = it.pr;
-    d.pc = it.pc;
-    d.capA = it.capA;
-    d.capAT = it.capAT;
-    d.smem = it.smem;
-    DevState* st = reinterpret_cast<DevState*>(b + it.o_st);
-    auto fillIter = [&](auto& a, auto* av, auto* atv, auto* cp, auto* rp, auto* xi, auto* xr, auto* xh, auto* yi,
-                        auto* yh) {
-        a.at_ptr = I(it.o_atptr);
-        a.at_idx = I(it.o_atidx);
-        a.at_val = atv;
-        a.a_ptr = I(it.o_aptr);
-        a.a_idx = I(it.o_aidx);
-        a.a_val = av;
-        a.cp = cp;
-        a.rp = rp;
-        a.xc = D(it.o_x64[0]);
-        a.xi = xi;
-        a.xr = xr;
-        a.xh = xh;
-        a.yc = D(it.o_y64[0]);
-        a.yi = yi;
-        a.yh = yh;
-        a.st = st;
-        a.m = it.lp.m;
-        a.n = it.lp.n;
-        a.max_iter = o.max_iter;
-        a.polish_max_iter = o.polish_max_iter;
-        a.N = o.termination_eval_frequency;
+bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
+    if (lim < 0.0) return false;
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= lim;
+}
+
+// Build, run and read back one pack.
+int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::time_point t0, pdlpx_result* results,
+                  const std::vector<int>& index, double* const* x_out, double* const* y_out, std::string& err) {
+    const int L = pk.L;
+    // positions, tiles
+    for (int l = 0; l < L; ++l) {
+        Item& it = *pk.items[l];
+        it.l = l;
+        it.r0 = pk.M;
+        it.c0 = pk.Nc;
+        it.z0 = pk.Z;
+        pk.M += it.lp.m;
+        pk.Nc += it.lp.n;
+        pk.Z += it.sc.a.nnz();
+        pk.nct += it.nct;
+        pk.nrt += it.nrt;
+    }
+    pk.layout();
+    std::vector<char> keep(L, 1);
+    std::vector<int4> ct, rt, lpt;
+    pk.tileLists(keep, ct, rt, lpt);
+    bool any_warm = false;
+    for (const Item* it : pk.items) any_warm |= it->in->warm_x != nullptr && it->in->warm_y != nullptr;
+
+    // host image: everything the kernels read, filled per LP in parallel
+    std::unique_ptr<char[]> img(new char[pk.image_end]);
+    std::unique_ptr<char[]> iters(any_warm ? new char[pk.iter_end - pk.image_end] : nullptr);
+    if (any_warm) std::memset(iters.get(), 0, pk.iter_end - pk.image_end);
+    reinterpret_cast<int32_t*>(img.get() + pk.o_aptr)[pk.M] = static_cast<int32_t>(pk.Z);
+    reinterpret_cast<int32_t*>(img.get() + pk.o_atptr)[pk.Nc] = static_cast<int32_t>(pk.Z);
+    std::memcpy(img.get() + pk.o_ctiles, ct.data(), sizeof(int4) * ct.size());
+    std::memcpy(img.get() + pk.o_rtiles, rt.data(), sizeof(int4) * rt.size());
+    std::memcpy(img.get() + pk.o_lpt, lpt.data(), sizeof(int4) * lpt.size());
+    parallelFor(L, [&](int l) { stageItem(pk, *pk.items[l], o, img.get(), iters.get()); });
+
+    PDLPX_BCK(cudaStreamCreateWithFlags(&pk.s, cudaStreamNonBlocking));
+    PDLPX_BCK(cudaMalloc(reinterpret_cast<void**>(&pk.d), pk.total));
+    cudaStream_t s = pk.s;
+    PDLPX_BCK(cudaMemcpyAsync(pk.d, img.get(), pk.image_end, cudaMemcpyHostToDevice, s));
+    if (any_warm)
+        PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.image_end, iters.get(), pk.iter_end - pk.image_end, cudaMemcpyHostToDevice, s));
+    else
+        PDLPX_BCK(cudaMemsetAsync(pk.d + pk.image_end, 0, pk.iter_end - pk.image_end, s));
+    PDLPX_BCK(cudaMemsetAsync(pk.d + pk.iter_end, 0, pk.total - pk.iter_end, s));
+    pk.makeArgs(o);
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PDLPX_BCK(cudaEventCreate(&ev0));
+    PDLPX_BCK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev_guard{ev0, ev1};
+    PDLPX_BCK(cudaEventRecord(ev0, s));
+    int launches = 0;
+
+    int* h_small = nullptr;  // pinned: counters[0] / per-LP flags
+    PDLPX_BCK(cudaMallocHost(reinterpret_cast<void**>(&h_small), 4 * static_cast<size_t>(std::max(L, 16))));
+    struct HFree {
+        void* p;
+        ~HFree() { cudaFreeHost(p); }
+    } h_guard{h_small};
+
+    auto capture = [&](cudaGraphExec_t& g, int& count, bool power) -> int32_t {
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        PDLPX_BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        count = power ? pk.launchPower(8) : pk.launchCycle(o.termination_eval_frequency);
+        PDLPX_BCK(cudaStreamEndCapture(s, &graph));
+        const cudaError_t ie = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        PDLPX_BCK(ie);
+        return PDLPX_OK;
     };
-    fillIter(d.it64, D(it.o_av64), D(it.o_atv64), reinterpret_cast<ColPack<double>*>(b + it.o_cp64),
-             reinterpret_cast<RowPack<double>*>(b + it.o_rp64), D(it.o_x64[1]), D(it.o_x64[2]), D(it.o_x64[3]),
-             D(it.o_y64[1]), D(it.o_y64[2]));
-    if (mixed)
-        fillIter(d.it32, F(it.o_av32), F(it.o_atv32), reinterpret_cast<ColPack<float>*>(b + it.o_cp32),
-                 reinterpret_cast<RowPack<float>*>(b + it.o_rp32), F(it.o_x32[0]), F(it.o_x32[1]), F(it.o_x32[2]),
-                 F(it.o_y32[0]), F(it.o_y32[1]));
-    auto fillCheck = [&](auto& c, const auto& itr) {
-        c.a_ptr = I(it.o_aptr);
-        c.a_idx = I(it.o_aidx);
-        c.a_val = D(it.o_av64);
-        c.at_ptr = I(it.o_atptr);
-        c.at_idx = I(it.o_atidx);
-        c.at_val = D(it.o_atv64);
-        c.xh = itr.xh;
-        c.xi = itr.xi;
-        c.yh = itr.yh;
-        c.yi = itr.yi;
-        c.c64 = D(it.o_c);
-        c.lb64 = D(it.o_lb);
-        c.ub64 = D(it.o_ub);
-        c.cs64 = D(it.o_cs);
-        c.tau64 = D(it.o_tau);
-        c.rl64 = D(it.o_rl);
-        c.ru64 = D(it.o_ru);
-        c.rs64 = D(it.o_rs);
-        c.sig64 = D(it.o_sig);
-        c.m = it.lp.m;
-        c.n = it.lp.n;
-        c.st = st;
-    };
-    fillCheck(d.ck64, d.it64);
-    if (mixed) fillCheck(d.ck32, d.it32);
-    d.a_v32 = mixed ? F(it.o_av32) : nullptr;
-    d.at_v32 = mixed ? F(it.o_atv32) : nullptr;
-    d.pi_x = D(it.o_pix);
-    d.pi_y = D(it.o_piy);
-    d.pi_xn = D(it.o_pixn);
-    d.part = D(it.o_part);
-    d.st = st;
-    d.dc = reinterpret_cast<DevConst*>(b + it.o_dc);
-    return d;
-}
 
-template <class F>
-void parallelFor(int count, F&& f) {
-    const int hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const int nt = std::min(hw, std::max(1, count));
-    std::vector<std::thread> ts;
-    std::atomic<int> next{0};
-    for (int t = 0; t < nt; ++t)
-        ts.emplace_back([&] {
-            for (int k = next++; k < count; k = next++) f(k);
-        });
-    for (auto& t : ts) t.join();
-}
+    // ---- power iteration of every LP
+    if (o.sv_max_iter > 0) {
+        int32_t rc = capture(pk.power, pk.power_launches, true);
+        if (rc != PDLPX_OK) return rc;
+        for (int guard = 0; guard < 2 + o.sv_max_iter / 8; ++guard) {
+            PDLPX_BCK(cudaGraphLaunch(pk.power, s));
+            launches += pk.power_launches;
+            PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.counters, 4, cudaMemcpyDeviceToHost, s));
+            PDLPX_BCK(cudaStreamSynchronize(s));
+            if (h_small[0] >= L) break;
+        }
+    }
+    packInitStep<<<(L + 127) / 128, 128, 0, s>>>(pk.args);
+    ++launches;
+    PDLPX_BCK(cudaGetLastError());
 
-#define PDLPX_BCK(call)                                                              \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);         \
-            return e_ == cudaErrorMemoryAllocation ? PDLPX_E_NOMEM : PDLPX_E_CUDA;   \
-        }                                                                            \
-    } while (0)
+    // ---- restart cycles
+    {
+        int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
+        if (rc != PDLPX_OK) return rc;
+    }
+    pk.active_tiles = pk.act_ct + pk.act_rt;
+    int cycles = 0;
+    while (true) {
+        if (timeUp(t0, o.max_solve_seconds)) break;
+        PDLPX_BCK(cudaGraphLaunch(pk.cycle, s));
+        launches += pk.cycle_launches;
+        ++cycles;
+        PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        int done = 0, fp64 = 0, live_tiles = 0;
+        for (int l = 0; l < L; ++l) {
+            done += h_small[l] & 1;
+            fp64 += (h_small[l] >> 1) & 1;
+            if (!(h_small[l] & 1)) live_tiles += pk.items[l]->nct + pk.items[l]->nrt;
+        }
+        if (o.verbose && cycles % 10 == 0) {
+            std::printf("PDLP batch  %7d iterations per LP  %d/%d LPs done  %d on FP64 iterates  [B200]\n",
+                        cycles * o.termination_eval_frequency, done, L, fp64);
+            std::fflush(stdout);
+        }
+        if (done >= L) break;
+        if (o.batch_compact && live_tiles < (pk.active_tiles * 3) / 5) {
+            for (int l = 0; l < L; ++l) keep[l] = !(h_small[l] & 1);
+            pk.tileLists(keep, ct, rt, lpt);
+            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, s));
+            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_rtiles, rt.data(), sizeof(int4) * rt.size(), cudaMemcpyHostToDevice, s));
+            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_lpt, lpt.data(), sizeof(int4) * lpt.size(), cudaMemcpyHostToDevice, s));
+            int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
+            if (rc != PDLPX_OK) return rc;
+            pk.active_tiles = pk.act_ct + pk.act_rt;
+        }
+    }
+    PDLPX_BCK(cudaEventRecord(ev1, s));
+    PDLPX_BCK(cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+
+    // ---- results
+    std::vector<DevState> fin(L);
+    PDLPX_BCK(cudaMemcpyAsync(fin.data(), pk.args.st, sizeof(DevState) * L, cudaMemcpyDeviceToHost, s));
+    std::vector<float> fx, fy;
+    std::vector<double> dx(pk.Nc), dy(pk.M);
+    if (pk.mixed) {
+        fx.resize(pk.Nc);
+        fy.resize(pk.M);
+        PDLPX_BCK(cudaMemcpyAsync(fx.data(), pk.args.it32.xh, 4 * static_cast<size_t>(pk.Nc), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(fy.data(), pk.args.it32.yh, 4 * static_cast<size_t>(pk.M), cudaMemcpyDeviceToHost, s));
+    }
+    PDLPX_BCK(cudaMemcpyAsync(dx.data(), pk.args.it64.xh, 8 * static_cast<size_t>(pk.Nc), cudaMemcpyDeviceToHost, s));
+    PDLPX_BCK(cudaMemcpyAsync(dy.data(), pk.args.it64.yh, 8 * static_cast<size_t>(pk.M), cudaMemcpyDeviceToHost, s));
+    PDLPX_BCK(cudaStreamSynchronize(s));
+    const bool out_of_time = timeUp(t0, o.max_solve_seconds);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    parallelFor(L, [&](int l) {
+        const Item& it = *pk.items[l];
+        const DevState& f = fin[l];
+        const int32_t m = it.lp.m, n = it.lp.n;
+        std::vector<double> xs(n), ys(m);
+        for (int32_t j = 0; j < n; ++j) xs[j] = f.prec == 0 ? static_cast<double>(fx[it.c0 + j]) : dx[it.c0 + j];
+        for (int32_t i = 0; i < m; ++i) ys[i] = f.prec == 0 ? static_cast<double>(fy[it.r0 + i]) : dy[it.r0 + i];
+        int32_t status;
+        if (f.done) {
+            status = f.status;
+            if (status == PDLPX_STATUS_ITER_LIMIT && out_of_time) status = PDLPX_STATUS_TIME_LIMIT;
+        } else {
+            status = f.converged ? PDLPX_STATUS_OPTIMAL : PDLPX_STATUS_TIME_LIMIT;
+        }
+        const ScaledLp& sc = it.sc;
+        std::vector<double> xo(n, 0.0), yo(m, 0.0);
+        double obj = 0.0;
+        if (status == PDLPX_STATUS_OPTIMAL) {
+            const double ic = 1.0 / sc.con_scale, io = 1.0 / sc.obj_scale;
+            double ov = it.lp.offset;
+            for (int32_t j = 0; j < n; ++j) {
+                double xj = xs[j] * sc.col_scale[j] * ic;
+                if (std::isfinite(it.lp.cl[j])) xj = std::max(xj, it.lp.cl[j]);
+                if (std::isfinite(it.lp.cu[j])) xj = std::min(xj, it.lp.cu[j]);
+                xo[j] = xj;
+                ov += it.lp.obj[j] * xj;
+            }
+            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
+            obj = ov;
+        } else if (status == PDLPX_STATUS_INFEASIBLE) {
+            const double io = 1.0 / sc.obj_scale;
+            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
+        } else if (status == PDLPX_STATUS_UNBOUNDED) {
+            const double ic = 1.0 / sc.con_scale;
+            for (int32_t j = 0; j < n; ++j) xo[j] = xs[j] * sc.col_scale[j] * ic;
+        }
+        const int k = index[l];
+        pdlpx_result& r = results[k];
+        std::memset(&r, 0, sizeof(r));
+        r.status = status;
+        r.objective = obj;
+        r.iterations = f.total;
+        r.work_units = static_cast<double>(f.total) *
+                       (4.0 * static_cast<double>(sc.a.nnz()) + 2.0 * static_cast<double>(m + n));
+        r.rel_primal_resid = f.pterm;
+        r.rel_dual_resid = f.dterm;
+        r.rel_gap = f.gap;
+        r.primal_objective = f.pobj;
+        r.dual_objective = f.dobj;
+        r.fp64_iterations = pk.mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
+        r.restarts = f.restarts;
+        r.step_size = f.step;
+        r.primal_weight = f.pw;
+        r.solve_seconds = secs;
+        r.device_seconds = ms * 1e-3;
+        r.used_gpu = 1;
+        r.kernel_launches = launches;
+        if (x_out && x_out[k]) std::memcpy(x_out[k], xo.data(), 8 * static_cast<size_t>(n));
+        if (y_out && y_out[k]) std::memcpy(y_out[k], yo.data(), 8 * static_cast<size_t>(m));
+    });
+    return PDLPX_OK;
+}
 
 }  // namespace
 
@@ -1197,8 +1062,6 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         return PDLPX_E_INVALID;
     }
     const bool mixed = o.precision != PDLPX_PREC_FP64;
-    int K = o.batch_cluster > 0 ? o.batch_cluster : 4;
-    K = std::max(1, std::min(K, kMaxCluster));
     std::vector<Item> items(count);
     std::vector<int32_t> codes(count, PDLPX_OK);
     parallelFor(count, [&](int k) {
@@ -1221,14 +1084,15 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         lp.rl.assign(in.row_lb, in.row_lb + in.m);
         lp.ru.assign(in.row_ub, in.row_ub + in.m);
         lp.offset = in.obj_offset;
-        buildScaled(lp, o, it.sc);
         it.trivial = lp.m == 0 || lp.n == 0;
-        it.gA = std::min(32, pickGroup(it.sc.a.nnz(), lp.m));
-        it.gAT = std::min(32, pickGroup(it.sc.a.nnz(), lp.n));
-        if (!it.trivial) {
-            layoutItem(it, mixed);
-            residency(it, K, mixed, o.batch_resident != 0);
-        }
+        if (it.trivial) return;
+        buildScaled(lp, o, it.sc);
+        const int64_t z = it.sc.a.nnz();
+        it.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, z, lp.n);
+        it.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, z, lp.m);
+        it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + rowsPerBlock(it.shapeP) - 1) / rowsPerBlock(it.shapeP));
+        it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + rowsPerBlock(it.shapeD) - 1) / rowsPerBlock(it.shapeD));
+        it.bytes = itemBytes(it, mixed);
     });
     for (int k = 0; k < count; ++k)
         if (codes[k] != PDLPX_OK) {
@@ -1237,15 +1101,11 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         }
     // Trivial LPs (no rows or no columns) are closed form, like pdlp.cpp:812-860, via the engine.
     std::vector<int> dev_items;
-    size_t total = 0;
     for (int k = 0; k < count; ++k) {
-        if (items[k].trivial) continue;
-        items[k].off = total;
-        total += items[k].bytes;
-        dev_items.push_back(k);
-    }
-    for (int k = 0; k < count; ++k) {
-        if (!items[k].trivial) continue;
+        if (!items[k].trivial) {
+            dev_items.push_back(k);
+            continue;
+        }
         Engine e;
         e.setOptions(o);
         const pdlpx_lp& in = lps[k];
@@ -1259,8 +1119,7 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         if (x_out && x_out[k] && !e.primal().empty()) std::memcpy(x_out[k], e.primal().data(), 8 * e.primal().size());
         if (y_out && y_out[k] && !e.dual().empty()) std::memcpy(y_out[k], e.dual().data(), 8 * e.dual().size());
     }
-    const int nd = static_cast<int>(dev_items.size());
-    if (nd == 0) return PDLPX_OK;
+    if (dev_items.empty()) return PDLPX_OK;
 
     int devcount = 0;
     if (cudaGetDeviceCount(&devcount) != cudaSuccess || devcount <= 0) {
@@ -1268,165 +1127,37 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         return PDLPX_E_NO_DEVICE;
     }
     PDLPX_BCK(cudaSetDevice((o.device >= 0 && o.device < devcount) ? o.device : 0));
-    // Host image of the whole arena, filled in parallel, uploaded in one copy.
-    std::vector<char> img(total);
-    parallelFor(nd, [&](int q) { stageItem(items[dev_items[q]], o, mixed, img.data()); });
-    char* dbase = nullptr;
-    PDLPX_BCK(cudaMalloc(reinterpret_cast<void**>(&dbase), total));
-    struct Free {
-        void* p;
-        ~Free() { cudaFree(p); }
-    } guard_arena{dbase};
-    cudaStream_t s = nullptr;
-    PDLPX_BCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    struct SFree {
-        cudaStream_t s;
-        ~SFree() { cudaStreamDestroy(s); }
-    } guard_stream{s};
-    PDLPX_BCK(cudaMemcpyAsync(dbase, img.data(), total, cudaMemcpyHostToDevice, s));
-    // Descriptors, order (largest first), queue.
-    std::vector<BatchLp> desc(nd);
-    for (int q = 0; q < nd; ++q) desc[q] = descriptor(items[dev_items[q]], dbase, o, mixed);
-    std::vector<int> order(nd);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return items[dev_items[a]].sc.a.nnz() > items[dev_items[b]].sc.a.nnz();
-    });
-    const size_t meta = al256(sizeof(BatchLp) * nd) + al256(sizeof(int) * nd) + 256;
-    char* dmeta = nullptr;
-    PDLPX_BCK(cudaMalloc(reinterpret_cast<void**>(&dmeta), meta));
-    struct Free guard_meta {
-        dmeta
-    };
-    BatchLp* d_desc = reinterpret_cast<BatchLp*>(dmeta);
-    int* d_order = reinterpret_cast<int*>(dmeta + al256(sizeof(BatchLp) * nd));
-    int* d_queue = reinterpret_cast<int*>(dmeta + al256(sizeof(BatchLp) * nd) + al256(sizeof(int) * nd));
-    PDLPX_BCK(cudaMemcpyAsync(d_desc, desc.data(), sizeof(BatchLp) * nd, cudaMemcpyHostToDevice, s));
-    PDLPX_BCK(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * nd, cudaMemcpyHostToDevice, s));
-    PDLPX_BCK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
-
-    // Launch: clusters of K CTAs, as many clusters as can be co-resident; the
-    // dynamic shared memory is the largest resident slice image of the batch.
-    int dyn = 0;
-    for (int q = 0; q < nd; ++q) dyn = std::max(dyn, items[dev_items[q]].smem ? items[dev_items[q]].sbytes : 0);
-    if (dyn > 0) PDLPX_BCK(cudaFuncSetAttribute(batchSolveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
-    cudaLaunchConfig_t cfg{};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = K;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kBlock, 1, 1);
-    cfg.dynamicSmemBytes = static_cast<size_t>(dyn);
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cfg.gridDim = dim3(K, 1, 1);
-    int max_clusters = 0;
-    PDLPX_BCK(cudaOccupancyMaxActiveClusters(&max_clusters, batchSolveKernel, &cfg));
-    const int nclusters = std::max(1, std::min(max_clusters, nd));
-    cfg.gridDim = dim3(K * nclusters, 1, 1);
-    cudaEvent_t e0, e1;
-    PDLPX_BCK(cudaEventCreate(&e0));
-    PDLPX_BCK(cudaEventCreate(&e1));
-    PDLPX_BCK(cudaEventRecord(e0, s));
-    PDLPX_BCK(cudaLaunchKernelEx(&cfg, batchSolveKernel, static_cast<const BatchLp*>(d_desc),
-                                 static_cast<const int*>(d_order), nd, d_queue));
-    PDLPX_BCK(cudaEventRecord(e1, s));
-    PDLPX_BCK(cudaEventSynchronize(e1));
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    PDLPX_BCK(cudaGetLastError());
-
-    // Results.
-    std::vector<DevState> fin(nd);
-    std::vector<std::vector<double>> xs(nd), ys(nd);
-    for (int q = 0; q < nd; ++q) {
-        const Item& it = items[dev_items[q]];
-        char* b = dbase + it.off;
-        PDLPX_BCK(cudaMemcpyAsync(&fin[q], b + it.o_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    size_t free_b = 0, total_b = 0;
+    PDLPX_BCK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = o.batch_pack_mb > 0 ? static_cast<size_t>(o.batch_pack_mb) << 20
+                                              : static_cast<size_t>(0.85 * static_cast<double>(free_b));
+    // Packs in input order: a new pack starts when the budget or 32-bit numbering would overflow.
+    const int64_t lim32 = std::numeric_limits<int32_t>::max() - 1;
+    size_t pos = 0;
+    while (pos < dev_items.size()) {
+        Pack pk;
+        pk.mixed = mixed;
+        std::vector<int> index;
+        size_t bytes = 0;
+        int64_t m = 0, n = 0, z = 0, tiles = 0;
+        while (pos < dev_items.size()) {
+            Item& it = items[dev_items[pos]];
+            const bool fits = bytes + it.bytes <= budget && m + it.lp.m < lim32 && n + it.lp.n < lim32 &&
+                              z + it.sc.a.nnz() < lim32 && tiles + it.nct + it.nrt < lim32;
+            if (!fits && !pk.items.empty()) break;
+            bytes += it.bytes;
+            m += it.lp.m;
+            n += it.lp.n;
+            z += it.sc.a.nnz();
+            tiles += it.nct + it.nrt;
+            pk.items.push_back(&it);
+            index.push_back(dev_items[pos]);
+            ++pos;
+        }
+        pk.L = static_cast<int>(pk.items.size());
+        const int32_t rc = solvePack(pk, o, t0, results, index, x_out, y_out, err);
+        if (rc != PDLPX_OK) return rc;
     }
-    PDLPX_BCK(cudaStreamSynchronize(s));
-    std::vector<std::vector<float>> fx(nd), fy(nd);
-    for (int q = 0; q < nd; ++q) {
-        const Item& it = items[dev_items[q]];
-        char* b = dbase + it.off;
-        const int32_t m = it.lp.m, n = it.lp.n;
-        xs[q].resize(n);
-        ys[q].resize(m);
-        if (fin[q].prec == 0) {
-            fx[q].resize(n);
-            fy[q].resize(m);
-            PDLPX_BCK(cudaMemcpyAsync(fx[q].data(), b + it.o_x32[2], 4 * static_cast<size_t>(n),
-                                      cudaMemcpyDeviceToHost, s));
-            PDLPX_BCK(cudaMemcpyAsync(fy[q].data(), b + it.o_y32[1], 4 * static_cast<size_t>(m),
-                                      cudaMemcpyDeviceToHost, s));
-        } else {
-            PDLPX_BCK(cudaMemcpyAsync(xs[q].data(), b + it.o_x64[3], 8 * static_cast<size_t>(n),
-                                      cudaMemcpyDeviceToHost, s));
-            PDLPX_BCK(cudaMemcpyAsync(ys[q].data(), b + it.o_y64[2], 8 * static_cast<size_t>(m),
-                                      cudaMemcpyDeviceToHost, s));
-        }
-    }
-    PDLPX_BCK(cudaStreamSynchronize(s));
-    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    parallelFor(nd, [&](int q) {
-        const int k = dev_items[q];
-        const Item& it = items[k];
-        const DevState& f = fin[q];
-        const int32_t m = it.lp.m, n = it.lp.n;
-        if (f.prec == 0) {
-            for (int32_t j = 0; j < n; ++j) xs[q][j] = fx[q][j];
-            for (int32_t i = 0; i < m; ++i) ys[q][i] = fy[q][i];
-        }
-        const ScaledLp& sc = it.sc;
-        pdlpx_result& r = results[k];
-        std::memset(&r, 0, sizeof(r));
-        int32_t status = f.done ? f.status : (f.converged ? PDLPX_STATUS_OPTIMAL : PDLPX_STATUS_ITER_LIMIT);
-        std::vector<double> xo(n, 0.0), yo(m, 0.0);
-        double obj = 0.0;
-        if (status == PDLPX_STATUS_OPTIMAL) {
-            const double ic = 1.0 / sc.con_scale, io = 1.0 / sc.obj_scale;
-            double ov = it.lp.offset;
-            for (int32_t j = 0; j < n; ++j) {
-                double xj = xs[q][j] * sc.col_scale[j] * ic;
-                if (std::isfinite(it.lp.cl[j])) xj = std::max(xj, it.lp.cl[j]);
-                if (std::isfinite(it.lp.cu[j])) xj = std::min(xj, it.lp.cu[j]);
-                xo[j] = xj;
-                ov += it.lp.obj[j] * xj;
-            }
-            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[q][i] * sc.row_scale[i] * io;
-            obj = ov;
-        } else if (status == PDLPX_STATUS_INFEASIBLE) {
-            const double io = 1.0 / sc.obj_scale;
-            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[q][i] * sc.row_scale[i] * io;
-        } else if (status == PDLPX_STATUS_UNBOUNDED) {
-            const double ic = 1.0 / sc.con_scale;
-            for (int32_t j = 0; j < n; ++j) xo[j] = xs[q][j] * sc.col_scale[j] * ic;
-        }
-        r.status = status;
-        r.objective = obj;
-        r.iterations = f.total;
-        r.work_units = static_cast<double>(f.total) *
-                       (4.0 * static_cast<double>(sc.a.nnz()) + 2.0 * static_cast<double>(m + n));
-        r.rel_primal_resid = f.pterm;
-        r.rel_dual_resid = f.dterm;
-        r.rel_gap = f.gap;
-        r.primal_objective = f.pobj;
-        r.dual_objective = f.dobj;
-        r.fp64_iterations = mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
-        r.restarts = f.restarts;
-        r.step_size = f.step;
-        r.primal_weight = f.pw;
-        r.solve_seconds = secs;
-        r.device_seconds = ms * 1e-3;
-        r.used_gpu = 1;
-        r.kernel_launches = 1;
-        if (x_out && x_out[k]) std::memcpy(x_out[k], xo.data(), 8 * static_cast<size_t>(n));
-        if (y_out && y_out[k]) std::memcpy(y_out[k], yo.data(), 8 * static_cast<size_t>(m));
-    });
     return PDLPX_OK;
 }
 

@@ -98,8 +98,8 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->autotune = 0;
     o->shape_primal = 0;
     o->shape_dual = 0;
-    o->batch_cluster = 0;
-    o->batch_resident = 1;
+    o->batch_pack_mb = 0;
+    o->batch_compact = 1;
 }
 
 const char* pdlpx_error_string(int32_t code) {

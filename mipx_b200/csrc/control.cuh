@@ -1,5 +1,5 @@
 // Controller logic of one check, shared by the single-LP graph (engine.cu) and the
-// batched persistent kernel (batch.cu): restart / primal weight / polish /
+// packed batch (batch.cu, one warp per LP): restart / primal weight / polish /
 // termination of PdlpSolver::solve (pdlp.cpp:2228-2469 main loop, 2592-2666
 // polish), FP64, executed by one thread.
 #pragma once

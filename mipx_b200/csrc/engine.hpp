@@ -83,7 +83,7 @@ private:
 // Threads per row for the CSR kernels, from the mean row length.
 int32_t pickGroup(int64_t nnz, int32_t rows);
 
-// Batched solve of independent LPs in one persistent cluster launch (batch.cu).
+// Batched solve of independent LPs packed into one device image (batch.cu).
 int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
                    double* const* x_out, double* const* y_out, std::string& err);
 

@@ -344,11 +344,12 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // before the solver state is consulted, so their latencies overlap.  The step
 // arithmetic is FP64 whatever the storage type (same association as the
 // reference: tau = step * tau_base / omega), results are rounded once on store.
+// primalRows handles the columns j0 + r * slab (r < R) below jend; the
+// single-LP kernel covers [0, n), the batched kernel one tile of one LP.
 template <int G, int R, int U, class T>
-__global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
+__device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jend, int koff) {
     constexpr int slab = kBlock / G;
     const int lane = threadIdx.x % G;
-    const int j0 = blockIdx.x * (slab * R) + threadIdx.x / G;
     const int* __restrict__ ptr = p.at_ptr;
     const ColPack<T>* __restrict__ cp = p.cp;
     const double* __restrict__ xcp = p.xc;
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
         q[r] = ColPack<T>{T(0), T(0), T(0), T(0)};
         xc[r] = 0.0;
         xi[r] = T(0);
-        if (j < p.n) {
+        if (j < jend) {
             b[r] = ptr[j];
             e[r] = ptr[j + 1];
             if (lane == 0) {
@@ -388,7 +389,7 @@ __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + r * slab;
-        if (lane != 0 || j >= p.n) continue;
+        if (lane != 0 || j >= jend) continue;
         const double xcd = xc[r], xid = xi[r];
         const double tau = step * static_cast<double>(q[r].tau) / pw;
         double xh = xcd - tau * (static_cast<double>(q[r].c) + s[r]);
@@ -402,12 +403,17 @@ __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
     }
 }
 
+template <int G, int R, int U, class T>
+__global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
+    constexpr int slab = kBlock / G;
+    primalRows<G, R, U, T>(p, blockIdx.x * (slab * R) + threadIdx.x / G, p.n, koff);
+}
+
 // Fused A x_refl + dual proximal step (pdlp_kernels.cu:94-157), same structure.
 template <int G, int R, int U, class T>
-__global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
+__device__ __forceinline__ void dualRows(const IterArgs<T>& p, int i0, int iend, int koff) {
     constexpr int slab = kBlock / G;
     const int lane = threadIdx.x % G;
-    const int i0 = blockIdx.x * (slab * R) + threadIdx.x / G;
     const int* __restrict__ ptr = p.a_ptr;
     const RowPack<T>* __restrict__ rp = p.rp;
     const double* __restrict__ ycp = p.yc;
@@ -424,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
         q[r] = RowPack<T>{T(0), T(0), T(0), T(0)};
         yc[r] = 0.0;
         yi[r] = T(0);
-        if (i < p.m) {
+        if (i < iend) {
             b[r] = ptr[i];
             e[r] = ptr[i + 1];
             if (lane == 0) {
@@ -447,7 +453,7 @@ __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = i0 + r * slab;
-        if (lane != 0 || i >= p.m) continue;
+        if (lane != 0 || i >= iend) continue;
         const double ycd = yc[r], yid = yi[r];
         const double sig = step * static_cast<double>(q[r].sigma) * pw;
         const double v = ycd + sig * s[r];
@@ -474,6 +480,12 @@ __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
         p.yc[i] = lam * yr + (1.0 - lam) * yid;
         if (last) p.yh[i] = static_cast<T>(py);
     }
+}
+
+template <int G, int R, int U, class T>
+__global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
+    constexpr int slab = kBlock / G;
+    dualRows<G, R, U, T>(p, blockIdx.x * (slab * R) + threadIdx.x / G, p.m, koff);
 }
 
 // ---- block reduction of NS slots with per-slot operators -------------------
@@ -594,12 +606,11 @@ __device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const De
 }
 
 // FP64 row pass of the check: A x_hat and all row metrics (pdlp_kernels.cu:280-371,
-// pdlp.cpp:1106-1120, 1185-1199, certificates pdlp.cpp:119-284).
+// pdlp.cpp:1106-1120, 1185-1199, certificates pdlp.cpp:119-284) over rows
+// lo + k * stride ... below hi; the block's partial slots go to out.
 template <int G, class T>
-__global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
-    const DevState* st = p.st;
-    if (st->done || st->prec != precTag<T>()) return;
-    const DevConst& dc = *p.dc;
+__device__ __forceinline__ void checkRowsRange(const CheckArgs<T>& p, const DevConst& dc, int lo, int hi, int stride,
+                                               double* out) {
     int ops[kRowSlots];
     double acc[kRowSlots];
 #pragma unroll
@@ -607,12 +618,11 @@ __global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
         ops[s] = rowSlotOp(s);
         acc[s] = slotInit(ops[s]);
     }
-    const int per_block = kBlock / G;
     const int lane = threadIdx.x % G;
     const bool adapt = dc.adaptive != 0;
-    for (int base = blockIdx.x * per_block; base < p.m; base += gridDim.x * per_block) {
+    for (int base = lo; base < hi; base += stride) {
         const int i = base + threadIdx.x / G;
-        const bool valid = i < p.m;
+        const bool valid = i < hi;
         double ax = 0.0;
         if (valid) ax = rowDot<G, double>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh);
         ax = groupSum<G>(ax);
@@ -626,16 +636,23 @@ __global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
             }
         }
     }
-    blockReduceSlots<kRowSlots>(acc, ops, p.part_rows + static_cast<size_t>(blockIdx.x) * kRowSlots);
+    blockReduceSlots<kRowSlots>(acc, ops, out);
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
+    const DevState* st = p.st;
+    if (st->done || st->prec != precTag<T>()) return;
+    constexpr int per_block = kBlock / G;
+    checkRowsRange<G, T>(p, *p.dc, blockIdx.x * per_block, p.m, gridDim.x * per_block,
+                         p.part_rows + static_cast<size_t>(blockIdx.x) * kRowSlots);
 }
 
 // FP64 column pass: A^T y_hat and A^T (y_hat - y_init) in one sweep, column
 // metrics (pdlp_kernels.cu:163-274, pdlp.cpp:1123-1184, certificates).
 template <int G, class T>
-__global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
-    const DevState* st = p.st;
-    if (st->done || st->prec != precTag<T>()) return;
-    const DevConst& dc = *p.dc;
+__device__ __forceinline__ void checkColsRange(const CheckArgs<T>& p, const DevConst& dc, int lo, int hi, int stride,
+                                               double* out) {
     int ops[kColSlots];
     double acc[kColSlots];
 #pragma unroll
@@ -643,12 +660,11 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
         ops[s] = colSlotOp(s);
         acc[s] = slotInit(ops[s]);
     }
-    const int per_block = kBlock / G;
     const int lane = threadIdx.x % G;
     const bool adapt = dc.adaptive != 0;
-    for (int base = blockIdx.x * per_block; base < p.n; base += gridDim.x * per_block) {
+    for (int base = lo; base < hi; base += stride) {
         const int j = base + threadIdx.x / G;
-        const bool valid = j < p.n;
+        const bool valid = j < hi;
         double aty = 0.0, atdy = 0.0;
         if (valid) rowDot2<G>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yh, p.yi, aty, atdy);
         aty = groupSum<G>(aty);
@@ -664,7 +680,16 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
             }
         }
     }
-    blockReduceSlots<kColSlots>(acc, ops, p.part_cols + static_cast<size_t>(blockIdx.x) * kColSlots);
+    blockReduceSlots<kColSlots>(acc, ops, out);
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
+    const DevState* st = p.st;
+    if (st->done || st->prec != precTag<T>()) return;
+    constexpr int per_block = kBlock / G;
+    checkColsRange<G, T>(p, *p.dc, blockIdx.x * per_block, p.n, gridDim.x * per_block,
+                         p.part_cols + static_cast<size_t>(blockIdx.x) * kColSlots);
 }
 
 // Restart copy x_init = x_cur = x_hat, y_init = y_cur = y_hat (pdlp_kernels.cu:377-405),

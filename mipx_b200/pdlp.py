@@ -128,8 +128,8 @@ class PdlpOptions:
     autotune: bool = False
     shape_primal: int = 0
     shape_dual: int = 0
-    batch_cluster: int = 0
-    batch_resident: bool = True
+    batch_pack_mb: int = 0
+    batch_compact: bool = True
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
