@@ -13,9 +13,10 @@ solve.  Metric: PDLP iterations per second (LPs/s and latency reported beside).
   (host scaling + H2D copies), solve, copy x and y back -- per step.
 * ``roofline``: the fused primal step (A^T y + Halpern step), the dominant
   kernel, timed alone with CUDA events on the engine's stream after the timed
-  region; algorithmic bytes per launch = 4(n+1) + 8 nnz + 4 m + 32 n (A^T CSR
-  pointers, indices, FP32 values, the y vector once, the packed column
-  constants and the current/anchor x read, reflected/current x written).
+  region; algorithmic bytes per launch = 4(n+1) + 8 nnz + 8 m + 40 n (A^T CSR
+  pointers, indices and FP32 values, the FP64 current y gathered once, the
+  packed FP32 column constants (16 B), FP64 current and FP32 anchor x read,
+  FP32 reflected and FP64 current x written).
 * ``cpu_baseline``: the reference's CPU PDLP (oracle/_ref, compiled from its
   sources; else the oracle restatement) on one host core, as the marginal rate
   between a 200- and a 400-iteration run of the same LP.
@@ -278,8 +279,8 @@ def main():
     # kernel timing for the roofline (dominant kernel: fused primal step)
     kt = solver.timeKernels(50)
     cfg = solver.launchConfig()
-    bytes_primal = 4 * (n + 1) + 8 * nnz + 4 * m + 32 * n
-    bytes_dual = 4 * (m + 1) + 8 * nnz + 4 * n + 28 * m
+    bytes_primal = 4 * (n + 1) + 8 * nnz + 8 * m + 40 * n
+    bytes_dual = 4 * (m + 1) + 8 * nnz + 4 * n + 36 * m
     peak, peak_kind = measured_peak_hbm()
     ach = bytes_primal / (kt["primal_ms"] * 1e-3) / 1e9
 

@@ -1,20 +1,23 @@
 // Packed batched PDLP (pdlpx_batch_solve).
 //
 // The LPs of a pack share one device image with global numbering: LP l owns
-// rows [r0_l, r0_l + m_l) and columns [c0_l, c0_l + n_l) of a block-diagonal
+// rows [r0_l, r0_l + mp_l) and columns [c0_l, c0_l + np_l) of a block-diagonal
 // A and A^T, so the gathers of the step kernels are those of the single-LP
-// kernels.  Rows and columns are cut into tiles that never straddle two LPs;
-// a tile is as tall as one block of the LP's launch shape covers.  One launch
-// of a step kernel covers every tile of every LP with that shape: the block
-// reads its tile and the tile's LP state, then runs the single-LP row bodies
-// (primalRows / dualRows) in the LP's current precision with the LP's own step
-// size, primal weight and Halpern count.  LPs restart, switch precision,
-// polish and finish independently: per-LP DevState / DevConst, and the
-// single-LP controlStep run by one warp per LP over the LP's tile partials in
-// fixed order.  A restart cycle of the whole pack -- N iterations, the FP64
-// check, the controllers, restart copies and FP32 -> FP64 hand-overs -- is one
-// CUDA graph launch.  When finished LPs leave enough tiles idle, the host drops
-// them from the tile lists and captures a smaller graph.
+// kernels.  Each LP's rows and columns are padded to whole tiles (a tile is as
+// tall as one block of the LP's launch shape covers; padded rows and columns
+// are empty, free and zero, and add nothing to any check term), and LPs with
+// the same launch shape are contiguous.  A step-kernel block therefore knows
+// its rows from its index alone; it loads the row pointers and its tile's
+// (LP, mode) word together, then runs the single-LP row bodies
+// (primalRowsFrom / dualRowsFrom) in the LP's current precision with the LP's
+// own step size, primal weight and Halpern count -- the same three dependent
+// load steps as the single-LP kernels.  LPs restart, switch precision, polish
+// and finish independently: per-LP DevState / DevConst, and the single-LP
+// controlStep run by one warp per LP over the LP's tile partials in fixed
+// order.  A restart cycle of the whole pack -- N iterations, the FP64 check, the
+// controllers, restart copies, FP32 -> FP64 hand-overs and the tile modes -- is
+// one CUDA graph launch.  When finished LPs leave enough tiles idle, the host
+// switches the launches to a list of the live tiles and captures a smaller graph.
 //
 // An LP's tiles, launch shape and reduction order depend on that LP alone, so
 // its result is bit-identical alone and in any mix (batch invariance).  A batch
@@ -39,13 +42,18 @@
 namespace pdlpx {
 namespace {
 
+// Tile modes (the .y of a tile's info word), refreshed at the end of every cycle.
+constexpr int kModeFp32 = 0, kModeFp64 = 1, kModeIdle = 2;
+
 struct PackArgs {
     IterArgs<float> it32;  // global arrays of the pack (st is set per tile)
     IterArgs<double> it64;
     CheckArgs<float> ck32;
     CheckArgs<double> ck64;
-    const int4* ctiles;  // column tiles: (LP, first column, end column, 0)
-    const int4* rtiles;  // row tiles
+    int4* ctinfo;        // column tiles: (LP, mode, first column, end column)
+    int4* rtinfo;        // row tiles
+    const int* clist;    // live column / row tile ids after compaction
+    const int* rlist;
     const int4* lpt;     // per LP: first column tile, column tiles, first row tile, row tiles
     DevState* st;
     const DevConst* dc;
@@ -58,11 +66,18 @@ struct PackArgs {
     double* pi_y;
     double* pi_xn;
     double* pi_part;      // [column tile][2]
-    int L, mixed, sv_max_iter;
+    int L, nct, nrt, mixed, sv_max_iter;
     double sv_tol;
 };
 
 constexpr int kCtlWarps = 4;  // LPs per block of the per-LP kernels
+
+// Resident blocks per SM the step kernels are compiled for: the tiles are
+// latency-bound, and 5 blocks (48 registers) measured faster than 3-4 blocks
+// (the compiler's own pick, 64-72 registers) and than 8 blocks with spills.
+#ifndef PDLPX_PACK_MIN_BLOCKS
+#define PDLPX_PACK_MIN_BLOCKS 5
+#endif
 
 __device__ __forceinline__ double combine(int op, double a, double b) {
     return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
@@ -87,67 +102,79 @@ __device__ __forceinline__ void warpTiles(const double* part, int first, int cou
 }
 
 // ---- PDHG step over one tile ------------------------------------------------
-template <int G, int R, int U>
-__global__ void __launch_bounds__(kBlock) packPrimal(PackArgs a, int tile0, int koff) {
-    const int4 t = a.ctiles[tile0 + blockIdx.x];
-    DevState* st = a.st + t.x;
-    if (st->done) return;
-    const int j0 = t.y + threadIdx.x / G;
-    if (st->prec == 0) {
+// A launch covers the tiles [tile0, tile0 + grid) of one shape whose rows start
+// at `base` (direct), or the live tiles list[list0 + b] of that shape (IND).
+template <int G, int R, int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_PACK_MIN_BLOCKS)
+    packPrimal(PackArgs a, int tile0, int base, int list0, int koff) {
+    constexpr int TR = (kBlock / G) * R;
+    const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int c0 = base + (tile - tile0) * TR;
+    const int j0 = c0 + static_cast<int>(threadIdx.x) / G;
+    int b[R], e[R];
+    rowBounds<G, R>(a.it64.at_ptr, j0, c0 + TR, b, e);
+    const int4 info = a.ctinfo[tile];
+    if (info.y == kModeIdle) return;
+    DevState* st = a.st + info.x;
+    if (info.y == kModeFp32) {
         IterArgs<float> p = a.it32;
         p.st = st;
-        primalRows<G, R, U, float>(p, j0, t.z, koff);
+        primalRowsFrom<G, R, U, float>(p, j0, c0 + TR, b, e, koff);
     } else {
         IterArgs<double> p = a.it64;
         p.st = st;
-        primalRows<G, R, U, double>(p, j0, t.z, koff);
+        primalRowsFrom<G, R, U, double>(p, j0, c0 + TR, b, e, koff);
     }
 }
 
-template <int G, int R, int U>
-__global__ void __launch_bounds__(kBlock) packDual(PackArgs a, int tile0, int koff) {
-    const int4 t = a.rtiles[tile0 + blockIdx.x];
-    DevState* st = a.st + t.x;
-    if (st->done) return;
-    const int i0 = t.y + threadIdx.x / G;
-    if (st->prec == 0) {
+template <int G, int R, int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_PACK_MIN_BLOCKS)
+    packDual(PackArgs a, int tile0, int base, int list0, int koff) {
+    constexpr int TR = (kBlock / G) * R;
+    const int tile = IND ? a.rlist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int r0 = base + (tile - tile0) * TR;
+    const int i0 = r0 + static_cast<int>(threadIdx.x) / G;
+    int b[R], e[R];
+    rowBounds<G, R>(a.it64.a_ptr, i0, r0 + TR, b, e);
+    const int4 info = a.rtinfo[tile];
+    if (info.y == kModeIdle) return;
+    DevState* st = a.st + info.x;
+    if (info.y == kModeFp32) {
         IterArgs<float> p = a.it32;
         p.st = st;
-        dualRows<G, R, U, float>(p, i0, t.z, koff);
+        dualRowsFrom<G, R, U, float>(p, i0, r0 + TR, b, e, koff);
     } else {
         IterArgs<double> p = a.it64;
         p.st = st;
-        dualRows<G, R, U, double>(p, i0, t.z, koff);
+        dualRowsFrom<G, R, U, double>(p, i0, r0 + TR, b, e, koff);
     }
 }
 
 // ---- FP64 check pass, one partial per tile -----------------------------------
-template <int G>
-__global__ void __launch_bounds__(kBlock) packCheckRows(PackArgs a, int tile0) {
-    const int tile = tile0 + blockIdx.x;
-    const int4 t = a.rtiles[tile];
-    const DevState* st = a.st + t.x;
-    if (st->done) return;
+template <int G, bool IND>
+__global__ void __launch_bounds__(kBlock) packCheckRows(PackArgs a, int tile0, int list0) {
+    const int tile = IND ? a.rlist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int4 t = a.rtinfo[tile];
+    if (t.y == kModeIdle) return;
     double* out = a.part_rows + static_cast<size_t>(tile) * kRowSlots;
     constexpr int per = kBlock / G;
-    if (st->prec == 0)
-        checkRowsRange<G, float>(a.ck32, a.dc[t.x], t.y, t.z, per, out);
+    if (t.y == kModeFp32)
+        checkRowsRange<G, float>(a.ck32, a.dc[t.x], t.z, t.w, per, out);
     else
-        checkRowsRange<G, double>(a.ck64, a.dc[t.x], t.y, t.z, per, out);
+        checkRowsRange<G, double>(a.ck64, a.dc[t.x], t.z, t.w, per, out);
 }
 
-template <int G>
-__global__ void __launch_bounds__(kBlock) packCheckCols(PackArgs a, int tile0) {
-    const int tile = tile0 + blockIdx.x;
-    const int4 t = a.ctiles[tile];
-    const DevState* st = a.st + t.x;
-    if (st->done) return;
+template <int G, bool IND>
+__global__ void __launch_bounds__(kBlock) packCheckCols(PackArgs a, int tile0, int list0) {
+    const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int4 t = a.ctinfo[tile];
+    if (t.y == kModeIdle) return;
     double* out = a.part_cols + static_cast<size_t>(tile) * kColSlots;
     constexpr int per = kBlock / G;
-    if (st->prec == 0)
-        checkColsRange<G, float>(a.ck32, a.dc[t.x], t.y, t.z, per, out);
+    if (t.y == kModeFp32)
+        checkColsRange<G, float>(a.ck32, a.dc[t.x], t.z, t.w, per, out);
     else
-        checkColsRange<G, double>(a.ck64, a.dc[t.x], t.y, t.z, per, out);
+        checkColsRange<G, double>(a.ck64, a.dc[t.x], t.z, t.w, per, out);
 }
 
 // ---- per-LP controller: one warp per LP ---------------------------------------
@@ -174,48 +201,51 @@ __global__ void __launch_bounds__(32 * kCtlWarps) packController(PackArgs a) {
 }
 
 // Restart copy (pdlp_kernels.cu:377-405) and FP32 -> FP64 hand-over per tile:
-// blocks [0, nct) take column tiles, the rest row tiles.
-__global__ void __launch_bounds__(kBlock) packRestart(PackArgs a, int nct) {
-    const bool col = static_cast<int>(blockIdx.x) < nct;
-    const int4 t = col ? a.ctiles[blockIdx.x] : a.rtiles[blockIdx.x - nct];
+// blocks [0, ncol) take column tiles, the rest row tiles (lists after compaction).
+__global__ void __launch_bounds__(kBlock) packRestart(PackArgs a, int ncol, int use_list) {
+    const bool col = static_cast<int>(blockIdx.x) < ncol;
+    const int k = col ? static_cast<int>(blockIdx.x) : static_cast<int>(blockIdx.x) - ncol;
+    const int tile = use_list ? (col ? a.clist[k] : a.rlist[k]) : k;
+    const int4 t = col ? a.ctinfo[tile] : a.rtinfo[tile];
+    if (t.y == kModeIdle) return;
     const DevState* st = a.st + t.x;
     if (st->done) return;
     const int prec = st->prec;
     const bool restart = st->restart != 0;
     const bool promote = prec == 0 && st->promote != 0;
     if (!restart && !promote) return;
-    for (int k = t.y + threadIdx.x; k < t.z; k += kBlock) {
+    for (int q = t.z + threadIdx.x; q < t.w; q += kBlock) {
         if (col) {
             if (prec == 0) {
                 if (restart) {
-                    const float v = a.it32.xh[k];
-                    a.it32.xi[k] = v;
-                    a.it32.xc[k] = v;
+                    const float v = a.it32.xh[q];
+                    a.it32.xi[q] = v;
+                    a.it32.xc[q] = v;
                 }
                 if (promote) {
-                    a.it64.xi[k] = a.it32.xi[k];
-                    a.it64.xh[k] = a.it32.xh[k];
+                    a.it64.xi[q] = a.it32.xi[q];
+                    a.it64.xh[q] = a.it32.xh[q];
                 }
             } else {
-                const double v = a.it64.xh[k];
-                a.it64.xi[k] = v;
-                a.it64.xc[k] = v;
+                const double v = a.it64.xh[q];
+                a.it64.xi[q] = v;
+                a.it64.xc[q] = v;
             }
         } else {
             if (prec == 0) {
                 if (restart) {
-                    const float v = a.it32.yh[k];
-                    a.it32.yi[k] = v;
-                    a.it32.yc[k] = v;
+                    const float v = a.it32.yh[q];
+                    a.it32.yi[q] = v;
+                    a.it32.yc[q] = v;
                 }
                 if (promote) {
-                    a.it64.yi[k] = a.it32.yi[k];
-                    a.it64.yh[k] = a.it32.yh[k];
+                    a.it64.yi[q] = a.it32.yi[q];
+                    a.it64.yh[q] = a.it32.yh[q];
                 }
             } else {
-                const double v = a.it64.yh[k];
-                a.it64.yi[k] = v;
-                a.it64.yc[k] = v;
+                const double v = a.it64.yh[q];
+                a.it64.yi[q] = v;
+                a.it64.yc[q] = v;
             }
         }
     }
@@ -233,16 +263,25 @@ __global__ void packFinish(PackArgs a) {
     a.flags[l] = (st->done ? 1 : 0) | (st->prec ? 2 : 0);
 }
 
+// Mode of every tile for the next cycle: idle once its LP is done, else its precision.
+__global__ void packModes(PackArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nct + a.nrt) return;
+    int4* info = k < a.nct ? a.ctinfo + k : a.rtinfo + (k - a.nct);
+    const DevState* st = a.st + info->x;
+    info->y = st->done ? kModeIdle : (st->prec ? kModeFp64 : kModeFp32);
+}
+
 // ---- power iteration on A^T A per LP (pdlp.cpp:748-795, 1985-2041) ---------------
 template <int G>
 __global__ void __launch_bounds__(kBlock) packPowerA(PackArgs a, int tile0) {
-    const int4 t = a.rtiles[tile0 + blockIdx.x];
+    const int4 t = a.rtinfo[tile0 + blockIdx.x];
     if (a.ps[t.x].done) return;
     constexpr int per = kBlock / G;
     const int lane = threadIdx.x % G;
-    for (int base = t.y; base < t.z; base += per) {
+    for (int base = t.z; base < t.w; base += per) {
         const int i = base + threadIdx.x / G;
-        const bool valid = i < t.z;
+        const bool valid = i < t.w;
         double s = 0.0;
         if (valid) {
             const int b = a.it64.a_ptr[i], e = a.it64.a_ptr[i + 1];
@@ -257,14 +296,14 @@ __global__ void __launch_bounds__(kBlock) packPowerA(PackArgs a, int tile0) {
 template <int G>
 __global__ void __launch_bounds__(kBlock) packPowerAt(PackArgs a, int tile0) {
     const int tile = tile0 + blockIdx.x;
-    const int4 t = a.ctiles[tile];
+    const int4 t = a.ctinfo[tile];
     if (a.ps[t.x].done) return;
     constexpr int per = kBlock / G;
     const int lane = threadIdx.x % G;
     double acc[2] = {0.0, 0.0};
-    for (int base = t.y; base < t.z; base += per) {
+    for (int base = t.z; base < t.w; base += per) {
         const int j = base + threadIdx.x / G;
-        const bool valid = j < t.z;
+        const bool valid = j < t.w;
         double s = 0.0;
         if (valid) {
             const int b = a.it64.at_ptr[j], e = a.it64.at_ptr[j + 1];
@@ -298,12 +337,12 @@ __global__ void __launch_bounds__(32 * kCtlWarps) packPowerFinish1(PackArgs a) {
 
 __global__ void __launch_bounds__(kBlock) packPowerNormalize(PackArgs a) {
     const int tile = blockIdx.x;
-    const int4 t = a.ctiles[tile];
+    const int4 t = a.ctinfo[tile];
     const PowerState& ps = a.ps[t.x];
     if (ps.done) return;
     const double s2 = ps.s2, nrm = ps.nrm;
     double acc[1] = {0.0};
-    for (int j = t.y + threadIdx.x; j < t.z; j += kBlock) {
+    for (int j = t.z + threadIdx.x; j < t.w; j += kBlock) {
         const double xn = a.pi_xn[j];
         const double d = xn - s2 * a.pi_x[j];
         acc[0] += d * d;
@@ -353,10 +392,13 @@ struct Item {
     ScaledLp sc;
     bool trivial = false;
     int shapeP = 0, shapeD = 0;
-    int nct = 0, nrt = 0;  // tiles
-    size_t bytes = 0;      // share of a pack's device image
+    int nct = 0, nrt = 0;      // tiles
+    int64_t np = 0, mp = 0;    // columns / rows padded to whole tiles
+    size_t bytes = 0;          // share of a pack's device image
     // position within its pack
-    int64_t r0 = 0, c0 = 0, z0 = 0;
+    int64_t r0 = 0, c0 = 0;    // first row, first column
+    int64_t za = 0, zt = 0;    // first entry of A / of A^T
+    int ct0 = 0, rt0 = 0;      // first column tile, first row tile
     int l = 0;
 };
 
@@ -364,11 +406,11 @@ size_t al256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
 
 // Device bytes an LP adds to a pack (image + scratch), for the pack split.
 size_t itemBytes(const Item& it, bool mixed) {
-    const size_t m = it.lp.m, n = it.lp.n, z = it.sc.a.nnz();
+    const size_t m = it.mp, n = it.np, z = it.sc.a.nnz();
     size_t b = 4 * (m + n) + z * (8 + 16 + (mixed ? 8 : 0));           // pointers, indices, values
     b += n * (32 + 40 + 8 + 24 + 24) + m * (32 + 32 + 8 + 16 + 8);     // packs, checks, FP64 iterates, power
     if (mixed) b += n * (16 + 12) + m * (16 + 8);
-    b += static_cast<size_t>(it.nct) * (16 + 8 * kColSlots + 16) + static_cast<size_t>(it.nrt) * (16 + 8 * kRowSlots);
+    b += static_cast<size_t>(it.nct) * (16 + 4 + 8 * kColSlots + 16) + static_cast<size_t>(it.nrt) * (16 + 4 + 8 * kRowSlots);
     b += sizeof(DevState) + sizeof(DevConst) + sizeof(PowerState) + 32;
     return b;
 }
@@ -399,9 +441,11 @@ void parallelFor(int count, F&& f) {
         }                                                                            \
     } while (0)
 
-// One launch of a step/check kernel class: tiles [begin, begin + count) of one shape.
+// One launch of a step / check kernel: the tiles of one shape class, all of them
+// (list0 < 0: tiles [tile0, tile0 + count) from row `base`) or `count` live ones
+// listed from list0.
 struct Launch {
-    int shape, begin, count;
+    int shape, tile0, base, count, list0;
 };
 
 // Device image and graphs of one pack.
@@ -409,24 +453,25 @@ struct Pack {
     std::vector<Item*> items;
     bool mixed = true;
     int L = 0;
-    int64_t M = 0, Nc = 0, Z = 0;
-    int nct = 0, nrt = 0;  // all tiles
+    int64_t M = 0, Nc = 0, Z = 0;  // padded rows, padded columns, entries
+    int nct = 0, nrt = 0;          // all tiles
     // arena layout
     size_t o_aptr, o_aidx, o_atptr, o_atidx, o_av32, o_atv32, o_av64, o_atv64, o_cp32, o_rp32, o_cp64, o_rp64;
     size_t o_c, o_lb, o_ub, o_cs, o_tau, o_rl, o_ru, o_rs, o_sig;
-    size_t o_st, o_dc, o_ps, o_ctiles, o_rtiles, o_lpt;
+    size_t o_st, o_dc, o_ps, o_ctinfo, o_rtinfo, o_lpt;
     size_t image_end;  // [0, image_end) is uploaded from the host image
     size_t o_xc, o_xi32, o_xr32, o_xh32, o_xi64, o_xr64, o_xh64, o_yc, o_yi32, o_yh32, o_yi64, o_yh64;
     size_t iter_end;   // [image_end, iter_end): iterates (zero or warm start)
-    size_t o_pix, o_piy, o_pixn, o_pipart, o_pcols, o_prows, o_flags, o_counters;
+    size_t o_pix, o_piy, o_pixn, o_pipart, o_pcols, o_prows, o_clist, o_rlist, o_flags, o_counters;
     size_t total;
     char* d = nullptr;
     cudaStream_t s = nullptr;
     cudaGraphExec_t cycle = nullptr, power = nullptr;
     int cycle_launches = 0, power_launches = 0;
-    int active_tiles = 0;  // tiles in the captured cycle graph
-    std::vector<Launch> lc, lr;  // launches of the current tile lists
-    int act_ct = 0, act_rt = 0;  // current (compacted) tile counts
+    std::vector<Launch> cls_c, cls_r;  // every tile, per shape class
+    std::vector<Launch> lc, lr;        // launches of the current cycle graph
+    bool listed = false;               // lc / lr run over the live-tile lists
+    int live_ct = 0, live_rt = 0;      // tiles in the current launches
     PackArgs args{};
 
     ~Pack() {
@@ -434,6 +479,51 @@ struct Pack {
         if (power) cudaGraphExecDestroy(power);
         if (d) cudaFree(d);
         if (s) cudaStreamDestroy(s);
+    }
+
+    // Positions: columns grouped by primal shape, rows by dual shape, LP order
+    // within a shape; each LP padded to whole tiles.
+    void place() {
+        for (int side = 0; side < 2; ++side) {
+            int64_t pos = 0, z = 0;
+            int tiles = 0;
+            std::vector<Launch>& cls = side == 0 ? cls_c : cls_r;
+            for (int shape = 0; shape < kNumShapes; ++shape) {
+                Launch c{shape, tiles, static_cast<int>(pos), 0, -1};
+                for (Item* it : items) {
+                    if ((side == 0 ? it->shapeP : it->shapeD) != shape) continue;
+                    if (side == 0) {
+                        it->c0 = pos;
+                        it->zt = z;
+                        it->ct0 = tiles;
+                        pos += it->np;
+                        tiles += it->nct;
+                    } else {
+                        it->r0 = pos;
+                        it->za = z;
+                        it->rt0 = tiles;
+                        pos += it->mp;
+                        tiles += it->nrt;
+                    }
+                    z += it->sc.a.nnz();
+                }
+                c.count = tiles - c.tile0;
+                if (c.count > 0) cls.push_back(c);
+            }
+            if (side == 0) {
+                Nc = pos;
+                nct = tiles;
+                Z = z;
+            } else {
+                M = pos;
+                nrt = tiles;
+            }
+        }
+        lc = cls_c;
+        lr = cls_r;
+        listed = false;
+        live_ct = nct;
+        live_rt = nrt;
     }
 
     void layout() {
@@ -468,8 +558,8 @@ struct Pack {
         o_st = take(sizeof(DevState) * L);
         o_dc = take(sizeof(DevConst) * L);
         o_ps = take(sizeof(PowerState) * L);
-        o_ctiles = take(sizeof(int4) * nct);
-        o_rtiles = take(sizeof(int4) * nrt);
+        o_ctinfo = take(sizeof(int4) * nct);
+        o_rtinfo = take(sizeof(int4) * nrt);
         o_lpt = take(sizeof(int4) * L);
         o_pix = take(8 * n);
         image_end = o;
@@ -491,6 +581,8 @@ struct Pack {
         o_pipart = take(16 * static_cast<size_t>(nct));
         o_pcols = take(8 * kColSlots * static_cast<size_t>(nct));
         o_prows = take(8 * kRowSlots * static_cast<size_t>(nrt));
+        o_clist = take(4 * static_cast<size_t>(nct));
+        o_rlist = take(4 * static_cast<size_t>(nrt));
         o_flags = take(4 * static_cast<size_t>(L));
         o_counters = take(64);
         total = o;
@@ -563,8 +655,10 @@ struct Pack {
         };
         fillCheck(a.ck64, a.it64);
         if (mixed) fillCheck(a.ck32, a.it32);
-        a.ctiles = P<int4>(o_ctiles);
-        a.rtiles = P<int4>(o_rtiles);
+        a.ctinfo = P<int4>(o_ctinfo);
+        a.rtinfo = P<int4>(o_rtinfo);
+        a.clist = P<int>(o_clist);
+        a.rlist = P<int>(o_rlist);
         a.lpt = P<int4>(o_lpt);
         a.st = P<DevState>(o_st);
         a.dc = P<DevConst>(o_dc);
@@ -578,49 +672,37 @@ struct Pack {
         a.pi_xn = P<double>(o_pixn);
         a.pi_part = P<double>(o_pipart);
         a.L = L;
+        a.nct = nct;
+        a.nrt = nrt;
         a.mixed = mixed ? 1 : 0;
         a.sv_max_iter = o.sv_max_iter;
         a.sv_tol = o.sv_tol;
     }
 
-    // Tile lists of the LPs with keep[l] set, grouped by launch shape (LP order
-    // within a shape), and the per-LP tile ranges.
-    void tileLists(const std::vector<char>& keep, std::vector<int4>& ct, std::vector<int4>& rt,
-                   std::vector<int4>& lpt) {
-        ct.clear();
-        rt.clear();
-        lpt.assign(L, make_int4(0, 0, 0, 0));
+    // Live-tile lists of the LPs with keep[l] set (shape class by shape class,
+    // tile order kept) and the launches over them.
+    void liveLists(const std::vector<char>& keep, std::vector<int>& cl, std::vector<int>& rl) {
+        cl.clear();
+        rl.clear();
         lc.clear();
         lr.clear();
         for (int side = 0; side < 2; ++side) {
-            std::vector<int4>& out = side == 0 ? ct : rt;
-            std::vector<Launch>& ls = side == 0 ? lc : lr;
-            for (int shape = 0; shape < kNumShapes; ++shape) {
-                const int begin = static_cast<int>(out.size());
-                for (int l = 0; l < L; ++l) {
-                    const Item& it = *items[l];
-                    if (!keep[l] || (side == 0 ? it.shapeP : it.shapeD) != shape) continue;
-                    const int per = rowsPerBlock(shape);
-                    const int64_t lo = side == 0 ? it.c0 : it.r0;
-                    const int64_t cnt = side == 0 ? it.lp.n : it.lp.m;
-                    const int first = static_cast<int>(out.size());
-                    for (int64_t b = 0; b < cnt; b += per)
-                        out.push_back(make_int4(l, static_cast<int>(lo + b), static_cast<int>(lo + std::min(cnt, b + per)), 0));
-                    const int count = static_cast<int>(out.size()) - first;
-                    if (side == 0) {
-                        lpt[l].x = first;
-                        lpt[l].y = count;
-                    } else {
-                        lpt[l].z = first;
-                        lpt[l].w = count;
-                    }
+            std::vector<int>& out = side == 0 ? cl : rl;
+            for (const Launch& c : side == 0 ? cls_c : cls_r) {
+                const int list0 = static_cast<int>(out.size());
+                for (const Item* it : items) {
+                    if (!keep[it->l] || (side == 0 ? it->shapeP : it->shapeD) != c.shape) continue;
+                    const int first = side == 0 ? it->ct0 : it->rt0;
+                    const int count = side == 0 ? it->nct : it->nrt;
+                    for (int k = 0; k < count; ++k) out.push_back(first + k);
                 }
-                const int count = static_cast<int>(out.size()) - begin;
-                if (count > 0) ls.push_back(Launch{shape, begin, count});
+                const int count = static_cast<int>(out.size()) - list0;
+                if (count > 0) (side == 0 ? lc : lr).push_back(Launch{c.shape, c.tile0, c.base, count, list0});
             }
         }
-        act_ct = static_cast<int>(ct.size());
-        act_rt = static_cast<int>(rt.size());
+        listed = true;
+        live_ct = static_cast<int>(cl.size());
+        live_rt = static_cast<int>(rl.size());
     }
 
     int launchCycle(int N) {
@@ -628,42 +710,59 @@ struct Pack {
         const PackArgs& a = args;
         for (int k = 1; k <= N; ++k) {
             for (const Launch& c : lc) {
-                PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU><<<c.count, kBlock, 0, s>>>(a, c.begin, k)));
+                if (listed) {
+                    PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+                } else {
+                    PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+                }
                 ++n;
             }
             for (const Launch& c : lr) {
-                PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU><<<c.count, kBlock, 0, s>>>(a, c.begin, k)));
+                if (listed) {
+                    PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+                } else {
+                    PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+                }
                 ++n;
             }
         }
         for (const Launch& c : lr) {
-            PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            if (listed) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
+            } else {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
+            }
             ++n;
         }
         for (const Launch& c : lc) {
-            PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            if (listed) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
+            } else {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
+            }
             ++n;
         }
         packController<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
-        if (act_ct + act_rt > 0) packRestart<<<act_ct + act_rt, kBlock, 0, s>>>(a, act_ct);
+        if (live_ct + live_rt > 0) packRestart<<<live_ct + live_rt, kBlock, 0, s>>>(a, live_ct, listed ? 1 : 0);
         packFinish<<<(L + 127) / 128, 128, 0, s>>>(a);
-        return n + 3;
+        packModes<<<(nct + nrt + 255) / 256, 256, 0, s>>>(a);
+        return n + 4;
     }
 
     int launchPower(int chunk) {
         int n = 0;
         const PackArgs& a = args;
         for (int it = 0; it < chunk; ++it) {
-            for (const Launch& c : lr) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerA<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            for (const Launch& c : cls_r) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerA<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
                 ++n;
             }
-            for (const Launch& c : lc) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerAt<GG><<<c.count, kBlock, 0, s>>>(a, c.begin)));
+            for (const Launch& c : cls_c) {
+                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerAt<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
                 ++n;
             }
             packPowerFinish1<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
-            if (act_ct > 0) packPowerNormalize<<<act_ct, kBlock, 0, s>>>(a);
+            packPowerNormalize<<<nct, kBlock, 0, s>>>(a);
             packPowerFinish2<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
             n += 3;
         }
@@ -671,60 +770,88 @@ struct Pack {
     }
 };
 
-// Host image of one LP's share of the pack.
+// Host image of one LP's share of the pack (its padded rows and columns included).
 void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img, char* iters) {
     const ScaledLp& sc = it.sc;
     const int32_t m = it.lp.m, n = it.lp.n, z = sc.a.nnz();
-    const int64_t r0 = it.r0, c0 = it.c0, z0 = it.z0;
+    const int64_t r0 = it.r0, c0 = it.c0, za = it.za, zt = it.zt, mp = it.mp, np = it.np;
+    const double inf = std::numeric_limits<double>::infinity();
     auto I = [&](size_t off) { return reinterpret_cast<int32_t*>(img + off); };
     auto F = [&](size_t off) { return reinterpret_cast<float*>(img + off); };
     auto D = [&](size_t off) { return reinterpret_cast<double*>(img + off); };
     int32_t* aptr = I(pk.o_aptr) + r0;
-    for (int32_t i = 0; i < m; ++i) aptr[i] = static_cast<int32_t>(z0 + sc.a.ptr[i]);
+    for (int64_t i = 0; i < mp; ++i) aptr[i] = static_cast<int32_t>(za + sc.a.ptr[std::min<int64_t>(i, m)]);
     int32_t* atptr = I(pk.o_atptr) + c0;
-    for (int32_t j = 0; j < n; ++j) atptr[j] = static_cast<int32_t>(z0 + sc.at.ptr[j]);
-    int32_t* aidx = I(pk.o_aidx) + z0;
-    int32_t* atidx = I(pk.o_atidx) + z0;
+    for (int64_t j = 0; j < np; ++j) atptr[j] = static_cast<int32_t>(zt + sc.at.ptr[std::min<int64_t>(j, n)]);
+    int32_t* aidx = I(pk.o_aidx) + za;
+    int32_t* atidx = I(pk.o_atidx) + zt;
     for (int32_t k = 0; k < z; ++k) {
         aidx[k] = static_cast<int32_t>(c0 + sc.a.idx[k]);
         atidx[k] = static_cast<int32_t>(r0 + sc.at.idx[k]);
     }
-    std::memcpy(D(pk.o_av64) + z0, sc.a.val.data(), 8 * static_cast<size_t>(z));
-    std::memcpy(D(pk.o_atv64) + z0, sc.at.val.data(), 8 * static_cast<size_t>(z));
+    std::memcpy(D(pk.o_av64) + za, sc.a.val.data(), 8 * static_cast<size_t>(z));
+    std::memcpy(D(pk.o_atv64) + zt, sc.at.val.data(), 8 * static_cast<size_t>(z));
+    // padding: empty, free rows and columns with zero cost and unit scales
+    auto col = [&](int64_t j, double& c, double& lb, double& ub, double& tau, double& cs) {
+        const bool real = j < n;
+        c = real ? sc.c[j] : 0.0;
+        lb = real ? sc.cl[j] : -inf;
+        ub = real ? sc.cu[j] : inf;
+        tau = real ? sc.tau[j] : 1.0;
+        cs = real ? sc.col_scale[j] : 1.0;
+    };
+    auto row = [&](int64_t i, double& sig, double& rl, double& ru, double& type, double& rs) {
+        const bool real = i < m;
+        sig = real ? sc.sigma[i] : 1.0;
+        rl = real ? sc.rl[i] : -inf;
+        ru = real ? sc.ru[i] : inf;
+        type = real ? static_cast<double>(sc.row_type[i]) : static_cast<double>(kRowRanged);
+        rs = real ? sc.row_scale[i] : 1.0;
+    };
+    for (int64_t j = 0; j < np; ++j) {
+        double c, lb, ub, tau, cs;
+        col(j, c, lb, ub, tau, cs);
+        reinterpret_cast<ColPack<double>*>(img + pk.o_cp64)[c0 + j] = ColPack<double>{c, lb, ub, tau};
+        if (pk.mixed)
+            reinterpret_cast<ColPack<float>*>(img + pk.o_cp32)[c0 + j] =
+                ColPack<float>{static_cast<float>(c), static_cast<float>(lb), static_cast<float>(ub), static_cast<float>(tau)};
+        D(pk.o_c)[c0 + j] = c;
+        D(pk.o_lb)[c0 + j] = lb;
+        D(pk.o_ub)[c0 + j] = ub;
+        D(pk.o_cs)[c0 + j] = cs;
+        D(pk.o_tau)[c0 + j] = tau;
+    }
+    for (int64_t i = 0; i < mp; ++i) {
+        double sig, rl, ru, type, rs;
+        row(i, sig, rl, ru, type, rs);
+        reinterpret_cast<RowPack<double>*>(img + pk.o_rp64)[r0 + i] = RowPack<double>{sig, rl, ru, type};
+        if (pk.mixed)
+            reinterpret_cast<RowPack<float>*>(img + pk.o_rp32)[r0 + i] =
+                RowPack<float>{static_cast<float>(sig), static_cast<float>(rl), static_cast<float>(ru), static_cast<float>(type)};
+        D(pk.o_rl)[r0 + i] = rl;
+        D(pk.o_ru)[r0 + i] = ru;
+        D(pk.o_rs)[r0 + i] = rs;
+        D(pk.o_sig)[r0 + i] = sig;
+    }
     if (pk.mixed) {
-        float* av = F(pk.o_av32) + z0;
-        float* atv = F(pk.o_atv32) + z0;
+        float* av = F(pk.o_av32) + za;
+        float* atv = F(pk.o_atv32) + zt;
         for (int32_t k = 0; k < z; ++k) {
             av[k] = static_cast<float>(sc.a.val[k]);
             atv[k] = static_cast<float>(sc.at.val[k]);
         }
-        auto* cp = reinterpret_cast<ColPack<float>*>(img + pk.o_cp32) + c0;
-        for (int32_t j = 0; j < n; ++j)
-            cp[j] = ColPack<float>{static_cast<float>(sc.c[j]), static_cast<float>(sc.cl[j]),
-                                   static_cast<float>(sc.cu[j]), static_cast<float>(sc.tau[j])};
-        auto* rp = reinterpret_cast<RowPack<float>*>(img + pk.o_rp32) + r0;
-        for (int32_t i = 0; i < m; ++i)
-            rp[i] = RowPack<float>{static_cast<float>(sc.sigma[i]), static_cast<float>(sc.rl[i]),
-                                   static_cast<float>(sc.ru[i]), static_cast<float>(sc.row_type[i])};
     }
-    auto* cp64 = reinterpret_cast<ColPack<double>*>(img + pk.o_cp64) + c0;
-    for (int32_t j = 0; j < n; ++j) cp64[j] = ColPack<double>{sc.c[j], sc.cl[j], sc.cu[j], sc.tau[j]};
-    auto* rp64 = reinterpret_cast<RowPack<double>*>(img + pk.o_rp64) + r0;
-    for (int32_t i = 0; i < m; ++i)
-        rp64[i] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
-    auto put = [&](size_t off, int64_t at, const std::vector<double>& v) {
-        if (!v.empty()) std::memcpy(D(off) + at, v.data(), 8 * v.size());
-    };
-    put(pk.o_c, c0, sc.c);
-    put(pk.o_lb, c0, sc.cl);
-    put(pk.o_ub, c0, sc.cu);
-    put(pk.o_cs, c0, sc.col_scale);
-    put(pk.o_tau, c0, sc.tau);
-    put(pk.o_rl, r0, sc.rl);
-    put(pk.o_ru, r0, sc.ru);
-    put(pk.o_rs, r0, sc.row_scale);
-    put(pk.o_sig, r0, sc.sigma);
-    // power-iteration start vector: mt19937(42) normals, normalised (pdlp.cpp:1990-2001)
+    // tiles: (LP, mode, first, end) -- padded tiles are whole
+    const int initial_mode = pk.mixed ? kModeFp32 : kModeFp64;
+    const int tp = rowsPerBlock(it.shapeP), td = rowsPerBlock(it.shapeD);
+    for (int k = 0; k < it.nct; ++k)
+        reinterpret_cast<int4*>(img + pk.o_ctinfo)[it.ct0 + k] =
+            make_int4(it.l, initial_mode, static_cast<int>(c0 + int64_t(k) * tp), static_cast<int>(c0 + int64_t(k + 1) * tp));
+    for (int k = 0; k < it.nrt; ++k)
+        reinterpret_cast<int4*>(img + pk.o_rtinfo)[it.rt0 + k] =
+            make_int4(it.l, initial_mode, static_cast<int>(r0 + int64_t(k) * td), static_cast<int>(r0 + int64_t(k + 1) * td));
+    reinterpret_cast<int4*>(img + pk.o_lpt)[it.l] = make_int4(it.ct0, it.nct, it.rt0, it.nrt);
+    // power-iteration start vector: mt19937(42) normals, normalised (pdlp.cpp:1990-2001); zero on padding
     {
         double* x0 = D(pk.o_pix) + c0;
         std::mt19937 rng(42);
@@ -737,6 +864,7 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
         xn = std::sqrt(xn);
         if (xn < 1e-15) xn = 1.0;
         for (int32_t j = 0; j < n; ++j) x0[j] /= xn;
+        for (int64_t j = n; j < np; ++j) x0[j] = 0.0;
     }
     // controller constants and initial state (as the single-LP solve)
     DevConst dc{};
@@ -830,23 +958,9 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
 int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::time_point t0, pdlpx_result* results,
                   const std::vector<int>& index, double* const* x_out, double* const* y_out, std::string& err) {
     const int L = pk.L;
-    // positions, tiles
-    for (int l = 0; l < L; ++l) {
-        Item& it = *pk.items[l];
-        it.l = l;
-        it.r0 = pk.M;
-        it.c0 = pk.Nc;
-        it.z0 = pk.Z;
-        pk.M += it.lp.m;
-        pk.Nc += it.lp.n;
-        pk.Z += it.sc.a.nnz();
-        pk.nct += it.nct;
-        pk.nrt += it.nrt;
-    }
+    for (int l = 0; l < L; ++l) pk.items[l]->l = l;
+    pk.place();
     pk.layout();
-    std::vector<char> keep(L, 1);
-    std::vector<int4> ct, rt, lpt;
-    pk.tileLists(keep, ct, rt, lpt);
     bool any_warm = false;
     for (const Item* it : pk.items) any_warm |= it->in->warm_x != nullptr && it->in->warm_y != nullptr;
 
@@ -856,9 +970,6 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
     if (any_warm) std::memset(iters.get(), 0, pk.iter_end - pk.image_end);
     reinterpret_cast<int32_t*>(img.get() + pk.o_aptr)[pk.M] = static_cast<int32_t>(pk.Z);
     reinterpret_cast<int32_t*>(img.get() + pk.o_atptr)[pk.Nc] = static_cast<int32_t>(pk.Z);
-    std::memcpy(img.get() + pk.o_ctiles, ct.data(), sizeof(int4) * ct.size());
-    std::memcpy(img.get() + pk.o_rtiles, rt.data(), sizeof(int4) * rt.size());
-    std::memcpy(img.get() + pk.o_lpt, lpt.data(), sizeof(int4) * lpt.size());
     parallelFor(L, [&](int l) { stageItem(pk, *pk.items[l], o, img.get(), iters.get()); });
 
     PDLPX_BCK(cudaStreamCreateWithFlags(&pk.s, cudaStreamNonBlocking));
@@ -928,7 +1039,8 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
         if (rc != PDLPX_OK) return rc;
     }
-    pk.active_tiles = pk.act_ct + pk.act_rt;
+    std::vector<char> keep(L, 1);
+    std::vector<int> cl, rl;
     int cycles = 0;
     while (true) {
         if (timeUp(t0, o.max_solve_seconds)) break;
@@ -949,15 +1061,15 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
             std::fflush(stdout);
         }
         if (done >= L) break;
-        if (o.batch_compact && live_tiles < (pk.active_tiles * 3) / 5) {
+        if (o.batch_compact && live_tiles < ((pk.live_ct + pk.live_rt) * 3) / 5) {
             for (int l = 0; l < L; ++l) keep[l] = !(h_small[l] & 1);
-            pk.tileLists(keep, ct, rt, lpt);
-            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_ctiles, ct.data(), sizeof(int4) * ct.size(), cudaMemcpyHostToDevice, s));
-            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_rtiles, rt.data(), sizeof(int4) * rt.size(), cudaMemcpyHostToDevice, s));
-            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_lpt, lpt.data(), sizeof(int4) * lpt.size(), cudaMemcpyHostToDevice, s));
+            pk.liveLists(keep, cl, rl);
+            if (!cl.empty())
+                PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_clist, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice, s));
+            if (!rl.empty())
+                PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_rlist, rl.data(), 4 * rl.size(), cudaMemcpyHostToDevice, s));
             int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
             if (rc != PDLPX_OK) return rc;
-            pk.active_tiles = pk.act_ct + pk.act_rt;
         }
     }
     PDLPX_BCK(cudaEventRecord(ev1, s));
@@ -1088,10 +1200,13 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         if (it.trivial) return;
         buildScaled(lp, o, it.sc);
         const int64_t z = it.sc.a.nnz();
-        it.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, z, lp.n);
-        it.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, z, lp.m);
-        it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + rowsPerBlock(it.shapeP) - 1) / rowsPerBlock(it.shapeP));
-        it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + rowsPerBlock(it.shapeD) - 1) / rowsPerBlock(it.shapeD));
+        it.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, z, lp.n, true);
+        it.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, z, lp.m, true);
+        const int tp = rowsPerBlock(it.shapeP), td = rowsPerBlock(it.shapeD);
+        it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + tp - 1) / tp);
+        it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + td - 1) / td);
+        it.np = static_cast<int64_t>(it.nct) * tp;
+        it.mp = static_cast<int64_t>(it.nrt) * td;
         it.bytes = itemBytes(it, mixed);
     });
     for (int k = 0; k < count; ++k)
@@ -1142,12 +1257,12 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         int64_t m = 0, n = 0, z = 0, tiles = 0;
         while (pos < dev_items.size()) {
             Item& it = items[dev_items[pos]];
-            const bool fits = bytes + it.bytes <= budget && m + it.lp.m < lim32 && n + it.lp.n < lim32 &&
+            const bool fits = bytes + it.bytes <= budget && m + it.mp < lim32 && n + it.np < lim32 &&
                               z + it.sc.a.nnz() < lim32 && tiles + it.nct + it.nrt < lim32;
             if (!fits && !pk.items.empty()) break;
             bytes += it.bytes;
-            m += it.lp.m;
-            n += it.lp.n;
+            m += it.mp;
+            n += it.np;
             z += it.sc.a.nnz();
             tiles += it.nct + it.nrt;
             pk.items.push_back(&it);

@@ -338,42 +338,51 @@ constexpr StepShape kShapes[] = {
 };
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
+// Row pointers of the R rows j0 + r * slab below jend handled by one G-lane
+// group (b = e = 0 past the end).
+template <int G, int R>
+__device__ __forceinline__ void rowBounds(const int* __restrict__ ptr, int j0, int jend, int (&b)[R], int (&e)[R]) {
+    constexpr int slab = kBlock / G;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + r * slab;
+        b[r] = 0;
+        e[r] = 0;
+        if (j < jend) {
+            b[r] = ptr[j];
+            e[r] = ptr[j + 1];
+        }
+    }
+}
+
 // Fused A^T y_cur + Halpern primal step (pdlp_kernels.cu:46-88 around a fused
-// SpMV).  All loads of the R columns -- row pointers, packed constants,
+// SpMV) of the columns j0 + r * slab (r < R) below jend, with their A^T row
+// bounds already loaded.  All loads of the R columns -- packed constants,
 // current / anchor x, then the A^T row entries and the y gathers -- are issued
 // before the solver state is consulted, so their latencies overlap.  The step
 // arithmetic is FP64 whatever the storage type (same association as the
 // reference: tau = step * tau_base / omega), results are rounded once on store.
-// primalRows handles the columns j0 + r * slab (r < R) below jend; the
-// single-LP kernel covers [0, n), the batched kernel one tile of one LP.
 template <int G, int R, int U, class T>
-__device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jend, int koff) {
+__device__ __forceinline__ void primalRowsFrom(const IterArgs<T>& p, int j0, int jend, const int (&b)[R],
+                                               const int (&e)[R], int koff) {
     constexpr int slab = kBlock / G;
     const int lane = threadIdx.x % G;
-    const int* __restrict__ ptr = p.at_ptr;
     const ColPack<T>* __restrict__ cp = p.cp;
     const double* __restrict__ xcp = p.xc;
     const T* __restrict__ xip = p.xi;
-    int b[R], e[R];
     ColPack<T> q[R];
     double xc[R];
     T xi[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + r * slab;
-        b[r] = 0;
-        e[r] = 0;
         q[r] = ColPack<T>{T(0), T(0), T(0), T(0)};
         xc[r] = 0.0;
         xi[r] = T(0);
-        if (j < jend) {
-            b[r] = ptr[j];
-            e[r] = ptr[j + 1];
-            if (lane == 0) {
-                q[r] = cp[j];
-                xc[r] = xcp[j];
-                xi[r] = xip[j];
-            }
+        if (j < jend && lane == 0) {
+            q[r] = cp[j];
+            xc[r] = xcp[j];
+            xi[r] = xip[j];
         }
     }
     double s[R];
@@ -403,6 +412,15 @@ __device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jen
     }
 }
 
+// primalRows handles the columns j0 + r * slab (r < R) below jend; the
+// single-LP kernel covers [0, n), the batched kernel one tile of one LP.
+template <int G, int R, int U, class T>
+__device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jend, int koff) {
+    int b[R], e[R];
+    rowBounds<G, R>(p.at_ptr, j0, jend, b, e);
+    primalRowsFrom<G, R, U, T>(p, j0, jend, b, e, koff);
+}
+
 template <int G, int R, int U, class T>
 __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
     constexpr int slab = kBlock / G;
@@ -411,33 +429,26 @@ __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
 
 // Fused A x_refl + dual proximal step (pdlp_kernels.cu:94-157), same structure.
 template <int G, int R, int U, class T>
-__device__ __forceinline__ void dualRows(const IterArgs<T>& p, int i0, int iend, int koff) {
+__device__ __forceinline__ void dualRowsFrom(const IterArgs<T>& p, int i0, int iend, const int (&b)[R],
+                                             const int (&e)[R], int koff) {
     constexpr int slab = kBlock / G;
     const int lane = threadIdx.x % G;
-    const int* __restrict__ ptr = p.a_ptr;
     const RowPack<T>* __restrict__ rp = p.rp;
     const double* __restrict__ ycp = p.yc;
     const T* __restrict__ yip = p.yi;
-    int b[R], e[R];
     RowPack<T> q[R];
     double yc[R];
     T yi[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = i0 + r * slab;
-        b[r] = 0;
-        e[r] = 0;
         q[r] = RowPack<T>{T(0), T(0), T(0), T(0)};
         yc[r] = 0.0;
         yi[r] = T(0);
-        if (i < iend) {
-            b[r] = ptr[i];
-            e[r] = ptr[i + 1];
-            if (lane == 0) {
-                q[r] = rp[i];
-                yc[r] = ycp[i];
-                yi[r] = yip[i];
-            }
+        if (i < iend && lane == 0) {
+            q[r] = rp[i];
+            yc[r] = ycp[i];
+            yi[r] = yip[i];
         }
     }
     double s[R];
@@ -480,6 +491,13 @@ __device__ __forceinline__ void dualRows(const IterArgs<T>& p, int i0, int iend,
         p.yc[i] = lam * yr + (1.0 - lam) * yid;
         if (last) p.yh[i] = static_cast<T>(py);
     }
+}
+
+template <int G, int R, int U, class T>
+__device__ __forceinline__ void dualRows(const IterArgs<T>& p, int i0, int iend, int koff) {
+    int b[R], e[R];
+    rowBounds<G, R>(p.a_ptr, i0, iend, b, e);
+    dualRowsFrom<G, R, U, T>(p, i0, iend, b, e, koff);
 }
 
 template <int G, int R, int U, class T>

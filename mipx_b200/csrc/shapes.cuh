@@ -65,6 +65,20 @@ inline int defaultShape(int64_t nnz, int32_t rows) {
     return 11;                   // G=64
 }
 
+// Default step shape of the packed batch: two rows per lane group so that a
+// block of a latency-bound tile keeps twice the loads in flight (measured on
+// B200 with 512 lognormal-sized LPs: 4 lanes x 2 rows for mean row lengths 8
+// and 20 beat the single-LP table's 4 x 1 and 8 x 1 by 20-30%).
+inline int batchShape(int64_t nnz, int32_t rows) {
+    const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
+    if (mean <= 3) return 1;     // G=1, R=2
+    if (mean <= 6) return 4;     // G=2, R=2
+    if (mean <= 24) return 6;    // G=4, R=2
+    if (mean <= 48) return 8;    // G=16
+    if (mean <= 128) return 9;   // G=32
+    return 11;                   // G=64
+}
+
 inline int shapeForGroup(int G) {
     for (int i = 0; i < kNumShapes; ++i)
         if (kShapes[i].G == G && kShapes[i].R == 1) return i;
@@ -73,13 +87,13 @@ inline int shapeForGroup(int G) {
 
 // Step shape of one matrix side from the options: a pinned shape index, else a
 // forced lane count, else the row-length table.
-inline int chooseShape(int pinned, int group, int64_t nnz, int32_t rows) {
+inline int chooseShape(int pinned, int group, int64_t nnz, int32_t rows, bool batch = false) {
     if (pinned > 0 && pinned <= kNumShapes) return pinned - 1;
     if (group > 0) {
         const int s = shapeForGroup(group);
         if (s >= 0) return s;
     }
-    return defaultShape(nnz, rows);
+    return batch ? batchShape(nnz, rows) : defaultShape(nnz, rows);
 }
 
 }  // namespace pdlpx
