@@ -124,7 +124,10 @@ typedef struct pdlpx_options {
                                          split into packs solved one after another */
     int32_t batch_compact;            /* pdlpx_batch_solve: 1 (default) drops finished LPs from the
                                          launches once they idle enough tiles; 0 never */
-    int32_t reserved[3];
+    int32_t batch_sell;               /* pdlpx_batch_solve: 1 (default) stores matrix sides with mean row
+                                         length <= 32 as sliced ELL (32-row slices, column-major, rows
+                                         sorted by length inside each 256-row tile); 0 keeps CSR */
+    int32_t reserved[2];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

@@ -7,21 +7,32 @@
 // tall as one block of the LP's launch shape covers; padded rows and columns
 // are empty, free and zero, and add nothing to any check term), and LPs with
 // the same launch shape are contiguous.  A step-kernel block therefore knows
-// its rows from its index alone; it loads the row pointers and its tile's
-// (LP, mode) word together, then runs the single-LP row bodies
-// (primalRowsFrom / dualRowsFrom) in the LP's current precision with the LP's
-// own step size, primal weight and Halpern count -- the same three dependent
-// load steps as the single-LP kernels.  LPs restart, switch precision, polish
-// and finish independently: per-LP DevState / DevConst, and the single-LP
-// controlStep run by one warp per LP over the LP's tile partials in fixed
-// order.  A restart cycle of the whole pack -- N iterations, the FP64 check, the
-// controllers, restart copies, FP32 -> FP64 hand-overs and the tile modes -- is
-// one CUDA graph launch.  When finished LPs leave enough tiles idle, the host
-// switches the launches to a list of the live tiles and captures a smaller graph.
+// its rows from its index alone; it loads its tile's (LP, mode) word beside
+// the first matrix loads, then runs the step in the LP's current precision
+// with the LP's own step size, primal weight and Halpern count.
 //
-// An LP's tiles, launch shape and reduction order depend on that LP alone, so
-// its result is bit-identical alone and in any mix (batch invariance).  A batch
-// larger than the device budget is split into packs solved one after another.
+// Matrix sides with short rows (mean <= 32 entries) are stored as sliced ELL:
+// 32-row slices, entries column-major inside a slice and padded to the
+// slice's longest row, so a warp's load of the k-th entries of its 32 rows is
+// one coalesced 128-byte (FP32) request and every thread owns one row; the
+// rows of each 256-row tile are renumbered longest first (stable) so a slice's
+// rows have similar lengths.  The renumbering is a relabelling of the LP's
+// variables and constraints, undone when the results are read back.  Long
+// rows keep CSR with a G-lane group per row.  The FP64 check pass and the
+// power iteration read CSR.
+//
+// LPs restart, switch precision, polish and finish independently: per-LP
+// DevState / DevConst, and the single-LP controlStep run by one warp per LP
+// over the LP's tile partials in fixed order.  A restart cycle of the whole
+// pack -- N iterations, the FP64 check, the controllers, restart copies, FP32
+// -> FP64 hand-overs and the tile modes -- is one CUDA graph launch.  When
+// finished LPs leave enough tiles idle, the host switches the launches to a
+// list of the live tiles and captures a smaller graph.
+//
+// An LP's tiles, launch shape, storage and reduction order depend on that LP
+// alone, so its result is bit-identical alone and in any mix (batch
+// invariance).  A batch larger than the device budget is split into packs
+// solved one after another.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -30,6 +41,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <numeric>
 #include <random>
 #include <thread>
 #include <vector>
@@ -45,11 +57,35 @@ namespace {
 // Tile modes (the .y of a tile's info word), refreshed at the end of every cycle.
 constexpr int kModeFp32 = 0, kModeFp64 = 1, kModeIdle = 2;
 
+// Sliced-ELL launch shapes follow the kNumShapes CSR shapes: entries per lane
+// per round U, one row per thread, kBlock rows per tile.
+constexpr int kSellU[] = {4, 8, 16};
+constexpr int kNumSell = 3;
+constexpr int kSlice = 32;  // rows per slice (one warp)
+
+__host__ __device__ constexpr bool isSell(int shape) { return shape >= kNumShapes; }
+// Rows one tile of a launch shape covers.
+inline int tileRows(int shape) { return isSell(shape) ? kBlock : rowsPerBlock(shape); }
+// Lanes per row of the CSR check and power kernels on that shape's tiles.
+inline int checkGroup(int shape) {
+    return isSell(shape) ? (kSellU[shape - kNumShapes] <= 4 ? 2 : (kSellU[shape - kNumShapes] <= 8 ? 4 : 8))
+                         : kShapes[shape].G;
+}
+
+struct SellSide {
+    const int2* hdr;  // per slice: first entry, entries per row (global slice = row / 32)
+    const int* idx;
+    const float* v32;
+    const double* v64;
+};
+
 struct PackArgs {
     IterArgs<float> it32;  // global arrays of the pack (st is set per tile)
     IterArgs<double> it64;
     CheckArgs<float> ck32;
     CheckArgs<double> ck64;
+    SellSide cs;         // A^T rows (primal step) of sliced-ELL shapes
+    SellSide rs;         // A rows (dual step)
     int4* ctinfo;        // column tiles: (LP, mode, first column, end column)
     int4* rtinfo;        // row tiles
     const int* clist;    // live column / row tile ids after compaction
@@ -72,11 +108,15 @@ struct PackArgs {
 
 constexpr int kCtlWarps = 4;  // LPs per block of the per-LP kernels
 
-// Resident blocks per SM the step kernels are compiled for: the tiles are
+// Resident blocks per SM the CSR step kernels are compiled for: the tiles are
 // latency-bound, and 5 blocks (48 registers) measured faster than 3-4 blocks
 // (the compiler's own pick, 64-72 registers) and than 8 blocks with spills.
 #ifndef PDLPX_PACK_MIN_BLOCKS
 #define PDLPX_PACK_MIN_BLOCKS 5
+#endif
+// Same for the sliced-ELL step kernels.
+#ifndef PDLPX_SELL_MIN_BLOCKS
+#define PDLPX_SELL_MIN_BLOCKS 4
 #endif
 
 __device__ __forceinline__ double combine(int op, double a, double b) {
@@ -101,7 +141,7 @@ __device__ __forceinline__ void warpTiles(const double* part, int first, int cou
         for (int off = 16; off > 0; off >>= 1) out[s] = combine(ops[s], out[s], __shfl_xor_sync(0xffffffffu, out[s], off));
 }
 
-// ---- PDHG step over one tile ------------------------------------------------
+// ---- PDHG step over one CSR tile --------------------------------------------
 // A launch covers the tiles [tile0, tile0 + grid) of one shape whose rows start
 // at `base` (direct), or the live tiles list[list0 + b] of that shape (IND).
 template <int G, int R, int U, bool IND>
@@ -147,6 +187,104 @@ __global__ void __launch_bounds__(kBlock, PDLPX_PACK_MIN_BLOCKS)
         IterArgs<double> p = a.it64;
         p.st = st;
         dualRowsFrom<G, R, U, double>(p, i0, r0 + TR, b, e, koff);
+    }
+}
+
+// ---- PDHG step over one sliced-ELL tile -------------------------------------
+// Dot product of this thread's row with x: entry k of the row sits at
+// hdr.x + k * 32 + lane; U entries are loaded per round, then their U gathers,
+// then the products are summed in entry order.
+// Entries past the row's end hold index 0 and value 0 (index 0 always exists).
+template <int U, class V, class X>
+__device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* __restrict__ val, int2 h, int lane,
+                                          const X* __restrict__ x) {
+    const int* ip = idx + h.x + lane;
+    const V* vp = val + h.x + lane;
+    double acc = 0.0;
+    for (int k0 = 0; k0 < h.y; k0 += U) {
+        int c[U];
+        V v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            const bool ok = k < h.y;
+            c[u] = ok ? __ldg(ip + k * kSlice) : 0;
+            v[u] = ok ? __ldg(vp + k * kSlice) : V(0);
+        }
+        X g[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) g[u] = __ldg(x + c[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc += static_cast<double>(v[u]) * static_cast<double>(g[u]);
+    }
+    return acc;
+}
+
+template <int U, class T>
+__device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
+                                               int koff) {
+    const ColPack<T> q = p.cp[j];
+    const double xc = p.xc[j];
+    const double xi = static_cast<double>(p.xi[j]);
+    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+    primalUpdate<T>(p, j, q, xc, xi, s, step, pw, lam, last);
+}
+
+template <int U, class T>
+__device__ __forceinline__ void dualSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int i, int2 h,
+                                             int koff) {
+    const RowPack<T> q = p.rp[i];
+    const double yc = p.yc[i];
+    const double yi = static_cast<double>(p.yi[i]);
+    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+    dualUpdate<T>(p, i, q, yc, yi, s, step, pw, lam, last);
+}
+
+template <int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packPrimalSell(PackArgs a, int tile0, int base, int list0, int koff) {
+    const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int j = base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x);
+    const int2 h = a.cs.hdr[j / kSlice];
+    const int4 info = a.ctinfo[tile];
+    if (info.y == kModeIdle) return;
+    DevState* st = a.st + info.x;
+    if (info.y == kModeFp32) {
+        IterArgs<float> p = a.it32;
+        p.st = st;
+        primalSellFrom<U, float>(p, a.cs.idx, a.cs.v32, j, h, koff);
+    } else {
+        IterArgs<double> p = a.it64;
+        p.st = st;
+        primalSellFrom<U, double>(p, a.cs.idx, a.cs.v64, j, h, koff);
+    }
+}
+
+template <int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packDualSell(PackArgs a, int tile0, int base, int list0, int koff) {
+    const int tile = IND ? a.rlist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    const int i = base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x);
+    const int2 h = a.rs.hdr[i / kSlice];
+    const int4 info = a.rtinfo[tile];
+    if (info.y == kModeIdle) return;
+    DevState* st = a.st + info.x;
+    if (info.y == kModeFp32) {
+        IterArgs<float> p = a.it32;
+        p.st = st;
+        dualSellFrom<U, float>(p, a.rs.idx, a.rs.v32, i, h, koff);
+    } else {
+        IterArgs<double> p = a.it64;
+        p.st = st;
+        dualSellFrom<U, double>(p, a.rs.idx, a.rs.v64, i, h, koff);
     }
 }
 
@@ -386,6 +524,44 @@ __global__ void packInitStep(PackArgs a) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+
+// One side of an LP in its pack numbering: new position -> original row
+// (order), original row -> new position (pos), and for sliced-ELL sides the
+// per-slice row lengths.
+struct SideOrder {
+    std::vector<int32_t> order, pos;
+    std::vector<int32_t> slice_len;
+    int64_t entries = 0;  // sliced-ELL entries (padded)
+};
+
+// Renumbering of `rows` CSR rows padded to `padded`: identity for CSR sides;
+// for sliced-ELL sides, rows sorted by length (longest first, stable) inside
+// each tile of `tile` rows, then the slice lengths.
+void orderSide(const std::vector<int32_t>& ptr, int32_t rows, int64_t padded, int tile, bool sell, SideOrder& so) {
+    so.order.resize(rows);
+    std::iota(so.order.begin(), so.order.end(), 0);
+    if (sell) {
+        for (int32_t t0 = 0; t0 < rows; t0 += tile) {
+            const int32_t t1 = std::min<int32_t>(rows, t0 + tile);
+            std::stable_sort(so.order.begin() + t0, so.order.begin() + t1, [&](int32_t a, int32_t b) {
+                return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
+            });
+        }
+        const int64_t slices = padded / kSlice;
+        so.slice_len.assign(slices, 0);
+        so.entries = 0;
+        for (int64_t s = 0; s < slices; ++s) {
+            int32_t len = 0;
+            for (int64_t r = s * kSlice; r < std::min<int64_t>(rows, (s + 1) * kSlice); ++r)
+                len = std::max(len, ptr[so.order[r] + 1] - ptr[so.order[r]]);
+            so.slice_len[s] = len;
+            so.entries += static_cast<int64_t>(len) * kSlice;
+        }
+    }
+    so.pos.resize(rows);
+    for (int32_t k = 0; k < rows; ++k) so.pos[so.order[k]] = k;
+}
+
 struct Item {
     const pdlpx_lp* in = nullptr;
     HostLp lp;
@@ -394,10 +570,12 @@ struct Item {
     int shapeP = 0, shapeD = 0;
     int nct = 0, nrt = 0;      // tiles
     int64_t np = 0, mp = 0;    // columns / rows padded to whole tiles
+    SideOrder cols, rows;      // renumbering of columns (A^T rows) and rows
     size_t bytes = 0;          // share of a pack's device image
     // position within its pack
     int64_t r0 = 0, c0 = 0;    // first row, first column
     int64_t za = 0, zt = 0;    // first entry of A / of A^T
+    int64_t ec = 0, er = 0;    // first sliced-ELL entry of A^T / of A
     int ct0 = 0, rt0 = 0;      // first column tile, first row tile
     int l = 0;
 };
@@ -410,6 +588,7 @@ size_t itemBytes(const Item& it, bool mixed) {
     size_t b = 4 * (m + n) + z * (8 + 16 + (mixed ? 8 : 0));           // pointers, indices, values
     b += n * (32 + 40 + 8 + 24 + 24) + m * (32 + 32 + 8 + 16 + 8);     // packs, checks, FP64 iterates, power
     if (mixed) b += n * (16 + 12) + m * (16 + 8);
+    b += static_cast<size_t>(it.cols.entries + it.rows.entries) * (4 + 8 + (mixed ? 4 : 0)) + (m + n) / 4;
     b += static_cast<size_t>(it.nct) * (16 + 4 + 8 * kColSlots + 16) + static_cast<size_t>(it.nrt) * (16 + 4 + 8 * kRowSlots);
     b += sizeof(DevState) + sizeof(DevConst) + sizeof(PowerState) + 32;
     return b;
@@ -441,6 +620,13 @@ void parallelFor(int count, F&& f) {
         }                                                                            \
     } while (0)
 
+#define PDLPX_SELL_SWITCH(S, CALL)                                   \
+    switch (S - kNumShapes) {                                        \
+        case 0: { constexpr int UU = kSellU[0]; CALL; } break;       \
+        case 1: { constexpr int UU = kSellU[1]; CALL; } break;       \
+        default: { constexpr int UU = kSellU[2]; CALL; } break;      \
+    }
+
 // One launch of a step / check kernel: the tiles of one shape class, all of them
 // (list0 < 0: tiles [tile0, tile0 + count) from row `base`) or `count` live ones
 // listed from list0.
@@ -448,15 +634,27 @@ struct Launch {
     int shape, tile0, base, count, list0;
 };
 
+// Shapes in placement order: sliced-ELL classes first (their rows start at 0
+// and stay aligned to whole slices), then the CSR classes.
+std::vector<int> placementOrder() {
+    std::vector<int> v;
+    for (int s = 0; s < kNumSell; ++s) v.push_back(kNumShapes + s);
+    for (int s = 0; s < kNumShapes; ++s) v.push_back(s);
+    return v;
+}
+
 // Device image and graphs of one pack.
 struct Pack {
     std::vector<Item*> items;
     bool mixed = true;
     int L = 0;
     int64_t M = 0, Nc = 0, Z = 0;  // padded rows, padded columns, entries
+    int64_t Ec = 0, Er = 0;        // sliced-ELL entries of A^T / A
+    int64_t Sc = 0, Sr = 0;        // slices (sliced-ELL prefix of the columns / rows, / 32)
     int nct = 0, nrt = 0;          // all tiles
     // arena layout
     size_t o_aptr, o_aidx, o_atptr, o_atidx, o_av32, o_atv32, o_av64, o_atv64, o_cp32, o_rp32, o_cp64, o_rp64;
+    size_t o_chdr, o_cidx, o_cv32, o_cv64, o_rhdr, o_ridx, o_rv32, o_rv64;
     size_t o_c, o_lb, o_ub, o_cs, o_tau, o_rl, o_ru, o_rs, o_sig;
     size_t o_st, o_dc, o_ps, o_ctinfo, o_rtinfo, o_lpt;
     size_t image_end;  // [0, image_end) is uploaded from the host image
@@ -485,28 +683,33 @@ struct Pack {
     // within a shape; each LP padded to whole tiles.
     void place() {
         for (int side = 0; side < 2; ++side) {
-            int64_t pos = 0, z = 0;
+            int64_t pos = 0, z = 0, ent = 0, sell_rows = 0;
             int tiles = 0;
             std::vector<Launch>& cls = side == 0 ? cls_c : cls_r;
-            for (int shape = 0; shape < kNumShapes; ++shape) {
+            for (int shape : placementOrder()) {
                 Launch c{shape, tiles, static_cast<int>(pos), 0, -1};
                 for (Item* it : items) {
                     if ((side == 0 ? it->shapeP : it->shapeD) != shape) continue;
                     if (side == 0) {
                         it->c0 = pos;
                         it->zt = z;
+                        it->ec = ent;
                         it->ct0 = tiles;
                         pos += it->np;
                         tiles += it->nct;
+                        ent += it->cols.entries;
                     } else {
                         it->r0 = pos;
                         it->za = z;
+                        it->er = ent;
                         it->rt0 = tiles;
                         pos += it->mp;
                         tiles += it->nrt;
+                        ent += it->rows.entries;
                     }
                     z += it->sc.a.nnz();
                 }
+                if (isSell(shape)) sell_rows = pos;
                 c.count = tiles - c.tile0;
                 if (c.count > 0) cls.push_back(c);
             }
@@ -514,9 +717,13 @@ struct Pack {
                 Nc = pos;
                 nct = tiles;
                 Z = z;
+                Ec = ent;
+                Sc = sell_rows / kSlice;
             } else {
                 M = pos;
                 nrt = tiles;
+                Er = ent;
+                Sr = sell_rows / kSlice;
             }
         }
         lc = cls_c;
@@ -542,6 +749,14 @@ struct Pack {
         o_atv32 = mixed ? take(4 * z) : 0;
         o_av64 = take(8 * z);
         o_atv64 = take(8 * z);
+        o_chdr = take(8 * static_cast<size_t>(std::max<int64_t>(Sc, 1)));
+        o_cidx = take(4 * static_cast<size_t>(Ec));
+        o_cv32 = mixed ? take(4 * static_cast<size_t>(Ec)) : 0;
+        o_cv64 = take(8 * static_cast<size_t>(Ec));
+        o_rhdr = take(8 * static_cast<size_t>(std::max<int64_t>(Sr, 1)));
+        o_ridx = take(4 * static_cast<size_t>(Er));
+        o_rv32 = mixed ? take(4 * static_cast<size_t>(Er)) : 0;
+        o_rv64 = take(8 * static_cast<size_t>(Er));
         o_cp32 = mixed ? take(16 * n) : 0;
         o_rp32 = mixed ? take(16 * m) : 0;
         o_cp64 = take(32 * n);
@@ -655,6 +870,8 @@ struct Pack {
         };
         fillCheck(a.ck64, a.it64);
         if (mixed) fillCheck(a.ck32, a.it32);
+        a.cs = SellSide{P<int2>(o_chdr), P<int>(o_cidx), mixed ? P<float>(o_cv32) : nullptr, P<double>(o_cv64)};
+        a.rs = SellSide{P<int2>(o_rhdr), P<int>(o_ridx), mixed ? P<float>(o_rv32) : nullptr, P<double>(o_rv64)};
         a.ctinfo = P<int4>(o_ctinfo);
         a.rtinfo = P<int4>(o_rtinfo);
         a.clist = P<int>(o_clist);
@@ -705,40 +922,62 @@ struct Pack {
         live_rt = static_cast<int>(rl.size());
     }
 
+    void launchPrimal(const Launch& c, int k) {
+        const PackArgs& a = args;
+        if (isSell(c.shape)) {
+            if (listed) {
+                PDLPX_SELL_SWITCH(c.shape, (packPrimalSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+            } else {
+                PDLPX_SELL_SWITCH(c.shape, (packPrimalSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+            }
+        } else if (listed) {
+            PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+        } else {
+            PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+        }
+    }
+
+    void launchDual(const Launch& c, int k) {
+        const PackArgs& a = args;
+        if (isSell(c.shape)) {
+            if (listed) {
+                PDLPX_SELL_SWITCH(c.shape, (packDualSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+            } else {
+                PDLPX_SELL_SWITCH(c.shape, (packDualSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+            }
+        } else if (listed) {
+            PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+        } else {
+            PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+        }
+    }
+
     int launchCycle(int N) {
         int n = 0;
         const PackArgs& a = args;
         for (int k = 1; k <= N; ++k) {
             for (const Launch& c : lc) {
-                if (listed) {
-                    PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
-                } else {
-                    PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
-                }
+                launchPrimal(c, k);
                 ++n;
             }
             for (const Launch& c : lr) {
-                if (listed) {
-                    PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
-                } else {
-                    PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
-                }
+                launchDual(c, k);
                 ++n;
             }
         }
         for (const Launch& c : lr) {
             if (listed) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packCheckRows<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
             } else {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckRows<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packCheckRows<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
             }
             ++n;
         }
         for (const Launch& c : lc) {
             if (listed) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packCheckCols<GG, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.list0)));
             } else {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packCheckCols<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packCheckCols<GG, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, 0)));
             }
             ++n;
         }
@@ -754,11 +993,11 @@ struct Pack {
         const PackArgs& a = args;
         for (int it = 0; it < chunk; ++it) {
             for (const Launch& c : cls_r) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerA<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packPowerA<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
                 ++n;
             }
             for (const Launch& c : cls_c) {
-                PDLPX_G_SWITCH(kShapes[c.shape].G, (packPowerAt<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
+                PDLPX_G_SWITCH(checkGroup(c.shape), (packPowerAt<GG><<<c.count, kBlock, 0, s>>>(a, c.tile0)));
                 ++n;
             }
             packPowerFinish1<<<(L + kCtlWarps - 1) / kCtlWarps, 32 * kCtlWarps, 0, s>>>(a);
@@ -770,47 +1009,90 @@ struct Pack {
     }
 };
 
-// Host image of one LP's share of the pack (its padded rows and columns included).
+// Host image of one LP's share of the pack, in the pack numbering (renumbered
+// sides, padded rows and columns included).
 void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img, char* iters) {
     const ScaledLp& sc = it.sc;
-    const int32_t m = it.lp.m, n = it.lp.n, z = sc.a.nnz();
+    const int32_t m = it.lp.m, n = it.lp.n;
     const int64_t r0 = it.r0, c0 = it.c0, za = it.za, zt = it.zt, mp = it.mp, np = it.np;
+    const SideOrder& co = it.cols;
+    const SideOrder& ro = it.rows;
     const double inf = std::numeric_limits<double>::infinity();
     auto I = [&](size_t off) { return reinterpret_cast<int32_t*>(img + off); };
     auto F = [&](size_t off) { return reinterpret_cast<float*>(img + off); };
     auto D = [&](size_t off) { return reinterpret_cast<double*>(img + off); };
-    int32_t* aptr = I(pk.o_aptr) + r0;
-    for (int64_t i = 0; i < mp; ++i) aptr[i] = static_cast<int32_t>(za + sc.a.ptr[std::min<int64_t>(i, m)]);
-    int32_t* atptr = I(pk.o_atptr) + c0;
-    for (int64_t j = 0; j < np; ++j) atptr[j] = static_cast<int32_t>(zt + sc.at.ptr[std::min<int64_t>(j, n)]);
-    int32_t* aidx = I(pk.o_aidx) + za;
-    int32_t* atidx = I(pk.o_atidx) + zt;
-    for (int32_t k = 0; k < z; ++k) {
-        aidx[k] = static_cast<int32_t>(c0 + sc.a.idx[k]);
-        atidx[k] = static_cast<int32_t>(r0 + sc.at.idx[k]);
+    // CSR of A (rows in pack order, columns renumbered) and of A^T; an entry keeps
+    // its place inside its row
+    {
+        int32_t* ptr = I(pk.o_aptr) + r0;
+        int32_t* idx = I(pk.o_aidx) + za;
+        double* v64 = D(pk.o_av64) + za;
+        float* v32 = pk.mixed ? F(pk.o_av32) + za : nullptr;
+        int64_t k = 0;
+        for (int64_t i = 0; i < mp; ++i) {
+            ptr[i] = static_cast<int32_t>(za + k);
+            if (i >= m) continue;
+            const int32_t old = ro.order[i];
+            for (int32_t q = sc.a.ptr[old]; q < sc.a.ptr[old + 1]; ++q, ++k) {
+                idx[k] = static_cast<int32_t>(c0 + co.pos[sc.a.idx[q]]);
+                v64[k] = sc.a.val[q];
+                if (v32) v32[k] = static_cast<float>(sc.a.val[q]);
+            }
+        }
     }
-    std::memcpy(D(pk.o_av64) + za, sc.a.val.data(), 8 * static_cast<size_t>(z));
-    std::memcpy(D(pk.o_atv64) + zt, sc.at.val.data(), 8 * static_cast<size_t>(z));
-    // padding: empty, free rows and columns with zero cost and unit scales
-    auto col = [&](int64_t j, double& c, double& lb, double& ub, double& tau, double& cs) {
-        const bool real = j < n;
-        c = real ? sc.c[j] : 0.0;
-        lb = real ? sc.cl[j] : -inf;
-        ub = real ? sc.cu[j] : inf;
-        tau = real ? sc.tau[j] : 1.0;
-        cs = real ? sc.col_scale[j] : 1.0;
+    {
+        int32_t* ptr = I(pk.o_atptr) + c0;
+        int32_t* idx = I(pk.o_atidx) + zt;
+        double* v64 = D(pk.o_atv64) + zt;
+        float* v32 = pk.mixed ? F(pk.o_atv32) + zt : nullptr;
+        int64_t k = 0;
+        for (int64_t j = 0; j < np; ++j) {
+            ptr[j] = static_cast<int32_t>(zt + k);
+            if (j >= n) continue;
+            const int32_t old = co.order[j];
+            for (int32_t q = sc.at.ptr[old]; q < sc.at.ptr[old + 1]; ++q, ++k) {
+                idx[k] = static_cast<int32_t>(r0 + ro.pos[sc.at.idx[q]]);
+                v64[k] = sc.at.val[q];
+                if (v32) v32[k] = static_cast<float>(sc.at.val[q]);
+            }
+        }
+    }
+    // sliced ELL of the renumbered sides that use it: slice s of the LP holds its
+    // rows 32 s .. 32 s + 31, entry k of lane l at first + k * 32 + l
+    auto sell = [&](const SideOrder& so, const Csr& a, const SideOrder& other, int64_t row0, int64_t other0,
+                    int64_t e0, size_t o_hdr, size_t o_idx, size_t o_v32, size_t o_v64) {
+        int2* hdr = reinterpret_cast<int2*>(img + o_hdr) + row0 / kSlice;
+        int32_t* idx = I(o_idx);
+        double* v64 = D(o_v64);
+        float* v32 = pk.mixed ? F(o_v32) : nullptr;
+        int64_t e = e0;
+        const int32_t rows = static_cast<int32_t>(so.order.size());
+        for (size_t s = 0; s < so.slice_len.size(); ++s) {
+            const int32_t len = so.slice_len[s];
+            hdr[s] = make_int2(static_cast<int>(e), len);
+            for (int32_t lane = 0; lane < kSlice; ++lane) {
+                const int64_t r = static_cast<int64_t>(s) * kSlice + lane;
+                const int32_t old = r < rows ? so.order[r] : -1;
+                const int32_t b = old >= 0 ? a.ptr[old] : 0, cnt = old >= 0 ? a.ptr[old + 1] - b : 0;
+                for (int32_t k = 0; k < len; ++k) {
+                    const int64_t at = e + static_cast<int64_t>(k) * kSlice + lane;
+                    const bool real = k < cnt;
+                    idx[at] = static_cast<int32_t>(real ? other0 + other.pos[a.idx[b + k]] : other0);
+                    v64[at] = real ? a.val[b + k] : 0.0;
+                    if (v32) v32[at] = real ? static_cast<float>(a.val[b + k]) : 0.0f;
+                }
+            }
+            e += static_cast<int64_t>(len) * kSlice;
+        }
     };
-    auto row = [&](int64_t i, double& sig, double& rl, double& ru, double& type, double& rs) {
-        const bool real = i < m;
-        sig = real ? sc.sigma[i] : 1.0;
-        rl = real ? sc.rl[i] : -inf;
-        ru = real ? sc.ru[i] : inf;
-        type = real ? static_cast<double>(sc.row_type[i]) : static_cast<double>(kRowRanged);
-        rs = real ? sc.row_scale[i] : 1.0;
-    };
+    if (isSell(it.shapeP)) sell(co, sc.at, ro, c0, r0, it.ec, pk.o_chdr, pk.o_cidx, pk.o_cv32, pk.o_cv64);
+    if (isSell(it.shapeD)) sell(ro, sc.a, co, r0, c0, it.er, pk.o_rhdr, pk.o_ridx, pk.o_rv32, pk.o_rv64);
+    // per-column / per-row constants; padding is empty, free, zero cost, unit scales
     for (int64_t j = 0; j < np; ++j) {
-        double c, lb, ub, tau, cs;
-        col(j, c, lb, ub, tau, cs);
+        const bool real = j < n;
+        const int32_t old = real ? co.order[j] : 0;
+        const double c = real ? sc.c[old] : 0.0, lb = real ? sc.cl[old] : -inf, ub = real ? sc.cu[old] : inf;
+        const double tau = real ? sc.tau[old] : 1.0, cs = real ? sc.col_scale[old] : 1.0;
         reinterpret_cast<ColPack<double>*>(img + pk.o_cp64)[c0 + j] = ColPack<double>{c, lb, ub, tau};
         if (pk.mixed)
             reinterpret_cast<ColPack<float>*>(img + pk.o_cp32)[c0 + j] =
@@ -822,8 +1104,11 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
         D(pk.o_tau)[c0 + j] = tau;
     }
     for (int64_t i = 0; i < mp; ++i) {
-        double sig, rl, ru, type, rs;
-        row(i, sig, rl, ru, type, rs);
+        const bool real = i < m;
+        const int32_t old = real ? ro.order[i] : 0;
+        const double sig = real ? sc.sigma[old] : 1.0, rl = real ? sc.rl[old] : -inf, ru = real ? sc.ru[old] : inf;
+        const double type = real ? static_cast<double>(sc.row_type[old]) : static_cast<double>(kRowRanged);
+        const double rs = real ? sc.row_scale[old] : 1.0;
         reinterpret_cast<RowPack<double>*>(img + pk.o_rp64)[r0 + i] = RowPack<double>{sig, rl, ru, type};
         if (pk.mixed)
             reinterpret_cast<RowPack<float>*>(img + pk.o_rp32)[r0 + i] =
@@ -833,17 +1118,9 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
         D(pk.o_rs)[r0 + i] = rs;
         D(pk.o_sig)[r0 + i] = sig;
     }
-    if (pk.mixed) {
-        float* av = F(pk.o_av32) + za;
-        float* atv = F(pk.o_atv32) + zt;
-        for (int32_t k = 0; k < z; ++k) {
-            av[k] = static_cast<float>(sc.a.val[k]);
-            atv[k] = static_cast<float>(sc.at.val[k]);
-        }
-    }
     // tiles: (LP, mode, first, end) -- padded tiles are whole
     const int initial_mode = pk.mixed ? kModeFp32 : kModeFp64;
-    const int tp = rowsPerBlock(it.shapeP), td = rowsPerBlock(it.shapeD);
+    const int tp = tileRows(it.shapeP), td = tileRows(it.shapeD);
     for (int k = 0; k < it.nct; ++k)
         reinterpret_cast<int4*>(img + pk.o_ctinfo)[it.ct0 + k] =
             make_int4(it.l, initial_mode, static_cast<int>(c0 + int64_t(k) * tp), static_cast<int>(c0 + int64_t(k + 1) * tp));
@@ -851,19 +1128,21 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
         reinterpret_cast<int4*>(img + pk.o_rtinfo)[it.rt0 + k] =
             make_int4(it.l, initial_mode, static_cast<int>(r0 + int64_t(k) * td), static_cast<int>(r0 + int64_t(k + 1) * td));
     reinterpret_cast<int4*>(img + pk.o_lpt)[it.l] = make_int4(it.ct0, it.nct, it.rt0, it.nrt);
-    // power-iteration start vector: mt19937(42) normals, normalised (pdlp.cpp:1990-2001); zero on padding
+    // power-iteration start vector: mt19937(42) normals over the original columns,
+    // normalised (pdlp.cpp:1990-2001), placed in the pack numbering; zero on padding
     {
         double* x0 = D(pk.o_pix) + c0;
+        std::vector<double> g(n);
         std::mt19937 rng(42);
         std::normal_distribution<double> dist(0.0, 1.0);
         double xn = 0.0;
         for (int32_t j = 0; j < n; ++j) {
-            x0[j] = dist(rng);
-            xn += x0[j] * x0[j];
+            g[j] = dist(rng);
+            xn += g[j] * g[j];
         }
         xn = std::sqrt(xn);
         if (xn < 1e-15) xn = 1.0;
-        for (int32_t j = 0; j < n; ++j) x0[j] /= xn;
+        for (int32_t j = 0; j < n; ++j) x0[co.pos[j]] = g[j] / xn;
         for (int64_t j = n; j < np; ++j) x0[j] = 0.0;
     }
     // controller constants and initial state (as the single-LP solve)
@@ -922,10 +1201,11 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
     auto IF = [&](size_t off) { return reinterpret_cast<float*>(iters + (off - pk.image_end)); };
     auto ID = [&](size_t off) { return reinterpret_cast<double*>(iters + (off - pk.image_end)); };
     const bool warm = it.in->warm_x != nullptr && it.in->warm_y != nullptr;
-    std::vector<double> wx(n, 0.0), wy(m, 0.0);
+    std::vector<double> wx(n, 0.0), wy(m, 0.0);  // pack numbering
     if (warm) {
-        for (int32_t j = 0; j < n; ++j) wx[j] = it.in->warm_x[j] / sc.col_scale[j] * sc.con_scale;
-        for (int32_t i = 0; i < m; ++i) wy[i] = it.in->warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+        for (int32_t j = 0; j < n; ++j) wx[co.pos[j]] = it.in->warm_x[j] / sc.col_scale[j] * sc.con_scale;
+        for (int32_t i = 0; i < m; ++i)
+            wy[ro.pos[i]] = it.in->warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
     }
     if (pk.mixed) {
         for (int32_t j = 0; j < n; ++j) {
@@ -1097,9 +1377,15 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         const Item& it = *pk.items[l];
         const DevState& f = fin[l];
         const int32_t m = it.lp.m, n = it.lp.n;
-        std::vector<double> xs(n), ys(m);
-        for (int32_t j = 0; j < n; ++j) xs[j] = f.prec == 0 ? static_cast<double>(fx[it.c0 + j]) : dx[it.c0 + j];
-        for (int32_t i = 0; i < m; ++i) ys[i] = f.prec == 0 ? static_cast<double>(fy[it.r0 + i]) : dy[it.r0 + i];
+        std::vector<double> xs(n), ys(m);  // original numbering
+        for (int32_t j = 0; j < n; ++j) {
+            const int64_t at = it.c0 + it.cols.pos[j];
+            xs[j] = f.prec == 0 ? static_cast<double>(fx[at]) : dx[at];
+        }
+        for (int32_t i = 0; i < m; ++i) {
+            const int64_t at = it.r0 + it.rows.pos[i];
+            ys[i] = f.prec == 0 ? static_cast<double>(fy[at]) : dy[at];
+        }
         int32_t status;
         if (f.done) {
             status = f.status;
@@ -1156,6 +1442,19 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
     return PDLPX_OK;
 }
 
+// Launch shape of one matrix side in the batch: a pinned shape (1..16 CSR,
+// 17..19 sliced ELL with 4 / 8 / 16 entries per round), a forced lane count,
+// sliced ELL for mean row lengths up to 32, else the batch CSR table.
+int batchSideShape(int pinned, int group, bool sell, int64_t nnz, int32_t rows) {
+    if (pinned > kNumShapes && pinned <= kNumShapes + kNumSell) return pinned - 1;
+    if (pinned > 0 || group > 0) return chooseShape(pinned, group, nnz, rows, true);
+    const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
+    // measured on 512 lognormal-sized LPs (mean 8 / 20 entries per column / row):
+    // 4 entries per round on the columns and 8 on the rows beat 8 / 16 by ~30%
+    if (sell && mean <= 32.0) return kNumShapes + (mean <= 8.0 ? 0 : 1);
+    return batchShape(nnz, rows);
+}
+
 }  // namespace
 
 int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
@@ -1200,13 +1499,15 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         if (it.trivial) return;
         buildScaled(lp, o, it.sc);
         const int64_t z = it.sc.a.nnz();
-        it.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, z, lp.n, true);
-        it.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, z, lp.m, true);
-        const int tp = rowsPerBlock(it.shapeP), td = rowsPerBlock(it.shapeD);
+        it.shapeP = batchSideShape(o.shape_primal, o.spmv_group_at, o.batch_sell != 0, z, lp.n);
+        it.shapeD = batchSideShape(o.shape_dual, o.spmv_group_a, o.batch_sell != 0, z, lp.m);
+        const int tp = tileRows(it.shapeP), td = tileRows(it.shapeD);
         it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + tp - 1) / tp);
         it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + td - 1) / td);
         it.np = static_cast<int64_t>(it.nct) * tp;
         it.mp = static_cast<int64_t>(it.nrt) * td;
+        orderSide(it.sc.at.ptr, lp.n, it.np, tp, isSell(it.shapeP), it.cols);
+        orderSide(it.sc.a.ptr, lp.m, it.mp, td, isSell(it.shapeD), it.rows);
         it.bytes = itemBytes(it, mixed);
     });
     for (int k = 0; k < count; ++k)
@@ -1254,17 +1555,19 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         pk.mixed = mixed;
         std::vector<int> index;
         size_t bytes = 0;
-        int64_t m = 0, n = 0, z = 0, tiles = 0;
+        int64_t m = 0, n = 0, z = 0, tiles = 0, ent = 0;
         while (pos < dev_items.size()) {
             Item& it = items[dev_items[pos]];
+            const int64_t e = std::max(it.cols.entries, it.rows.entries);
             const bool fits = bytes + it.bytes <= budget && m + it.mp < lim32 && n + it.np < lim32 &&
-                              z + it.sc.a.nnz() < lim32 && tiles + it.nct + it.nrt < lim32;
+                              z + it.sc.a.nnz() < lim32 && tiles + it.nct + it.nrt < lim32 && ent + e < lim32;
             if (!fits && !pk.items.empty()) break;
             bytes += it.bytes;
             m += it.mp;
             n += it.np;
             z += it.sc.a.nnz();
             tiles += it.nct + it.nrt;
+            ent += e;
             pk.items.push_back(&it);
             index.push_back(dev_items[pos]);
             ++pos;

@@ -338,6 +338,54 @@ constexpr StepShape kShapes[] = {
 };
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
+// Halpern primal step of column j given s = (A^T y_cur)_j: projected gradient
+// step, reflection, averaging with the anchor (pdlp_kernels.cu:46-88).  FP64
+// arithmetic with the reference's association (tau = step * tau_base / omega).
+template <class T>
+__device__ __forceinline__ void primalUpdate(const IterArgs<T>& p, int j, const ColPack<T>& q, double xcd, double xid,
+                                             double s, double step, double pw, double lam, bool last) {
+    const double tau = step * static_cast<double>(q.tau) / pw;
+    double xh = xcd - tau * (static_cast<double>(q.c) + s);
+    const double lb = q.lb, ub = q.ub;
+    if (xh < lb) xh = lb;
+    if (xh > ub) xh = ub;
+    const double xr = 2.0 * xh - xcd;
+    p.xr[j] = static_cast<T>(xr);
+    p.xc[j] = lam * xr + (1.0 - lam) * xid;
+    if (last) p.xh[j] = static_cast<T>(xh);
+}
+
+// Dual proximal step of row i given s = (A x_refl)_i (pdlp_kernels.cu:94-157):
+// the projection of y + sigma (A x_refl) by row type, reflection, averaging.
+template <class T>
+__device__ __forceinline__ void dualUpdate(const IterArgs<T>& p, int i, const RowPack<T>& q, double ycd, double yid,
+                                           double s, double step, double pw, double lam, bool last) {
+    const double sig = step * static_cast<double>(q.sigma) * pw;
+    const double v = ycd + sig * s;
+    const double rl = q.rl, ru = q.ru;
+    const int type = static_cast<int>(q.type);
+    double py;
+    if (type == 0) {
+        py = v - sig * rl;
+    } else if (type == 1) {
+        py = v - sig * ru;
+        if (py < 0.0) py = 0.0;
+    } else if (type == 2) {
+        py = v - sig * rl;
+        if (py > 0.0) py = 0.0;
+    } else {
+        if (v >= sig * ru)
+            py = v - sig * ru;
+        else if (v <= sig * rl)
+            py = v - sig * rl;
+        else
+            py = 0.0;
+    }
+    const double yr = 2.0 * py - ycd;
+    p.yc[i] = lam * yr + (1.0 - lam) * yid;
+    if (last) p.yh[i] = static_cast<T>(py);
+}
+
 // Row pointers of the R rows j0 + r * slab below jend handled by one G-lane
 // group (b = e = 0 past the end).
 template <int G, int R>
@@ -399,16 +447,7 @@ __device__ __forceinline__ void primalRowsFrom(const IterArgs<T>& p, int j0, int
     for (int r = 0; r < R; ++r) {
         const int j = j0 + r * slab;
         if (lane != 0 || j >= jend) continue;
-        const double xcd = xc[r], xid = xi[r];
-        const double tau = step * static_cast<double>(q[r].tau) / pw;
-        double xh = xcd - tau * (static_cast<double>(q[r].c) + s[r]);
-        const double lb = q[r].lb, ub = q[r].ub;
-        if (xh < lb) xh = lb;
-        if (xh > ub) xh = ub;
-        const double xr = 2.0 * xh - xcd;
-        p.xr[j] = static_cast<T>(xr);
-        p.xc[j] = lam * xr + (1.0 - lam) * xid;
-        if (last) p.xh[j] = static_cast<T>(xh);
+        primalUpdate<T>(p, j, q[r], xc[r], static_cast<double>(xi[r]), s[r], step, pw, lam, last);
     }
 }
 
@@ -465,31 +504,7 @@ __device__ __forceinline__ void dualRowsFrom(const IterArgs<T>& p, int i0, int i
     for (int r = 0; r < R; ++r) {
         const int i = i0 + r * slab;
         if (lane != 0 || i >= iend) continue;
-        const double ycd = yc[r], yid = yi[r];
-        const double sig = step * static_cast<double>(q[r].sigma) * pw;
-        const double v = ycd + sig * s[r];
-        const double rl = q[r].rl, ru = q[r].ru;
-        const int type = static_cast<int>(q[r].type);
-        double py;
-        if (type == 0) {
-            py = v - sig * rl;
-        } else if (type == 1) {
-            py = v - sig * ru;
-            if (py < 0.0) py = 0.0;
-        } else if (type == 2) {
-            py = v - sig * rl;
-            if (py > 0.0) py = 0.0;
-        } else {
-            if (v >= sig * ru)
-                py = v - sig * ru;
-            else if (v <= sig * rl)
-                py = v - sig * rl;
-            else
-                py = 0.0;
-        }
-        const double yr = 2.0 * py - ycd;
-        p.yc[i] = lam * yr + (1.0 - lam) * yid;
-        if (last) p.yh[i] = static_cast<T>(py);
+        dualUpdate<T>(p, i, q[r], yc[r], static_cast<double>(yi[r]), s[r], step, pw, lam, last);
     }
 }
 

@@ -130,6 +130,7 @@ class PdlpOptions:
     shape_dual: int = 0
     batch_pack_mb: int = 0
     batch_compact: bool = True
+    batch_sell: bool = True
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()

@@ -121,3 +121,26 @@ def test_batch_matches_single_lp_solves():
         q = s.solve()
         assert r.status == q.status == Status.Optimal
         assert abs(r.objective - q.objective) <= 2e-6 * (1 + abs(q.objective))
+
+
+def test_batch_sliced_ell_matches_csr():
+    """The sliced-ELL storage (rows renumbered by length inside each tile) and
+    the CSR storage of the same LPs reach the same answers, and the renumbering
+    is undone in the returned x and y."""
+    lps = _mix(1600, (150, 700, 1600, 3000))
+    o = dict(verbose=False, **TIGHT)
+    sell = batch_solve(lps, PdlpOptions(batch_sell=True, **o))
+    csr = batch_solve(lps, PdlpOptions(batch_sell=False, **o))
+    for lp, (r, x, y), (q, u, v) in zip(lps, sell, csr):
+        assert r.status == q.status == Status.Optimal
+        assert abs(r.objective - q.objective) <= 2e-6 * (1 + abs(q.objective))
+        a = lp.matrix
+        ax = np.array([a.values[a.row_starts[i]:a.row_starts[i + 1]] @ x[a.col_indices[a.row_starts[i]:a.row_starts[i + 1]]]
+                       for i in range(lp.num_rows)])
+        viol = np.maximum(lp.row_lower - ax, 0) + np.maximum(ax - lp.row_upper, 0)
+        assert np.linalg.norm(viol) <= 1e-5 * (1 + np.linalg.norm(np.r_[lp.row_lower[np.isfinite(lp.row_lower)],
+                                                                          lp.row_upper[np.isfinite(lp.row_upper)]]))
+        # a renumbering left in place would move entries by O(1); both solves
+        # approximate the same (nondegenerate) primal-dual pair
+        assert np.linalg.norm(x - u) <= 1e-2 * (1 + np.linalg.norm(u))
+        assert np.linalg.norm(y - v) <= 1e-2 * (1 + np.linalg.norm(v))
