@@ -20,6 +20,9 @@ solve.  Metric: PDLP iterations per second (LPs/s and latency reported beside).
 * ``cpu_baseline``: the reference's CPU PDLP (oracle/_ref, compiled from its
   sources; else the oracle restatement) on one host core, as the marginal rate
   between a 200- and a 400-iteration run of the same LP.
+* ``batch``: the batched workload (512 lognormal-sized random sparse LPs, one
+  ``pdlpx_batch_solve`` call, 1e-6 relative KKT): LPs/s on the device and end to
+  end, beside the single-LP FP64 engine's LPs/s on a sample of the same LPs.
 
 ``--impl reference`` times the reference's CPU implementation alone (rank 0;
 other ranks exit).  With ``--gpus N`` under torchrun each rank solves its own
@@ -56,6 +59,8 @@ def parse():
     p.add_argument("--supplies", type=int, default=1000)
     p.add_argument("--demands", type=int, default=1000)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batch", action="store_true", help="skip the 512-LP batched workload")
+    p.add_argument("--batch-lps", type=int, default=512)
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--profile", type=int, default=0, metavar="ITERS",
                    help="profiling run: one solve of the workload capped at ITERS iterations, no JSON line")
@@ -199,6 +204,43 @@ def cpu_baseline(lp, budget_iters=(200, 400)) -> dict:
             "seconds": sum(times)}
 
 
+def batch_workload(rank, world, local, count=512, single_sample=16) -> dict:
+    """The batched workload: `count` random sparse LPs of lognormal size (median
+    1,500 rows, sigma 0.8, clipped to [200, 20,000], n = 2.5 m, 4-12 nonzeros per
+    column, seeds 1000 + k) solved to 1e-6 relative KKT by one pdlpx_batch_solve
+    call, against the single-LP FP64 engine on the first `single_sample` LPs.
+    Under torchrun each rank solves its own copy (independent LPs shard with no
+    collective)."""
+    from mipx_b200 import generators as G
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver, Precision, Status, batch_solve
+    tol = dict(primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local)
+    sizes = G.batch_sizes(count, seed=5)
+    lps = [G.random_lp(m, n, 4, 12, 1000 + k)[0] for k, (m, n) in enumerate(sizes)]
+    batch_solve(lps[:4], PdlpOptions(verbose=False, max_iter=400, **tol))  # warm-up (module load)
+    t0 = time.perf_counter()
+    out = batch_solve(lps, PdlpOptions(verbose=False, **tol))
+    wall = time.perf_counter() - t0
+    dev = out[0][0].device_seconds
+    ok = sum(1 for r, _, _ in out if r.status == Status.Optimal)
+    single = 0.0
+    for lp in lps[:single_sample]:
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, precision=Precision.FP64, **tol))
+        s.load(lp)
+        single += s.solve().device_seconds
+    nnz = sum(lp.matrix.numNonzeros() for lp in lps)
+    lps_dev = count / dev
+    single_rate = single_sample / single
+    return {"workload": f"{count} random sparse LPs, lognormal sizes (median m 1500, n = 2.5 m), {nnz} nonzeros, "
+                        "to 1e-6 rel KKT, one pdlpx_batch_solve call",
+            "lps_per_sec": lps_dev, "e2e_lps_per_sec": count / wall, "device_s": dev, "wall_s": wall,
+            "optimal": ok, "iterations_total": int(sum(r.iterations for r, _, _ in out)),
+            "iterations_max": int(max(r.iterations for r, _, _ in out)),
+            "single_lp_fp64_lps_per_sec": single_rate,
+            "single_lp_fp64_sample": f"first {single_sample} LPs, one FP64 single-LP solve each (device time)",
+            "speedup_vs_single_lp_fp64": lps_dev / single_rate}
+
+
 def run_reference(args, rank, pg):
     if rank != 0:
         return
@@ -304,6 +346,8 @@ def main():
     e2e_t = max_over_ranks(pg, e2e_t)
     e2e_val = sum_over_ranks(pg, float(e2e_iters)) / e2e_t
 
+    batch = None if args.no_batch else batch_workload(rank, world, local, args.batch_lps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -341,6 +385,7 @@ def main():
                          "traffic": traffic, "algorithmic_bytes": bytes_primal,
                          "dual_step_GBps": bytes_dual / (kt["dual_ms"] * 1e-3) / 1e9},
             "cpu_baseline": cpu,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

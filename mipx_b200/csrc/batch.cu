@@ -1336,8 +1336,9 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
             if (!(h_small[l] & 1)) live_tiles += pk.items[l]->nct + pk.items[l]->nrt;
         }
         if (o.verbose && cycles % 10 == 0) {
-            std::printf("PDLP batch  %7d iterations per LP  %d/%d LPs done  %d on FP64 iterates  [B200]\n",
-                        cycles * o.termination_eval_frequency, done, L, fp64);
+            std::printf("PDLP batch  %7d iterations per LP  %d/%d LPs done  %d on FP64 iterates  %d live tiles  %.3fs  [B200]\n",
+                        cycles * o.termination_eval_frequency, done, L, fp64, live_tiles,
+                        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
             std::fflush(stdout);
         }
         if (done >= L) break;
