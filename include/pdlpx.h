@@ -246,6 +246,57 @@ typedef struct pdlpx_lp {
 int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts,
                           pdlpx_result* results, double* const* x_out, double* const* y_out);
 
+/* ---- request server: LP solves as they arrive, continuously batched ----
+ * No counterpart in the reference (the MIP search there calls PdlpSolver::solve
+ * once per LP).  Submitted LPs are copied and scaled by a pool of host threads,
+ * then packed with whatever else is waiting into packs solved by the batched
+ * engine, several packs at a time on their own CUDA streams, within a device
+ * memory budget; a request that arrives while packs run starts in the next
+ * pack as soon as a stream and memory are free, and each LP's result is
+ * available as soon as the restart cycle that finishes it returns.  An LP's
+ * result does not depend on what it was packed with (bit-identical alone and
+ * in any mix, same options). */
+typedef struct pdlpx_server pdlpx_server;
+
+typedef struct pdlpx_server_config {
+    double budget_bytes;   /* device bytes of the packs in flight; 0 = 85% of free memory */
+    int32_t max_packs;     /* packs solved at the same time (streams), default 4 */
+    int32_t max_pack_lps;  /* LPs per pack, default 64 */
+    int32_t prep_threads;  /* host threads copying and scaling submitted LPs, 0 = half the cores */
+    int32_t queue_limit;   /* unfinished requests before submit returns PDLPX_E_BUSY, default 100000 */
+    int32_t reserved[4];
+} pdlpx_server_config;
+
+typedef struct pdlpx_server_stats {
+    int64_t submitted, completed; /* requests */
+    int64_t waiting;              /* submitted, not yet in a running pack */
+    int64_t running;              /* in a running pack */
+    int32_t packs_running, reserved0;
+    double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s; /* submit -> result */
+    double lps_per_sec;           /* completed / (last completion - first submission) */
+    double bytes_in_flight;       /* device bytes of the running packs */
+} pdlpx_server_stats;
+
+void pdlpx_server_config_default(pdlpx_server_config* c);
+int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config* cfg, pdlpx_server** out);
+/* Stops the running packs between restart cycles (their unfinished requests end
+ * with status TimeLimit), joins the threads and frees everything. */
+int32_t pdlpx_server_destroy(pdlpx_server* s);
+/* Copies the LP (and its warm start, if both warm_x and warm_y are given). */
+int32_t pdlpx_server_submit(pdlpx_server* s, const pdlpx_lp* lp, int64_t* ticket);
+/* Warm start from a finished, unreleased request: its x when the sizes match,
+ * its y for the first rows (rows beyond it, e.g. appended cuts, start at 0). */
+int32_t pdlpx_server_submit_warm(pdlpx_server* s, const pdlpx_lp* lp, int64_t warm_ticket, int64_t* ticket);
+int32_t pdlpx_server_poll(pdlpx_server* s, int64_t ticket, int32_t* done);
+/* Waits up to timeout_seconds (< 0: no limit); PDLPX_E_TIMEOUT if unfinished. */
+int32_t pdlpx_server_wait(pdlpx_server* s, int64_t ticket, double timeout_seconds, pdlpx_result* out);
+int32_t pdlpx_server_get_solution(const pdlpx_server* s, int64_t ticket, double* x, int32_t n, double* y,
+                                  int32_t m);
+/* Forgets a finished request (its solution can no longer be read or warm-start another). */
+int32_t pdlpx_server_release(pdlpx_server* s, int64_t ticket);
+int32_t pdlpx_server_get_stats(const pdlpx_server* s, pdlpx_server_stats* out);
+const char* pdlpx_server_last_error(const pdlpx_server* s);
+
 /* ---- device kernels exposed for parity tests (host buffers in and out) ---- */
 /* y = A x with the engine's SpMV kernel.  precision: PDLPX_PREC_MIXED (FP32 values,
  * FP32 x, FP32 accumulation) or PDLPX_PREC_FP64.  group: threads per row (0 = auto). */

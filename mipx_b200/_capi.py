@@ -67,6 +67,17 @@ class GenLp(C.Structure):
 
 
 # (name, restype, argtypes) of every entry point declared in include/pdlpx.h
+class ServerConfig(C.Structure):
+    _fields_ = [("budget_bytes", f64), ("max_packs", i32), ("max_pack_lps", i32), ("prep_threads", i32),
+                ("queue_limit", i32), ("reserved", i32 * 4)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("waiting", C.c_int64), ("running", C.c_int64),
+                ("packs_running", i32), ("reserved0", i32), ("p50_latency_s", f64), ("p99_latency_s", f64),
+                ("mean_latency_s", f64), ("max_latency_s", f64), ("lps_per_sec", f64), ("bytes_in_flight", f64)]
+
+
 SIGNATURES = [
     ("pdlpx_options_default", None, [C.POINTER(Options)]),
     ("pdlpx_error_string", C.c_char_p, [i32]),
@@ -99,6 +110,17 @@ SIGNATURES = [
     ("pdlpx_get_launch_config", i32, [C.c_void_p, P_i32, P_i32, P_i32, P_i32]),
     ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),
                                 C.POINTER(P_f64), C.POINTER(P_f64)]),
+    ("pdlpx_server_config_default", None, [C.POINTER(ServerConfig)]),
+    ("pdlpx_server_create", i32, [C.POINTER(Options), C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    ("pdlpx_server_destroy", i32, [C.c_void_p]),
+    ("pdlpx_server_submit", i32, [C.c_void_p, C.POINTER(Lp), C.POINTER(C.c_int64)]),
+    ("pdlpx_server_submit_warm", i32, [C.c_void_p, C.POINTER(Lp), C.c_int64, C.POINTER(C.c_int64)]),
+    ("pdlpx_server_poll", i32, [C.c_void_p, C.c_int64, P_i32]),
+    ("pdlpx_server_wait", i32, [C.c_void_p, C.c_int64, f64, C.POINTER(Result)]),
+    ("pdlpx_server_get_solution", i32, [C.c_void_p, C.c_int64, P_f64, i32, P_f64, i32]),
+    ("pdlpx_server_release", i32, [C.c_void_p, C.c_int64]),
+    ("pdlpx_server_get_stats", i32, [C.c_void_p, C.POINTER(ServerStats)]),
+    ("pdlpx_server_last_error", C.c_char_p, [C.c_void_p]),
     ("pdlpx_csr_spmv", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, i32, i32]),
     ("pdlpx_row_violation", i32, [i32, i32, i32, P_i32, P_i32, P_f64, P_f64, P_f64, P_f64, P_f64, P_f64]),
     ("pdlpx_row_violation_noalloc", i32, [i32, i32, i32] + [C.c_void_p] * 8),

@@ -49,6 +49,7 @@
 #include "control.cuh"
 #include "engine.hpp"
 #include "kernels.cuh"
+#include "pack.hpp"
 #include "shapes.cuh"
 
 namespace pdlpx {
@@ -563,8 +564,8 @@ void orderSide(const std::vector<int32_t>& ptr, int32_t rows, int64_t padded, in
 }
 
 struct Item {
-    const pdlpx_lp* in = nullptr;
     HostLp lp;
+    std::vector<double> warm_x, warm_y;  // warm start in original space (both or neither)
     ScaledLp sc;
     bool trivial = false;
     int shapeP = 0, shapeD = 0;
@@ -672,11 +673,16 @@ struct Pack {
     int live_ct = 0, live_rt = 0;      // tiles in the current launches
     PackArgs args{};
 
+    // Stream-ordered allocation: packs of a request server come and go while
+    // other packs run, and a plain free would wait for the whole device.
     ~Pack() {
         if (cycle) cudaGraphExecDestroy(cycle);
         if (power) cudaGraphExecDestroy(power);
-        if (d) cudaFree(d);
-        if (s) cudaStreamDestroy(s);
+        if (d) cudaFreeAsync(d, s);
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
     }
 
     // Positions: columns grouped by primal shape, rows by dual shape, LP order
@@ -1200,12 +1206,12 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
     // iterate arrays start at image_end in the arena and at 0 in `iters`
     auto IF = [&](size_t off) { return reinterpret_cast<float*>(iters + (off - pk.image_end)); };
     auto ID = [&](size_t off) { return reinterpret_cast<double*>(iters + (off - pk.image_end)); };
-    const bool warm = it.in->warm_x != nullptr && it.in->warm_y != nullptr;
+    const bool warm = !it.warm_x.empty();
     std::vector<double> wx(n, 0.0), wy(m, 0.0);  // pack numbering
     if (warm) {
-        for (int32_t j = 0; j < n; ++j) wx[co.pos[j]] = it.in->warm_x[j] / sc.col_scale[j] * sc.con_scale;
+        for (int32_t j = 0; j < n; ++j) wx[co.pos[j]] = it.warm_x[j] / sc.col_scale[j] * sc.con_scale;
         for (int32_t i = 0; i < m; ++i)
-            wy[ro.pos[i]] = it.in->warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+            wy[ro.pos[i]] = it.warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
     }
     if (pk.mixed) {
         for (int32_t j = 0; j < n; ++j) {
@@ -1234,15 +1240,97 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= lim;
 }
 
-// Build, run and read back one pack.
-int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::time_point t0, pdlpx_result* results,
-                  const std::vector<int>& index, double* const* x_out, double* const* y_out, std::string& err) {
+// Read one finished (or stopped) LP back from the device and unscale it
+// (pdlp.cpp:2678-2712): x = x_hat * col_scale / con_scale clamped to the
+// original bounds, y = sign * y_hat * row_scale / obj_scale, in the LP's
+// original numbering.
+int32_t collectLp(const Pack& pk, int l, bool out_of_time, double secs, double dev_s, int launches, LpOutcome& out,
+                  std::string& err) {
+    const Item& it = *pk.items[l];
+    cudaStream_t s = pk.s;
+    const int32_t m = it.lp.m, n = it.lp.n;
+    DevState f{};
+    PDLPX_BCK(cudaMemcpyAsync(&f, pk.args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    PDLPX_BCK(cudaStreamSynchronize(s));
+    std::vector<double> xs(n), ys(m);  // original numbering, scaled space
+    if (f.prec == 0) {
+        std::vector<float> fx(it.np), fy(it.mp);
+        PDLPX_BCK(cudaMemcpyAsync(fx.data(), pk.args.it32.xh + it.c0, 4 * fx.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(fy.data(), pk.args.it32.yh + it.r0, 4 * fy.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        for (int32_t j = 0; j < n; ++j) xs[j] = fx[it.cols.pos[j]];
+        for (int32_t i = 0; i < m; ++i) ys[i] = fy[it.rows.pos[i]];
+    } else {
+        std::vector<double> dx(it.np), dy(it.mp);
+        PDLPX_BCK(cudaMemcpyAsync(dx.data(), pk.args.it64.xh + it.c0, 8 * dx.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(dy.data(), pk.args.it64.yh + it.r0, 8 * dy.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        for (int32_t j = 0; j < n; ++j) xs[j] = dx[it.cols.pos[j]];
+        for (int32_t i = 0; i < m; ++i) ys[i] = dy[it.rows.pos[i]];
+    }
+    int32_t status;
+    if (f.done) {
+        status = f.status;
+        if (status == PDLPX_STATUS_ITER_LIMIT && out_of_time) status = PDLPX_STATUS_TIME_LIMIT;
+    } else {
+        status = f.converged ? PDLPX_STATUS_OPTIMAL : PDLPX_STATUS_TIME_LIMIT;
+    }
+    const ScaledLp& sc = it.sc;
+    out.x.assign(n, 0.0);
+    out.y.assign(m, 0.0);
+    double obj = 0.0;
+    if (status == PDLPX_STATUS_OPTIMAL) {
+        const double ic = 1.0 / sc.con_scale, io = 1.0 / sc.obj_scale;
+        double ov = it.lp.offset;
+        for (int32_t j = 0; j < n; ++j) {
+            double xj = xs[j] * sc.col_scale[j] * ic;
+            if (std::isfinite(it.lp.cl[j])) xj = std::max(xj, it.lp.cl[j]);
+            if (std::isfinite(it.lp.cu[j])) xj = std::min(xj, it.lp.cu[j]);
+            out.x[j] = xj;
+            ov += it.lp.obj[j] * xj;
+        }
+        for (int32_t i = 0; i < m; ++i) out.y[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
+        obj = ov;
+    } else if (status == PDLPX_STATUS_INFEASIBLE) {
+        const double io = 1.0 / sc.obj_scale;
+        for (int32_t i = 0; i < m; ++i) out.y[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
+    } else if (status == PDLPX_STATUS_UNBOUNDED) {
+        const double ic = 1.0 / sc.con_scale;
+        for (int32_t j = 0; j < n; ++j) out.x[j] = xs[j] * sc.col_scale[j] * ic;
+    }
+    pdlpx_result& r = out.r;
+    std::memset(&r, 0, sizeof(r));
+    r.status = status;
+    r.objective = obj;
+    r.iterations = f.total;
+    r.work_units = static_cast<double>(f.total) * (4.0 * static_cast<double>(sc.a.nnz()) + 2.0 * static_cast<double>(m + n));
+    r.rel_primal_resid = f.pterm;
+    r.rel_dual_resid = f.dterm;
+    r.rel_gap = f.gap;
+    r.primal_objective = f.pobj;
+    r.dual_objective = f.dobj;
+    r.fp64_iterations = pk.mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
+    r.restarts = f.restarts;
+    r.step_size = f.step;
+    r.primal_weight = f.pw;
+    r.solve_seconds = secs;
+    r.device_seconds = dev_s;
+    r.used_gpu = 1;
+    r.kernel_launches = launches;
+    return PDLPX_OK;
+}
+
+// Build and run one pack; `done(l, outcome)` is called from this thread for
+// every LP as soon as a cycle finds it finished (and for the rest when the
+// time limit or `stop` ends the pack).
+int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::time_point t0,
+                  const std::atomic<int>* stop, const LpDone& done, std::string& err) {
     const int L = pk.L;
     for (int l = 0; l < L; ++l) pk.items[l]->l = l;
     pk.place();
     pk.layout();
     bool any_warm = false;
-    for (const Item* it : pk.items) any_warm |= it->in->warm_x != nullptr && it->in->warm_y != nullptr;
+    for (const Item* it : pk.items) any_warm |= !it->warm_x.empty();
 
     // host image: everything the kernels read, filled per LP in parallel
     std::unique_ptr<char[]> img(new char[pk.image_end]);
@@ -1253,7 +1341,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
     parallelFor(L, [&](int l) { stageItem(pk, *pk.items[l], o, img.get(), iters.get()); });
 
     PDLPX_BCK(cudaStreamCreateWithFlags(&pk.s, cudaStreamNonBlocking));
-    PDLPX_BCK(cudaMalloc(reinterpret_cast<void**>(&pk.d), pk.total));
+    PDLPX_BCK(cudaMallocAsync(reinterpret_cast<void**>(&pk.d), pk.total, pk.s));
     cudaStream_t s = pk.s;
     PDLPX_BCK(cudaMemcpyAsync(pk.d, img.get(), pk.image_end, cudaMemcpyHostToDevice, s));
     if (any_warm)
@@ -1275,13 +1363,18 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
     } ev_guard{ev0, ev1};
     PDLPX_BCK(cudaEventRecord(ev0, s));
     int launches = 0;
+    auto deviceSeconds = [&]() -> double {
+        float ms = 0.0f;
+        if (cudaEventRecord(ev1, s) == cudaSuccess && cudaEventSynchronize(ev1) == cudaSuccess)
+            cudaEventElapsedTime(&ms, ev0, ev1);
+        return 1e-3 * ms;
+    };
+    auto hostSeconds = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
 
-    int* h_small = nullptr;  // pinned: counters[0] / per-LP flags
-    PDLPX_BCK(cudaMallocHost(reinterpret_cast<void**>(&h_small), 4 * static_cast<size_t>(std::max(L, 16))));
-    struct HFree {
-        void* p;
-        ~HFree() { cudaFreeHost(p); }
-    } h_guard{h_small};
+    // counters[0] / per-LP flags (pageable: a pinned allocation would
+    // synchronize the device, which other packs share)
+    std::vector<int> h_flags(std::max(L, 16));
+    int* h_small = h_flags.data();
 
     auto capture = [&](cudaGraphExec_t& g, int& count, bool power) -> int32_t {
         if (g) {
@@ -1297,6 +1390,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         PDLPX_BCK(ie);
         return PDLPX_OK;
     };
+    auto stopped = [&]() { return stop != nullptr && stop->load(std::memory_order_relaxed) != 0; };
 
     // ---- power iteration of every LP
     if (o.sv_max_iter > 0) {
@@ -1307,41 +1401,54 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
             launches += pk.power_launches;
             PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.counters, 4, cudaMemcpyDeviceToHost, s));
             PDLPX_BCK(cudaStreamSynchronize(s));
-            if (h_small[0] >= L) break;
+            if (h_small[0] >= L || stopped()) break;
         }
     }
     packInitStep<<<(L + 127) / 128, 128, 0, s>>>(pk.args);
     ++launches;
     PDLPX_BCK(cudaGetLastError());
 
-    // ---- restart cycles
+    // ---- restart cycles; finished LPs are read back after the cycle that ends them
     {
         int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
         if (rc != PDLPX_OK) return rc;
     }
-    std::vector<char> keep(L, 1);
+    std::vector<char> keep(L, 1), collected(L, 0);
     std::vector<int> cl, rl;
-    int cycles = 0;
-    while (true) {
-        if (timeUp(t0, o.max_solve_seconds)) break;
+    int cycles = 0, ncollected = 0;
+    while (ncollected < L) {
+        if (timeUp(t0, o.max_solve_seconds) || stopped()) break;
         PDLPX_BCK(cudaGraphLaunch(pk.cycle, s));
         launches += pk.cycle_launches;
         ++cycles;
         PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
-        int done = 0, fp64 = 0, live_tiles = 0;
+        int done_count = 0, fp64 = 0, live_tiles = 0;
+        bool fresh = false;
         for (int l = 0; l < L; ++l) {
-            done += h_small[l] & 1;
+            done_count += h_small[l] & 1;
             fp64 += (h_small[l] >> 1) & 1;
             if (!(h_small[l] & 1)) live_tiles += pk.items[l]->nct + pk.items[l]->nrt;
+            fresh |= (h_small[l] & 1) && !collected[l];
+        }
+        if (fresh) {
+            const double dev_s = deviceSeconds(), secs = hostSeconds();
+            for (int l = 0; l < L; ++l) {
+                if (!(h_small[l] & 1) || collected[l]) continue;
+                LpOutcome out;
+                const int32_t rc = collectLp(pk, l, false, secs, dev_s, launches, out, err);
+                if (rc != PDLPX_OK) return rc;
+                collected[l] = 1;
+                ++ncollected;
+                done(l, std::move(out));
+            }
         }
         if (o.verbose && cycles % 10 == 0) {
             std::printf("PDLP batch  %7d iterations per LP  %d/%d LPs done  %d on FP64 iterates  %d live tiles  %.3fs  [B200]\n",
-                        cycles * o.termination_eval_frequency, done, L, fp64, live_tiles,
-                        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+                        cycles * o.termination_eval_frequency, done_count, L, fp64, live_tiles, hostSeconds());
             std::fflush(stdout);
         }
-        if (done >= L) break;
+        if (done_count >= L) break;
         if (o.batch_compact && live_tiles < ((pk.live_ct + pk.live_rt) * 3) / 5) {
             for (int l = 0; l < L; ++l) keep[l] = !(h_small[l] & 1);
             pk.liveLists(keep, cl, rl);
@@ -1353,93 +1460,18 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
             if (rc != PDLPX_OK) return rc;
         }
     }
-    PDLPX_BCK(cudaEventRecord(ev1, s));
-    PDLPX_BCK(cudaEventSynchronize(ev1));
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-
-    // ---- results
-    std::vector<DevState> fin(L);
-    PDLPX_BCK(cudaMemcpyAsync(fin.data(), pk.args.st, sizeof(DevState) * L, cudaMemcpyDeviceToHost, s));
-    std::vector<float> fx, fy;
-    std::vector<double> dx(pk.Nc), dy(pk.M);
-    if (pk.mixed) {
-        fx.resize(pk.Nc);
-        fy.resize(pk.M);
-        PDLPX_BCK(cudaMemcpyAsync(fx.data(), pk.args.it32.xh, 4 * static_cast<size_t>(pk.Nc), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaMemcpyAsync(fy.data(), pk.args.it32.yh, 4 * static_cast<size_t>(pk.M), cudaMemcpyDeviceToHost, s));
+    // LPs the time limit or the stop request left unfinished
+    if (ncollected < L) {
+        const double dev_s = deviceSeconds(), secs = hostSeconds();
+        const bool out_of_time = timeUp(t0, o.max_solve_seconds);
+        for (int l = 0; l < L; ++l) {
+            if (collected[l]) continue;
+            LpOutcome out;
+            const int32_t rc = collectLp(pk, l, out_of_time, secs, dev_s, launches, out, err);
+            if (rc != PDLPX_OK) return rc;
+            done(l, std::move(out));
+        }
     }
-    PDLPX_BCK(cudaMemcpyAsync(dx.data(), pk.args.it64.xh, 8 * static_cast<size_t>(pk.Nc), cudaMemcpyDeviceToHost, s));
-    PDLPX_BCK(cudaMemcpyAsync(dy.data(), pk.args.it64.yh, 8 * static_cast<size_t>(pk.M), cudaMemcpyDeviceToHost, s));
-    PDLPX_BCK(cudaStreamSynchronize(s));
-    const bool out_of_time = timeUp(t0, o.max_solve_seconds);
-    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    parallelFor(L, [&](int l) {
-        const Item& it = *pk.items[l];
-        const DevState& f = fin[l];
-        const int32_t m = it.lp.m, n = it.lp.n;
-        std::vector<double> xs(n), ys(m);  // original numbering
-        for (int32_t j = 0; j < n; ++j) {
-            const int64_t at = it.c0 + it.cols.pos[j];
-            xs[j] = f.prec == 0 ? static_cast<double>(fx[at]) : dx[at];
-        }
-        for (int32_t i = 0; i < m; ++i) {
-            const int64_t at = it.r0 + it.rows.pos[i];
-            ys[i] = f.prec == 0 ? static_cast<double>(fy[at]) : dy[at];
-        }
-        int32_t status;
-        if (f.done) {
-            status = f.status;
-            if (status == PDLPX_STATUS_ITER_LIMIT && out_of_time) status = PDLPX_STATUS_TIME_LIMIT;
-        } else {
-            status = f.converged ? PDLPX_STATUS_OPTIMAL : PDLPX_STATUS_TIME_LIMIT;
-        }
-        const ScaledLp& sc = it.sc;
-        std::vector<double> xo(n, 0.0), yo(m, 0.0);
-        double obj = 0.0;
-        if (status == PDLPX_STATUS_OPTIMAL) {
-            const double ic = 1.0 / sc.con_scale, io = 1.0 / sc.obj_scale;
-            double ov = it.lp.offset;
-            for (int32_t j = 0; j < n; ++j) {
-                double xj = xs[j] * sc.col_scale[j] * ic;
-                if (std::isfinite(it.lp.cl[j])) xj = std::max(xj, it.lp.cl[j]);
-                if (std::isfinite(it.lp.cu[j])) xj = std::min(xj, it.lp.cu[j]);
-                xo[j] = xj;
-                ov += it.lp.obj[j] * xj;
-            }
-            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
-            obj = ov;
-        } else if (status == PDLPX_STATUS_INFEASIBLE) {
-            const double io = 1.0 / sc.obj_scale;
-            for (int32_t i = 0; i < m; ++i) yo[i] = sc.obj_sign * ys[i] * sc.row_scale[i] * io;
-        } else if (status == PDLPX_STATUS_UNBOUNDED) {
-            const double ic = 1.0 / sc.con_scale;
-            for (int32_t j = 0; j < n; ++j) xo[j] = xs[j] * sc.col_scale[j] * ic;
-        }
-        const int k = index[l];
-        pdlpx_result& r = results[k];
-        std::memset(&r, 0, sizeof(r));
-        r.status = status;
-        r.objective = obj;
-        r.iterations = f.total;
-        r.work_units = static_cast<double>(f.total) *
-                       (4.0 * static_cast<double>(sc.a.nnz()) + 2.0 * static_cast<double>(m + n));
-        r.rel_primal_resid = f.pterm;
-        r.rel_dual_resid = f.dterm;
-        r.rel_gap = f.gap;
-        r.primal_objective = f.pobj;
-        r.dual_objective = f.dobj;
-        r.fp64_iterations = pk.mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
-        r.restarts = f.restarts;
-        r.step_size = f.step;
-        r.primal_weight = f.pw;
-        r.solve_seconds = secs;
-        r.device_seconds = ms * 1e-3;
-        r.used_gpu = 1;
-        r.kernel_launches = launches;
-        if (x_out && x_out[k]) std::memcpy(x_out[k], xo.data(), 8 * static_cast<size_t>(n));
-        if (y_out && y_out[k]) std::memcpy(y_out[k], yo.data(), 8 * static_cast<size_t>(m));
-    });
     return PDLPX_OK;
 }
 
@@ -1456,94 +1488,178 @@ int batchSideShape(int pinned, int group, bool sell, int64_t nnz, int32_t rows) 
     return batchShape(nnz, rows);
 }
 
-}  // namespace
+// Copy, validate and scale one LP; choose its launch shapes and storage.
+int32_t prepareItem(const pdlpx_lp& in, const pdlpx_options& o, Item& it) {
+    HostLp& lp = it.lp;
+    lp.m = in.m;
+    lp.n = in.n;
+    lp.maximize = in.sense == PDLPX_MAXIMIZE;
+    if (in.m < 0 || in.n < 0 || !canonicalCsr(in.m, in.n, in.nnz, in.row_ptr, in.col_idx, in.val, lp.a) ||
+        (in.n > 0 && (in.obj == nullptr || in.col_lb == nullptr || in.col_ub == nullptr)) ||
+        (in.m > 0 && (in.row_lb == nullptr || in.row_ub == nullptr)))
+        return PDLPX_E_INVALID;
+    lp.obj.assign(in.obj, in.obj + in.n);
+    lp.cl.assign(in.col_lb, in.col_lb + in.n);
+    lp.cu.assign(in.col_ub, in.col_ub + in.n);
+    lp.rl.assign(in.row_lb, in.row_lb + in.m);
+    lp.ru.assign(in.row_ub, in.row_ub + in.m);
+    lp.offset = in.obj_offset;
+    if (in.warm_x != nullptr && in.warm_y != nullptr) {
+        it.warm_x.assign(in.warm_x, in.warm_x + in.n);
+        it.warm_y.assign(in.warm_y, in.warm_y + in.m);
+    }
+    it.trivial = lp.m == 0 || lp.n == 0;
+    if (it.trivial) return PDLPX_OK;
+    const bool mixed = o.precision != PDLPX_PREC_FP64;
+    buildScaled(lp, o, it.sc);
+    const int64_t z = it.sc.a.nnz();
+    it.shapeP = batchSideShape(o.shape_primal, o.spmv_group_at, o.batch_sell != 0, z, lp.n);
+    it.shapeD = batchSideShape(o.shape_dual, o.spmv_group_a, o.batch_sell != 0, z, lp.m);
+    const int tp = tileRows(it.shapeP), td = tileRows(it.shapeD);
+    it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + tp - 1) / tp);
+    it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + td - 1) / td);
+    it.np = static_cast<int64_t>(it.nct) * tp;
+    it.mp = static_cast<int64_t>(it.nrt) * td;
+    orderSide(it.sc.at.ptr, lp.n, it.np, tp, isSell(it.shapeP), it.cols);
+    orderSide(it.sc.a.ptr, lp.m, it.mp, td, isSell(it.shapeD), it.rows);
+    it.bytes = itemBytes(it, mixed);
+    return PDLPX_OK;
+}
 
-int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
-                   double* const* x_out, double* const* y_out, std::string& err) {
-    const auto t0 = std::chrono::steady_clock::now();
+// Closed-form LPs (no rows or no columns) through the single-LP engine's host
+// path (pdlp.cpp:812-860).
+int32_t solveTrivialItem(const Item& it, const pdlpx_options& o, LpOutcome& out, std::string& err) {
+    Engine e;
+    e.setOptions(o);
+    const HostLp& lp = it.lp;
+    int32_t rc = e.load(lp.m, lp.n, lp.a.nnz(), lp.a.ptr.data(), lp.a.idx.data(), lp.a.val.data(), lp.obj.data(),
+                        lp.cl.data(), lp.cu.data(), lp.rl.data(), lp.ru.data(),
+                        lp.maximize ? PDLPX_MAXIMIZE : PDLPX_MINIMIZE, lp.offset);
+    if (rc == PDLPX_OK) rc = e.solve(&out.r);
+    if (rc != PDLPX_OK) {
+        err = e.last_error;
+        return rc;
+    }
+    out.x = e.primal();
+    out.y = e.dual();
+    return PDLPX_OK;
+}
+
+bool optionsSupported(const pdlpx_options& o, std::string& err) {
     if (o.anderson_acceleration && o.anderson_window_size >= 2) {
         err = "anderson_acceleration is not available in the device engine";
-        return PDLPX_E_INVALID;
+        return false;
     }
     if (o.adaptive_step) {
         err = "adaptive_step is not available in the batched solve";
-        return PDLPX_E_INVALID;
+        return false;
     }
     if (o.termination_eval_frequency <= 0) {
         err = "termination_eval_frequency must be positive";
-        return PDLPX_E_INVALID;
+        return false;
     }
-    const bool mixed = o.precision != PDLPX_PREC_FP64;
-    std::vector<Item> items(count);
-    std::vector<int32_t> codes(count, PDLPX_OK);
-    parallelFor(count, [&](int k) {
-        Item& it = items[k];
-        it.in = &lps[k];
-        const pdlpx_lp& in = lps[k];
-        HostLp& lp = it.lp;
-        lp.m = in.m;
-        lp.n = in.n;
-        lp.maximize = in.sense == PDLPX_MAXIMIZE;
-        if (in.m < 0 || in.n < 0 || !canonicalCsr(in.m, in.n, in.nnz, in.row_ptr, in.col_idx, in.val, lp.a) ||
-            (in.n > 0 && (in.obj == nullptr || in.col_lb == nullptr || in.col_ub == nullptr)) ||
-            (in.m > 0 && (in.row_lb == nullptr || in.row_ub == nullptr))) {
-            codes[k] = PDLPX_E_INVALID;
-            return;
-        }
-        lp.obj.assign(in.obj, in.obj + in.n);
-        lp.cl.assign(in.col_lb, in.col_lb + in.n);
-        lp.cu.assign(in.col_ub, in.col_ub + in.n);
-        lp.rl.assign(in.row_lb, in.row_lb + in.m);
-        lp.ru.assign(in.row_ub, in.row_ub + in.m);
-        lp.offset = in.obj_offset;
-        it.trivial = lp.m == 0 || lp.n == 0;
-        if (it.trivial) return;
-        buildScaled(lp, o, it.sc);
-        const int64_t z = it.sc.a.nnz();
-        it.shapeP = batchSideShape(o.shape_primal, o.spmv_group_at, o.batch_sell != 0, z, lp.n);
-        it.shapeD = batchSideShape(o.shape_dual, o.spmv_group_a, o.batch_sell != 0, z, lp.m);
-        const int tp = tileRows(it.shapeP), td = tileRows(it.shapeD);
-        it.nct = static_cast<int>((static_cast<int64_t>(lp.n) + tp - 1) / tp);
-        it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + td - 1) / td);
-        it.np = static_cast<int64_t>(it.nct) * tp;
-        it.mp = static_cast<int64_t>(it.nrt) * td;
-        orderSide(it.sc.at.ptr, lp.n, it.np, tp, isSell(it.shapeP), it.cols);
-        orderSide(it.sc.a.ptr, lp.m, it.mp, td, isSell(it.shapeD), it.rows);
-        it.bytes = itemBytes(it, mixed);
-    });
-    for (int k = 0; k < count; ++k)
-        if (codes[k] != PDLPX_OK) {
-            err = "invalid LP at index " + std::to_string(k);
-            return codes[k];
-        }
-    // Trivial LPs (no rows or no columns) are closed form, like pdlp.cpp:812-860, via the engine.
-    std::vector<int> dev_items;
-    for (int k = 0; k < count; ++k) {
-        if (!items[k].trivial) {
-            dev_items.push_back(k);
-            continue;
-        }
-        Engine e;
-        e.setOptions(o);
-        const pdlpx_lp& in = lps[k];
-        int32_t rc = e.load(in.m, in.n, in.nnz, in.row_ptr, in.col_idx, in.val, in.obj, in.col_lb, in.col_ub,
-                            in.row_lb, in.row_ub, in.sense, in.obj_offset);
-        if (rc == PDLPX_OK) rc = e.solve(&results[k]);
-        if (rc != PDLPX_OK) {
-            err = e.last_error;
-            return rc;
-        }
-        if (x_out && x_out[k] && !e.primal().empty()) std::memcpy(x_out[k], e.primal().data(), 8 * e.primal().size());
-        if (y_out && y_out[k] && !e.dual().empty()) std::memcpy(y_out[k], e.dual().data(), 8 * e.dual().size());
-    }
-    if (dev_items.empty()) return PDLPX_OK;
+    return true;
+}
 
+int32_t selectDevice(const pdlpx_options& o, std::string& err) {
     int devcount = 0;
     if (cudaGetDeviceCount(&devcount) != cudaSuccess || devcount <= 0) {
         err = "no CUDA device visible";
         return PDLPX_E_NO_DEVICE;
     }
     PDLPX_BCK(cudaSetDevice((o.device >= 0 && o.device < devcount) ? o.device : 0));
+    return PDLPX_OK;
+}
+
+// Solve one pack of prepared items on the current device.
+int32_t runPack(const std::vector<Item*>& items, const pdlpx_options& o, std::chrono::steady_clock::time_point t0,
+                const std::atomic<int>* stop, const LpDone& done, std::string& err) {
+    Pack pk;
+    pk.mixed = o.precision != PDLPX_PREC_FP64;
+    pk.items = items;
+    pk.L = static_cast<int>(items.size());
+    if (pk.L == 0) return PDLPX_OK;
+    return solvePack(pk, o, t0, stop, done, err);
+}
+
+}  // namespace
+
+struct PreparedLp {
+    Item item;
+};
+
+void PreparedLpDeleter::operator()(PreparedLp* p) const { delete p; }
+
+int32_t prepareLp(const pdlpx_lp& lp, const pdlpx_options& o, PreparedPtr& out, std::string& err) {
+    if (!optionsSupported(o, err)) return PDLPX_E_INVALID;
+    PreparedPtr p(new PreparedLp());
+    const int32_t rc = prepareItem(lp, o, p->item);
+    if (rc != PDLPX_OK) {
+        err = "invalid LP (CSR structure, sizes or missing arrays)";
+        return rc;
+    }
+    out = std::move(p);
+    return PDLPX_OK;
+}
+
+bool preparedTrivial(const PreparedLp& p) { return p.item.trivial; }
+size_t preparedBytes(const PreparedLp& p) { return p.item.bytes; }
+int32_t preparedRows(const PreparedLp& p) { return p.item.lp.m; }
+int32_t preparedCols(const PreparedLp& p) { return p.item.lp.n; }
+
+int32_t solvePreparedTrivial(const PreparedLp& p, const pdlpx_options& o, LpOutcome& out, std::string& err) {
+    return solveTrivialItem(p.item, o, out, err);
+}
+
+int32_t solvePrepared(const std::vector<PreparedLp*>& lps, const pdlpx_options& o, const std::atomic<int>* stop,
+                      const LpDone& done, std::string& err) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!optionsSupported(o, err)) return PDLPX_E_INVALID;
+    std::vector<Item*> items;
+    for (PreparedLp* p : lps) {
+        if (p->item.trivial) {
+            err = "trivial LPs are solved on the host, not in a pack";
+            return PDLPX_E_INVALID;
+        }
+        items.push_back(&p->item);
+    }
+    if (items.empty()) return PDLPX_OK;
+    int32_t rc = selectDevice(o, err);
+    if (rc != PDLPX_OK) return rc;
+    return runPack(items, o, t0, stop, done, err);
+}
+
+int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
+                   double* const* x_out, double* const* y_out, std::string& err) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!optionsSupported(o, err)) return PDLPX_E_INVALID;
+    std::vector<Item> items(count);
+    std::vector<int32_t> codes(count, PDLPX_OK);
+    parallelFor(count, [&](int k) { codes[k] = prepareItem(lps[k], o, items[k]); });
+    for (int k = 0; k < count; ++k)
+        if (codes[k] != PDLPX_OK) {
+            err = "invalid LP at index " + std::to_string(k);
+            return codes[k];
+        }
+    auto deliver = [&](int k, LpOutcome& out) {
+        results[k] = out.r;
+        if (x_out && x_out[k] && !out.x.empty()) std::memcpy(x_out[k], out.x.data(), 8 * out.x.size());
+        if (y_out && y_out[k] && !out.y.empty()) std::memcpy(y_out[k], out.y.data(), 8 * out.y.size());
+    };
+    std::vector<int> dev_items;
+    for (int k = 0; k < count; ++k) {
+        if (!items[k].trivial) {
+            dev_items.push_back(k);
+            continue;
+        }
+        LpOutcome out;
+        const int32_t rc = solveTrivialItem(items[k], o, out, err);
+        if (rc != PDLPX_OK) return rc;
+        deliver(k, out);
+    }
+    if (dev_items.empty()) return PDLPX_OK;
+    int32_t rc = selectDevice(o, err);
+    if (rc != PDLPX_OK) return rc;
     size_t free_b = 0, total_b = 0;
     PDLPX_BCK(cudaMemGetInfo(&free_b, &total_b));
     const size_t budget = o.batch_pack_mb > 0 ? static_cast<size_t>(o.batch_pack_mb) << 20
@@ -1552,8 +1668,7 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
     const int64_t lim32 = std::numeric_limits<int32_t>::max() - 1;
     size_t pos = 0;
     while (pos < dev_items.size()) {
-        Pack pk;
-        pk.mixed = mixed;
+        std::vector<Item*> pack;
         std::vector<int> index;
         size_t bytes = 0;
         int64_t m = 0, n = 0, z = 0, tiles = 0, ent = 0;
@@ -1562,19 +1677,18 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
             const int64_t e = std::max(it.cols.entries, it.rows.entries);
             const bool fits = bytes + it.bytes <= budget && m + it.mp < lim32 && n + it.np < lim32 &&
                               z + it.sc.a.nnz() < lim32 && tiles + it.nct + it.nrt < lim32 && ent + e < lim32;
-            if (!fits && !pk.items.empty()) break;
+            if (!fits && !pack.empty()) break;
             bytes += it.bytes;
             m += it.mp;
             n += it.np;
             z += it.sc.a.nnz();
             tiles += it.nct + it.nrt;
             ent += e;
-            pk.items.push_back(&it);
+            pack.push_back(&it);
             index.push_back(dev_items[pos]);
             ++pos;
         }
-        pk.L = static_cast<int>(pk.items.size());
-        const int32_t rc = solvePack(pk, o, t0, results, index, x_out, y_out, err);
+        rc = runPack(pack, o, t0, nullptr, [&](int l, LpOutcome&& out) { deliver(index[l], out); }, err);
         if (rc != PDLPX_OK) return rc;
     }
     return PDLPX_OK;

@@ -1,0 +1,533 @@
+// Request server over the packed batch engine (pdlpx_server_* in pdlpx.h).
+//
+// Three kinds of host threads:
+//   * preparation workers copy nothing (submit already copied the LP) but scale
+//     it and choose its pack layout (prepareLp), in parallel;
+//   * one dispatcher forms a pack from every prepared request that is waiting,
+//     up to max_pack_lps and within the device budget left by the packs in
+//     flight, whenever fewer than max_packs packs run;
+//   * one worker per pack runs it on its own CUDA stream (solvePrepared) and
+//     completes each request as soon as the restart cycle that finishes it
+//     returns.
+// So requests that arrive while packs run are admitted as soon as a stream and
+// memory free up, and the packs' kernels overlap on the device.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "engine.hpp"
+#include "pack.hpp"
+#include "pdlpx.h"
+
+namespace pdlpx {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// Owned copy of a caller's pdlpx_lp.
+struct OwnedLp {
+    int32_t m = 0, n = 0, nnz = 0, sense = PDLPX_MINIMIZE;
+    double offset = 0.0;
+    std::vector<int32_t> ptr, idx;
+    std::vector<double> val, obj, cl, cu, rl, ru, wx, wy;
+
+    bool copy(const pdlpx_lp& in) {
+        if (in.m < 0 || in.n < 0 || in.nnz < 0 || (in.m > 0 && in.row_ptr == nullptr) ||
+            (in.nnz > 0 && (in.col_idx == nullptr || in.val == nullptr)) ||
+            (in.n > 0 && (in.obj == nullptr || in.col_lb == nullptr || in.col_ub == nullptr)) ||
+            (in.m > 0 && (in.row_lb == nullptr || in.row_ub == nullptr)))
+            return false;
+        m = in.m;
+        n = in.n;
+        nnz = in.nnz;
+        sense = in.sense;
+        offset = in.obj_offset;
+        ptr.assign(in.row_ptr ? in.row_ptr : nullptr, in.row_ptr ? in.row_ptr + m + 1 : nullptr);
+        if (ptr.empty()) ptr.assign(1, 0);
+        idx.assign(in.col_idx, in.col_idx + nnz);
+        val.assign(in.val, in.val + nnz);
+        obj.assign(in.obj, in.obj + n);
+        cl.assign(in.col_lb, in.col_lb + n);
+        cu.assign(in.col_ub, in.col_ub + n);
+        rl.assign(in.row_lb, in.row_lb + m);
+        ru.assign(in.row_ub, in.row_ub + m);
+        if (in.warm_x != nullptr && in.warm_y != nullptr) {
+            wx.assign(in.warm_x, in.warm_x + n);
+            wy.assign(in.warm_y, in.warm_y + m);
+        }
+        return true;
+    }
+
+    pdlpx_lp view() const {
+        pdlpx_lp v{};
+        v.m = m;
+        v.n = n;
+        v.nnz = nnz;
+        v.row_ptr = ptr.data();
+        v.col_idx = idx.data();
+        v.val = val.data();
+        v.obj = obj.data();
+        v.col_lb = cl.data();
+        v.col_ub = cu.data();
+        v.row_lb = rl.data();
+        v.row_ub = ru.data();
+        v.sense = sense;
+        v.obj_offset = offset;
+        v.warm_x = wx.empty() ? nullptr : wx.data();
+        v.warm_y = wy.empty() ? nullptr : wy.data();
+        return v;
+    }
+};
+
+enum ReqState { kQueued = 0, kPrepared = 1, kRunning = 2, kDone = 3 };
+
+struct Request {
+    int64_t ticket = 0;
+    OwnedLp raw;
+    PreparedPtr prep;
+    size_t bytes = 0;
+    Clock::time_point submitted, finished;
+    int state = kQueued;
+    int32_t code = PDLPX_OK;
+    std::string err;
+    LpOutcome out;
+};
+
+double quantile(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * static_cast<double>(v.size() - 1);
+    const size_t lo = static_cast<size_t>(pos);
+    const size_t hi = std::min(v.size() - 1, lo + 1);
+    return v[lo] + (pos - static_cast<double>(lo)) * (v[hi] - v[lo]);
+}
+
+}  // namespace
+
+class Server {
+public:
+    Server(const pdlpx_options& o, const pdlpx_server_config& c, size_t budget) : opt_(o), cfg_(c), budget_(budget) {}
+
+    ~Server() { shutdown(); }
+
+    void start() {
+        const int prep = cfg_.prep_threads > 0
+                             ? cfg_.prep_threads
+                             : std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / 2);
+        for (int k = 0; k < prep; ++k) prep_threads_.emplace_back([this] { prepLoop(); });
+        dispatcher_ = std::thread([this] { dispatchLoop(); });
+    }
+
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (closed_) return;
+            closed_ = true;
+            stop_.store(1);
+        }
+        cv_prep_.notify_all();
+        cv_dispatch_.notify_all();
+        for (auto& t : prep_threads_) t.join();
+        if (dispatcher_.joinable()) dispatcher_.join();
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_packs_.wait(lk, [this] { return packs_running_ == 0; });
+        // requests that never reached a pack
+        for (auto& kv : reqs_) {
+            Request& r = *kv.second;
+            if (r.state != kDone) {
+                r.state = kDone;
+                r.code = PDLPX_E_INVALID;
+                r.err = "server shut down before the request was solved";
+                r.finished = Clock::now();
+            }
+        }
+        cv_done_.notify_all();
+    }
+
+    int32_t submit(const pdlpx_lp& lp, int64_t warm_ticket, int64_t* ticket, std::string& err) {
+        auto req = std::make_unique<Request>();
+        if (!req->raw.copy(lp)) {
+            err = "invalid LP (sizes or missing arrays)";
+            return PDLPX_E_INVALID;
+        }
+        std::lock_guard<std::mutex> g(mu_);
+        if (closed_) {
+            err = "server is shut down";
+            return PDLPX_E_INVALID;
+        }
+        if (submitted_ - completed_ >= static_cast<int64_t>(cfg_.queue_limit)) {
+            err = "request queue is full";
+            return PDLPX_E_BUSY;
+        }
+        if (warm_ticket >= 0) {
+            auto it = reqs_.find(warm_ticket);
+            if (it == reqs_.end() || it->second->state != kDone || it->second->code != PDLPX_OK) {
+                err = "warm-start ticket is unknown, unfinished or failed";
+                return PDLPX_E_UNKNOWN_TICKET;
+            }
+            const LpOutcome& w = it->second->out;
+            if (static_cast<int32_t>(w.x.size()) == req->raw.n && !w.x.empty()) {
+                req->raw.wx = w.x;
+                req->raw.wy.assign(req->raw.m, 0.0);
+                const size_t k = std::min(w.y.size(), req->raw.wy.size());
+                std::copy(w.y.begin(), w.y.begin() + static_cast<std::ptrdiff_t>(k), req->raw.wy.begin());
+            }
+        }
+        const int64_t t = next_ticket_++;
+        req->ticket = t;
+        req->submitted = Clock::now();
+        if (submitted_ == 0) first_submit_ = req->submitted;
+        ++submitted_;
+        *ticket = t;
+        prep_q_.push_back(t);
+        reqs_.emplace(t, std::move(req));
+        cv_prep_.notify_one();
+        return PDLPX_OK;
+    }
+
+    int32_t poll(int64_t ticket, int32_t* done) const {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return PDLPX_E_UNKNOWN_TICKET;
+        *done = it->second->state == kDone ? 1 : 0;
+        return PDLPX_OK;
+    }
+
+    int32_t wait(int64_t ticket, double timeout, pdlpx_result* out, std::string& err) {
+        std::unique_lock<std::mutex> lk(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return PDLPX_E_UNKNOWN_TICKET;
+        Request* r = it->second.get();
+        auto ready = [r] { return r->state == kDone; };
+        if (timeout < 0.0) {
+            cv_done_.wait(lk, ready);
+        } else if (!cv_done_.wait_for(lk, std::chrono::duration<double>(timeout), ready)) {
+            err = "request still running";
+            return PDLPX_E_TIMEOUT;
+        }
+        if (r->code != PDLPX_OK) {
+            err = r->err;
+            return r->code;
+        }
+        if (out) *out = r->out.r;
+        return PDLPX_OK;
+    }
+
+    int32_t solution(int64_t ticket, double* x, int32_t n, double* y, int32_t m, std::string& err) const {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return PDLPX_E_UNKNOWN_TICKET;
+        const Request& r = *it->second;
+        if (r.state != kDone || r.code != PDLPX_OK) {
+            err = "request unfinished or failed";
+            return PDLPX_E_INVALID;
+        }
+        if ((x && n != static_cast<int32_t>(r.out.x.size())) || (y && m != static_cast<int32_t>(r.out.y.size()))) {
+            err = "solution sizes do not match the LP";
+            return PDLPX_E_INVALID;
+        }
+        if (x && n > 0) std::memcpy(x, r.out.x.data(), 8 * static_cast<size_t>(n));
+        if (y && m > 0) std::memcpy(y, r.out.y.data(), 8 * static_cast<size_t>(m));
+        return PDLPX_OK;
+    }
+
+    int32_t release(int64_t ticket) {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return PDLPX_E_UNKNOWN_TICKET;
+        if (it->second->state != kDone) return PDLPX_E_BUSY;
+        reqs_.erase(it);
+        return PDLPX_OK;
+    }
+
+    void stats(pdlpx_server_stats* s) const {
+        std::lock_guard<std::mutex> g(mu_);
+        std::memset(s, 0, sizeof(*s));
+        s->submitted = submitted_;
+        s->completed = completed_;
+        int64_t waiting = 0, running = 0;
+        for (const auto& kv : reqs_) {
+            const int st = kv.second->state;
+            waiting += st == kQueued || st == kPrepared;
+            running += st == kRunning;
+        }
+        s->waiting = waiting;
+        s->running = running;
+        s->packs_running = packs_running_;
+        s->p50_latency_s = quantile(latencies_, 0.50);
+        s->p99_latency_s = quantile(latencies_, 0.99);
+        double sum = 0.0, mx = 0.0;
+        for (double v : latencies_) {
+            sum += v;
+            mx = std::max(mx, v);
+        }
+        s->mean_latency_s = latencies_.empty() ? 0.0 : sum / static_cast<double>(latencies_.size());
+        s->max_latency_s = mx;
+        const double span = completed_ > 0 ? std::chrono::duration<double>(last_complete_ - first_submit_).count() : 0.0;
+        s->lps_per_sec = span > 0.0 ? static_cast<double>(completed_) / span : 0.0;
+        s->bytes_in_flight = static_cast<double>(bytes_in_flight_);
+    }
+
+private:
+    // Completion of one request (mu_ held).
+    void finishLocked(Request& r) {
+        r.state = kDone;
+        r.finished = Clock::now();
+        r.prep.reset();
+        ++completed_;
+        last_complete_ = r.finished;
+        latencies_.push_back(std::chrono::duration<double>(r.finished - r.submitted).count());
+    }
+
+    void prepLoop() {
+        while (true) {
+            Request* r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_prep_.wait(lk, [this] { return closed_ || !prep_q_.empty(); });
+                if (closed_) return;
+                r = reqs_.at(prep_q_.front()).get();
+                prep_q_.pop_front();
+            }
+            // r stays valid: a request is only erased once done
+            std::string err;
+            PreparedPtr p;
+            int32_t rc = prepareLp(r->raw.view(), opt_, p, err);
+            LpOutcome trivial;
+            if (rc == PDLPX_OK && preparedTrivial(*p)) rc = solvePreparedTrivial(*p, opt_, trivial, err);
+            std::lock_guard<std::mutex> g(mu_);
+            if (rc != PDLPX_OK) {
+                r->code = rc;
+                r->err = err;
+                finishLocked(*r);
+                cv_done_.notify_all();
+            } else if (preparedTrivial(*p)) {
+                r->out = std::move(trivial);
+                finishLocked(*r);
+                cv_done_.notify_all();
+            } else {
+                r->bytes = preparedBytes(*p);
+                r->prep = std::move(p);
+                r->state = kPrepared;
+                ready_q_.push_back(r->ticket);
+                cv_dispatch_.notify_one();
+            }
+        }
+    }
+
+    void dispatchLoop() {
+        const int max_packs = std::max(1, cfg_.max_packs);
+        const size_t max_lps = static_cast<size_t>(std::max(1, cfg_.max_pack_lps));
+        while (true) {
+            std::vector<Request*> pack;
+            size_t bytes = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_dispatch_.wait(lk, [&] {
+                    if (closed_) return true;
+                    if (ready_q_.empty() || packs_running_ >= max_packs) return false;
+                    const size_t head = reqs_.at(ready_q_.front())->bytes;
+                    return bytes_in_flight_ == 0 || bytes_in_flight_ + head <= budget_;
+                });
+                if (closed_) return;
+                while (!ready_q_.empty() && pack.size() < max_lps) {
+                    Request* r = reqs_.at(ready_q_.front()).get();
+                    if (!pack.empty() && bytes_in_flight_ + bytes + r->bytes > budget_) break;
+                    bytes += r->bytes;
+                    r->state = kRunning;
+                    pack.push_back(r);
+                    ready_q_.pop_front();
+                }
+                bytes_in_flight_ += bytes;
+                ++packs_running_;
+            }
+            std::thread([this, pack, bytes] { runPack(pack, bytes); }).detach();
+        }
+    }
+
+    void runPack(std::vector<Request*> pack, size_t bytes) {
+        std::vector<PreparedLp*> lps;
+        for (Request* r : pack) lps.push_back(r->prep.get());
+        std::string err;
+        const int32_t rc = solvePrepared(lps, opt_, &stop_, [&](int l, LpOutcome&& out) {
+            std::lock_guard<std::mutex> g(mu_);
+            Request& r = *pack[l];
+            r.out = std::move(out);
+            finishLocked(r);
+            cv_done_.notify_all();
+        }, err);
+        std::lock_guard<std::mutex> g(mu_);
+        for (Request* r : pack) {
+            if (r->state == kDone) continue;
+            r->code = rc != PDLPX_OK ? rc : PDLPX_E_CUDA;
+            r->err = rc != PDLPX_OK ? err : "pack ended without a result";
+            finishLocked(*r);
+        }
+        bytes_in_flight_ -= bytes;
+        --packs_running_;
+        cv_done_.notify_all();
+        cv_dispatch_.notify_all();
+        cv_packs_.notify_all();
+    }
+
+    const pdlpx_options opt_;
+    const pdlpx_server_config cfg_;
+    const size_t budget_;
+    mutable std::mutex mu_;
+    std::condition_variable cv_prep_, cv_dispatch_, cv_done_, cv_packs_;
+    std::unordered_map<int64_t, std::unique_ptr<Request>> reqs_;
+    std::deque<int64_t> prep_q_, ready_q_;
+    std::vector<std::thread> prep_threads_;
+    std::thread dispatcher_;
+    std::atomic<int> stop_{0};
+    bool closed_ = false;
+    int packs_running_ = 0;
+    size_t bytes_in_flight_ = 0;
+    int64_t next_ticket_ = 1, submitted_ = 0, completed_ = 0;
+    Clock::time_point first_submit_, last_complete_;
+    std::vector<double> latencies_;
+};
+
+}  // namespace pdlpx
+
+struct pdlpx_server {
+    std::unique_ptr<pdlpx::Server> impl;
+    mutable std::mutex err_mu;
+    std::string last_error;
+    void setError(const std::string& e) {
+        std::lock_guard<std::mutex> g(err_mu);
+        last_error = e;
+    }
+};
+
+extern "C" {
+
+void pdlpx_server_config_default(pdlpx_server_config* c) {
+    if (c == nullptr) return;
+    std::memset(c, 0, sizeof(*c));
+    c->budget_bytes = 0.0;
+    c->max_packs = 4;
+    c->max_pack_lps = 64;
+    c->prep_threads = 0;
+    c->queue_limit = 100000;
+}
+
+int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config* cfg, pdlpx_server** out) {
+    if (out == nullptr) return PDLPX_E_INVALID;
+    *out = nullptr;
+    try {
+        pdlpx_options o;
+        pdlpx_options_default(&o);
+        if (opts) o = *opts;
+        pdlpx_server_config c;
+        pdlpx_server_config_default(&c);
+        if (cfg) c = *cfg;
+        if (c.queue_limit <= 0) c.queue_limit = 100000;
+        int devcount = 0;
+        if (cudaGetDeviceCount(&devcount) != cudaSuccess || devcount <= 0) {
+            cudaGetLastError();
+            pdlpx::setGlobalError("no CUDA device visible");
+            return PDLPX_E_NO_DEVICE;
+        }
+        cudaSetDevice((o.device >= 0 && o.device < devcount) ? o.device : 0);
+        size_t budget = static_cast<size_t>(c.budget_bytes > 0.0 ? c.budget_bytes : 0.0);
+        if (budget == 0) {
+            size_t free_b = 0, total_b = 0;
+            if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+                pdlpx::setGlobalError("cudaMemGetInfo failed");
+                return PDLPX_E_CUDA;
+            }
+            budget = static_cast<size_t>(0.85 * static_cast<double>(free_b));
+        }
+        auto* s = new pdlpx_server();
+        s->impl = std::make_unique<pdlpx::Server>(o, c, budget);
+        s->impl->start();
+        *out = s;
+        return PDLPX_OK;
+    } catch (const std::bad_alloc&) {
+        return PDLPX_E_NOMEM;
+    } catch (...) {
+        return PDLPX_E_INVALID;
+    }
+}
+
+int32_t pdlpx_server_destroy(pdlpx_server* s) {
+    if (s == nullptr) return PDLPX_E_INVALID;
+    s->impl->shutdown();
+    delete s;
+    return PDLPX_OK;
+}
+
+static int32_t submitCommon(pdlpx_server* s, const pdlpx_lp* lp, int64_t warm, int64_t* ticket) {
+    if (s == nullptr || lp == nullptr || ticket == nullptr) return PDLPX_E_INVALID;
+    try {
+        std::string err;
+        const int32_t rc = s->impl->submit(*lp, warm, ticket, err);
+        if (rc != PDLPX_OK) s->setError(err);
+        return rc;
+    } catch (const std::bad_alloc&) {
+        s->setError("host allocation failed");
+        return PDLPX_E_NOMEM;
+    }
+}
+
+int32_t pdlpx_server_submit(pdlpx_server* s, const pdlpx_lp* lp, int64_t* ticket) {
+    return submitCommon(s, lp, -1, ticket);
+}
+
+int32_t pdlpx_server_submit_warm(pdlpx_server* s, const pdlpx_lp* lp, int64_t warm_ticket, int64_t* ticket) {
+    if (warm_ticket < 0) return PDLPX_E_INVALID;
+    return submitCommon(s, lp, warm_ticket, ticket);
+}
+
+int32_t pdlpx_server_poll(pdlpx_server* s, int64_t ticket, int32_t* done) {
+    if (s == nullptr || done == nullptr) return PDLPX_E_INVALID;
+    return s->impl->poll(ticket, done);
+}
+
+int32_t pdlpx_server_wait(pdlpx_server* s, int64_t ticket, double timeout_seconds, pdlpx_result* out) {
+    if (s == nullptr) return PDLPX_E_INVALID;
+    std::string err;
+    const int32_t rc = s->impl->wait(ticket, timeout_seconds, out, err);
+    if (rc != PDLPX_OK) s->setError(err);
+    return rc;
+}
+
+int32_t pdlpx_server_get_solution(const pdlpx_server* s, int64_t ticket, double* x, int32_t n, double* y,
+                                  int32_t m) {
+    if (s == nullptr) return PDLPX_E_INVALID;
+    std::string err;
+    const int32_t rc = s->impl->solution(ticket, x, n, y, m, err);
+    if (rc != PDLPX_OK) const_cast<pdlpx_server*>(s)->setError(err);
+    return rc;
+}
+
+int32_t pdlpx_server_release(pdlpx_server* s, int64_t ticket) {
+    if (s == nullptr) return PDLPX_E_INVALID;
+    return s->impl->release(ticket);
+}
+
+int32_t pdlpx_server_get_stats(const pdlpx_server* s, pdlpx_server_stats* out) {
+    if (s == nullptr || out == nullptr) return PDLPX_E_INVALID;
+    s->impl->stats(out);
+    return PDLPX_OK;
+}
+
+const char* pdlpx_server_last_error(const pdlpx_server* s) {
+    if (s == nullptr) return "";
+    return s->last_error.c_str();
+}
+
+}  // extern "C"

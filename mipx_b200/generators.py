@@ -8,6 +8,8 @@
   variables, 2,000 rows, 2M unit nonzeros).
 * ``powerlaw_lp``    -- large LP with power-law column counts (500,000 x
   2,000,000, counts in [2, 2000] with mean 10, 1% of rows scaled by 1e3).
+* ``node_lp``        -- branch-and-bound node LP of a base LP: integer-marked
+  columns fixed to floor/ceil of x0 and random cuts appended (serving workload).
 * ``batch_sizes``    -- row counts of the 512-LP batch, lognormal(median 1,500,
   sigma 0.8) clipped to [200, 20,000], n = 2.5 m.
 """
@@ -71,3 +73,46 @@ def batch_sizes(count: int = 512, median: float = 1500.0, sigma: float = 0.8, lo
 
 def batch_lps(count: int = 512, seed: int = 5, **kw) -> list[LpProblem]:
     return [random_lp(m, n, 4, 12, seed * 100003 + k)[0] for k, (m, n) in enumerate(batch_sizes(count, seed=seed, **kw))]
+
+
+def integer_marks(n: int, frac: float = 0.3, seed: int = 3) -> np.ndarray:
+    """Integrality marks of the serving workload's base LP: a seeded 30% of the columns."""
+    return np.random.default_rng(seed).random(n) < frac
+
+
+def node_lp(base: LpProblem, x0: np.ndarray, is_int: np.ndarray, seed: int, fix_lo: float = 0.01,
+            fix_hi: float = 0.05, cuts_max: int = 50, cut_nnz: tuple[int, int] = (20, 200)) -> LpProblem:
+    """A branch-and-bound node LP of `base`: a random 1-5% of the integer-marked
+    columns fixed to floor or ceil of x0, then 0-50 random cuts a x <= a x0 +
+    U[0,1] with 20-200 N(0,1) entries each, appended after the base rows (so a
+    parent's duals warm-start the first rows)."""
+    rng = np.random.default_rng(seed)
+    ints = np.flatnonzero(is_int)
+    lo, hi = max(1, int(round(fix_lo * ints.size))), max(1, int(round(fix_hi * ints.size)))
+    fix = rng.choice(ints, size=int(rng.integers(lo, hi + 1)), replace=False)
+    val = np.where(rng.random(fix.size) < 0.5, np.floor(x0[fix]), np.ceil(x0[fix]))
+    cl, cu = base.col_lower.copy(), base.col_upper.copy()
+    cl[fix] = np.clip(val, cl[fix], cu[fix])
+    cu[fix] = cl[fix]
+    a = base.matrix
+    rows, starts, idx, vals, rl, ru = [], [a.row_starts], [a.col_indices], [a.values], [base.row_lower], [base.row_upper]
+    ncut = int(rng.integers(0, cuts_max + 1))
+    nnz = int(a.values.size)
+    cut_ptr = []
+    for _ in range(ncut):
+        k = int(rng.integers(cut_nnz[0], cut_nnz[1] + 1))
+        cols = np.sort(rng.choice(base.num_cols, size=k, replace=False)).astype(np.int32)
+        v = rng.standard_normal(k)
+        idx.append(cols)
+        vals.append(v)
+        nnz += k
+        cut_ptr.append(nnz)
+        rl.append(np.array([-np.inf]))
+        ru.append(np.array([float(v @ x0[cols]) + float(rng.random())]))
+    rp = np.concatenate([a.row_starts, np.array(cut_ptr, dtype=np.int32)]).astype(np.int32)
+    m = base.num_rows + ncut
+    mat = SparseMatrix(m, base.num_cols, values=np.concatenate(vals), col_indices=np.concatenate(idx).astype(np.int32),
+                       row_starts=rp)
+    return LpProblem(name=f"{base.name}_node{seed}", sense=base.sense, num_cols=base.num_cols, num_rows=m,
+                     obj=base.obj.copy(), col_lower=cl, col_upper=cu, row_lower=np.concatenate(rl),
+                     row_upper=np.concatenate(ru), matrix=mat, obj_offset=base.obj_offset)

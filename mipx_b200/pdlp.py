@@ -445,6 +445,86 @@ def batch_solve(problems: Sequence[LpProblem], options: PdlpOptions, warm: Seque
     return [(LpResult.from_c(res[k]), xs[k], ys[k]) for k in range(len(problems))]
 
 
+class Server:
+    """LP solves as they arrive (``pdlpx_server_*``): submitted LPs are packed
+    with whatever else is waiting and solved several packs at a time on the
+    device; each result is available as soon as it is finished.
+
+    ``submit(lp, warm=None)`` returns a ticket; ``warm`` is an ``(x, y)`` pair or
+    the ticket of a finished request.  ``wait(ticket)`` returns
+    ``(LpResult, x, y)``.  ``stats()`` reports p50/p99 latency and LPs/s."""
+
+    def __init__(self, options: PdlpOptions, budget_bytes: float = 0.0, max_packs: int = 4,
+                 max_pack_lps: int = 64, prep_threads: int = 0, queue_limit: int = 100000):
+        self._lib = _capi.load()
+        cfg = _capi.ServerConfig()
+        self._lib.pdlpx_server_config_default(C.byref(cfg))
+        cfg.budget_bytes = float(budget_bytes)
+        cfg.max_packs = int(max_packs)
+        cfg.max_pack_lps = int(max_pack_lps)
+        cfg.prep_threads = int(prep_threads)
+        cfg.queue_limit = int(queue_limit)
+        self._h = C.c_void_p()
+        _capi.check(self._lib.pdlpx_server_create(C.byref(options.to_c()), C.byref(cfg), C.byref(self._h)))
+        self._dims: dict[int, tuple[int, int]] = {}
+
+    def _check(self, code: int) -> None:
+        if code != 0:
+            raise _capi.PdlpxError(code, self._lib.pdlpx_server_last_error(self._h).decode())
+
+    def submit(self, lp: LpProblem, warm=None) -> int:
+        keep: list = []
+        t = C.c_int64()
+        if isinstance(warm, (int, np.integer)):
+            c_lp = lp.to_c(keep, None, None)
+            self._check(self._lib.pdlpx_server_submit_warm(self._h, C.byref(c_lp), int(warm), C.byref(t)))
+        else:
+            wx, wy = warm if warm is not None else (None, None)
+            c_lp = lp.to_c(keep, wx, wy)
+            self._check(self._lib.pdlpx_server_submit(self._h, C.byref(c_lp), C.byref(t)))
+        self._dims[t.value] = (lp.num_cols, lp.num_rows)
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = C.c_int32()
+        self._check(self._lib.pdlpx_server_poll(self._h, int(ticket), C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        r = _capi.Result()
+        self._check(self._lib.pdlpx_server_wait(self._h, int(ticket), float(timeout), C.byref(r)))
+        n, m = self._dims[ticket]
+        x, y = np.zeros(n), np.zeros(m)
+        self._check(self._lib.pdlpx_server_get_solution(self._h, int(ticket), _pd(x), n, _pd(y), m))
+        return LpResult.from_c(r), x, y
+
+    def release(self, ticket: int) -> None:
+        self._check(self._lib.pdlpx_server_release(self._h, int(ticket)))
+        self._dims.pop(ticket, None)
+
+    def stats(self) -> dict:
+        s = _capi.ServerStats()
+        self._check(self._lib.pdlpx_server_get_stats(self._h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_ if not name.startswith("reserved")}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.pdlpx_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def csr_spmv(matrix: SparseMatrix, x, precision: Precision = Precision.Mixed, group: int = 0) -> np.ndarray:
     """y = A x with the engine's device SpMV kernel (parity entry point)."""
     lib = _capi.load()
