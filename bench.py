@@ -23,6 +23,8 @@ solve.  Metric: PDLP iterations per second (LPs/s and latency reported beside).
 * ``batch``: the batched workload (512 lognormal-sized random sparse LPs, one
   ``pdlpx_batch_solve`` call, 1e-6 relative KKT): LPs/s on the device and end to
   end, beside the single-LP FP64 engine's LPs/s on a sample of the same LPs.
+* ``serving``: the request server on a Poisson stream of branch-and-bound node
+  LPs of a 20,000 x 50,000 base LP: p50/p99 latency and LPs/s.
 
 ``--impl reference`` times the reference's CPU implementation alone (rank 0;
 other ranks exit).  With ``--gpus N`` under torchrun each rank solves its own
@@ -61,6 +63,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the 512-LP batched workload")
     p.add_argument("--batch-lps", type=int, default=512)
+    p.add_argument("--no-serving", action="store_true", help="skip the node-LP serving workload")
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--profile", type=int, default=0, metavar="ITERS",
                    help="profiling run: one solve of the workload capped at ITERS iterations, no JSON line")
@@ -241,6 +244,52 @@ def batch_workload(rank, world, local, count=512, single_sample=16) -> dict:
             "speedup_vs_single_lp_fp64": lps_dev / single_rate}
 
 
+def serving_workload(local, requests=64, rate=500.0, single_sample=4) -> dict:
+    """The serving workload: a 20,000 x 50,000 random sparse base LP (4-12
+    nonzeros per column, 30% of the columns marked integer), solved once through
+    the request server, then `requests` branch-and-bound node LPs (1-5% of the
+    integer columns fixed to floor/ceil of x0, 0-50 appended cuts of 20-200
+    nonzeros) arriving as a Poisson stream at `rate` per second, each
+    warm-started from the base request; latency is submit -> result."""
+    from mipx_b200 import generators as G
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver, Precision, Server, Status
+    tol = dict(primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, verbose=False, device=local)
+    base, x0 = G.random_lp(20000, 50000, 4, 12, 101)
+    ints = G.integer_marks(base.num_cols)
+    nodes = [G.node_lp(base, x0, ints, 1000 + k) for k in range(requests)]
+    arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, requests))
+    with Server(PdlpOptions(**tol)) as srv:
+        tb = srv.submit(base)
+        srv.wait(tb)
+        start = time.perf_counter()
+        tickets = []
+        for k, nd in enumerate(nodes):
+            d = start + arrivals[k] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(nd, warm=tb))
+        res = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+    single = 0.0
+    for nd in nodes[:single_sample]:
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(precision=Precision.FP64, **tol))
+        s.load(nd)
+        single += s.solve().device_seconds
+    # the server's clock starts at the base request; count the node stream only
+    span = max(r.solve_seconds for r, _, _ in res)
+    lats = st["p50_latency_s"], st["p99_latency_s"]
+    lps = requests / (time.perf_counter() - start) if res else 0.0
+    return {"workload": f"{requests} node LPs of a 20000 x 50000 base LP ({base.matrix.numNonzeros()} nonzeros), "
+                        f"Poisson arrivals at {rate:g}/s, warm-started from the base, to 1e-6 rel KKT",
+            "p50_latency_s": lats[0], "p99_latency_s": lats[1], "lps_per_sec": lps,
+            "optimal": sum(1 for r, _, _ in res if r.status == Status.Optimal),
+            "iterations_median": float(np.median([r.iterations for r, _, _ in res])),
+            "single_lp_fp64_lps_per_sec": single_sample / single,
+            "single_lp_fp64_sample": f"first {single_sample} node LPs, one FP64 single-LP solve each (device time)",
+            "speedup_vs_single_lp_fp64": lps / (single_sample / single), "solve_seconds_max": span}
+
+
 def run_reference(args, rank, pg):
     if rank != 0:
         return
@@ -347,6 +396,7 @@ def main():
     e2e_val = sum_over_ranks(pg, float(e2e_iters)) / e2e_t
 
     batch = None if args.no_batch else batch_workload(rank, world, local, args.batch_lps)
+    serving = None if args.no_serving else serving_workload(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -386,6 +436,7 @@ def main():
                          "dual_step_GBps": bytes_dual / (kt["dual_ms"] * 1e-3) / 1e9},
             "cpu_baseline": cpu,
             "batch": batch,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

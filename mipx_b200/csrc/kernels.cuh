@@ -605,8 +605,15 @@ __device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const De
     const double g = c + aty;
     const double lbT = static_cast<double>(static_cast<T>(lb));
     const double ubT = static_cast<double>(static_cast<T>(ub));
+    // A fixed column (lb == ub) admits a reduced cost of either sign, so it adds
+    // no dual residual.  (The reference tests the lower bound first,
+    // pdlp.cpp:1134-1140, and counts a negative reduced cost of a fixed column,
+    // which never vanishes: LPs with fixed columns whose reduced cost is negative
+    // cannot reach its tolerance.)
     double dr;
-    if (xh <= lbT + 1e-12 && hl)
+    if (hl && hu && lb == ub)
+        dr = 0.0;
+    else if (xh <= lbT + 1e-12 && hl)
         dr = fmin(g, 0.0);
     else if (xh >= ubT - 1e-12 && hu)
         dr = fmax(g, 0.0);

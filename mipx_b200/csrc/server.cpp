@@ -98,7 +98,7 @@ struct Request {
     OwnedLp raw;
     PreparedPtr prep;
     size_t bytes = 0;
-    Clock::time_point submitted, finished;
+    Clock::time_point submitted, ready, finished;
     int state = kQueued;
     int32_t code = PDLPX_OK;
     std::string err;
@@ -285,7 +285,6 @@ private:
     void finishLocked(Request& r) {
         r.state = kDone;
         r.finished = Clock::now();
-        r.prep.reset();
         ++completed_;
         last_complete_ = r.finished;
         latencies_.push_back(std::chrono::duration<double>(r.finished - r.submitted).count());
@@ -321,6 +320,7 @@ private:
                 r->bytes = preparedBytes(*p);
                 r->prep = std::move(p);
                 r->state = kPrepared;
+                r->ready = Clock::now();
                 ready_q_.push_back(r->ticket);
                 cv_dispatch_.notify_one();
             }
@@ -335,13 +335,28 @@ private:
             size_t bytes = 0;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_dispatch_.wait(lk, [&] {
-                    if (closed_) return true;
-                    if (ready_q_.empty() || packs_running_ >= max_packs) return false;
-                    const size_t head = reqs_.at(ready_q_.front())->bytes;
-                    return bytes_in_flight_ == 0 || bytes_in_flight_ + head <= budget_;
-                });
-                if (closed_) return;
+                // A pack starts when a stream and memory are free and either a full
+                // pack is ready or the oldest ready request has waited the batching
+                // window (a pack runs for many restart cycles, so a short wait that
+                // fills it costs less latency than it saves).
+                const auto window = std::chrono::milliseconds(std::max(0, cfg_.batch_window_ms));
+                while (true) {
+                    if (closed_) return;
+                    bool can = !ready_q_.empty() && packs_running_ < max_packs;
+                    if (can) {
+                        const Request& head = *reqs_.at(ready_q_.front());
+                        can = bytes_in_flight_ == 0 || bytes_in_flight_ + head.bytes <= budget_;
+                        if (can && ready_q_.size() < max_lps) {
+                            const auto due = head.ready + window;
+                            if (Clock::now() < due) {
+                                cv_dispatch_.wait_until(lk, due);
+                                continue;
+                            }
+                        }
+                    }
+                    if (can) break;
+                    cv_dispatch_.wait(lk);
+                }
                 while (!ready_q_.empty() && pack.size() < max_lps) {
                     Request* r = reqs_.at(ready_q_.front()).get();
                     if (!pack.empty() && bytes_in_flight_ + bytes + r->bytes > budget_) break;
@@ -357,20 +372,34 @@ private:
         }
     }
 
+    // The pack owns its prepared LPs until it returns (the engine reads every
+    // LP of the pack until the last one finishes), and a finished request may be
+    // released by its client at once, so completion is tracked here, never by
+    // reading a request after it was completed.
     void runPack(std::vector<Request*> pack, size_t bytes) {
+        std::vector<PreparedPtr> preps;
         std::vector<PreparedLp*> lps;
-        for (Request* r : pack) lps.push_back(r->prep.get());
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            for (Request* r : pack) {
+                preps.push_back(std::move(r->prep));
+                lps.push_back(preps.back().get());
+            }
+        }
+        std::vector<char> finished(pack.size(), 0);
         std::string err;
         const int32_t rc = solvePrepared(lps, opt_, &stop_, [&](int l, LpOutcome&& out) {
             std::lock_guard<std::mutex> g(mu_);
+            finished[l] = 1;
             Request& r = *pack[l];
             r.out = std::move(out);
             finishLocked(r);
             cv_done_.notify_all();
         }, err);
         std::lock_guard<std::mutex> g(mu_);
-        for (Request* r : pack) {
-            if (r->state == kDone) continue;
+        for (size_t k = 0; k < pack.size(); ++k) {
+            if (finished[k]) continue;
+            Request* r = pack[k];
             r->code = rc != PDLPX_OK ? rc : PDLPX_E_CUDA;
             r->err = rc != PDLPX_OK ? err : "pack ended without a result";
             finishLocked(*r);
@@ -419,9 +448,10 @@ void pdlpx_server_config_default(pdlpx_server_config* c) {
     std::memset(c, 0, sizeof(*c));
     c->budget_bytes = 0.0;
     c->max_packs = 4;
-    c->max_pack_lps = 64;
+    c->max_pack_lps = 32;
     c->prep_threads = 0;
     c->queue_limit = 100000;
+    c->batch_window_ms = 50;
 }
 
 int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config* cfg, pdlpx_server** out) {

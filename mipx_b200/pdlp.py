@@ -455,7 +455,8 @@ class Server:
     ``(LpResult, x, y)``.  ``stats()`` reports p50/p99 latency and LPs/s."""
 
     def __init__(self, options: PdlpOptions, budget_bytes: float = 0.0, max_packs: int = 4,
-                 max_pack_lps: int = 64, prep_threads: int = 0, queue_limit: int = 100000):
+                 max_pack_lps: int = 32, prep_threads: int = 0, queue_limit: int = 100000,
+                 batch_window_ms: int = 50):
         self._lib = _capi.load()
         cfg = _capi.ServerConfig()
         self._lib.pdlpx_server_config_default(C.byref(cfg))
@@ -464,6 +465,7 @@ class Server:
         cfg.max_pack_lps = int(max_pack_lps)
         cfg.prep_threads = int(prep_threads)
         cfg.queue_limit = int(queue_limit)
+        cfg.batch_window_ms = int(batch_window_ms)
         self._h = C.c_void_p()
         _capi.check(self._lib.pdlpx_server_create(C.byref(options.to_c()), C.byref(cfg), C.byref(self._h)))
         self._dims: dict[int, tuple[int, int]] = {}

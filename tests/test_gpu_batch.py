@@ -144,3 +144,24 @@ def test_batch_sliced_ell_matches_csr():
         # approximate the same (nondegenerate) primal-dual pair
         assert np.linalg.norm(x - u) <= 1e-2 * (1 + np.linalg.norm(u))
         assert np.linalg.norm(y - v) <= 1e-2 * (1 + np.linalg.norm(v))
+
+
+def test_fixed_column_with_negative_reduced_cost_converges():
+    """min -2 x1 - x2  s.t.  x1 + x2 <= 1.5,  x1 fixed at 1,  0 <= x2 <= 10:  x = (1, 0.5),
+    objective -2.5; the fixed column's reduced cost is negative at the optimum, which
+    must not count as dual residual (single-LP engine and batch)."""
+    from mipx_b200.pdlp import LpProblem, PdlpSolver, SparseMatrix
+    lp = LpProblem(num_cols=2, obj=np.array([-2.0, -1.0]), col_lower=np.array([1.0, 0.0]),
+                   col_upper=np.array([1.0, 10.0]), num_rows=1, row_lower=np.array([-np.inf]),
+                   row_upper=np.array([1.5]),
+                   matrix=SparseMatrix(1, 2, values=np.array([1.0, 1.0]), col_indices=np.array([0, 1], np.int32),
+                                       row_starts=np.array([0, 2], np.int32)))
+    o = PdlpOptions(max_iter=200000, **TIGHT)
+    s = PdlpSolver()
+    s.setOptions(o)
+    s.load(lp)
+    r = s.solve()
+    assert r.status == Status.Optimal and abs(r.objective + 2.5) <= 1e-5, r
+    (q, x, _), = batch_solve([lp], o)
+    assert q.status == Status.Optimal and abs(q.objective + 2.5) <= 1e-5, q
+    np.testing.assert_allclose(x, [1.0, 0.5], atol=1e-5)
