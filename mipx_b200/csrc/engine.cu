@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <random>
 
@@ -158,7 +159,13 @@ struct DeviceLp {
     int gA = 1, gAT = 1;        // lanes per row of the check / power kernels
     int shapeP = 0, shapeD = 0;  // step kernel shapes (kShapes index): primal (A^T), dual (A)
     bool tuned = false;
-    int nb_rows = 1, nb_cols = 1, nb_pi = 1;
+    int nb_rows = 1, nb_cols = 1, nb_pi = 1;  // check / power partial blocks (all launches)
+    // Rows of A (nlD) and of A^T (nlP) far longer than the rest come first in
+    // the device numbering and get their own launches: lane counts gLA / gLAT,
+    // step shapes shapeLD / shapeLP; the other rows use gA / gAT, shapeD / shapeP.
+    int nlD = 0, nlP = 0, gLA = 1, gLAT = 1, shapeLD = 0, shapeLP = 0;
+    int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
+    std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
 
     int *a_ptr = nullptr, *a_idx = nullptr, *at_ptr = nullptr, *at_idx = nullptr;
     float *a_v32 = nullptr, *at_v32 = nullptr;
@@ -296,21 +303,66 @@ IterArgs<double> iterArgs<double>(const DeviceLp& d, const pdlpx_options& o) {
     return d.iter64(o);
 }
 
+// Step launches of one iteration on each side: the long rows (if any), then the rest.
+template <class T>
+int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s) {
+    int n = 0;
+    if (d.nlP > 0) {
+        PDLPX_SHAPE_SWITCH(d.shapeLP,
+                           (primalStep<GG, RR, UU, T><<<gridForShape(d.nlP, d.shapeLP), kBlock, 0, s>>>(ia, k, 0, d.nlP)));
+        ++n;
+    }
+    if (d.n > d.nlP) {
+        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gridForShape(d.n - d.nlP, d.shapeP), kBlock, 0, s>>>(
+                                         ia, k, d.nlP, d.n)));
+        ++n;
+    }
+    return n;
+}
+template <class T>
+int launchDual(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s) {
+    int n = 0;
+    if (d.nlD > 0) {
+        PDLPX_SHAPE_SWITCH(d.shapeLD,
+                           (dualStep<GG, RR, UU, T><<<gridForShape(d.nlD, d.shapeLD), kBlock, 0, s>>>(ia, k, 0, d.nlD)));
+        ++n;
+    }
+    if (d.m > d.nlD) {
+        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gridForShape(d.m - d.nlD, d.shapeD), kBlock, 0, s>>>(
+                                         ia, k, d.nlD, d.m)));
+        ++n;
+    }
+    return n;
+}
+// FP64 check pass: short rows write partials [0, nb_*_s), long rows the rest.
+template <class T>
+int launchChecks(const DeviceLp& d, const CheckArgs<T>& ca, cudaStream_t s) {
+    PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows_s, kBlock, 0, s>>>(ca, d.nlD, d.m, 0)));
+    PDLPX_G_SWITCH(d.gAT, (checkCols<GG, T><<<d.nb_cols_s, kBlock, 0, s>>>(ca, d.nlP, d.n, 0)));
+    int n = 2;
+    if (d.nlD > 0) {
+        PDLPX_G_SWITCH(d.gLA, (checkRows<GG, T><<<d.nb_rows - d.nb_rows_s, kBlock, 0, s>>>(ca, 0, d.nlD, d.nb_rows_s)));
+        ++n;
+    }
+    if (d.nlP > 0) {
+        PDLPX_G_SWITCH(d.gLAT, (checkCols<GG, T><<<d.nb_cols - d.nb_cols_s, kBlock, 0, s>>>(ca, 0, d.nlP, d.nb_cols_s)));
+        ++n;
+    }
+    return n;
+}
+
 // One restart cycle: N fused iterations, check, controller, restart copy.
 template <class T>
 int launchCycle(DeviceLp& d, const pdlpx_options& o) {
     const IterArgs<T> ia = iterArgs<T>(d, o);
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
-    const int gp = gridForShape(d.n, d.shapeP), gd = gridForShape(d.m, d.shapeD);
     int launches = 0;
     for (int k = 1; k <= o.termination_eval_frequency; ++k) {
-        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, k)));
-        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, k)));
-        launches += 2;
+        launches += launchPrimal<T>(d, ia, k, s);
+        launches += launchDual<T>(d, ia, k, s);
     }
-    PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
-    PDLPX_G_SWITCH(d.gAT, (checkCols<GG, T><<<d.nb_cols, kBlock, 0, s>>>(ca)));
+    launches += launchChecks<T>(d, ca, s) - 2;
     controller<<<1, kBlock, 0, s>>>(d.st, d.dc, d.part_rows, d.part_cols, sizeof(T) == 8 ? 1 : 0);
     const int nb = std::max(1, std::min(gridFor(std::max(d.m, d.n), 1), 8 * d.sms));
     restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc);
@@ -329,8 +381,17 @@ int launchPowerChunk(DeviceLp& d, const PowerArgs& pa, const PowerMat<V>& mt, in
     cudaStream_t s = d.stream;
     int launches = 0;
     for (int it = 0; it < chunk; ++it) {
-        PDLPX_G_SWITCH(d.gA, (powerA<GG, V><<<gridFor(d.m, d.gA), kBlock, 0, s>>>(pa, mt)));
-        PDLPX_G_SWITCH(d.gAT, (powerAt<GG, V><<<d.nb_pi, kBlock, 0, s>>>(pa, mt)));
+        // A x for every row before A^T y reads it
+        PDLPX_G_SWITCH(d.gA, (powerA<GG, V><<<gridFor(d.m - d.nlD, d.gA), kBlock, 0, s>>>(pa, mt, d.nlD, d.m)));
+        if (d.nlD > 0) {
+            PDLPX_G_SWITCH(d.gLA, (powerA<GG, V><<<gridFor(d.nlD, d.gLA), kBlock, 0, s>>>(pa, mt, 0, d.nlD)));
+            ++launches;
+        }
+        PDLPX_G_SWITCH(d.gAT, (powerAt<GG, V><<<d.nb_pi_s, kBlock, 0, s>>>(pa, mt, d.nlP, d.n, 0)));
+        if (d.nlP > 0) {
+            PDLPX_G_SWITCH(d.gLAT, (powerAt<GG, V><<<d.nb_pi - d.nb_pi_s, kBlock, 0, s>>>(pa, mt, 0, d.nlP, d.nb_pi_s)));
+            ++launches;
+        }
         powerFinish1<<<1, kBlock, 0, s>>>(pa);
         powerNormalize<<<d.nb_pi, kBlock, 0, s>>>(pa);
         powerFinish2<<<1, kBlock, 0, s>>>(pa);
@@ -354,6 +415,21 @@ void packRows(const ScaledLp& sc, std::vector<RowPack<T>>& out) {
                             static_cast<T>(sc.row_type[i])};
 }
 
+// Vectors between the original numbering and the device numbering
+// (pos: original -> device; empty = identity).
+void toDevice(std::vector<double>& v, const std::vector<int32_t>& pos) {
+    if (pos.empty()) return;
+    std::vector<double> w(v.size());
+    for (size_t k = 0; k < v.size(); ++k) w[pos[k]] = v[k];
+    v.swap(w);
+}
+void fromDevice(std::vector<double>& v, const std::vector<int32_t>& pos) {
+    if (pos.empty()) return;
+    std::vector<double> w(v.size());
+    for (size_t k = 0; k < v.size(); ++k) w[k] = v[pos[k]];
+    v.swap(w);
+}
+
 bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
     if (lim < 0.0) return false;
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= lim;
@@ -361,8 +437,97 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
 
 }  // namespace
 
+// Rows of one matrix side far longer than the rest (more entries than
+// max(64, 8 x the mean)): the renumbering that puts them first, longest first,
+// the other rows after them in their original order.  Returns their count
+// (0 and an empty order: no such rows, identity).
+static int32_t longRowsFirst(const Csr& a, std::vector<int32_t>& order) {
+    order.clear();
+    const int32_t rows = a.rows;
+    if (rows == 0) return 0;
+    const double mean = static_cast<double>(a.nnz()) / rows;
+    const int32_t thr = std::max<int32_t>(64, static_cast<int32_t>(8.0 * mean));
+    std::vector<int32_t> lng, sht;
+    for (int32_t i = 0; i < rows; ++i) (a.ptr[i + 1] - a.ptr[i] > thr ? lng : sht).push_back(i);
+    if (lng.empty()) return 0;
+    std::stable_sort(lng.begin(), lng.end(),
+                     [&](int32_t x, int32_t y) { return a.ptr[x + 1] - a.ptr[x] > a.ptr[y + 1] - a.ptr[y]; });
+    order = lng;
+    order.insert(order.end(), sht.begin(), sht.end());
+    return static_cast<int32_t>(lng.size());
+}
+
+// The scaled LP with its rows in order `ro` and columns in order `co` (new
+// position -> original; empty = identity); rpos / cpos receive original ->
+// new.  Entries keep their place inside their row.
+static void permuteScaled(const ScaledLp& sc, const std::vector<int32_t>& ro, const std::vector<int32_t>& co,
+                          ScaledLp& out, std::vector<int32_t>& rpos, std::vector<int32_t>& cpos) {
+    const int32_t m = sc.a.rows, n = sc.a.cols;
+    auto inverse = [](const std::vector<int32_t>& ord, int32_t k, std::vector<int32_t>& pos) {
+        pos.resize(k);
+        for (int32_t q = 0; q < k; ++q) pos[ord.empty() ? q : ord[q]] = q;
+    };
+    inverse(ro, m, rpos);
+    inverse(co, n, cpos);
+    auto oldRow = [&](int32_t i) { return ro.empty() ? i : ro[i]; };
+    auto oldCol = [&](int32_t j) { return co.empty() ? j : co[j]; };
+    out.obj_sign = sc.obj_sign;
+    out.obj_scale = sc.obj_scale;
+    out.con_scale = sc.con_scale;
+    out.precond_pw = sc.precond_pw;
+    auto permuteCsr = [](const Csr& a, int32_t rows, int32_t cols, const std::function<int32_t(int32_t)>& old,
+                         const std::vector<int32_t>& idxPos, Csr& b) {
+        b.rows = rows;
+        b.cols = cols;
+        b.ptr.assign(1, 0);
+        b.ptr.reserve(rows + 1);
+        b.idx.clear();
+        b.val.clear();
+        b.idx.reserve(a.idx.size());
+        b.val.reserve(a.val.size());
+        for (int32_t r = 0; r < rows; ++r) {
+            const int32_t o = old(r);
+            for (int32_t k = a.ptr[o]; k < a.ptr[o + 1]; ++k) {
+                b.idx.push_back(idxPos[a.idx[k]]);
+                b.val.push_back(a.val[k]);
+            }
+            b.ptr.push_back(static_cast<int32_t>(b.idx.size()));
+        }
+    };
+    permuteCsr(sc.a, m, n, oldRow, cpos, out.a);
+    permuteCsr(sc.at, n, m, oldCol, rpos, out.at);
+    auto cols = [&](const std::vector<double>& v, std::vector<double>& w) {
+        w.resize(n);
+        for (int32_t j = 0; j < n; ++j) w[j] = v[oldCol(j)];
+    };
+    auto rowsOf = [&](const std::vector<double>& v, std::vector<double>& w) {
+        w.resize(m);
+        for (int32_t i = 0; i < m; ++i) w[i] = v[oldRow(i)];
+    };
+    cols(sc.c, out.c);
+    cols(sc.cl, out.cl);
+    cols(sc.cu, out.cu);
+    cols(sc.col_scale, out.col_scale);
+    cols(sc.tau, out.tau);
+    rowsOf(sc.rl, out.rl);
+    rowsOf(sc.ru, out.ru);
+    rowsOf(sc.row_scale, out.row_scale);
+    rowsOf(sc.sigma, out.sigma);
+    out.row_type.resize(m);
+    for (int32_t i = 0; i < m; ++i) out.row_type[i] = sc.row_type[oldRow(i)];
+}
+
+// Launch shape of the long rows of one side, from their mean length.
+static int longShape(int64_t nnz, int32_t rows) {
+    const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
+    if (mean <= 128) return 9;   // G=32
+    if (mean <= 384) return 11;  // G=64
+    if (mean <= 768) return 13;  // G=128, U=8
+    return 15;                   // G=256, U=8
+}
+
 // Build (or rebuild) the device image of the scaled LP.
-static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, const pdlpx_options& o,
+static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in, const pdlpx_options& o,
                            std::string& err) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
@@ -376,18 +541,36 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc, co
     d.device = dev;
     PDLPX_CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
     PDLPX_CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    // Skewed sides: long rows first in the device numbering (identity otherwise).
+    std::vector<int32_t> ro, co;
+    d.nlD = longRowsFirst(sc_in.a, ro);
+    d.nlP = longRowsFirst(sc_in.at, co);
+    ScaledLp permuted;
+    if (d.nlD > 0 || d.nlP > 0) permuteScaled(sc_in, ro, co, permuted, d.rpos, d.cpos);
+    const ScaledLp& sc = (d.nlD > 0 || d.nlP > 0) ? permuted : sc_in;
+    if (d.nlD == 0) d.rpos.clear();
+    if (d.nlP == 0) d.cpos.clear();
     d.m = sc.a.rows;
     d.n = sc.a.cols;
     d.nnz = sc.a.nnz();
     d.mixed = o.precision != PDLPX_PREC_FP64;
     const int64_t m = d.m, n = d.n, nnz = d.nnz;
-    d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz, d.m);
-    d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz, d.n);
-    d.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, nnz, d.m);
-    d.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, nnz, d.n);
+    const int64_t zlD = d.nlD > 0 ? sc.a.ptr[d.nlD] : 0, zlP = d.nlP > 0 ? sc.at.ptr[d.nlP] : 0;
+    const int32_t msD = d.m - d.nlD, msP = d.n - d.nlP;  // short rows
+    d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz - zlD, msD);
+    d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz - zlP, msP);
+    d.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, nnz - zlD, msD);
+    d.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, nnz - zlP, msP);
+    d.gLA = d.nlD > 0 ? std::min(256, pickGroup(zlD, d.nlD)) : 1;
+    d.gLAT = d.nlP > 0 ? std::min(256, pickGroup(zlP, d.nlP)) : 1;
+    d.shapeLD = longShape(zlD, d.nlD);
+    d.shapeLP = longShape(zlP, d.nlP);
     const int cap = 4 * d.sms;
-    d.nb_rows = std::max(1, std::min(gridFor(m, d.gA), cap));
-    d.nb_cols = std::max(1, std::min(gridFor(n, d.gAT), cap));
+    d.nb_rows_s = std::max(1, std::min(gridFor(msD, d.gA), cap));
+    d.nb_cols_s = std::max(1, std::min(gridFor(msP, d.gAT), cap));
+    d.nb_rows = d.nb_rows_s + (d.nlD > 0 ? std::max(1, std::min(gridFor(d.nlD, d.gLA), cap)) : 0);
+    d.nb_cols = d.nb_cols_s + (d.nlP > 0 ? std::max(1, std::min(gridFor(d.nlP, d.gLAT), cap)) : 0);
+    d.nb_pi_s = d.nb_cols_s;
     d.nb_pi = d.nb_cols;
 
     // Arena layout.
@@ -559,14 +742,14 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
         }
     } guard{e0, e1};
     auto timeShape = [&](bool primal, int shape, float& ms) -> int32_t {
-        const int grid = primal ? gridForShape(d.n, shape) : gridForShape(d.m, shape);
+        const int grid = primal ? gridForShape(d.n - d.nlP, shape) : gridForShape(d.m - d.nlD, shape);
         constexpr int reps = 5;
         for (int r = 0; r <= reps; ++r) {
             if (r == 1) PDLPX_CK(cudaEventRecord(e0, s));
             if (primal) {
-                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1)));
+                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1, d.nlP, d.n)));
             } else {
-                PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1)));
+                PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1, d.nlD, d.m)));
             }
         }
         PDLPX_CK(cudaEventRecord(e1, s));
@@ -868,6 +1051,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
         xn = std::sqrt(xn);
         if (xn < 1e-15) xn = 1.0;
         for (auto& v : x0) v /= xn;
+        toDevice(x0, d.cpos);
         PDLPX_CK(cudaMemcpyAsync(d.pi_x, x0.data(), 8 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
         PowerState ps0{1.0, 0.0, 0.0, 0, opt_.sv_max_iter <= 0 ? 1 : 0};
         *d.h_ps = ps0;
@@ -977,6 +1161,8 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
         wy.resize(m);
         for (int32_t j = 0; j < n; ++j) wx[j] = warm_x_[j] / sc_.col_scale[j] * sc_.con_scale;
         for (int32_t i = 0; i < m; ++i) wy[i] = warm_y_[i] * sc_.obj_scale / (sc_.obj_sign * sc_.row_scale[i]);
+        toDevice(wx, d.cpos);
+        toDevice(wy, d.rpos);
     }
     if (d.mixed) {
         std::vector<float> fx(n, 0.0f), fy(m, 0.0f);
@@ -1088,6 +1274,8 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
             PDLPX_CK(cudaMemcpyAsync(yh.data(), d.yh64, 8 * static_cast<size_t>(m), cudaMemcpyDeviceToHost, s));
             PDLPX_CK(cudaStreamSynchronize(s));
         }
+        fromDevice(xh, d.cpos);
+        fromDevice(yh, d.rpos);
     }
     objective_ = 0.0;
     if (status == PDLPX_STATUS_OPTIMAL) {
@@ -1149,23 +1337,17 @@ int32_t timeStepKernels(DeviceLp& d, const pdlpx_options& o, int reps, float ms[
     const IterArgs<T> ia = iterArgs<T>(d, o);
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
-    const int gp = gridForShape(d.n, d.shapeP), gd = gridForShape(d.m, d.shapeD);
     cudaEvent_t ev[4];
     for (auto& e : ev) PDLPX_CK(cudaEventCreate(&e));
-    // warm-up launch of each
-    PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, 1)));
-    PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    // warm-up launch of each; a step's time covers its long- and short-row launches
+    launchPrimal<T>(d, ia, 1, s);
+    launchDual<T>(d, ia, 1, s);
     PDLPX_CK(cudaEventRecord(ev[0], s));
-    for (int r = 0; r < reps; ++r)
-        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gp, kBlock, 0, s>>>(ia, 1)));
+    for (int r = 0; r < reps; ++r) launchPrimal<T>(d, ia, 1, s);
     PDLPX_CK(cudaEventRecord(ev[1], s));
-    for (int r = 0; r < reps; ++r)
-        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gd, kBlock, 0, s>>>(ia, 1)));
+    for (int r = 0; r < reps; ++r) launchDual<T>(d, ia, 1, s);
     PDLPX_CK(cudaEventRecord(ev[2], s));
-    for (int r = 0; r < reps; ++r) {
-        PDLPX_G_SWITCH(d.gA, (checkRows<GG, T><<<d.nb_rows, kBlock, 0, s>>>(ca)));
-        PDLPX_G_SWITCH(d.gAT, (checkCols<GG, T><<<d.nb_cols, kBlock, 0, s>>>(ca)));
-    }
+    for (int r = 0; r < reps; ++r) launchChecks<T>(d, ca, s);
     PDLPX_CK(cudaEventRecord(ev[3], s));
     PDLPX_CK(cudaGetLastError());
     PDLPX_CK(cudaEventSynchronize(ev[3]));
@@ -1212,8 +1394,8 @@ int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd
     if (!dev_) return PDLPX_E_NOT_LOADED;
     if (ga) *ga = kShapes[dev_->shapeD].G;
     if (gat) *gat = kShapes[dev_->shapeP].G;
-    if (bp) *bp = gridForShape(dev_->n, dev_->shapeP);
-    if (bd) *bd = gridForShape(dev_->m, dev_->shapeD);
+    if (bp) *bp = gridForShape(dev_->n - dev_->nlP, dev_->shapeP);
+    if (bd) *bd = gridForShape(dev_->m - dev_->nlD, dev_->shapeD);
     return PDLPX_OK;
 }
 

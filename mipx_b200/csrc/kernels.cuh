@@ -460,10 +460,13 @@ __device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jen
     primalRowsFrom<G, R, U, T>(p, j0, jend, b, e, koff);
 }
 
+// Columns [begin, end) of A^T (the engine launches long and short columns
+// separately when their lengths are far apart).
 template <int G, int R, int U, class T>
-__global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff) {
+__global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff, int begin, int end) {
     constexpr int slab = kBlock / G;
-    primalRows<G, R, U, T>(p, blockIdx.x * (slab * R) + threadIdx.x / G, p.n, koff);
+    primalRows<G, R, U, T>(p, begin + static_cast<int>(blockIdx.x) * (slab * R) + static_cast<int>(threadIdx.x) / G, end,
+                           koff);
 }
 
 // Fused A x_refl + dual proximal step (pdlp_kernels.cu:94-157), same structure.
@@ -516,9 +519,10 @@ __device__ __forceinline__ void dualRows(const IterArgs<T>& p, int i0, int iend,
 }
 
 template <int G, int R, int U, class T>
-__global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff) {
+__global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff, int begin, int end) {
     constexpr int slab = kBlock / G;
-    dualRows<G, R, U, T>(p, blockIdx.x * (slab * R) + threadIdx.x / G, p.m, koff);
+    dualRows<G, R, U, T>(p, begin + static_cast<int>(blockIdx.x) * (slab * R) + static_cast<int>(threadIdx.x) / G, end,
+                         koff);
 }
 
 // ---- block reduction of NS slots with per-slot operators -------------------
@@ -679,13 +683,14 @@ __device__ __forceinline__ void checkRowsRange(const CheckArgs<T>& p, const DevC
     blockReduceSlots<kRowSlots>(acc, ops, out);
 }
 
+// Rows [begin, end), block partials from slot part0 on.
 template <int G, class T>
-__global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p) {
+__global__ void __launch_bounds__(kBlock) checkRows(CheckArgs<T> p, int begin, int end, int part0) {
     const DevState* st = p.st;
     if (st->done || st->prec != precTag<T>()) return;
     constexpr int per_block = kBlock / G;
-    checkRowsRange<G, T>(p, *p.dc, blockIdx.x * per_block, p.m, gridDim.x * per_block,
-                         p.part_rows + static_cast<size_t>(blockIdx.x) * kRowSlots);
+    checkRowsRange<G, T>(p, *p.dc, begin + static_cast<int>(blockIdx.x) * per_block, end, gridDim.x * per_block,
+                         p.part_rows + static_cast<size_t>(part0 + blockIdx.x) * kRowSlots);
 }
 
 // FP64 column pass: A^T y_hat and A^T (y_hat - y_init) in one sweep, column
@@ -724,12 +729,12 @@ __device__ __forceinline__ void checkColsRange(const CheckArgs<T>& p, const DevC
 }
 
 template <int G, class T>
-__global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p) {
+__global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p, int begin, int end, int part0) {
     const DevState* st = p.st;
     if (st->done || st->prec != precTag<T>()) return;
     constexpr int per_block = kBlock / G;
-    checkColsRange<G, T>(p, *p.dc, blockIdx.x * per_block, p.n, gridDim.x * per_block,
-                         p.part_cols + static_cast<size_t>(blockIdx.x) * kColSlots);
+    checkColsRange<G, T>(p, *p.dc, begin + static_cast<int>(blockIdx.x) * per_block, end, gridDim.x * per_block,
+                         p.part_cols + static_cast<size_t>(part0 + blockIdx.x) * kColSlots);
 }
 
 // Restart copy x_init = x_cur = x_hat, y_init = y_cur = y_hat (pdlp_kernels.cu:377-405),
@@ -791,25 +796,25 @@ struct PowerMat {
     const V* at_val;
 };
 template <int G, class V>
-__global__ void __launch_bounds__(kBlock) powerA(PowerArgs a, PowerMat<V> mt) {
+__global__ void __launch_bounds__(kBlock) powerA(PowerArgs a, PowerMat<V> mt, int begin, int end) {
     if (a.ps->done) return;
     const int t = blockIdx.x * kBlock + threadIdx.x;
-    const int i = t / G, lane = t % G;
-    const bool valid = i < a.m;
+    const int i = begin + t / G, lane = t % G;
+    const bool valid = i < end;
     double s = 0.0;
     if (valid) s = rowDot<G, double>(mt.a_ptr[i], mt.a_ptr[i + 1], lane, mt.a_idx, mt.a_val, a.x);
     s = groupSum<G>(s);
     if (valid && lane == 0) a.y[i] = s;
 }
 template <int G, class V>
-__global__ void __launch_bounds__(kBlock) powerAt(PowerArgs a, PowerMat<V> mt) {
+__global__ void __launch_bounds__(kBlock) powerAt(PowerArgs a, PowerMat<V> mt, int begin, int end, int part0) {
     if (a.ps->done) return;
     const int per_block = kBlock / G;
     const int lane = threadIdx.x % G;
     double acc[2] = {0.0, 0.0};
-    for (int base = blockIdx.x * per_block; base < a.n; base += gridDim.x * per_block) {
+    for (int base = begin + static_cast<int>(blockIdx.x) * per_block; base < end; base += gridDim.x * per_block) {
         const int j = base + threadIdx.x / G;
-        const bool valid = j < a.n;
+        const bool valid = j < end;
         double s = 0.0;
         if (valid) s = rowDot<G, double>(mt.at_ptr[j], mt.at_ptr[j + 1], lane, mt.at_idx, mt.at_val, a.y);
         s = groupSum<G>(s);
@@ -820,7 +825,7 @@ __global__ void __launch_bounds__(kBlock) powerAt(PowerArgs a, PowerMat<V> mt) {
         }
     }
     const int ops[2] = {OP_SUM, OP_SUM};
-    blockReduceSlots<2>(acc, ops, a.part + static_cast<size_t>(blockIdx.x) * 2);
+    blockReduceSlots<2>(acc, ops, a.part + static_cast<size_t>(part0 + blockIdx.x) * 2);
 }
 __global__ void powerFinish1(PowerArgs a);
 __global__ void __launch_bounds__(kBlock) powerNormalize(PowerArgs a);
