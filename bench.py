@@ -67,6 +67,11 @@ def parse():
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--profile", type=int, default=0, metavar="ITERS",
                    help="profiling run: one solve of the workload capped at ITERS iterations, no JSON line")
+    p.add_argument("--profile-batch", type=int, default=0, metavar="LPS",
+                   help="profiling run: one pdlpx_batch_solve of the first LPS LPs of the batched workload")
+    p.add_argument("--profile-large", type=int, default=0, metavar="M",
+                   help="profiling run: one solve of an M x 4M power-law LP (column counts 2-2000, mean 10)")
+    p.add_argument("--profile-iters", type=int, default=2000, help="iteration cap of --profile-batch / --profile-large")
     return p.parse_args()
 
 
@@ -207,6 +212,29 @@ def cpu_baseline(lp, budget_iters=(200, 400)) -> dict:
             "seconds": sum(times)}
 
 
+def profile_run(args, local) -> None:
+    """Capped runs of the batched and large workloads for ncu (no JSON line)."""
+    from mipx_b200 import generators as G
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver, batch_solve
+    o = PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local,
+                    max_iter=args.profile_iters)
+    if args.profile_batch:
+        sizes = G.batch_sizes(512, seed=5)[:args.profile_batch]
+        lps = [G.random_lp(m, n, 4, 12, 1000 + k)[0] for k, (m, n) in enumerate(sizes)]
+        out = batch_solve(lps, o)
+        print(f"profile batch: {len(lps)} LPs, {sum(r.iterations for r, _, _ in out)} LP-iterations, "
+              f"device {out[0][0].device_seconds:.3f}s, launches {out[0][0].kernel_launches}", flush=True)
+    if args.profile_large:
+        m = args.profile_large
+        lp, _ = G.powerlaw_lp(m, 4 * m, 2, 2000, 10.0, 0.01, 1e3, 11)
+        s = PdlpSolver()
+        s.setOptions(o)
+        s.load(lp)
+        r = s.solve()
+        print(f"profile large: {m} x {4 * m}, {lp.matrix.numNonzeros()} nnz, {r.iterations} iterations, "
+              f"device {r.device_seconds:.3f}s, config {s.launchConfig()}", flush=True)
+
+
 def batch_workload(rank, world, local, count=512, single_sample=16) -> dict:
     """The batched workload: `count` random sparse LPs of lognormal size (median
     1,500 rows, sigma 0.8, clipped to [200, 20,000], n = 2.5 m, 4-12 nonzeros per
@@ -318,6 +346,9 @@ def main():
     rank, world, local, pg = dist_init(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, pg)
+        return
+    if args.profile_batch or args.profile_large:
+        profile_run(args, local)
         return
     import torch
 

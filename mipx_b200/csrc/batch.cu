@@ -115,9 +115,11 @@ constexpr int kCtlWarps = 4;  // LPs per block of the per-LP kernels
 #ifndef PDLPX_PACK_MIN_BLOCKS
 #define PDLPX_PACK_MIN_BLOCKS 5
 #endif
-// Same for the sliced-ELL step kernels.
+// Same for the sliced-ELL step kernels: 8 blocks (32 registers) measured 28%
+// faster per iteration of the 512-LP pack than 4 blocks in the FP32 phase and
+// equal in the FP64 phase.
 #ifndef PDLPX_SELL_MIN_BLOCKS
-#define PDLPX_SELL_MIN_BLOCKS 4
+#define PDLPX_SELL_MIN_BLOCKS 8
 #endif
 
 __device__ __forceinline__ double combine(int op, double a, double b) {
@@ -1482,9 +1484,10 @@ int batchSideShape(int pinned, int group, bool sell, int64_t nnz, int32_t rows) 
     if (pinned > kNumShapes && pinned <= kNumShapes + kNumSell) return pinned - 1;
     if (pinned > 0 || group > 0) return chooseShape(pinned, group, nnz, rows, true);
     const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
-    // measured on 512 lognormal-sized LPs (mean 8 / 20 entries per column / row):
-    // 4 entries per round on the columns and 8 on the rows beat 8 / 16 by ~30%
-    if (sell && mean <= 32.0) return kNumShapes + (mean <= 8.0 ? 0 : 1);
+    // measured on 512 lognormal-sized LPs (mean 8 / 20 entries per column / row,
+    // us per iteration of the full pack, FP32 / FP64 phase): 4 entries per round
+    // on the columns and 8 on the rows 127 / 132; 8 and 8: 181 / 171
+    if (sell && mean <= 32.0) return kNumShapes + (mean <= 12.0 ? 0 : 1);
     return batchShape(nnz, rows);
 }
 
