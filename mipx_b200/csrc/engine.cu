@@ -21,6 +21,7 @@
 
 #include "engine.hpp"
 #include "kernels.cuh"
+#include "anderson.cuh"
 #include "control.cuh"
 #include "shapes.cuh"
 
@@ -183,6 +184,12 @@ struct DeviceLp {
     double *prev_ax = nullptr, *prev_xh = nullptr;
     double *pi_x = nullptr, *pi_y = nullptr, *pi_xn = nullptr, *pi_part = nullptr;
     double *part_rows = nullptr, *part_cols = nullptr;
+    // Anderson acceleration at restarts (anderson.cuh); aa_w = 0 when off.
+    int aa_w = 0, aa_nb = 1;
+    double *aa_X = nullptr, *aa_R = nullptr, *aa_out = nullptr, *aa_part = nullptr, *aa_gram = nullptr,
+           *aa_work = nullptr;
+    int* aa_order = nullptr;
+    AaState* aa_st = nullptr;
     DevState* st = nullptr;
     DevConst* dc = nullptr;
     PowerState* ps = nullptr;
@@ -254,6 +261,26 @@ struct DeviceLp {
         a.max_iter = o.max_iter;
         a.polish_max_iter = o.polish_max_iter;
         a.N = o.termination_eval_frequency;
+        return a;
+    }
+    AaArgs aaArgs(double reg) const {
+        AaArgs a{};
+        a.X = aa_X;
+        a.Rr = aa_R;
+        a.out = aa_out;
+        a.part = aa_part;
+        a.gram = aa_gram;
+        a.work = aa_work;
+        a.order = aa_order;
+        a.as = aa_st;
+        a.st = st;
+        a.lb = lb64;
+        a.ub = ub64;
+        a.n = n;
+        a.m = m;
+        a.w = aa_w;
+        a.nb = aa_nb;
+        a.reg = reg;
         return a;
     }
     template <class T>
@@ -365,7 +392,20 @@ int launchCycle(DeviceLp& d, const pdlpx_options& o) {
     launches += launchChecks<T>(d, ca, s) - 2;
     controller<<<1, kBlock, 0, s>>>(d.st, d.dc, d.part_rows, d.part_cols, sizeof(T) == 8 ? 1 : 0);
     const int nb = std::max(1, std::min(gridFor(std::max(d.m, d.n), 1), 8 * d.sms));
-    restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc);
+    const AaArgs aa = d.aaArgs(o.anderson_regularization);
+    if (d.aa_w > 0) {
+        aaStore<T><<<d.aa_nb, kBlock, 0, s>>>(aa, ia.xh, ia.xi, ia.yh, ia.yi);
+        aaSolve<<<1, 32, 0, s>>>(aa);
+        aaExtrapolate<<<d.aa_nb, kBlock, 0, s>>>(aa);
+        aaDecide<<<1, 32, 0, s>>>(aa);
+        launches += 4;
+    }
+    restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc,
+                                         d.aa_w > 0 ? &d.aa_st->accepted : nullptr);
+    if (d.aa_w > 0) {
+        aaApply<T><<<nb, kBlock, 0, s>>>(aa, ia.xi, ia.yi, ia.xc, ia.yc);
+        ++launches;
+    }
     launches += 4;
     if (sizeof(T) == 4 && d.mixed) {
         PromoteArgs pa{d.xi32, d.xh32, d.yi32, d.yh32, d.xi64, d.xh64, d.yi64, d.yh64, d.st, d.n, d.m};
@@ -603,6 +643,22 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     const size_t o_pi_x = take(8 * n), o_pi_y = take(8 * m), o_pi_xn = take(8 * n),
                  o_pi_part = take(8 * 2 * d.nb_pi);
     const size_t o_prow = take(8 * kRowSlots * d.nb_rows), o_pcol = take(8 * kColSlots * d.nb_cols);
+    // Anderson ring (2 w (n + m) doubles), extrapolation scratch, partials, Gram matrix.
+    d.aa_w = o.anderson_acceleration && o.anderson_window_size >= 2 ? o.anderson_window_size : 0;
+    const size_t dim = static_cast<size_t>(n) + static_cast<size_t>(m);
+    size_t o_aa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (d.aa_w > 0) {
+        const size_t w = static_cast<size_t>(d.aa_w);
+        d.aa_nb = std::max(1, std::min(gridFor(static_cast<int64_t>(dim), 1), 4 * d.sms));
+        o_aa[0] = take(8 * w * dim);
+        o_aa[1] = take(8 * w * dim);
+        o_aa[2] = take(8 * dim);
+        o_aa[3] = take(8 * static_cast<size_t>(d.aa_nb) * std::max<size_t>(w, 2));
+        o_aa[4] = take(8 * w * w);
+        o_aa[5] = take(8 * (2 * w * w + 2 * w));
+        o_aa[6] = take(4 * w);
+        o_aa[7] = take(sizeof(AaState));
+    }
     const size_t o_st = take(sizeof(DevState)), o_dc = take(sizeof(DevConst)), o_ps = take(sizeof(PowerState));
     d.arena_bytes = off;
     PDLPX_CK(cudaMalloc(reinterpret_cast<void**>(&d.arena), d.arena_bytes));
@@ -654,6 +710,16 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.pi_part = reinterpret_cast<double*>(b + o_pi_part);
     d.part_rows = reinterpret_cast<double*>(b + o_prow);
     d.part_cols = reinterpret_cast<double*>(b + o_pcol);
+    if (d.aa_w > 0) {
+        d.aa_X = reinterpret_cast<double*>(b + o_aa[0]);
+        d.aa_R = reinterpret_cast<double*>(b + o_aa[1]);
+        d.aa_out = reinterpret_cast<double*>(b + o_aa[2]);
+        d.aa_part = reinterpret_cast<double*>(b + o_aa[3]);
+        d.aa_gram = reinterpret_cast<double*>(b + o_aa[4]);
+        d.aa_work = reinterpret_cast<double*>(b + o_aa[5]);
+        d.aa_order = reinterpret_cast<int*>(b + o_aa[6]);
+        d.aa_st = reinterpret_cast<AaState*>(b + o_aa[7]);
+    }
     d.st = reinterpret_cast<DevState*>(b + o_st);
     d.dc = reinterpret_cast<DevConst*>(b + o_dc);
     d.ps = reinterpret_cast<PowerState*>(b + o_ps);
@@ -982,8 +1048,8 @@ int32_t Engine::solve(pdlpx_result* out) {
         last_error = "solve before load";
         return PDLPX_E_NOT_LOADED;
     }
-    if (opt_.anderson_acceleration && opt_.anderson_window_size >= 2) {
-        last_error = "anderson_acceleration is not available in the device engine";
+    if (opt_.anderson_acceleration && opt_.anderson_window_size > 64) {
+        last_error = "anderson_window_size above 64";
         return PDLPX_E_INVALID;
     }
     if (opt_.termination_eval_frequency <= 0) {
@@ -1006,7 +1072,9 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     std::memset(out, 0, sizeof(*out));
     used_gpu_ = false;
     const bool want_mixed = opt_.precision != PDLPX_PREC_FP64;
-    if (!dev_ || dev_->mixed != want_mixed || (opt_.adaptive_step != 0) != (dev_->prev_ax != nullptr)) {
+    const int want_aa = opt_.anderson_acceleration && opt_.anderson_window_size >= 2 ? opt_.anderson_window_size : 0;
+    if (!dev_ || dev_->mixed != want_mixed || (opt_.adaptive_step != 0) != (dev_->prev_ax != nullptr) ||
+        dev_->aa_w != want_aa) {
         const int32_t rc = buildDevice(dev_, sc_, opt_, err);
         if (rc != PDLPX_OK) {
             dev_.reset();
@@ -1190,6 +1258,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
             PDLPX_CK(cudaMemcpyAsync(p, wy.data(), 8 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
         PDLPX_CK(cudaStreamSynchronize(s));
     }
+    if (d.aa_st) PDLPX_CK(cudaMemsetAsync(d.aa_st, 0, sizeof(AaState), s));
     if (d.prev_ax) {
         PDLPX_CK(cudaMemsetAsync(d.prev_ax, 0, 8 * static_cast<size_t>(m), s));
         PDLPX_CK(cudaMemsetAsync(d.prev_xh, 0, 8 * static_cast<size_t>(n), s));

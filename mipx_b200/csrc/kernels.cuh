@@ -738,11 +738,15 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p, int begin, i
 }
 
 // Restart copy x_init = x_cur = x_hat, y_init = y_cur = y_hat (pdlp_kernels.cu:377-405),
-// executed only when the controller decided to restart.
+// executed only when the controller decided to restart, and skipped when `skip`
+// (the Anderson step's verdict, or null) says the extrapolated point was written
+// instead.
 template <class T>
 __global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n, int m, const T* xh,
-                                                     const T* yh, T* xi, T* yi, double* xc, double* yc) {
+                                                     const T* yh, T* xi, T* yi, double* xc, double* yc,
+                                                     const int* skip) {
     if (st->done || st->prec != precTag<T>() || !st->restart) return;
+    if (skip != nullptr && *skip) return;
     for (int k = blockIdx.x * kBlock + threadIdx.x; k < (n > m ? n : m); k += gridDim.x * kBlock) {
         if (k < n) {
             const T v = xh[k];

@@ -36,6 +36,9 @@ def quiet(**kw) -> PdlpOptions:
 
 
 TIGHT = dict(primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
+# Launch-shape and batching knobs of the device engine: no meaning for the
+# reference, left at their defaults when the cases are replayed.
+ENGINE_ONLY = {"autotune", "shape_primal", "shape_dual", "batch_pack_mb", "batch_compact", "batch_sell"}
 
 CASES = {
     # name: (problem builder, options) -- options follow the mipx test that uses the LP
@@ -62,6 +65,11 @@ CASES = {
     "medium_tight": (F.medium_lp, quiet(max_iter=500000, **TIGHT)),
     "medium_norescale": (F.medium_lp, quiet(max_iter=500000, do_bound_obj_rescaling=False)),
     "medium_polish7": (F.medium_lp, quiet(max_iter=500000, polish_primal_tol=1e-7, polish_dual_tol=1e-7)),
+    # Anderson acceleration at restarts (test_pdlp.cpp:1204-1310)
+    "simple_anderson": (F.simple_lp, quiet(max_iter=50000, anderson_acceleration=True, anderson_window_size=5)),
+    "simple_anderson_w2": (F.simple_lp, quiet(max_iter=50000, anderson_acceleration=True, anderson_window_size=2)),
+    "equality_anderson": (F.equality_lp, quiet(max_iter=100000, anderson_acceleration=True, anderson_window_size=5)),
+    "medium_anderson": (F.medium_lp, quiet(max_iter=500000, anderson_acceleration=True, anderson_window_size=5)),
 }
 GENERATED = {
     # name: (m, n, lo, hi, seed)
@@ -69,6 +77,10 @@ GENERATED = {
     "rand_200x500": (200, 500, 4, 12, 4),
     "rand_500x1250": (500, 1250, 4, 12, 5),
     "rand_2000x5000": (2000, 5000, 4, 12, 1),
+}
+# Generated LPs solved with Anderson acceleration (window 5), same tolerances.
+GENERATED_AA = {
+    "rand_500x1250_anderson": (500, 1250, 4, 12, 5),
 }
 
 # LPs too large for the reference's CPU PDLP in a test budget: HiGHS optimum only.
@@ -101,17 +113,21 @@ def main() -> None:
     todo = [(k, b(), o) for k, (b, o) in CASES.items()]
     for name, (m, n, lo, hi, seed) in GENERATED.items():
         todo.append((name, G.random_lp(m, n, lo, hi, seed)[0], quiet(max_iter=500000, **TIGHT)))
+    for name, (m, n, lo, hi, seed) in GENERATED_AA.items():
+        todo.append((name, G.random_lp(m, n, lo, hi, seed)[0],
+                     quiet(max_iter=500000, anderson_acceleration=True, anderson_window_size=5, **TIGHT)))
     for name, lp, opts in todo:
         res, x, y = O.ref_solve(lp, opts)
         entry = {
             "status": int(res.status), "objective": res.objective, "iterations": res.iterations,
             "work_units": res.work_units, "m": lp.num_rows, "n": lp.num_cols,
             "options": {k: (int(v) if isinstance(v, bool) else v) for k, v in vars(opts).items()
-                        if k != "stop_flag" and not isinstance(v, object.__class__)},
+                        if k != "stop_flag" and k not in ENGINE_ONLY and not isinstance(v, object.__class__)},
         }
         entry["options"] = {k: (v if not hasattr(v, "value") else int(v)) for k, v in entry["options"].items()}
-        if name in GENERATED:
-            entry["generator"] = dict(zip(("m", "n", "nnz_lo", "nnz_hi", "seed"), GENERATED[name]))
+        if name in GENERATED or name in GENERATED_AA:
+            gen = GENERATED.get(name) or GENERATED_AA[name]
+            entry["generator"] = dict(zip(("m", "n", "nnz_lo", "nnz_hi", "seed"), gen))
             entry["highs_objective"] = highs_objective(lp)
         index[name] = entry
         arrays[f"{name}__x"] = x

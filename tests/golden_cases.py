@@ -24,6 +24,8 @@ BUILDERS = {
     "large_rhs": F.large_rhs_lp, "equality": F.equality_lp, "equality_polish": F.equality_lp,
     "filter": F.filter_lp, "maximize": F.maximize_lp, "ranged": F.ranged_lp, "medium": F.medium_lp,
     "medium_tight": F.medium_lp, "medium_norescale": F.medium_lp, "medium_polish7": F.medium_lp,
+    "simple_anderson": F.simple_lp, "simple_anderson_w2": F.simple_lp, "equality_anderson": F.equality_lp,
+    "medium_anderson": F.medium_lp,
 }
 
 
