@@ -255,7 +255,8 @@ int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_option
  * pack as soon as a stream and memory are free, and each LP's result is
  * available as soon as the restart cycle that finishes it returns.  An LP's
  * result does not depend on what it was packed with (bit-identical alone and
- * in any mix, same options). */
+ * in any mix, same options); a family member's result does not depend on the
+ * other members of its family pack. */
 typedef struct pdlpx_server pdlpx_server;
 
 typedef struct pdlpx_server_config {
@@ -266,7 +267,11 @@ typedef struct pdlpx_server_config {
     int32_t queue_limit;   /* unfinished requests before submit returns PDLPX_E_BUSY, default 100000 */
     int32_t batch_window_ms; /* a pack starts when max_pack_lps requests are ready or the oldest ready
                                 request has waited this long (default 50; 0 = start at once) */
-    int32_t reserved[3];
+    int32_t families;      /* 1 (default): a request submitted with a warm-start ticket whose rows begin
+                              with the ticket's rows unchanged (a branch-and-bound node: new bounds,
+                              appended rows) is solved in a family pack with the other nodes of that
+                              ticket -- the shared rows stored once, FP64 iterates; 0: regular packs */
+    int32_t reserved[2];
 } pdlpx_server_config;
 
 typedef struct pdlpx_server_stats {

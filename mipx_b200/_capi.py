@@ -69,7 +69,7 @@ class GenLp(C.Structure):
 # (name, restype, argtypes) of every entry point declared in include/pdlpx.h
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", f64), ("max_packs", i32), ("max_pack_lps", i32), ("prep_threads", i32),
-                ("queue_limit", i32), ("batch_window_ms", i32), ("reserved", i32 * 3)]
+                ("queue_limit", i32), ("batch_window_ms", i32), ("families", i32), ("reserved", i32 * 2)]
 
 
 class ServerStats(C.Structure):

@@ -1019,6 +1019,57 @@ struct Pack {
 
 // Host image of one LP's share of the pack, in the pack numbering (renumbered
 // sides, padded rows and columns included).
+// Controller constants and initial solver state of one LP (as the single-LP
+// solve sets them up); nb_rows / nb_cols are its partial counts.
+void lpState(const Item& it, const pdlpx_options& o, bool mixed, int nb_rows, int nb_cols, DevConst& dc, DevState& st) {
+    const ScaledLp& sc = it.sc;
+    const int32_t m = it.lp.m, n = it.lp.n;
+    dc.m = m;
+    dc.n = n;
+    dc.N = o.termination_eval_frequency;
+    dc.max_iter = o.max_iter;
+    dc.polish_max_iter = o.polish_max_iter;
+    dc.linf = o.optimality_norm == PDLPX_NORM_LINF;
+    dc.update_pw = o.update_primal_weight != 0;
+    dc.enable_polish = o.enable_polishing != 0;
+    dc.mixed = mixed;
+    dc.fp64_switch = o.fp64_switch != 0;
+    dc.adaptive = 0;
+    dc.precond_refresh = o.preconditioner_refresh != 0;
+    dc.nb_rows = nb_rows;
+    dc.nb_cols = nb_cols;
+    dc.stall_limit = 10;
+    dc.primal_tol = o.primal_tol;
+    dc.dual_tol = o.dual_tol;
+    dc.opt_tol = o.optimality_tol;
+    dc.polish_ptol = o.polish_primal_tol;
+    dc.polish_dtol = o.polish_dual_tol;
+    dc.kp = o.pid_kp;
+    dc.ki = o.pid_ki;
+    dc.kd = o.pid_kd;
+    dc.ismooth = o.pid_i_smooth;
+    dc.suff = o.restart_sufficient_decay;
+    dc.nec = o.restart_necessary_decay;
+    dc.art = o.restart_artificial_fraction;
+    terminationNorms(it.lp, o.optimality_norm, dc.c_norm, dc.b_norm);
+    dc.obj_sign = sc.obj_sign;
+    dc.obj_scale = sc.obj_scale;
+    dc.con_scale = sc.con_scale;
+    dc.offset = it.lp.offset;
+    dc.precond_ratio = o.preconditioner_refresh_ratio;
+    dc.switch_score = 30.0;
+    st.step = 1.0;
+    st.pw = o.primal_weight;
+    st.prec = mixed ? 0 : 1;
+    st.fpe0 = -1.0;
+    st.last_fpe = std::numeric_limits<double>::infinity();
+    st.best_pw = st.pw;
+    st.best_score = std::numeric_limits<double>::infinity();
+    st.best_kkt = std::numeric_limits<double>::infinity();
+    st.precond_pw = sc.precond_pw;
+    st.switch_total = -1;
+}
+
 void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img, char* iters) {
     const ScaledLp& sc = it.sc;
     const int32_t m = it.lp.m, n = it.lp.n;
@@ -1155,52 +1206,9 @@ void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img
     }
     // controller constants and initial state (as the single-LP solve)
     DevConst dc{};
-    dc.m = m;
-    dc.n = n;
-    dc.N = o.termination_eval_frequency;
-    dc.max_iter = o.max_iter;
-    dc.polish_max_iter = o.polish_max_iter;
-    dc.linf = o.optimality_norm == PDLPX_NORM_LINF;
-    dc.update_pw = o.update_primal_weight != 0;
-    dc.enable_polish = o.enable_polishing != 0;
-    dc.mixed = pk.mixed;
-    dc.fp64_switch = o.fp64_switch != 0;
-    dc.adaptive = 0;
-    dc.precond_refresh = o.preconditioner_refresh != 0;
-    dc.nb_rows = it.nrt;
-    dc.nb_cols = it.nct;
-    dc.stall_limit = 10;
-    dc.primal_tol = o.primal_tol;
-    dc.dual_tol = o.dual_tol;
-    dc.opt_tol = o.optimality_tol;
-    dc.polish_ptol = o.polish_primal_tol;
-    dc.polish_dtol = o.polish_dual_tol;
-    dc.kp = o.pid_kp;
-    dc.ki = o.pid_ki;
-    dc.kd = o.pid_kd;
-    dc.ismooth = o.pid_i_smooth;
-    dc.suff = o.restart_sufficient_decay;
-    dc.nec = o.restart_necessary_decay;
-    dc.art = o.restart_artificial_fraction;
-    terminationNorms(it.lp, o.optimality_norm, dc.c_norm, dc.b_norm);
-    dc.obj_sign = sc.obj_sign;
-    dc.obj_scale = sc.obj_scale;
-    dc.con_scale = sc.con_scale;
-    dc.offset = it.lp.offset;
-    dc.precond_ratio = o.preconditioner_refresh_ratio;
-    dc.switch_score = 30.0;
-    reinterpret_cast<DevConst*>(img + pk.o_dc)[it.l] = dc;
     DevState st{};
-    st.step = 1.0;
-    st.pw = o.primal_weight;
-    st.prec = pk.mixed ? 0 : 1;
-    st.fpe0 = -1.0;
-    st.last_fpe = std::numeric_limits<double>::infinity();
-    st.best_pw = st.pw;
-    st.best_score = std::numeric_limits<double>::infinity();
-    st.best_kkt = std::numeric_limits<double>::infinity();
-    st.precond_pw = sc.precond_pw;
-    st.switch_total = -1;
+    lpState(it, o, pk.mixed, it.nrt, it.nct, dc, st);
+    reinterpret_cast<DevConst*>(img + pk.o_dc)[it.l] = dc;
     reinterpret_cast<DevState*>(img + pk.o_st)[it.l] = st;
     reinterpret_cast<PowerState*>(img + pk.o_ps)[it.l] = PowerState{1.0, 0.0, 0.0, 0, o.sv_max_iter <= 0 ? 1 : 0};
     // warm start, scaled like pdlp.cpp:1812-1827 (iters is null when no LP of the pack has one)
@@ -1242,34 +1250,11 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= lim;
 }
 
-// Read one finished (or stopped) LP back from the device and unscale it
-// (pdlp.cpp:2678-2712): x = x_hat * col_scale / con_scale clamped to the
-// original bounds, y = sign * y_hat * row_scale / obj_scale, in the LP's
-// original numbering.
-int32_t collectLp(const Pack& pk, int l, bool out_of_time, double secs, double dev_s, int launches, LpOutcome& out,
-                  std::string& err) {
-    const Item& it = *pk.items[l];
-    cudaStream_t s = pk.s;
+// Status, unscaled solution and result record of one LP from its final solver
+// state and its pdhg iterates xs, ys (scaled space, original numbering).
+void finishOutcome(const Item& it, const DevState& f, const std::vector<double>& xs, const std::vector<double>& ys,
+                   bool mixed, bool out_of_time, double secs, double dev_s, int launches, LpOutcome& out) {
     const int32_t m = it.lp.m, n = it.lp.n;
-    DevState f{};
-    PDLPX_BCK(cudaMemcpyAsync(&f, pk.args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-    PDLPX_BCK(cudaStreamSynchronize(s));
-    std::vector<double> xs(n), ys(m);  // original numbering, scaled space
-    if (f.prec == 0) {
-        std::vector<float> fx(it.np), fy(it.mp);
-        PDLPX_BCK(cudaMemcpyAsync(fx.data(), pk.args.it32.xh + it.c0, 4 * fx.size(), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaMemcpyAsync(fy.data(), pk.args.it32.yh + it.r0, 4 * fy.size(), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaStreamSynchronize(s));
-        for (int32_t j = 0; j < n; ++j) xs[j] = fx[it.cols.pos[j]];
-        for (int32_t i = 0; i < m; ++i) ys[i] = fy[it.rows.pos[i]];
-    } else {
-        std::vector<double> dx(it.np), dy(it.mp);
-        PDLPX_BCK(cudaMemcpyAsync(dx.data(), pk.args.it64.xh + it.c0, 8 * dx.size(), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaMemcpyAsync(dy.data(), pk.args.it64.yh + it.r0, 8 * dy.size(), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaStreamSynchronize(s));
-        for (int32_t j = 0; j < n; ++j) xs[j] = dx[it.cols.pos[j]];
-        for (int32_t i = 0; i < m; ++i) ys[i] = dy[it.rows.pos[i]];
-    }
     int32_t status;
     if (f.done) {
         status = f.status;
@@ -1311,7 +1296,7 @@ int32_t collectLp(const Pack& pk, int l, bool out_of_time, double secs, double d
     r.rel_gap = f.gap;
     r.primal_objective = f.pobj;
     r.dual_objective = f.dobj;
-    r.fp64_iterations = pk.mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
+    r.fp64_iterations = mixed ? (f.switch_total >= 0 ? f.total - f.switch_total : 0) : f.total;
     r.restarts = f.restarts;
     r.step_size = f.step;
     r.primal_weight = f.pw;
@@ -1319,6 +1304,37 @@ int32_t collectLp(const Pack& pk, int l, bool out_of_time, double secs, double d
     r.device_seconds = dev_s;
     r.used_gpu = 1;
     r.kernel_launches = launches;
+}
+
+// Read one finished (or stopped) LP back from the device and unscale it
+// (pdlp.cpp:2678-2712): x = x_hat * col_scale / con_scale clamped to the
+// original bounds, y = sign * y_hat * row_scale / obj_scale, in the LP's
+// original numbering.
+int32_t collectLp(const Pack& pk, int l, bool out_of_time, double secs, double dev_s, int launches, LpOutcome& out,
+                  std::string& err) {
+    const Item& it = *pk.items[l];
+    cudaStream_t s = pk.s;
+    const int32_t m = it.lp.m, n = it.lp.n;
+    DevState f{};
+    PDLPX_BCK(cudaMemcpyAsync(&f, pk.args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    PDLPX_BCK(cudaStreamSynchronize(s));
+    std::vector<double> xs(n), ys(m);  // original numbering, scaled space
+    if (f.prec == 0) {
+        std::vector<float> fx(it.np), fy(it.mp);
+        PDLPX_BCK(cudaMemcpyAsync(fx.data(), pk.args.it32.xh + it.c0, 4 * fx.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(fy.data(), pk.args.it32.yh + it.r0, 4 * fy.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        for (int32_t j = 0; j < n; ++j) xs[j] = fx[it.cols.pos[j]];
+        for (int32_t i = 0; i < m; ++i) ys[i] = fy[it.rows.pos[i]];
+    } else {
+        std::vector<double> dx(it.np), dy(it.mp);
+        PDLPX_BCK(cudaMemcpyAsync(dx.data(), pk.args.it64.xh + it.c0, 8 * dx.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(dy.data(), pk.args.it64.yh + it.r0, 8 * dy.size(), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        for (int32_t j = 0; j < n; ++j) xs[j] = dx[it.cols.pos[j]];
+        for (int32_t i = 0; i < m; ++i) ys[i] = dy[it.rows.pos[i]];
+    }
+    finishOutcome(it, f, xs, ys, pk.mixed, out_of_time, secs, dev_s, launches, out);
     return PDLPX_OK;
 }
 
@@ -1585,6 +1601,8 @@ int32_t runPack(const std::vector<Item*>& items, const pdlpx_options& o, std::ch
     return solvePack(pk, o, t0, stop, done, err);
 }
 
+#include "family.cuh"
+
 }  // namespace
 
 struct PreparedLp {
@@ -1630,6 +1648,63 @@ int32_t solvePrepared(const std::vector<PreparedLp*>& lps, const pdlpx_options& 
     int32_t rc = selectDevice(o, err);
     if (rc != PDLPX_OK) return rc;
     return runPack(items, o, t0, stop, done, err);
+}
+
+FamilyPtr makeFamilyBase(const pdlpx_lp& base) {
+    auto f = std::make_shared<FamilyBase>();
+    Csr a;
+    if (base.m <= 0 || base.n <= 0 || base.row_ptr == nullptr ||
+        !canonicalCsr(base.m, base.n, base.nnz, base.row_ptr, base.col_idx, base.val, a))
+        return nullptr;
+    f->m = base.m;
+    f->n = base.n;
+    f->ptr = std::move(a.ptr);
+    f->idx = std::move(a.idx);
+    f->val = std::move(a.val);
+    return f;
+}
+
+bool familyMember(const PreparedLp& p, const FamilyBase& f, const pdlpx_options& o) {
+    const HostLp& lp = p.item.lp;
+    if (p.item.trivial || o.matrix_zero_tol > 0.0 || f.m <= 0 || lp.n != f.n || lp.m < f.m) return false;
+    const size_t z = static_cast<size_t>(f.ptr[f.m]);
+    return std::equal(f.ptr.begin(), f.ptr.end(), lp.a.ptr.begin()) &&
+           std::memcmp(lp.a.idx.data(), f.idx.data(), 4 * z) == 0 &&
+           std::memcmp(lp.a.val.data(), f.val.data(), 8 * z) == 0;
+}
+
+size_t familyMemberBytes(const PreparedLp& p, const FamilyBase& f) {
+    const HostLp& lp = p.item.lp;
+    const int64_t extra = lp.m - f.m, zk = lp.a.nnz() - f.ptr[f.m];
+    const size_t lane = familyPackBytes(f.n, f.m, 0, 0, 0, famBlocks(f.n), famBlocks(f.m)) / kFam;
+    const size_t shared = (24 * static_cast<size_t>(f.ptr[f.m]) + 4 * static_cast<size_t>(f.m + f.n)) / kFam;
+    return lane + shared + 120 * static_cast<size_t>(extra) + 28 * static_cast<size_t>(zk);
+}
+
+int32_t solveFamily(const FamilyBase& f, const std::vector<PreparedLp*>& lps, const pdlpx_options& o,
+                    const std::atomic<int>* stop, const LpDone& done, std::string& err) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!optionsSupported(o, err)) return PDLPX_E_INVALID;
+    if (lps.empty()) return PDLPX_OK;
+    if (static_cast<int>(lps.size()) > kFam) {
+        err = "a family pack holds at most 32 LPs";
+        return PDLPX_E_INVALID;
+    }
+    FamPack fp;
+    fp.base = &f;
+    fp.n = f.n;
+    fp.mb = f.m;
+    for (PreparedLp* p : lps) {
+        if (!familyMember(*p, f, o)) {
+            err = "LP is not a member of the family (columns or base rows differ)";
+            return PDLPX_E_INVALID;
+        }
+        fp.items.push_back(&p->item);
+    }
+    fp.L = static_cast<int>(fp.items.size());
+    int32_t rc = selectDevice(o, err);
+    if (rc != PDLPX_OK) return rc;
+    return solveFamilyPack(fp, o, t0, stop, done, err);
 }
 
 int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,

@@ -1,0 +1,1004 @@
+// Family packs: node LPs that share the leading rows of one base matrix.
+//
+// Branch-and-bound node LPs of one base LP (bound changes on integer columns
+// and a few appended cut rows) have the same
+// constraint matrix in their first m_b rows.  A family pack stores those rows
+// once and runs up to 32 node LPs over them in the same sweep: one warp per
+// matrix row or column, one lane per LP.  The warp loads a row's entries once
+// (coalesced, broadcast by shuffle) and every lane gathers its own LP's value
+// of each entry; per-LP vectors are interleaved [row or column][32 lanes], so
+// each gather of the warp is one 256-byte request instead of 32 scattered
+// sectors, and the matrix bytes of an iteration are shared by all its LPs.
+//
+// Each LP keeps its own scaling (Ruiz row / column factors, Pock-Chambolle
+// step sizes, bound and objective rescaling, exactly as a separate solve
+// computes them, pdlp.cpp:469-669): the shared values are the original ones and
+// the scaled product is formed on the fly, (A_l x)_i = r_li sum_j a_ij (c_lj x_j).
+// The primal step stores c .* x_refl and the dual step r .* y_cur next to the
+// iterates, so the gathers need no scale factor.  Rows an LP appends after the
+// base rows ("cut rows") are its own CSR rows, handled by a warp per row in the
+// dual step and, for the primal step, by a per-column list of the appended
+// entries of every LP.
+//
+// Iterates are FP64 throughout (the shared matrix is read once per iteration,
+// so the per-LP vectors are the traffic); per-LP DevState / DevConst and the
+// single-LP controlStep, restart, polish and termination rules as in the packed
+// batch.  Lane l's arithmetic and reduction order depend on LP l alone, so a
+// node LP's result is the same in a family of one and in any mix.
+
+constexpr int kFam = 32;  // lanes (LPs) per family pack
+constexpr unsigned kFull = 0xffffffffu;
+
+struct FamArgs {
+    const int* a_ptr;     // base rows (original values)
+    const int* a_idx;
+    const double* a_val;
+    const int* at_ptr;    // base rows transposed
+    const int* at_idx;
+    const double* at_val;
+    const int* k_ptr;     // appended rows of all LPs
+    const int* k_idx;
+    const double* k_val;
+    const int* k_lane;    // LP of each appended row
+    const int* kt_ptr;    // appended entries by column: row, LP, value
+    const int* kt_row;
+    const int* kt_lane;
+    const double* kt_val;
+    const ColPack<double>* cp;  // [n][32]
+    const double* cs;           // column scale [n][32]
+    double *xc, *xi, *xh, *xs;  // [n][32]; xs = column scale * x_refl
+    const RowPack<double>* rp;  // [m_b][32] then [K]
+    const double* rs;           // row scale
+    double *yc, *yi, *yh, *ys;  // ys = row scale * y_cur
+    DevState* st;
+    const DevConst* dc;
+    PowerState* ps;
+    int* flags;
+    int* counters;
+    double* part_rows;  // [block][32][kRowSlots]
+    double* part_cols;  // [block][32][kColSlots]
+    double *pi_x, *pi_y, *pi_xn, *pi_part;
+    int n, mb, K, L;
+    int gb, gk;           // step / power blocks over base rows, appended rows
+    int nbr, nbk, nbc;    // check blocks: base rows, appended rows, columns
+    int max_iter, polish_max_iter, N, sv_max_iter;
+    double sv_tol;
+};
+
+__device__ __forceinline__ size_t fIdx(int r, int l) { return static_cast<size_t>(r) * kFam + l; }
+__device__ __forceinline__ size_t fCut(const FamArgs& a, int q) { return static_cast<size_t>(a.mb) * kFam + q; }
+
+// Dot product of one shared row with lane l's vector get(entry index): the warp
+// loads up to 32 entries with one coalesced load per array, broadcasts them by
+// shuffle and every active lane gathers its own value (four independent
+// products per round).  The loop bounds are warp-uniform.
+template <class Get>
+__device__ __forceinline__ double famDot(const int* __restrict__ idx, const double* __restrict__ val, int b, int e,
+                                         int l, bool on, Get get) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int c0 = b; c0 < e; c0 += 32) {
+        const int cnt = min(32, e - c0);
+        int mc = 0;
+        double mv = 0.0;
+        if (l < cnt) {
+            mc = __ldg(idx + c0 + l);
+            mv = __ldg(val + c0 + l);
+        }
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            const int q0 = __shfl_sync(kFull, mc, k), q1 = __shfl_sync(kFull, mc, k + 1);
+            const int q2 = __shfl_sync(kFull, mc, k + 2), q3 = __shfl_sync(kFull, mc, k + 3);
+            const double v0 = __shfl_sync(kFull, mv, k), v1 = __shfl_sync(kFull, mv, k + 1);
+            const double v2 = __shfl_sync(kFull, mv, k + 2), v3 = __shfl_sync(kFull, mv, k + 3);
+            double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+            if (on) {
+                g0 = get(q0);
+                g1 = get(q1);
+                g2 = get(q2);
+                g3 = get(q3);
+            }
+            s0 += v0 * g0;
+            s1 += v1 * g1;
+            s2 += v2 * g2;
+            s3 += v3 * g3;
+        }
+        for (; k < cnt; ++k) {
+            const int q = __shfl_sync(kFull, mc, k);
+            const double v = __shfl_sync(kFull, mv, k);
+            const double g = on ? get(q) : 0.0;
+            s0 += v * g;
+        }
+    }
+    return (s0 + s1) + (s2 + s3);
+}
+
+// Sum of one appended row of LP lp against get(column): lanes stride over the
+// entries, fixed-order butterfly; every lane returns the sum.
+template <class Get>
+__device__ __forceinline__ double famCutDot(const FamArgs& a, int q, int l, Get get) {
+    double s = 0.0;
+    for (int k = a.k_ptr[q] + l; k < a.k_ptr[q + 1]; k += 32) s += a.k_val[k] * get(a.k_idx[k]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(kFull, s, off);
+    return s;
+}
+
+// Dual proximal step of one row (pdlp_kernels.cu:94-157, as dualUpdate) given
+// s = (A_l x_refl)_i; returns the new current y, py the pdhg y.
+__device__ __forceinline__ double famDualStep(const RowPack<double>& q, double yc, double yi, double s, double step,
+                                              double pw, double lam, double& py) {
+    const double sig = step * q.sigma * pw;
+    const double v = yc + sig * s;
+    const int type = static_cast<int>(q.type);
+    if (type == 0) {
+        py = v - sig * q.rl;
+    } else if (type == 1) {
+        py = v - sig * q.ru;
+        if (py < 0.0) py = 0.0;
+    } else if (type == 2) {
+        py = v - sig * q.rl;
+        if (py > 0.0) py = 0.0;
+    } else {
+        if (v >= sig * q.ru)
+            py = v - sig * q.ru;
+        else if (v <= sig * q.rl)
+            py = v - sig * q.rl;
+        else
+            py = 0.0;
+    }
+    const double yr = 2.0 * py - yc;
+    return lam * yr + (1.0 - lam) * yi;
+}
+
+// ---- PDHG step -----------------------------------------------------------------
+// Primal: one warp per column j; (A_l^T y)_j = c_lj (sum_i a_ij ys_il + appended entries).
+__global__ void __launch_bounds__(kBlock) famPrimal(FamArgs a, int koff) {
+    const int j = static_cast<int>(blockIdx.x) * kWarps + static_cast<int>(threadIdx.x >> 5);
+    const int l = threadIdx.x & 31;
+    if (j >= a.n) return;
+    bool last = false;
+    const bool on = l < a.L && active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N);
+    if (__ballot_sync(kFull, on) == 0) return;
+    const size_t q = fIdx(j, l);
+    ColPack<double> c{0.0, 0.0, 0.0, 0.0};
+    double cs = 1.0, xc = 0.0, xi = 0.0;
+    if (on) {
+        c = a.cp[q];
+        cs = a.cs[q];
+        xc = a.xc[q];
+        xi = a.xi[q];
+    }
+    const double* ys = a.ys;
+    double s = famDot(a.at_idx, a.at_val, a.at_ptr[j], a.at_ptr[j + 1], l, on,
+                      [&](int i) { return __ldg(ys + fIdx(i, l)); });
+    for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k)
+        if (on && a.kt_lane[k] == l) s += a.kt_val[k] * ys[fCut(a, a.kt_row[k])];
+    if (!on) return;
+    const DevState* st = a.st + l;
+    const double step = st->step, pw = st->pw;
+    const int kk = st->inner + koff;
+    const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
+    const double tau = step * c.tau / pw;
+    double xh = xc - tau * (c.c + cs * s);
+    if (xh < c.lb) xh = c.lb;
+    if (xh > c.ub) xh = c.ub;
+    const double xr = 2.0 * xh - xc;
+    a.xc[q] = lam * xr + (1.0 - lam) * xi;
+    a.xs[q] = cs * xr;
+    if (last) a.xh[q] = xh;
+}
+
+// Dual: blocks [0, gb) one warp per base row, then one warp per appended row.
+__global__ void __launch_bounds__(kBlock) famDual(FamArgs a, int koff) {
+    const int w = static_cast<int>(threadIdx.x >> 5);
+    const int l = threadIdx.x & 31;
+    const double* xs = a.xs;
+    if (static_cast<int>(blockIdx.x) < a.gb) {
+        const int i = static_cast<int>(blockIdx.x) * kWarps + w;
+        if (i >= a.mb) return;
+        bool last = false;
+        const bool on = l < a.L && active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N);
+        if (__ballot_sync(kFull, on) == 0) return;
+        const size_t q = fIdx(i, l);
+        RowPack<double> r{0.0, 0.0, 0.0, 0.0};
+        double rs = 1.0, yc = 0.0, yi = 0.0;
+        if (on) {
+            r = a.rp[q];
+            rs = a.rs[q];
+            yc = a.yc[q];
+            yi = a.yi[q];
+        }
+        const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on,
+                                [&](int j) { return __ldg(xs + fIdx(j, l)); });
+        if (!on) return;
+        const DevState* st = a.st + l;
+        const int kk = st->inner + koff;
+        const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
+        double py;
+        const double yn = famDualStep(r, yc, yi, rs * s, st->step, st->pw, lam, py);
+        a.yc[q] = yn;
+        a.ys[q] = rs * yn;
+        if (last) a.yh[q] = py;
+        return;
+    }
+    const int qq = (static_cast<int>(blockIdx.x) - a.gb) * kWarps + w;
+    if (qq >= a.K) return;
+    const int lp = a.k_lane[qq];
+    bool last = false;
+    if (!active(a.st + lp, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;  // warp-uniform
+    const double s = famCutDot(a, qq, l, [&](int j) { return __ldg(xs + fIdx(j, lp)); });
+    if (l != 0) return;
+    const size_t q = fCut(a, qq);
+    const DevState* st = a.st + lp;
+    const int kk = st->inner + koff;
+    const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
+    const double rs = a.rs[q], yc = a.yc[q];
+    double py;
+    const double yn = famDualStep(a.rp[q], yc, a.yi[q], rs * s, st->step, st->pw, lam, py);
+    a.yc[q] = yn;
+    a.ys[q] = rs * yn;
+    if (last) a.yh[q] = py;
+}
+
+// ---- FP64 check pass: per-lane block partials [block][32][NS] -----------------------
+template <int NS>
+__device__ __forceinline__ void famBlockReduce(const double (&acc)[NS], const int (&ops)[NS], double* out) {
+    __shared__ double red[kWarps][kFam][NS];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) red[w][l][s] = acc[s];
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            double v = red[0][l][s];
+            for (int k = 1; k < kWarps; ++k) v = combine(ops[s], v, red[k][l][s]);
+            out[static_cast<size_t>(l) * NS + s] = v;
+        }
+    }
+}
+
+__device__ __forceinline__ bool famChecking(const FamArgs& a, int l) {
+    return l < a.L && !a.st[l].done && a.st[l].prec == 1;
+}
+
+// Rows: blocks [0, nbr) stride over the base rows, [nbr, nbr + nbk) over the
+// appended rows (their terms go to the lane of their LP).
+__global__ void __launch_bounds__(kBlock) famCheckRows(FamArgs a) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    int ops[kRowSlots];
+    double acc[kRowSlots];
+#pragma unroll
+    for (int s = 0; s < kRowSlots; ++s) {
+        ops[s] = rowSlotOp(s);
+        acc[s] = slotInit(ops[s]);
+    }
+    const double *xh = a.xh, *cs = a.cs;
+    if (static_cast<int>(blockIdx.x) < a.nbr) {
+        const bool on = famChecking(a, l);
+        for (int i = static_cast<int>(blockIdx.x) * kWarps + w; i < a.mb; i += a.nbr * kWarps) {
+            const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on, [&](int j) {
+                const size_t c = fIdx(j, l);
+                return cs[c] * xh[c];
+            });
+            if (on) {
+                const size_t q = fIdx(i, l);
+                const RowPack<double> r = a.rp[q];
+                const double rsv = a.rs[q];
+                accRowMetrics(acc, a.dc[l], rsv * s, r.rl, r.ru, rsv, a.yh[q], a.yi[q]);
+            }
+        }
+    } else {
+        const int b = static_cast<int>(blockIdx.x) - a.nbr;
+        for (int qq = b * kWarps + w; qq < a.K; qq += a.nbk * kWarps) {
+            const int lp = a.k_lane[qq];
+            if (!famChecking(a, lp)) continue;  // warp-uniform
+            const double s = famCutDot(a, qq, l, [&](int j) {
+                const size_t c = fIdx(j, lp);
+                return cs[c] * xh[c];
+            });
+            if (l == lp) {
+                const size_t q = fCut(a, qq);
+                const RowPack<double> r = a.rp[q];
+                const double rsv = a.rs[q];
+                accRowMetrics(acc, a.dc[lp], rsv * s, r.rl, r.ru, rsv, a.yh[q], a.yi[q]);
+            }
+        }
+    }
+    famBlockReduce<kRowSlots>(acc, ops, a.part_rows + static_cast<size_t>(blockIdx.x) * kFam * kRowSlots);
+}
+
+// Columns: A_l^T y_hat and A_l^T (y_hat - y_init), column metrics.
+__global__ void __launch_bounds__(kBlock) famCheckCols(FamArgs a) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    int ops[kColSlots];
+    double acc[kColSlots];
+#pragma unroll
+    for (int s = 0; s < kColSlots; ++s) {
+        ops[s] = colSlotOp(s);
+        acc[s] = slotInit(ops[s]);
+    }
+    const bool on = famChecking(a, l);
+    const double *yh = a.yh, *yi = a.yi, *rs = a.rs;
+    for (int j = static_cast<int>(blockIdx.x) * kWarps + w; j < a.n; j += a.nbc * kWarps) {
+        const int b = a.at_ptr[j], e = a.at_ptr[j + 1];
+        double aty = famDot(a.at_idx, a.at_val, b, e, l, on, [&](int i) {
+            const size_t q = fIdx(i, l);
+            return rs[q] * yh[q];
+        });
+        double atdy = famDot(a.at_idx, a.at_val, b, e, l, on, [&](int i) {
+            const size_t q = fIdx(i, l);
+            return rs[q] * (yh[q] - yi[q]);
+        });
+        for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k) {
+            if (!on || a.kt_lane[k] != l) continue;
+            const size_t q = fCut(a, a.kt_row[k]);
+            aty += a.kt_val[k] * (rs[q] * yh[q]);
+            atdy += a.kt_val[k] * (rs[q] * (yh[q] - yi[q]));
+        }
+        if (on) {
+            const size_t c = fIdx(j, l);
+            const ColPack<double> p = a.cp[c];
+            const double csv = a.cs[c];
+            accColMetrics<double>(acc, a.dc[l], a.xh[c], a.xi[c], p.c, p.lb, p.ub, csv, csv * aty, csv * atdy);
+        }
+    }
+    famBlockReduce<kColSlots>(acc, ops, a.part_cols + static_cast<size_t>(blockIdx.x) * kFam * kColSlots);
+}
+
+// Fixed-order reduction of LP l's partials over nb blocks across one warp.
+template <int NS>
+__device__ __forceinline__ void famLanes(const double* part, int nb, int l, int lane, const int (&ops)[NS],
+                                         double (&out)[NS]) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) out[s] = slotInit(ops[s]);
+    for (int b = lane; b < nb; b += 32) {
+        const double* p = part + (static_cast<size_t>(b) * kFam + l) * NS;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) out[s] = combine(ops[s], out[s], p[s]);
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) out[s] = combine(ops[s], out[s], __shfl_xor_sync(kFull, out[s], off));
+}
+
+// One warp per LP: reduce its partials, run the single-LP controller step.
+__global__ void __launch_bounds__(32 * kCtlWarps) famController(FamArgs a) {
+    const int l = static_cast<int>(blockIdx.x) * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L) return;
+    DevState* st = a.st + l;
+    if (st->done) return;
+    int rops[kRowSlots], cops[kColSlots];
+#pragma unroll
+    for (int s = 0; s < kRowSlots; ++s) rops[s] = rowSlotOp(s);
+#pragma unroll
+    for (int s = 0; s < kColSlots; ++s) cops[s] = colSlotOp(s);
+    double rows[kRowSlots], cols[kColSlots];
+    famLanes<kRowSlots>(a.part_rows, a.nbr + a.nbk, l, lane, rops, rows);
+    famLanes<kColSlots>(a.part_cols, a.nbc, l, lane, cops, cols);
+    if (lane == 0) {
+        DevState s = *st;
+        controlStep(s, a.dc[l], rows, cols);
+        *st = s;
+    }
+}
+
+// Restart copy (pdlp_kernels.cu:377-405) of the LPs whose controller restarted:
+// anchor = current = pdhg; the scaled y gathered by the primal step follows y_cur.
+__global__ void __launch_bounds__(kBlock) famRestart(FamArgs a) {
+    const size_t ncol = static_cast<size_t>(a.n) * kFam, nrow = static_cast<size_t>(a.mb) * kFam;
+    const size_t total = ncol + nrow + static_cast<size_t>(a.K);
+    for (size_t t = static_cast<size_t>(blockIdx.x) * kBlock + threadIdx.x; t < total;
+         t += static_cast<size_t>(gridDim.x) * kBlock) {
+        int l;
+        if (t < ncol + nrow)
+            l = static_cast<int>(t % kFam);
+        else
+            l = a.k_lane[t - ncol - nrow];
+        if (l >= a.L) continue;
+        const DevState* st = a.st + l;
+        if (st->done || !st->restart) continue;
+        if (t < ncol) {
+            const double v = a.xh[t];
+            a.xi[t] = v;
+            a.xc[t] = v;
+        } else {
+            const size_t r = t - ncol;
+            const double v = a.yh[r];
+            a.yi[r] = v;
+            a.yc[r] = v;
+            a.ys[r] = a.rs[r] * v;
+        }
+    }
+}
+
+__global__ void famFinish(FamArgs a) {
+    const int l = threadIdx.x;
+    if (l >= a.L) return;
+    a.flags[l] = (a.st[l].done ? 1 : 0) | 2;
+}
+
+// ---- power iteration on A_l^T A_l per lane (pdlp.cpp:748-795, 1985-2041) -------------
+__global__ void __launch_bounds__(kBlock) famPowerA(FamArgs a) {
+    const int w = static_cast<int>(threadIdx.x >> 5);
+    const int l = threadIdx.x & 31;
+    const double *px = a.pi_x, *cs = a.cs;
+    if (static_cast<int>(blockIdx.x) < a.gb) {
+        const int i = static_cast<int>(blockIdx.x) * kWarps + w;
+        if (i >= a.mb) return;
+        const bool on = l < a.L && !a.ps[l].done;
+        if (__ballot_sync(kFull, on) == 0) return;
+        const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on, [&](int j) {
+            const size_t c = fIdx(j, l);
+            return cs[c] * px[c];
+        });
+        if (on) a.pi_y[fIdx(i, l)] = a.rs[fIdx(i, l)] * s;
+        return;
+    }
+    const int qq = (static_cast<int>(blockIdx.x) - a.gb) * kWarps + w;
+    if (qq >= a.K) return;
+    const int lp = a.k_lane[qq];
+    if (a.ps[lp].done) return;
+    const double s = famCutDot(a, qq, l, [&](int j) {
+        const size_t c = fIdx(j, lp);
+        return cs[c] * px[c];
+    });
+    if (l == 0) a.pi_y[fCut(a, qq)] = a.rs[fCut(a, qq)] * s;
+}
+
+__global__ void __launch_bounds__(kBlock) famPowerAt(FamArgs a) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const bool on = l < a.L && !a.ps[l].done;
+    const double *py = a.pi_y, *rs = a.rs;
+    double acc[2] = {0.0, 0.0};
+    for (int j = static_cast<int>(blockIdx.x) * kWarps + w; j < a.n; j += a.nbc * kWarps) {
+        double s = famDot(a.at_idx, a.at_val, a.at_ptr[j], a.at_ptr[j + 1], l, on, [&](int i) {
+            const size_t q = fIdx(i, l);
+            return rs[q] * py[q];
+        });
+        for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k)
+            if (on && a.kt_lane[k] == l) {
+                const size_t q = fCut(a, a.kt_row[k]);
+                s += a.kt_val[k] * (rs[q] * py[q]);
+            }
+        if (on) {
+            const size_t c = fIdx(j, l);
+            const double xn = a.cs[c] * s;
+            a.pi_xn[c] = xn;
+            acc[0] += a.pi_x[c] * xn;
+            acc[1] += xn * xn;
+        }
+    }
+    const int ops[2] = {OP_SUM, OP_SUM};
+    famBlockReduce<2>(acc, ops, a.pi_part + static_cast<size_t>(blockIdx.x) * kFam * 2);
+}
+
+__global__ void __launch_bounds__(32 * kCtlWarps) famPowerFinish1(FamArgs a) {
+    const int l = static_cast<int>(blockIdx.x) * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L || a.ps[l].done) return;
+    const int ops[2] = {OP_SUM, OP_SUM};
+    double out[2];
+    famLanes<2>(a.pi_part, a.nbc, l, lane, ops, out);
+    if (lane == 0) {
+        a.ps[l].s2 = out[0];
+        a.ps[l].nrm = sqrt(out[1]);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) famPowerNormalize(FamArgs a) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const bool on = l < a.L && !a.ps[l].done;
+    double acc[2] = {0.0, 0.0};
+    if (on) {
+        const double s2 = a.ps[l].s2, nrm = a.ps[l].nrm;
+        for (int j = static_cast<int>(blockIdx.x) * kWarps + w; j < a.n; j += a.nbc * kWarps) {
+            const size_t c = fIdx(j, l);
+            const double xn = a.pi_xn[c];
+            const double d = xn - s2 * a.pi_x[c];
+            acc[0] += d * d;
+            if (nrm >= 1e-15) a.pi_x[c] = xn / nrm;
+        }
+    }
+    const int ops[2] = {OP_SUM, OP_SUM};
+    famBlockReduce<2>(acc, ops, a.pi_part + static_cast<size_t>(blockIdx.x) * kFam * 2);
+}
+
+__global__ void __launch_bounds__(32 * kCtlWarps) famPowerFinish2(FamArgs a) {
+    const int l = static_cast<int>(blockIdx.x) * kCtlWarps + static_cast<int>(threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (l >= a.L || a.ps[l].done) return;
+    const int ops[2] = {OP_SUM, OP_SUM};
+    double out[2];
+    famLanes<2>(a.pi_part, a.nbc, l, lane, ops, out);
+    if (lane == 0) {
+        PowerState& p = a.ps[l];
+        p.resid = sqrt(out[0]);
+        p.iter += 1;
+        if (p.nrm < 1e-15 || p.resid < a.sv_tol * fabs(p.s2) || p.iter >= a.sv_max_iter) {
+            p.done = 1;
+            atomicAdd(a.counters, 1);
+        }
+    }
+}
+
+// Step size from the spectral-norm estimate (0.998 / ||A_l||_2, pdlp.cpp:796-800).
+__global__ void famInitStep(FamArgs a) {
+    const int l = threadIdx.x;
+    if (l >= a.L) return;
+    DevState& s = a.st[l];
+    const double step = 0.998 / sqrt(fmax(a.ps[l].s2, 1e-12));
+    s.step = step;
+    s.tau_fac = static_cast<float>(step / s.pw);
+    s.sig_fac = static_cast<float>(step * s.pw);
+}
+
+// ---------------------------------------------------------------------------
+// Host side of a family pack
+// ---------------------------------------------------------------------------
+struct FamPack {
+    const FamilyBase* base = nullptr;
+    std::vector<Item*> items;
+    int L = 0, n = 0, mb = 0, K = 0;
+    int64_t Zb = 0, Zk = 0;
+    std::vector<int> qfirst;  // first appended row of each lane
+    size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane;
+    size_t o_ktptr, o_ktrow, o_ktlane, o_ktval, o_cp, o_cs, o_rp, o_rs, o_st, o_dc, o_ps, o_pix;
+    size_t image_end;
+    size_t o_xc, o_xi, o_xh, o_xs, o_yc, o_yi, o_yh, o_ys;
+    size_t iter_end;
+    size_t o_piy, o_pixn, o_pipart, o_prows, o_pcols, o_flags, o_counters;
+    size_t total;
+    char* d = nullptr;
+    cudaStream_t s = nullptr;
+    cudaGraphExec_t cycle = nullptr, power = nullptr;
+    int cycle_launches = 0, power_launches = 0;
+    FamArgs args{};
+
+    ~FamPack() {
+        if (cycle) cudaGraphExecDestroy(cycle);
+        if (power) cudaGraphExecDestroy(power);
+        if (d) cudaFreeAsync(d, s);
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+
+    size_t rowsAll() const { return static_cast<size_t>(mb) * kFam + static_cast<size_t>(K); }
+    size_t colsAll() const { return static_cast<size_t>(n) * kFam; }
+
+    void layout(int nbr, int nbk, int nbc) {
+        size_t off = 0;
+        auto take = [&](size_t bytes) {
+            const size_t at = off;
+            off += al256(bytes);
+            return at;
+        };
+        const size_t R = rowsAll(), C = colsAll();
+        o_aptr = take(4 * (static_cast<size_t>(mb) + 1));
+        o_aidx = take(4 * static_cast<size_t>(Zb));
+        o_aval = take(8 * static_cast<size_t>(Zb));
+        o_atptr = take(4 * (static_cast<size_t>(n) + 1));
+        o_atidx = take(4 * static_cast<size_t>(Zb));
+        o_atval = take(8 * static_cast<size_t>(Zb));
+        o_kptr = take(4 * (static_cast<size_t>(K) + 1));
+        o_kidx = take(4 * static_cast<size_t>(Zk));
+        o_kval = take(8 * static_cast<size_t>(Zk));
+        o_klane = take(4 * static_cast<size_t>(K));
+        o_ktptr = take(4 * (static_cast<size_t>(n) + 1));
+        o_ktrow = take(4 * static_cast<size_t>(Zk));
+        o_ktlane = take(4 * static_cast<size_t>(Zk));
+        o_ktval = take(8 * static_cast<size_t>(Zk));
+        o_cp = take(32 * C);
+        o_cs = take(8 * C);
+        o_rp = take(32 * R);
+        o_rs = take(8 * R);
+        o_st = take(sizeof(DevState) * kFam);
+        o_dc = take(sizeof(DevConst) * kFam);
+        o_ps = take(sizeof(PowerState) * kFam);
+        o_pix = take(8 * C);
+        image_end = off;
+        o_xc = take(8 * C);
+        o_xi = take(8 * C);
+        o_xh = take(8 * C);
+        o_xs = take(8 * C);
+        o_yc = take(8 * R);
+        o_yi = take(8 * R);
+        o_yh = take(8 * R);
+        o_ys = take(8 * R);
+        iter_end = off;
+        o_piy = take(8 * R);
+        o_pixn = take(8 * C);
+        o_pipart = take(8 * 2 * kFam * static_cast<size_t>(nbc));
+        o_prows = take(8 * kRowSlots * kFam * static_cast<size_t>(nbr + nbk));
+        o_pcols = take(8 * kColSlots * kFam * static_cast<size_t>(nbc));
+        o_flags = take(4 * kFam);
+        o_counters = take(16);
+        total = off;
+    }
+};
+
+// Device bytes of a family pack of L members with the given appended rows / entries.
+size_t familyPackBytes(int64_t n, int64_t mb, int64_t zb, int64_t K, int64_t zk, int nbc, int nbrk) {
+    const size_t C = static_cast<size_t>(n) * kFam, R = static_cast<size_t>(mb) * kFam + static_cast<size_t>(K);
+    size_t b = 4 * static_cast<size_t>(mb + n + 2) + 24 * static_cast<size_t>(zb);
+    b += 4 * static_cast<size_t>(K + n + 2) + 28 * static_cast<size_t>(zk) + 4 * static_cast<size_t>(K);
+    b += C * (32 + 8 + 8 * 6) + R * (32 + 8 + 8 * 5);
+    b += 8 * kFam * (2 * static_cast<size_t>(nbc) + kRowSlots * static_cast<size_t>(nbrk) + kColSlots * static_cast<size_t>(nbc));
+    return b + 64 * 1024;
+}
+
+int famBlocks(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kWarps - 1) / kWarps)); }
+
+// Build the image, run the power iteration and the restart cycles of one family
+// pack; `done(l, outcome)` as for a regular pack.
+int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady_clock::time_point t0,
+                        const std::atomic<int>* stop, const LpDone& done, std::string& err) {
+    const int L = fp.L, n = fp.n, mb = fp.mb;
+    const FamilyBase& fb = *fp.base;
+    int sms = 148;
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    // appended rows of every lane, in lane order
+    fp.qfirst.assign(L + 1, 0);
+    fp.K = 0;
+    fp.Zk = 0;
+    for (int l = 0; l < L; ++l) {
+        const Item& it = *fp.items[l];
+        fp.qfirst[l] = fp.K;
+        fp.K += it.lp.m - mb;
+        fp.Zk += it.lp.a.ptr[it.lp.m] - it.lp.a.ptr[mb];
+    }
+    fp.qfirst[L] = fp.K;
+    fp.Zb = fb.ptr[mb];
+    const int K = fp.K;
+    const int gb = famBlocks(mb), gk = K > 0 ? famBlocks(K) : 0;
+    const int cap = 4 * sms;
+    const int nbr = std::min(gb, cap), nbk = K > 0 ? std::min(gk, cap) : 0, nbc = std::min(famBlocks(n), cap);
+    fp.layout(nbr, nbk, nbc);
+
+    // ---- host image
+    std::unique_ptr<char[]> img(new char[fp.image_end]);
+    std::unique_ptr<char[]> iters(new char[fp.iter_end - fp.image_end]);
+    char* H = img.get();
+    auto I = [&](size_t off) { return reinterpret_cast<int32_t*>(H + off); };
+    auto D = [&](size_t off) { return reinterpret_cast<double*>(H + off); };
+    auto ID = [&](size_t off) { return reinterpret_cast<double*>(iters.get() + (off - fp.image_end)); };
+    std::memcpy(I(fp.o_aptr), fb.ptr.data(), 4 * (static_cast<size_t>(mb) + 1));
+    std::memcpy(I(fp.o_aidx), fb.idx.data(), 4 * static_cast<size_t>(fp.Zb));
+    std::memcpy(D(fp.o_aval), fb.val.data(), 8 * static_cast<size_t>(fp.Zb));
+    {
+        Csr a;
+        a.rows = mb;
+        a.cols = n;
+        a.ptr = fb.ptr;
+        a.idx = fb.idx;
+        a.val = fb.val;
+        Csr at;
+        transposeCsr(a, at);
+        std::memcpy(I(fp.o_atptr), at.ptr.data(), 4 * (static_cast<size_t>(n) + 1));
+        std::memcpy(I(fp.o_atidx), at.idx.data(), 4 * static_cast<size_t>(fp.Zb));
+        std::memcpy(D(fp.o_atval), at.val.data(), 8 * static_cast<size_t>(fp.Zb));
+    }
+    {
+        // appended rows, then their entries by column (row order inside a column)
+        int32_t* kp = I(fp.o_kptr);
+        int32_t* ki = I(fp.o_kidx);
+        double* kv = D(fp.o_kval);
+        int32_t* kl = I(fp.o_klane);
+        std::vector<int32_t> colcnt(static_cast<size_t>(n) + 1, 0);
+        int64_t z = 0;
+        int q = 0;
+        for (int l = 0; l < L; ++l) {
+            const Csr& a = fp.items[l]->lp.a;
+            for (int32_t i = mb; i < a.rows; ++i, ++q) {
+                kp[q] = static_cast<int32_t>(z);
+                kl[q] = l;
+                for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k, ++z) {
+                    ki[z] = a.idx[k];
+                    kv[z] = a.val[k];
+                    ++colcnt[a.idx[k] + 1];
+                }
+            }
+        }
+        kp[K] = static_cast<int32_t>(z);
+        int32_t* ktp = I(fp.o_ktptr);
+        for (int32_t j = 0; j < n; ++j) colcnt[j + 1] += colcnt[j];
+        std::memcpy(ktp, colcnt.data(), 4 * (static_cast<size_t>(n) + 1));
+        int32_t* ktr = I(fp.o_ktrow);
+        int32_t* ktl = I(fp.o_ktlane);
+        double* ktv = D(fp.o_ktval);
+        for (int qq = 0; qq < K; ++qq)
+            for (int32_t k = kp[qq]; k < kp[qq + 1]; ++k) {
+                const int32_t at = colcnt[ki[k]]++;
+                ktr[at] = qq;
+                ktl[at] = kl[qq];
+                ktv[at] = kv[k];
+            }
+    }
+    // per-lane constants, state, power start vector and iterates
+    const double inf = std::numeric_limits<double>::infinity();
+    std::vector<double> g(n);
+    {
+        std::mt19937 rng(42);
+        std::normal_distribution<double> dist(0.0, 1.0);
+        double xn = 0.0;
+        for (int32_t j = 0; j < n; ++j) {
+            g[j] = dist(rng);
+            xn += g[j] * g[j];
+        }
+        xn = std::sqrt(xn);
+        if (xn < 1e-15) xn = 1.0;
+        for (auto& v : g) v /= xn;
+    }
+    ColPack<double>* cp = reinterpret_cast<ColPack<double>*>(H + fp.o_cp);
+    RowPack<double>* rp = reinterpret_cast<RowPack<double>*>(H + fp.o_rp);
+    double *cs = D(fp.o_cs), *rs = D(fp.o_rs), *pix = D(fp.o_pix);
+    double *xc = ID(fp.o_xc), *xi = ID(fp.o_xi), *xh = ID(fp.o_xh), *xsv = ID(fp.o_xs);
+    double *yc = ID(fp.o_yc), *yi = ID(fp.o_yi), *yh = ID(fp.o_yh), *ysv = ID(fp.o_ys);
+    const size_t Rb = static_cast<size_t>(mb) * kFam;
+    parallelFor(kFam, [&](int l) {
+        if (l >= L) {
+            for (int32_t j = 0; j < n; ++j) {
+                const size_t c = static_cast<size_t>(j) * kFam + l;
+                cp[c] = ColPack<double>{0.0, -inf, inf, 1.0};
+                cs[c] = 1.0;
+                pix[c] = xc[c] = xi[c] = xh[c] = xsv[c] = 0.0;
+            }
+            for (int32_t i = 0; i < mb; ++i) {
+                const size_t r = static_cast<size_t>(i) * kFam + l;
+                rp[r] = RowPack<double>{1.0, -inf, inf, static_cast<double>(kRowRanged)};
+                rs[r] = 1.0;
+                yc[r] = yi[r] = yh[r] = ysv[r] = 0.0;
+            }
+            return;
+        }
+        const Item& it = *fp.items[l];
+        const ScaledLp& sc = it.sc;
+        const int32_t m = it.lp.m;
+        std::vector<double> wx(n, 0.0), wy(m, 0.0);
+        if (!it.warm_x.empty()) {
+            for (int32_t j = 0; j < n; ++j) wx[j] = it.warm_x[j] / sc.col_scale[j] * sc.con_scale;
+            for (int32_t i = 0; i < m; ++i) wy[i] = it.warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+        }
+        for (int32_t j = 0; j < n; ++j) {
+            const size_t c = static_cast<size_t>(j) * kFam + l;
+            cp[c] = ColPack<double>{sc.c[j], sc.cl[j], sc.cu[j], sc.tau[j]};
+            cs[c] = sc.col_scale[j];
+            pix[c] = g[j];
+            xc[c] = xi[c] = xh[c] = wx[j];
+            xsv[c] = sc.col_scale[j] * wx[j];
+        }
+        for (int32_t i = 0; i < m; ++i) {
+            const size_t r = i < mb ? static_cast<size_t>(i) * kFam + l : Rb + static_cast<size_t>(fp.qfirst[l] + i - mb);
+            rp[r] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
+            rs[r] = sc.row_scale[i];
+            yc[r] = yi[r] = yh[r] = wy[i];
+            ysv[r] = sc.row_scale[i] * wy[i];
+        }
+        DevConst dc{};
+        DevState st{};
+        lpState(it, o, false, nbr + nbk, nbc, dc, st);
+        reinterpret_cast<DevConst*>(H + fp.o_dc)[l] = dc;
+        reinterpret_cast<DevState*>(H + fp.o_st)[l] = st;
+        reinterpret_cast<PowerState*>(H + fp.o_ps)[l] = PowerState{1.0, 0.0, 0.0, 0, o.sv_max_iter <= 0 ? 1 : 0};
+    });
+    for (int l = L; l < kFam; ++l) {
+        reinterpret_cast<DevConst*>(H + fp.o_dc)[l] = DevConst{};
+        DevState st{};
+        st.done = 1;
+        reinterpret_cast<DevState*>(H + fp.o_st)[l] = st;
+        reinterpret_cast<PowerState*>(H + fp.o_ps)[l] = PowerState{1.0, 0.0, 0.0, 0, 1};
+    }
+
+    // ---- device image
+    PDLPX_BCK(cudaStreamCreateWithFlags(&fp.s, cudaStreamNonBlocking));
+    PDLPX_BCK(cudaMallocAsync(reinterpret_cast<void**>(&fp.d), fp.total, fp.s));
+    cudaStream_t s = fp.s;
+    PDLPX_BCK(cudaMemcpyAsync(fp.d, H, fp.image_end, cudaMemcpyHostToDevice, s));
+    PDLPX_BCK(cudaMemcpyAsync(fp.d + fp.image_end, iters.get(), fp.iter_end - fp.image_end, cudaMemcpyHostToDevice, s));
+    PDLPX_BCK(cudaMemsetAsync(fp.d + fp.iter_end, 0, fp.total - fp.iter_end, s));
+    {
+        FamArgs& a = fp.args;
+        char* d = fp.d;
+        auto Pi = [&](size_t off) { return reinterpret_cast<int*>(d + off); };
+        auto Pd = [&](size_t off) { return reinterpret_cast<double*>(d + off); };
+        a.a_ptr = Pi(fp.o_aptr);
+        a.a_idx = Pi(fp.o_aidx);
+        a.a_val = Pd(fp.o_aval);
+        a.at_ptr = Pi(fp.o_atptr);
+        a.at_idx = Pi(fp.o_atidx);
+        a.at_val = Pd(fp.o_atval);
+        a.k_ptr = Pi(fp.o_kptr);
+        a.k_idx = Pi(fp.o_kidx);
+        a.k_val = Pd(fp.o_kval);
+        a.k_lane = Pi(fp.o_klane);
+        a.kt_ptr = Pi(fp.o_ktptr);
+        a.kt_row = Pi(fp.o_ktrow);
+        a.kt_lane = Pi(fp.o_ktlane);
+        a.kt_val = Pd(fp.o_ktval);
+        a.cp = reinterpret_cast<const ColPack<double>*>(d + fp.o_cp);
+        a.cs = Pd(fp.o_cs);
+        a.xc = Pd(fp.o_xc);
+        a.xi = Pd(fp.o_xi);
+        a.xh = Pd(fp.o_xh);
+        a.xs = Pd(fp.o_xs);
+        a.rp = reinterpret_cast<const RowPack<double>*>(d + fp.o_rp);
+        a.rs = Pd(fp.o_rs);
+        a.yc = Pd(fp.o_yc);
+        a.yi = Pd(fp.o_yi);
+        a.yh = Pd(fp.o_yh);
+        a.ys = Pd(fp.o_ys);
+        a.st = reinterpret_cast<DevState*>(d + fp.o_st);
+        a.dc = reinterpret_cast<const DevConst*>(d + fp.o_dc);
+        a.ps = reinterpret_cast<PowerState*>(d + fp.o_ps);
+        a.flags = Pi(fp.o_flags);
+        a.counters = Pi(fp.o_counters);
+        a.part_rows = Pd(fp.o_prows);
+        a.part_cols = Pd(fp.o_pcols);
+        a.pi_x = Pd(fp.o_pix);
+        a.pi_y = Pd(fp.o_piy);
+        a.pi_xn = Pd(fp.o_pixn);
+        a.pi_part = Pd(fp.o_pipart);
+        a.n = n;
+        a.mb = mb;
+        a.K = K;
+        a.L = L;
+        a.gb = gb;
+        a.gk = gk;
+        a.nbr = nbr;
+        a.nbk = nbk;
+        a.nbc = nbc;
+        a.max_iter = o.max_iter;
+        a.polish_max_iter = o.polish_max_iter;
+        a.N = o.termination_eval_frequency;
+        a.sv_max_iter = o.sv_max_iter;
+        a.sv_tol = o.sv_tol;
+    }
+    const FamArgs args = fp.args;
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PDLPX_BCK(cudaEventCreate(&ev0));
+    PDLPX_BCK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev_guard{ev0, ev1};
+    PDLPX_BCK(cudaEventRecord(ev0, s));
+    int launches = 0;
+    auto deviceSeconds = [&]() -> double {
+        float ms = 0.0f;
+        if (cudaEventRecord(ev1, s) == cudaSuccess && cudaEventSynchronize(ev1) == cudaSuccess)
+            cudaEventElapsedTime(&ms, ev0, ev1);
+        return 1e-3 * ms;
+    };
+    auto hostSeconds = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    auto stopped = [&]() { return stop != nullptr && stop->load(std::memory_order_relaxed) != 0; };
+    std::vector<int> h_flags(kFam);
+    const int nct = famBlocks(n), stepRows = gb + gk;
+    const int ctl = (L + kCtlWarps - 1) / kCtlWarps;
+    const int nrs = std::max(1, std::min<int>(static_cast<int>((fp.colsAll() + fp.rowsAll() + kBlock - 1) / kBlock), 8 * sms));
+    auto capture = [&](cudaGraphExec_t& gx, int& count, bool power) -> int32_t {
+        cudaGraph_t graph = nullptr;
+        PDLPX_BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        count = 0;
+        if (power) {
+            for (int r = 0; r < 8; ++r) {
+                famPowerA<<<stepRows, kBlock, 0, s>>>(args);
+                famPowerAt<<<nbc, kBlock, 0, s>>>(args);
+                famPowerFinish1<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
+                famPowerNormalize<<<nbc, kBlock, 0, s>>>(args);
+                famPowerFinish2<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
+                count += 5;
+            }
+        } else {
+            for (int k = 1; k <= o.termination_eval_frequency; ++k) {
+                famPrimal<<<nct, kBlock, 0, s>>>(args, k);
+                famDual<<<stepRows, kBlock, 0, s>>>(args, k);
+                count += 2;
+            }
+            famCheckRows<<<nbr + nbk, kBlock, 0, s>>>(args);
+            famCheckCols<<<nbc, kBlock, 0, s>>>(args);
+            famController<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
+            famRestart<<<nrs, kBlock, 0, s>>>(args);
+            famFinish<<<1, kFam, 0, s>>>(args);
+            count += 5;
+        }
+        PDLPX_BCK(cudaStreamEndCapture(s, &graph));
+        const cudaError_t ie = cudaGraphInstantiate(&gx, graph, 0);
+        cudaGraphDestroy(graph);
+        PDLPX_BCK(ie);
+        return PDLPX_OK;
+    };
+
+    // ---- power iteration of every lane
+    if (o.sv_max_iter > 0) {
+        int32_t rc = capture(fp.power, fp.power_launches, true);
+        if (rc != PDLPX_OK) return rc;
+        for (int guard = 0; guard < 2 + o.sv_max_iter / 8; ++guard) {
+            PDLPX_BCK(cudaGraphLaunch(fp.power, s));
+            launches += fp.power_launches;
+            PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), args.counters, 4, cudaMemcpyDeviceToHost, s));
+            PDLPX_BCK(cudaStreamSynchronize(s));
+            if (h_flags[0] >= L || stopped()) break;
+        }
+    }
+    famInitStep<<<1, kFam, 0, s>>>(args);
+    ++launches;
+    PDLPX_BCK(cudaGetLastError());
+
+    // ---- restart cycles
+    {
+        int32_t rc = capture(fp.cycle, fp.cycle_launches, false);
+        if (rc != PDLPX_OK) return rc;
+    }
+    std::vector<char> collected(L, 0);
+    int ncollected = 0, cycles = 0;
+    auto collect = [&](int l, bool out_of_time, double secs, double dev_s) -> int32_t {
+        const Item& it = *fp.items[l];
+        const int32_t m = it.lp.m;
+        DevState f{};
+        std::vector<double> xv(n), yv(m);
+        PDLPX_BCK(cudaMemcpyAsync(&f, args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpy2DAsync(xv.data(), 8, args.xh + l, 8 * kFam, 8, n, cudaMemcpyDeviceToHost, s));
+        if (mb > 0)
+            PDLPX_BCK(cudaMemcpy2DAsync(yv.data(), 8, args.yh + l, 8 * kFam, 8, mb, cudaMemcpyDeviceToHost, s));
+        if (m > mb)
+            PDLPX_BCK(cudaMemcpyAsync(yv.data() + mb, args.yh + Rb + fp.qfirst[l], 8 * static_cast<size_t>(m - mb),
+                                      cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        LpOutcome out;
+        finishOutcome(it, f, xv, yv, false, out_of_time, secs, dev_s, launches, out);
+        collected[l] = 1;
+        ++ncollected;
+        done(l, std::move(out));
+        return PDLPX_OK;
+    };
+    while (ncollected < L) {
+        if (timeUp(t0, o.max_solve_seconds) || stopped()) break;
+        PDLPX_BCK(cudaGraphLaunch(fp.cycle, s));
+        launches += fp.cycle_launches;
+        ++cycles;
+        PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        int done_count = 0;
+        bool fresh = false;
+        for (int l = 0; l < L; ++l) {
+            done_count += h_flags[l] & 1;
+            fresh |= (h_flags[l] & 1) && !collected[l];
+        }
+        if (fresh) {
+            const double dev_s = deviceSeconds(), secs = hostSeconds();
+            for (int l = 0; l < L; ++l) {
+                if (!(h_flags[l] & 1) || collected[l]) continue;
+                const int32_t rc = collect(l, false, secs, dev_s);
+                if (rc != PDLPX_OK) return rc;
+            }
+        }
+        if (o.verbose && cycles % 10 == 0) {
+            std::printf("PDLP family %7d iterations per LP  %d/%d LPs done  %d shared rows  %d appended rows  %.3fs  [B200]\n",
+                        cycles * o.termination_eval_frequency, done_count, L, mb, K, hostSeconds());
+            std::fflush(stdout);
+        }
+        if (done_count >= L) break;
+    }
+    if (ncollected < L) {
+        const double dev_s = deviceSeconds(), secs = hostSeconds();
+        const bool out_of_time = timeUp(t0, o.max_solve_seconds);
+        for (int l = 0; l < L; ++l) {
+            if (collected[l]) continue;
+            const int32_t rc = collect(l, out_of_time, secs, dev_s);
+            if (rc != PDLPX_OK) return rc;
+        }
+    }
+    return PDLPX_OK;
+}

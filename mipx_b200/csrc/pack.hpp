@@ -52,4 +52,30 @@ int32_t preparedCols(const PreparedLp& p);
 int32_t solvePrepared(const std::vector<PreparedLp*>& lps, const pdlpx_options& o, const std::atomic<int>* stop,
                       const LpDone& done, std::string& err);
 
+// ---- families: node LPs of one base LP ---------------------------------------
+// Branch-and-bound node LPs keep the base LP's constraint rows (bounds,
+// objective and row bounds may change) and may append rows after them.  Up to
+// kFamilyLanes such LPs are solved as one family pack: the base rows stored
+// once, one lane per LP (family.cuh).
+constexpr int kFamilyLanes = 32;
+
+struct FamilyBase {
+    int32_t m = 0, n = 0;           // base rows, columns
+    std::vector<int32_t> ptr, idx;  // canonical CSR of the base rows, original values
+    std::vector<double> val;
+};
+using FamilyPtr = std::shared_ptr<const FamilyBase>;
+
+// Canonical copy of an LP's rows as a family base (null for an invalid LP or one without rows).
+FamilyPtr makeFamilyBase(const pdlpx_lp& base);
+// Whether a prepared LP is a member: same columns, the base rows first and
+// unchanged, options that keep the original matrix (no zero filter).
+bool familyMember(const PreparedLp& p, const FamilyBase& f, const pdlpx_options& o);
+// Device bytes a member adds to a family pack (its lane plus its share of the base rows).
+size_t familyMemberBytes(const PreparedLp& p, const FamilyBase& f);
+// Solve up to kFamilyLanes members of one family as one pack on the current
+// device (FP64 iterates, per-LP scaling and state); `done` as for solvePrepared.
+int32_t solveFamily(const FamilyBase& f, const std::vector<PreparedLp*>& lps, const pdlpx_options& o,
+                    const std::atomic<int>* stop, const LpDone& done, std::string& err);
+
 }  // namespace pdlpx

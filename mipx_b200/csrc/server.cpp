@@ -9,6 +9,11 @@
 //   * one worker per pack runs it on its own CUDA stream (solvePrepared) and
 //     completes each request as soon as the restart cycle that finishes it
 //     returns.
+// A request submitted with a warm-start ticket whose constraint rows start with
+// the ticket's rows unchanged (a branch-and-bound node of that LP: new bounds,
+// appended cut rows) joins the ticket's family; the dispatcher packs members
+// of one family together and runs them as a family pack (solveFamily: the
+// base rows stored once, one lane per LP).
 // So requests that arrive while packs run are admitted as soon as a stream and
 // memory free up, and the packs' kernels overlap on the device.
 #include <algorithm>
@@ -103,6 +108,8 @@ struct Request {
     int32_t code = PDLPX_OK;
     std::string err;
     LpOutcome out;
+    FamilyPtr fam_self;  // this LP as a family base (built when a node first links to it)
+    FamilyPtr family;    // base of the family this request belongs to, or null
 };
 
 double quantile(std::vector<double> v, double q) {
@@ -177,7 +184,12 @@ public:
                 err = "warm-start ticket is unknown, unfinished or failed";
                 return PDLPX_E_UNKNOWN_TICKET;
             }
-            const LpOutcome& w = it->second->out;
+            Request& base = *it->second;
+            if (cfg_.families && base.raw.m > 0 && base.raw.n == req->raw.n && base.raw.m <= req->raw.m) {
+                if (!base.fam_self) base.fam_self = makeFamilyBase(base.raw.view());
+                req->family = base.fam_self;  // confirmed against the prepared LP
+            }
+            const LpOutcome& w = base.out;
             if (static_cast<int32_t>(w.x.size()) == req->raw.n && !w.x.empty()) {
                 req->raw.wx = w.x;
                 req->raw.wy.assign(req->raw.m, 0.0);
@@ -317,7 +329,8 @@ private:
                 finishLocked(*r);
                 cv_done_.notify_all();
             } else {
-                r->bytes = preparedBytes(*p);
+                if (r->family && !familyMember(*p, *r->family, opt_)) r->family = nullptr;
+                r->bytes = r->family ? familyMemberBytes(*p, *r->family) : preparedBytes(*p);
                 r->prep = std::move(p);
                 r->state = kPrepared;
                 r->ready = Clock::now();
@@ -357,18 +370,30 @@ private:
                     if (can) break;
                     cv_dispatch_.wait(lk);
                 }
-                while (!ready_q_.empty() && pack.size() < max_lps) {
+                // the head request's family (or the requests outside any family),
+                // in arrival order
+                const FamilyPtr fam = reqs_.at(ready_q_.front())->family;
+                const size_t cap = fam ? std::min<size_t>(max_lps, kFamilyLanes) : max_lps;
+                std::deque<int64_t> rest;
+                while (!ready_q_.empty()) {
                     Request* r = reqs_.at(ready_q_.front()).get();
-                    if (!pack.empty() && bytes_in_flight_ + bytes + r->bytes > budget_) break;
-                    bytes += r->bytes;
-                    r->state = kRunning;
-                    pack.push_back(r);
+                    const bool take = r->family == fam && pack.size() < cap &&
+                                      (pack.empty() || bytes_in_flight_ + bytes + r->bytes <= budget_);
+                    if (take) {
+                        bytes += r->bytes;
+                        r->state = kRunning;
+                        pack.push_back(r);
+                    } else {
+                        rest.push_back(ready_q_.front());
+                    }
                     ready_q_.pop_front();
                 }
+                ready_q_.swap(rest);
                 bytes_in_flight_ += bytes;
                 ++packs_running_;
             }
             std::thread([this, pack, bytes] { runPack(pack, bytes); }).detach();
+            pack.clear();
         }
     }
 
@@ -379,8 +404,10 @@ private:
     void runPack(std::vector<Request*> pack, size_t bytes) {
         std::vector<PreparedPtr> preps;
         std::vector<PreparedLp*> lps;
+        FamilyPtr fam;
         {
             std::lock_guard<std::mutex> g(mu_);
+            fam = pack.front()->family;
             for (Request* r : pack) {
                 preps.push_back(std::move(r->prep));
                 lps.push_back(preps.back().get());
@@ -388,14 +415,16 @@ private:
         }
         std::vector<char> finished(pack.size(), 0);
         std::string err;
-        const int32_t rc = solvePrepared(lps, opt_, &stop_, [&](int l, LpOutcome&& out) {
+        auto done = [&](int l, LpOutcome&& out) {
             std::lock_guard<std::mutex> g(mu_);
             finished[l] = 1;
             Request& r = *pack[l];
             r.out = std::move(out);
             finishLocked(r);
             cv_done_.notify_all();
-        }, err);
+        };
+        const int32_t rc = fam ? solveFamily(*fam, lps, opt_, &stop_, done, err)
+                               : solvePrepared(lps, opt_, &stop_, done, err);
         std::lock_guard<std::mutex> g(mu_);
         for (size_t k = 0; k < pack.size(); ++k) {
             if (finished[k]) continue;
@@ -452,6 +481,7 @@ void pdlpx_server_config_default(pdlpx_server_config* c) {
     c->prep_threads = 0;
     c->queue_limit = 100000;
     c->batch_window_ms = 50;
+    c->families = 1;
 }
 
 int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config* cfg, pdlpx_server** out) {

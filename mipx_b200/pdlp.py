@@ -452,11 +452,13 @@ class Server:
 
     ``submit(lp, warm=None)`` returns a ticket; ``warm`` is an ``(x, y)`` pair or
     the ticket of a finished request.  ``wait(ticket)`` returns
-    ``(LpResult, x, y)``.  ``stats()`` reports p50/p99 latency and LPs/s."""
+    ``(LpResult, x, y)``.  ``stats()`` reports p50/p99 latency and LPs/s.
+    With ``families`` on, requests warm-started from a ticket whose rows they
+    keep unchanged (branch-and-bound nodes of that LP) run in family packs."""
 
     def __init__(self, options: PdlpOptions, budget_bytes: float = 0.0, max_packs: int = 4,
                  max_pack_lps: int = 32, prep_threads: int = 0, queue_limit: int = 100000,
-                 batch_window_ms: int = 50):
+                 batch_window_ms: int = 50, families: bool = True):
         self._lib = _capi.load()
         cfg = _capi.ServerConfig()
         self._lib.pdlpx_server_config_default(C.byref(cfg))
@@ -466,6 +468,7 @@ class Server:
         cfg.prep_threads = int(prep_threads)
         cfg.queue_limit = int(queue_limit)
         cfg.batch_window_ms = int(batch_window_ms)
+        cfg.families = int(bool(families))
         self._h = C.c_void_p()
         _capi.check(self._lib.pdlpx_server_create(C.byref(options.to_c()), C.byref(cfg), C.byref(self._h)))
         self._dims: dict[int, tuple[int, int]] = {}

@@ -146,3 +146,85 @@ def test_server_release_while_pack_still_runs():
                     pending.discard(t)
             time.sleep(0.002)
         assert not pending
+
+
+# ---------------------------------------------------------------------------
+# Family packs: node LPs warm-started from a base ticket share its rows
+# ---------------------------------------------------------------------------
+def _family(seed=51, count=8, m=2000, n=5000):
+    base, x0 = G.random_lp(m, n, 4, 12, seed)
+    ints = G.integer_marks(base.num_cols)
+    return base, [G.node_lp(base, x0, ints, 100 + k) for k in range(count)]
+
+
+def _solve_nodes(base, nodes, opts, **cfg):
+    with Server(opts, **cfg) as srv:
+        tb = srv.submit(base)
+        srv.wait(tb, timeout=300)
+        tickets = [srv.submit(nd, warm=tb) for nd in nodes]
+        return [srv.wait(t, timeout=300) for t in tickets]
+
+
+def test_family_results_same_alone_and_in_mix():
+    """A node LP's family-pack result is bit-identical in a family of one and
+    packed with seven other nodes of the same base (one lane per LP, lane
+    arithmetic independent of the other lanes)."""
+    base, nodes = _family()
+    o = PdlpOptions(**TIGHT)
+    mix = _solve_nodes(base, nodes, o, max_packs=1, max_pack_lps=32, batch_window_ms=500)
+    for k in (0, 3, 7):
+        alone = _solve_nodes(base, [nodes[k]], o, max_packs=1)[0]
+        (r, x, y), (q, u, v) = mix[k], alone
+        assert r.status == q.status == Status.Optimal
+        assert r.iterations == q.iterations and r.objective == q.objective
+        np.testing.assert_array_equal(x, u)
+        np.testing.assert_array_equal(y, v)
+        assert r.fp64_iterations == r.iterations  # family packs iterate in FP64
+
+
+def test_family_matches_single_lp_fp64():
+    """Family results against the single-LP FP64 engine on the same node LPs:
+    same status, objectives within 2e-6 (1 + |obj|) (both at 1e-6 relative KKT),
+    primal feasibility of the returned x within the tolerance."""
+    from mipx_b200.pdlp import PdlpSolver, Precision
+    base, nodes = _family(seed=52, count=6)
+    o = PdlpOptions(**TIGHT)
+    fam = _solve_nodes(base, nodes, o, max_packs=1, batch_window_ms=500)
+    for nd, (r, x, _) in zip(nodes, fam):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(precision=Precision.FP64, **TIGHT))
+        s.load(nd)
+        q = s.solve()
+        assert r.status == q.status
+        if q.status != Status.Optimal:
+            continue
+        assert abs(r.objective - q.objective) <= 2e-6 * (1 + abs(q.objective)), (r.objective, q.objective)
+        assert np.all(x >= nd.col_lower - 1e-9) and np.all(x <= nd.col_upper + 1e-9)
+        assert r.rel_primal_resid <= 1e-6 and r.rel_dual_resid <= 1e-6
+
+
+def test_family_member_check_and_regular_fallback():
+    """An LP linked to the ticket whose base rows differ (one value changed) or
+    whose columns differ is solved in a regular pack and still reaches the optimum;
+    a family pack and the regular packs run side by side."""
+    base, nodes = _family(seed=53, count=3)
+    changed = G.node_lp(base, np.zeros(base.num_cols), G.integer_marks(base.num_cols), 7)
+    changed.matrix.values[5] *= 1.5
+    o = PdlpOptions(**TIGHT)
+    with Server(o, max_packs=3) as srv:
+        tb = srv.submit(base)
+        srv.wait(tb, timeout=300)
+        tickets = [srv.submit(nd, warm=tb) for nd in nodes + [changed]]
+        res = [srv.wait(t, timeout=300) for t in tickets]
+    for r, _, _ in res:
+        assert r.status == Status.Optimal
+    assert res[-1][0].fp64_iterations < res[-1][0].iterations  # regular mixed-precision pack
+
+
+def test_family_off_uses_regular_packs():
+    base, nodes = _family(seed=54, count=2)
+    o = PdlpOptions(**TIGHT)
+    res = _solve_nodes(base, nodes, o, families=False)
+    for r, _, _ in res:
+        assert r.status == Status.Optimal
+        assert r.fp64_iterations < r.iterations
