@@ -71,7 +71,10 @@ def parse():
                    help="profiling run: one pdlpx_batch_solve of the first LPS LPs of the batched workload")
     p.add_argument("--profile-large", type=int, default=0, metavar="M",
                    help="profiling run: one solve of an M x 4M power-law LP (column counts 2-2000, mean 10)")
-    p.add_argument("--profile-iters", type=int, default=2000, help="iteration cap of --profile-batch / --profile-large")
+    p.add_argument("--profile-family", type=int, default=0, metavar="LPS",
+                   help="profiling run: LPS node LPs of the serving workload's base LP as one family pack")
+    p.add_argument("--profile-iters", type=int, default=2000,
+                   help="iteration cap of --profile-batch / --profile-large / --profile-family")
     return p.parse_args()
 
 
@@ -224,6 +227,19 @@ def profile_run(args, local) -> None:
         out = batch_solve(lps, o)
         print(f"profile batch: {len(lps)} LPs, {sum(r.iterations for r, _, _ in out)} LP-iterations, "
               f"device {out[0][0].device_seconds:.3f}s, launches {out[0][0].kernel_launches}", flush=True)
+    if args.profile_family:
+        from mipx_b200.pdlp import Server
+        base, x0 = G.random_lp(20000, 50000, 4, 12, 101)
+        ints = G.integer_marks(base.num_cols)
+        nodes = [G.node_lp(base, x0, ints, 1000 + k) for k in range(args.profile_family)]
+        with Server(o, max_packs=1, max_pack_lps=32, batch_window_ms=2000) as srv:
+            tb = srv.submit(base)
+            srv.wait(tb)
+            t0 = time.perf_counter()
+            res = [srv.wait(t) for t in [srv.submit(nd, warm=tb) for nd in nodes]]
+            wall = time.perf_counter() - t0
+        print(f"profile family: {len(nodes)} node LPs, {sum(r.iterations for r, _, _ in res)} LP-iterations, "
+              f"device {max(r.device_seconds for r, _, _ in res):.3f}s, wall {wall:.3f}s", flush=True)
     if args.profile_large:
         m = args.profile_large
         lp, _ = G.powerlaw_lp(m, 4 * m, 2, 2000, 10.0, 0.01, 1e3, 11)
@@ -347,7 +363,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, pg)
         return
-    if args.profile_batch or args.profile_large:
+    if args.profile_batch or args.profile_large or args.profile_family:
         profile_run(args, local)
         return
     import torch

@@ -27,6 +27,11 @@
 // node LP's result is the same in a family of one and in any mix.
 
 constexpr int kFam = 32;  // lanes (LPs) per family pack
+// Consecutive columns / base rows one warp of a step kernel walks as one
+// contiguous entry range (their CSR entries are adjacent), so a warp keeps
+// several rows' loads and gathers in flight instead of one short row's.
+constexpr int kFamColsPerWarp = 4;
+constexpr int kFamRowsPerWarp = 2;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct FamArgs {
@@ -40,6 +45,7 @@ struct FamArgs {
     const int* k_idx;
     const double* k_val;
     const int* k_lane;    // LP of each appended row
+    const int* k_first;   // [33] first appended row of each lane
     const int* kt_ptr;    // appended entries by column: row, LP, value
     const int* kt_row;
     const int* kt_lane;
@@ -55,12 +61,14 @@ struct FamArgs {
     PowerState* ps;
     int* flags;
     int* counters;
+    const unsigned* live;  // bit l: LP l had not finished at the end of the last cycle
     double* part_rows;  // [block][32][kRowSlots]
     double* part_cols;  // [block][32][kColSlots]
     double *pi_x, *pi_y, *pi_xn, *pi_part;
     int n, mb, K, L;
-    int gb, gk;           // step / power blocks over base rows, appended rows
-    int nbr, nbk, nbc;    // check blocks: base rows, appended rows, columns
+    int gb, gk;           // power blocks over base rows, appended rows (one row per warp)
+    int gp, gd;           // step blocks: columns, base rows (kFamColsPerWarp / kFamRowsPerWarp per warp)
+    int nbr, nbk, nbc;    // check blocks: base rows, appended rows (one per lane, or none), columns
     int max_iter, polish_max_iter, N, sv_max_iter;
     double sv_tol;
 };
@@ -70,8 +78,9 @@ __device__ __forceinline__ size_t fCut(const FamArgs& a, int q) { return static_
 
 // Dot product of one shared row with lane l's vector get(entry index): the warp
 // loads up to 32 entries with one coalesced load per array, broadcasts them by
-// shuffle and every active lane gathers its own value (four independent
-// products per round).  The loop bounds are warp-uniform.
+// shuffle and every active lane gathers its own values, eight gathers in flight
+// per round before the products wait on them.  The loop bounds are
+// warp-uniform; the slots of a round past the row's end gather nothing.
 template <class Get>
 __device__ __forceinline__ double famDot(const int* __restrict__ idx, const double* __restrict__ val, int b, int e,
                                          int l, bool on, Get get) {
@@ -84,33 +93,80 @@ __device__ __forceinline__ double famDot(const int* __restrict__ idx, const doub
             mc = __ldg(idx + c0 + l);
             mv = __ldg(val + c0 + l);
         }
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4) {
-            const int q0 = __shfl_sync(kFull, mc, k), q1 = __shfl_sync(kFull, mc, k + 1);
-            const int q2 = __shfl_sync(kFull, mc, k + 2), q3 = __shfl_sync(kFull, mc, k + 3);
-            const double v0 = __shfl_sync(kFull, mv, k), v1 = __shfl_sync(kFull, mv, k + 1);
-            const double v2 = __shfl_sync(kFull, mv, k + 2), v3 = __shfl_sync(kFull, mv, k + 3);
-            double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
-            if (on) {
-                g0 = get(q0);
-                g1 = get(q1);
-                g2 = get(q2);
-                g3 = get(q3);
+        for (int k = 0; k < cnt; k += 8) {
+            int q[8];
+            double v[8], g[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                q[u] = __shfl_sync(kFull, mc, (k + u) & 31);
+                v[u] = __shfl_sync(kFull, mv, (k + u) & 31);
             }
-            s0 += v0 * g0;
-            s1 += v1 * g1;
-            s2 += v2 * g2;
-            s3 += v3 * g3;
-        }
-        for (; k < cnt; ++k) {
-            const int q = __shfl_sync(kFull, mc, k);
-            const double v = __shfl_sync(kFull, mv, k);
-            const double g = on ? get(q) : 0.0;
-            s0 += v * g;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) g[u] = (on && k + u < cnt) ? get(q[u]) : 0.0;
+            s0 += v[0] * g[0];
+            s1 += v[1] * g[1];
+            s2 += v[2] * g[2];
+            s3 += v[3] * g[3];
+            s0 += v[4] * g[4];
+            s1 += v[5] * g[5];
+            s2 += v[6] * g[6];
+            s3 += v[7] * g[7];
         }
     }
     return (s0 + s1) + (s2 + s3);
 }
+
+// famDot over R consecutive rows whose entries are adjacent: bnd[0..R] are
+// their CSR bounds (rows past the last real one empty).  Entries are taken in
+// order, eight gathers per round; each product goes to the accumulator of its
+// row (warp-uniform predicates), so every row is summed in entry order.
+template <int R, class Get>
+__device__ __forceinline__ void famDotRows(const int* __restrict__ idx, const double* __restrict__ val,
+                                           const int (&bnd)[R + 1], int l, bool on, Get get, double (&s)[R]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = 0.0;
+    const int b = bnd[0], e = bnd[R];
+    for (int c0 = b; c0 < e; c0 += 32) {
+        const int cnt = min(32, e - c0);
+        int mc = 0;
+        double mv = 0.0;
+        if (l < cnt) {
+            mc = __ldg(idx + c0 + l);
+            mv = __ldg(val + c0 + l);
+        }
+        for (int k = 0; k < cnt; k += 8) {
+            int q[8];
+            double v[8], g[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                q[u] = __shfl_sync(kFull, mc, (k + u) & 31);
+                v[u] = __shfl_sync(kFull, mv, (k + u) & 31);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) g[u] = (on && k + u < cnt) ? get(q[u]) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int pos = c0 + k + u;
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (pos >= bnd[r] && pos < bnd[r + 1]) s[r] += v[u] * g[u];
+            }
+        }
+    }
+}
+
+// CSR bounds of the rows first .. first + R - 1 (clipped to `rows`) from one
+// coalesced load: bnd[r] = ptr[first + min(r, count)].
+template <int R>
+__device__ __forceinline__ int famBounds(const int* __restrict__ ptr, int first, int rows, int l, int (&bnd)[R + 1]) {
+    const int count = min(R, rows - first);
+    const int p = l <= count ? __ldg(ptr + first + l) : 0;
+#pragma unroll
+    for (int r = 0; r <= R; ++r) bnd[r] = __shfl_sync(kFull, p, min(r, count));
+    return count;
+}
+
+__device__ __forceinline__ void famPrefetch(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // Sum of one appended row of LP lp against get(column): lanes stride over the
 // entries, fixed-order butterfly; every lane returns the sum.
@@ -151,77 +207,102 @@ __device__ __forceinline__ double famDualStep(const RowPack<double>& q, double y
 }
 
 // ---- PDHG step -----------------------------------------------------------------
-// Primal: one warp per column j; (A_l^T y)_j = c_lj (sum_i a_ij ys_il + appended entries).
-__global__ void __launch_bounds__(kBlock) famPrimal(FamArgs a, int koff) {
-    const int j = static_cast<int>(blockIdx.x) * kWarps + static_cast<int>(threadIdx.x >> 5);
+// Primal: one warp per kFamColsPerWarp consecutive columns;
+// (A_l^T y)_j = c_lj (sum_i a_ij ys_il + appended entries).  Lanes of LPs
+// still running gather at once (the live mask of the last cycle); the solver
+// state -- iteration limits inside the cycle, step, weight -- is read after
+// the sums, and the per-lane column data is prefetched into L2 meanwhile.
+__global__ void __launch_bounds__(kBlock, 4) famPrimal(FamArgs a, int koff) {
+    constexpr int R = kFamColsPerWarp;
+    const int j0 = (static_cast<int>(blockIdx.x) * kWarps + static_cast<int>(threadIdx.x >> 5)) * R;
     const int l = threadIdx.x & 31;
-    if (j >= a.n) return;
-    bool last = false;
-    const bool on = l < a.L && active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N);
-    if (__ballot_sync(kFull, on) == 0) return;
-    const size_t q = fIdx(j, l);
-    ColPack<double> c{0.0, 0.0, 0.0, 0.0};
-    double cs = 1.0, xc = 0.0, xi = 0.0;
-    if (on) {
-        c = a.cp[q];
-        cs = a.cs[q];
-        xc = a.xc[q];
-        xi = a.xi[q];
-    }
+    if (j0 >= a.n) return;
+    const bool live = (*a.live >> l) & 1u;
+    if (__ballot_sync(kFull, live) == 0) return;
+    int bnd[R + 1], kbd[R + 1];
+    const int nr = famBounds<R>(a.at_ptr, j0, a.n, l, bnd);
+    famBounds<R>(a.kt_ptr, j0, a.n, l, kbd);
+    if (live)
+        for (int r = 0; r < nr; ++r) {
+            const size_t q = fIdx(j0 + r, l);
+            famPrefetch(a.cp + q);
+            famPrefetch(a.cs + q);
+            famPrefetch(a.xc + q);
+            famPrefetch(a.xi + q);
+        }
     const double* ys = a.ys;
-    double s = famDot(a.at_idx, a.at_val, a.at_ptr[j], a.at_ptr[j + 1], l, on,
-                      [&](int i) { return __ldg(ys + fIdx(i, l)); });
-    for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k)
-        if (on && a.kt_lane[k] == l) s += a.kt_val[k] * ys[fCut(a, a.kt_row[k])];
-    if (!on) return;
+    double s[R];
+    famDotRows<R>(a.at_idx, a.at_val, bnd, l, live, [&](int i) { return __ldg(ys + fIdx(i, l)); }, s);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        for (int k = kbd[r]; k < kbd[r + 1]; ++k)
+            if (live && a.kt_lane[k] == l) s[r] += a.kt_val[k] * ys[fCut(a, a.kt_row[k])];
+    bool last = false;
+    if (!live || !active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;
     const DevState* st = a.st + l;
     const double step = st->step, pw = st->pw;
     const int kk = st->inner + koff;
     const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
-    const double tau = step * c.tau / pw;
-    double xh = xc - tau * (c.c + cs * s);
-    if (xh < c.lb) xh = c.lb;
-    if (xh > c.ub) xh = c.ub;
-    const double xr = 2.0 * xh - xc;
-    a.xc[q] = lam * xr + (1.0 - lam) * xi;
-    a.xs[q] = cs * xr;
-    if (last) a.xh[q] = xh;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (r >= nr) break;
+        const size_t q = fIdx(j0 + r, l);
+        const ColPack<double> c = a.cp[q];
+        const double cs = a.cs[q], xc = a.xc[q], xi = a.xi[q];
+        const double tau = step * c.tau / pw;
+        double xh = xc - tau * (c.c + cs * s[r]);
+        if (xh < c.lb) xh = c.lb;
+        if (xh > c.ub) xh = c.ub;
+        const double xr = 2.0 * xh - xc;
+        a.xc[q] = lam * xr + (1.0 - lam) * xi;
+        a.xs[q] = cs * xr;
+        if (last) a.xh[q] = xh;
+    }
 }
 
-// Dual: blocks [0, gb) one warp per base row, then one warp per appended row.
-__global__ void __launch_bounds__(kBlock) famDual(FamArgs a, int koff) {
+// Dual: blocks [0, gd) one warp per kFamRowsPerWarp base rows, then one warp
+// per appended row.
+__global__ void __launch_bounds__(kBlock, 4) famDual(FamArgs a, int koff) {
     const int w = static_cast<int>(threadIdx.x >> 5);
     const int l = threadIdx.x & 31;
     const double* xs = a.xs;
-    if (static_cast<int>(blockIdx.x) < a.gb) {
-        const int i = static_cast<int>(blockIdx.x) * kWarps + w;
-        if (i >= a.mb) return;
+    if (static_cast<int>(blockIdx.x) < a.gd) {
+        constexpr int R = kFamRowsPerWarp;
+        const int i0 = (static_cast<int>(blockIdx.x) * kWarps + w) * R;
+        if (i0 >= a.mb) return;
+        const bool live = (*a.live >> l) & 1u;
+        if (__ballot_sync(kFull, live) == 0) return;
+        int bnd[R + 1];
+        const int nr = famBounds<R>(a.a_ptr, i0, a.mb, l, bnd);
+        if (live)
+            for (int r = 0; r < nr; ++r) {
+                const size_t q = fIdx(i0 + r, l);
+                famPrefetch(a.rp + q);
+                famPrefetch(a.rs + q);
+                famPrefetch(a.yc + q);
+                famPrefetch(a.yi + q);
+            }
+        double s[R];
+        famDotRows<R>(a.a_idx, a.a_val, bnd, l, live, [&](int j) { return __ldg(xs + fIdx(j, l)); }, s);
         bool last = false;
-        const bool on = l < a.L && active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N);
-        if (__ballot_sync(kFull, on) == 0) return;
-        const size_t q = fIdx(i, l);
-        RowPack<double> r{0.0, 0.0, 0.0, 0.0};
-        double rs = 1.0, yc = 0.0, yi = 0.0;
-        if (on) {
-            r = a.rp[q];
-            rs = a.rs[q];
-            yc = a.yc[q];
-            yi = a.yi[q];
-        }
-        const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on,
-                                [&](int j) { return __ldg(xs + fIdx(j, l)); });
-        if (!on) return;
+        if (!live || !active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;
         const DevState* st = a.st + l;
         const int kk = st->inner + koff;
         const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
-        double py;
-        const double yn = famDualStep(r, yc, yi, rs * s, st->step, st->pw, lam, py);
-        a.yc[q] = yn;
-        a.ys[q] = rs * yn;
-        if (last) a.yh[q] = py;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r >= nr) break;
+            const size_t q = fIdx(i0 + r, l);
+            const double rs = a.rs[q], yc = a.yc[q];
+            double py;
+            const double yn = famDualStep(a.rp[q], yc, a.yi[q], rs * s[r], st->step, st->pw, lam, py);
+            a.yc[q] = yn;
+            a.ys[q] = rs * yn;
+            if (last) a.yh[q] = py;
+        }
         return;
     }
-    const int qq = (static_cast<int>(blockIdx.x) - a.gb) * kWarps + w;
+    const int qq = (static_cast<int>(blockIdx.x) - a.gd) * kWarps + w;
     if (qq >= a.K) return;
     const int lp = a.k_lane[qq];
     bool last = false;
@@ -262,8 +343,9 @@ __device__ __forceinline__ bool famChecking(const FamArgs& a, int l) {
     return l < a.L && !a.st[l].done && a.st[l].prec == 1;
 }
 
-// Rows: blocks [0, nbr) stride over the base rows, [nbr, nbr + nbk) over the
-// appended rows (their terms go to the lane of their LP).
+// Rows: blocks [0, nbr) stride over the base rows; block nbr + l takes the
+// appended rows of lane l (their terms go to lane l's partial), so an LP's
+// reduction order does not depend on the other LPs of the pack.
 __global__ void __launch_bounds__(kBlock) famCheckRows(FamArgs a) {
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     int ops[kRowSlots];
@@ -289,10 +371,10 @@ __global__ void __launch_bounds__(kBlock) famCheckRows(FamArgs a) {
             }
         }
     } else {
-        const int b = static_cast<int>(blockIdx.x) - a.nbr;
-        for (int qq = b * kWarps + w; qq < a.K; qq += a.nbk * kWarps) {
-            const int lp = a.k_lane[qq];
-            if (!famChecking(a, lp)) continue;  // warp-uniform
+        const int lp = static_cast<int>(blockIdx.x) - a.nbr;
+        const bool live = famChecking(a, lp);  // block-uniform
+        const int q1 = a.k_first[lp + 1];
+        for (int qq = a.k_first[lp] + w; live && qq < q1; qq += kWarps) {
             const double s = famCutDot(a, qq, l, [&](int j) {
                 const size_t c = fIdx(j, lp);
                 return cs[c] * xh[c];
@@ -376,7 +458,12 @@ __global__ void __launch_bounds__(32 * kCtlWarps) famController(FamArgs a) {
 #pragma unroll
     for (int s = 0; s < kColSlots; ++s) cops[s] = colSlotOp(s);
     double rows[kRowSlots], cols[kColSlots];
-    famLanes<kRowSlots>(a.part_rows, a.nbr + a.nbk, l, lane, rops, rows);
+    famLanes<kRowSlots>(a.part_rows, a.nbr, l, lane, rops, rows);
+    if (a.nbk > 0) {  // this LP's appended rows: the partial of lane l in block nbr + l
+        const double* p = a.part_rows + (static_cast<size_t>(a.nbr + l) * kFam + l) * kRowSlots;
+#pragma unroll
+        for (int s = 0; s < kRowSlots; ++s) rows[s] = combine(rops[s], rows[s], p[s]);
+    }
     famLanes<kColSlots>(a.part_cols, a.nbc, l, lane, cops, cols);
     if (lane == 0) {
         DevState s = *st;
@@ -416,8 +503,10 @@ __global__ void __launch_bounds__(kBlock) famRestart(FamArgs a) {
 
 __global__ void famFinish(FamArgs a) {
     const int l = threadIdx.x;
-    if (l >= a.L) return;
-    a.flags[l] = (a.st[l].done ? 1 : 0) | 2;
+    const bool done = l >= a.L || a.st[l].done;
+    const unsigned live = __ballot_sync(kFull, !done);
+    if (l == 0) *const_cast<unsigned*>(a.live) = live;
+    if (l < a.L) a.flags[l] = (done ? 1 : 0) | 2;
 }
 
 // ---- power iteration on A_l^T A_l per lane (pdlp.cpp:748-795, 1985-2041) -------------
@@ -544,7 +633,7 @@ struct FamPack {
     int L = 0, n = 0, mb = 0, K = 0;
     int64_t Zb = 0, Zk = 0;
     std::vector<int> qfirst;  // first appended row of each lane
-    size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane;
+    size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane, o_kfirst, o_live;
     size_t o_ktptr, o_ktrow, o_ktlane, o_ktval, o_cp, o_cs, o_rp, o_rs, o_st, o_dc, o_ps, o_pix;
     size_t image_end;
     size_t o_xc, o_xi, o_xh, o_xs, o_yc, o_yi, o_yh, o_ys;
@@ -588,6 +677,8 @@ struct FamPack {
         o_kidx = take(4 * static_cast<size_t>(Zk));
         o_kval = take(8 * static_cast<size_t>(Zk));
         o_klane = take(4 * static_cast<size_t>(K));
+        o_kfirst = take(4 * (kFam + 1));
+        o_live = take(4);
         o_ktptr = take(4 * (static_cast<size_t>(n) + 1));
         o_ktrow = take(4 * static_cast<size_t>(Zk));
         o_ktlane = take(4 * static_cast<size_t>(Zk));
@@ -659,8 +750,10 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
     fp.Zb = fb.ptr[mb];
     const int K = fp.K;
     const int gb = famBlocks(mb), gk = K > 0 ? famBlocks(K) : 0;
+    const int gp = famBlocks((static_cast<int64_t>(n) + kFamColsPerWarp - 1) / kFamColsPerWarp);
+    const int gd = famBlocks((static_cast<int64_t>(mb) + kFamRowsPerWarp - 1) / kFamRowsPerWarp);
     const int cap = 4 * sms;
-    const int nbr = std::min(gb, cap), nbk = K > 0 ? std::min(gk, cap) : 0, nbc = std::min(famBlocks(n), cap);
+    const int nbr = std::min(gb, cap), nbk = K > 0 ? L : 0, nbc = std::min(famBlocks(n), cap);
     fp.layout(nbr, nbk, nbc);
 
     // ---- host image
@@ -708,6 +801,9 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
             }
         }
         kp[K] = static_cast<int32_t>(z);
+        int32_t* kf = I(fp.o_kfirst);
+        for (int l = 0; l <= kFam; ++l) kf[l] = fp.qfirst[std::min(l, L)];
+        *reinterpret_cast<uint32_t*>(H + fp.o_live) = L >= kFam ? ~0u : ((1u << L) - 1u);
         int32_t* ktp = I(fp.o_ktptr);
         for (int32_t j = 0; j < n; ++j) colcnt[j + 1] += colcnt[j];
         std::memcpy(ktp, colcnt.data(), 4 * (static_cast<size_t>(n) + 1));
@@ -819,6 +915,8 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         a.k_idx = Pi(fp.o_kidx);
         a.k_val = Pd(fp.o_kval);
         a.k_lane = Pi(fp.o_klane);
+        a.k_first = Pi(fp.o_kfirst);
+        a.live = reinterpret_cast<const unsigned*>(d + fp.o_live);
         a.kt_ptr = Pi(fp.o_ktptr);
         a.kt_row = Pi(fp.o_ktrow);
         a.kt_lane = Pi(fp.o_ktlane);
@@ -851,6 +949,8 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         a.K = K;
         a.L = L;
         a.gb = gb;
+        a.gp = gp;
+        a.gd = gd;
         a.gk = gk;
         a.nbr = nbr;
         a.nbk = nbk;
@@ -884,7 +984,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
     auto hostSeconds = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
     auto stopped = [&]() { return stop != nullptr && stop->load(std::memory_order_relaxed) != 0; };
     std::vector<int> h_flags(kFam);
-    const int nct = famBlocks(n), stepRows = gb + gk;
+    const int stepRows = gb + gk;
     const int ctl = (L + kCtlWarps - 1) / kCtlWarps;
     const int nrs = std::max(1, std::min<int>(static_cast<int>((fp.colsAll() + fp.rowsAll() + kBlock - 1) / kBlock), 8 * sms));
     auto capture = [&](cudaGraphExec_t& gx, int& count, bool power) -> int32_t {
@@ -902,8 +1002,8 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
             }
         } else {
             for (int k = 1; k <= o.termination_eval_frequency; ++k) {
-                famPrimal<<<nct, kBlock, 0, s>>>(args, k);
-                famDual<<<stepRows, kBlock, 0, s>>>(args, k);
+                famPrimal<<<gp, kBlock, 0, s>>>(args, k);
+                famDual<<<gd + gk, kBlock, 0, s>>>(args, k);
                 count += 2;
             }
             famCheckRows<<<nbr + nbk, kBlock, 0, s>>>(args);
