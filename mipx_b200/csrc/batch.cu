@@ -1667,6 +1667,8 @@ FamilyPtr makeFamilyBase(const pdlpx_lp& base) {
 bool familyMember(const PreparedLp& p, const FamilyBase& f, const pdlpx_options& o) {
     const HostLp& lp = p.item.lp;
     if (p.item.trivial || o.matrix_zero_tol > 0.0 || f.m <= 0 || lp.n != f.n || lp.m < f.m) return false;
+    // gather offsets (index x 32) of the shared rows are int32
+    if (static_cast<int64_t>(std::max(f.m, f.n)) * kFamilyLanes >= std::numeric_limits<int32_t>::max()) return false;
     const size_t z = static_cast<size_t>(f.ptr[f.m]);
     return std::equal(f.ptr.begin(), f.ptr.end(), lp.a.ptr.begin()) &&
            std::memcmp(lp.a.idx.data(), f.idx.data(), 4 * z) == 0 &&

@@ -35,8 +35,8 @@ constexpr int kFamRowsPerWarp = 2;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct FamArgs {
-    const int* a_ptr;     // base rows (original values)
-    const int* a_idx;
+    const int* a_ptr;     // base rows (original values); the entry indices are
+    const int* a_idx;     // stored times 32, the offset of the entry's slot of lane 0
     const double* a_val;
     const int* at_ptr;    // base rows transposed
     const int* at_idx;
@@ -118,14 +118,27 @@ __device__ __forceinline__ double famDot(const int* __restrict__ idx, const doub
 
 // famDot over R consecutive rows whose entries are adjacent: bnd[0..R] are
 // their CSR bounds (rows past the last real one empty).  Entries are taken in
-// order, eight gathers per round; each product goes to the accumulator of its
-// row (warp-uniform predicates), so every row is summed in entry order.
+// order, eight gathers per round, into one running sum that is handed to the
+// row's slot when the entry position crosses the row's end (a warp-uniform
+// test; the next bound comes by shuffle from the lane that loaded it), so
+// every row is summed in entry order with one multiply-add per entry.
 template <int R, class Get>
 __device__ __forceinline__ void famDotRows(const int* __restrict__ idx, const double* __restrict__ val,
-                                           const int (&bnd)[R + 1], int l, bool on, Get get, double (&s)[R]) {
+                                           const int (&bnd)[R + 1], int pl, int l, bool on, Get get, double (&s)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) s[r] = 0.0;
     const int b = bnd[0], e = bnd[R];
+    int cr = 0;
+    int nextb = bnd[1];
+    double acc = 0.0;
+    auto flush = [&]() {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (r == cr) s[r] = acc;
+        acc = 0.0;
+        ++cr;
+        nextb = __shfl_sync(kFull, pl, min(cr + 1, R));
+    };
     for (int c0 = b; c0 < e; c0 += 32) {
         const int cnt = min(32, e - c0);
         int mc = 0;
@@ -134,7 +147,9 @@ __device__ __forceinline__ void famDotRows(const int* __restrict__ idx, const do
             mc = __ldg(idx + c0 + l);
             mv = __ldg(val + c0 + l);
         }
-        for (int k = 0; k < cnt; k += 8) {
+        // full rounds of eight, then one masked round for the rest
+        auto round = [&](int k, auto masked) {
+            constexpr bool M = decltype(masked)::value;
             int q[8];
             double v[8], g[8];
 #pragma unroll
@@ -143,26 +158,34 @@ __device__ __forceinline__ void famDotRows(const int* __restrict__ idx, const do
                 v[u] = __shfl_sync(kFull, mv, (k + u) & 31);
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) g[u] = (on && k + u < cnt) ? get(q[u]) : 0.0;
+            for (int u = 0; u < 8; ++u) g[u] = (on && (!M || k + u < cnt)) ? get(q[u]) : 0.0;
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
+                if (M && k + u >= cnt) break;
                 const int pos = c0 + k + u;
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (pos >= bnd[r] && pos < bnd[r + 1]) s[r] += v[u] * g[u];
+                while (pos >= nextb) flush();
+                acc += v[u] * g[u];
             }
-        }
+        };
+        int k = 0;
+        for (; k + 8 <= cnt; k += 8) round(k, std::false_type{});
+        if (k < cnt) round(k, std::true_type{});
     }
+    while (cr < R) flush();
 }
 
 // CSR bounds of the rows first .. first + R - 1 (clipped to `rows`) from one
-// coalesced load: bnd[r] = ptr[first + min(r, count)].
+// coalesced load: bnd[r] = ptr[first + min(r, count)];
+// pl is this lane's loaded bound (lane r holds bnd[r]; lanes past the last
+// real row hold the last bound).
 template <int R>
-__device__ __forceinline__ int famBounds(const int* __restrict__ ptr, int first, int rows, int l, int (&bnd)[R + 1]) {
+__device__ __forceinline__ int famBounds(const int* __restrict__ ptr, int first, int rows, int l, int (&bnd)[R + 1],
+                                         int& pl) {
     const int count = min(R, rows - first);
-    const int p = l <= count ? __ldg(ptr + first + l) : 0;
+    const int p = __ldg(ptr + first + min(l, count));
 #pragma unroll
     for (int r = 0; r <= R; ++r) bnd[r] = __shfl_sync(kFull, p, min(r, count));
+    pl = p;
     return count;
 }
 
@@ -219,9 +242,9 @@ __global__ void __launch_bounds__(kBlock, 4) famPrimal(FamArgs a, int koff) {
     if (j0 >= a.n) return;
     const bool live = (*a.live >> l) & 1u;
     if (__ballot_sync(kFull, live) == 0) return;
-    int bnd[R + 1], kbd[R + 1];
-    const int nr = famBounds<R>(a.at_ptr, j0, a.n, l, bnd);
-    famBounds<R>(a.kt_ptr, j0, a.n, l, kbd);
+    int bnd[R + 1], kbd[R + 1], pl, pk;
+    const int nr = famBounds<R>(a.at_ptr, j0, a.n, l, bnd, pl);
+    famBounds<R>(a.kt_ptr, j0, a.n, l, kbd, pk);
     if (live)
         for (int r = 0; r < nr; ++r) {
             const size_t q = fIdx(j0 + r, l);
@@ -232,7 +255,7 @@ __global__ void __launch_bounds__(kBlock, 4) famPrimal(FamArgs a, int koff) {
         }
     const double* ys = a.ys;
     double s[R];
-    famDotRows<R>(a.at_idx, a.at_val, bnd, l, live, [&](int i) { return __ldg(ys + fIdx(i, l)); }, s);
+    famDotRows<R>(a.at_idx, a.at_val, bnd, pl, l, live, [&](int i) { return __ldg(ys + (static_cast<size_t>(i) + l)); }, s);
 #pragma unroll
     for (int r = 0; r < R; ++r)
         for (int k = kbd[r]; k < kbd[r + 1]; ++k)
@@ -272,8 +295,8 @@ __global__ void __launch_bounds__(kBlock, 4) famDual(FamArgs a, int koff) {
         if (i0 >= a.mb) return;
         const bool live = (*a.live >> l) & 1u;
         if (__ballot_sync(kFull, live) == 0) return;
-        int bnd[R + 1];
-        const int nr = famBounds<R>(a.a_ptr, i0, a.mb, l, bnd);
+        int bnd[R + 1], pl;
+        const int nr = famBounds<R>(a.a_ptr, i0, a.mb, l, bnd, pl);
         if (live)
             for (int r = 0; r < nr; ++r) {
                 const size_t q = fIdx(i0 + r, l);
@@ -283,7 +306,7 @@ __global__ void __launch_bounds__(kBlock, 4) famDual(FamArgs a, int koff) {
                 famPrefetch(a.yi + q);
             }
         double s[R];
-        famDotRows<R>(a.a_idx, a.a_val, bnd, l, live, [&](int j) { return __ldg(xs + fIdx(j, l)); }, s);
+        famDotRows<R>(a.a_idx, a.a_val, bnd, pl, l, live, [&](int j) { return __ldg(xs + (static_cast<size_t>(j) + l)); }, s);
         bool last = false;
         if (!live || !active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;
         const DevState* st = a.st + l;
@@ -360,7 +383,7 @@ __global__ void __launch_bounds__(kBlock) famCheckRows(FamArgs a) {
         const bool on = famChecking(a, l);
         for (int i = static_cast<int>(blockIdx.x) * kWarps + w; i < a.mb; i += a.nbr * kWarps) {
             const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on, [&](int j) {
-                const size_t c = fIdx(j, l);
+                const size_t c = static_cast<size_t>(j) + l;
                 return cs[c] * xh[c];
             });
             if (on) {
@@ -405,11 +428,11 @@ __global__ void __launch_bounds__(kBlock) famCheckCols(FamArgs a) {
     for (int j = static_cast<int>(blockIdx.x) * kWarps + w; j < a.n; j += a.nbc * kWarps) {
         const int b = a.at_ptr[j], e = a.at_ptr[j + 1];
         double aty = famDot(a.at_idx, a.at_val, b, e, l, on, [&](int i) {
-            const size_t q = fIdx(i, l);
+            const size_t q = static_cast<size_t>(i) + l;
             return rs[q] * yh[q];
         });
         double atdy = famDot(a.at_idx, a.at_val, b, e, l, on, [&](int i) {
-            const size_t q = fIdx(i, l);
+            const size_t q = static_cast<size_t>(i) + l;
             return rs[q] * (yh[q] - yi[q]);
         });
         for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k) {
@@ -520,7 +543,7 @@ __global__ void __launch_bounds__(kBlock) famPowerA(FamArgs a) {
         const bool on = l < a.L && !a.ps[l].done;
         if (__ballot_sync(kFull, on) == 0) return;
         const double s = famDot(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], l, on, [&](int j) {
-            const size_t c = fIdx(j, l);
+            const size_t c = static_cast<size_t>(j) + l;
             return cs[c] * px[c];
         });
         if (on) a.pi_y[fIdx(i, l)] = a.rs[fIdx(i, l)] * s;
@@ -544,7 +567,7 @@ __global__ void __launch_bounds__(kBlock) famPowerAt(FamArgs a) {
     double acc[2] = {0.0, 0.0};
     for (int j = static_cast<int>(blockIdx.x) * kWarps + w; j < a.n; j += a.nbc * kWarps) {
         double s = famDot(a.at_idx, a.at_val, a.at_ptr[j], a.at_ptr[j + 1], l, on, [&](int i) {
-            const size_t q = fIdx(i, l);
+            const size_t q = static_cast<size_t>(i) + l;
             return rs[q] * py[q];
         });
         for (int k = a.kt_ptr[j]; k < a.kt_ptr[j + 1]; ++k)
@@ -764,7 +787,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
     auto D = [&](size_t off) { return reinterpret_cast<double*>(H + off); };
     auto ID = [&](size_t off) { return reinterpret_cast<double*>(iters.get() + (off - fp.image_end)); };
     std::memcpy(I(fp.o_aptr), fb.ptr.data(), 4 * (static_cast<size_t>(mb) + 1));
-    std::memcpy(I(fp.o_aidx), fb.idx.data(), 4 * static_cast<size_t>(fp.Zb));
+    for (int64_t k = 0; k < fp.Zb; ++k) I(fp.o_aidx)[k] = fb.idx[k] * kFam;
     std::memcpy(D(fp.o_aval), fb.val.data(), 8 * static_cast<size_t>(fp.Zb));
     {
         Csr a;
@@ -776,7 +799,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         Csr at;
         transposeCsr(a, at);
         std::memcpy(I(fp.o_atptr), at.ptr.data(), 4 * (static_cast<size_t>(n) + 1));
-        std::memcpy(I(fp.o_atidx), at.idx.data(), 4 * static_cast<size_t>(fp.Zb));
+        for (int64_t k = 0; k < fp.Zb; ++k) I(fp.o_atidx)[k] = at.idx[k] * kFam;
         std::memcpy(D(fp.o_atval), at.val.data(), 8 * static_cast<size_t>(fp.Zb));
     }
     {
