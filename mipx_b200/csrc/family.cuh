@@ -34,6 +34,18 @@ constexpr int kFamColsPerWarp = 4;
 constexpr int kFamRowsPerWarp = 2;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Per-lane step parameters of the running cycle, structure of arrays so that a
+// warp reads its 32 LPs' values with one coalesced load each (the solver state
+// itself is an array of structures: 32 lanes would touch 32 cache lines per
+// field).  Written at the end of every cycle (and before the first) from the
+// controller's state; allow = iterations this cycle (0 when finished).
+struct FamLane {
+    double step[kFam];
+    double pw[kFam];
+    int inner[kFam];
+    int allow[kFam];
+};
+
 struct FamArgs {
     const int* a_ptr;     // base rows (original values); the entry indices are
     const int* a_idx;     // stored times 32, the offset of the entry's slot of lane 0
@@ -62,6 +74,7 @@ struct FamArgs {
     int* flags;
     int* counters;
     const unsigned* live;  // bit l: LP l had not finished at the end of the last cycle
+    FamLane* lanes;
     double* part_rows;  // [block][32][kRowSlots]
     double* part_cols;  // [block][32][kColSlots]
     double *pi_x, *pi_y, *pi_xn, *pi_part;
@@ -260,11 +273,11 @@ __global__ void __launch_bounds__(kBlock, 4) famPrimal(FamArgs a, int koff) {
     for (int r = 0; r < R; ++r)
         for (int k = kbd[r]; k < kbd[r + 1]; ++k)
             if (live && a.kt_lane[k] == l) s[r] += a.kt_val[k] * ys[fCut(a, a.kt_row[k])];
-    bool last = false;
-    if (!live || !active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;
-    const DevState* st = a.st + l;
-    const double step = st->step, pw = st->pw;
-    const int kk = st->inner + koff;
+    const int allow = a.lanes->allow[l];
+    if (!live || koff > allow) return;
+    const bool last = koff == allow;
+    const double step = a.lanes->step[l], pw = a.lanes->pw[l];
+    const int kk = a.lanes->inner[l] + koff;
     const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -307,10 +320,11 @@ __global__ void __launch_bounds__(kBlock, 4) famDual(FamArgs a, int koff) {
             }
         double s[R];
         famDotRows<R>(a.a_idx, a.a_val, bnd, pl, l, live, [&](int j) { return __ldg(xs + (static_cast<size_t>(j) + l)); }, s);
-        bool last = false;
-        if (!live || !active(a.st + l, 1, koff, a.max_iter, a.polish_max_iter, last, a.N)) return;
-        const DevState* st = a.st + l;
-        const int kk = st->inner + koff;
+        const int allow = a.lanes->allow[l];
+        if (!live || koff > allow) return;
+        const bool last = koff == allow;
+        const double step = a.lanes->step[l], pw = a.lanes->pw[l];
+        const int kk = a.lanes->inner[l] + koff;
         const double lam = static_cast<double>(kk) / static_cast<double>(kk + 1);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -318,7 +332,7 @@ __global__ void __launch_bounds__(kBlock, 4) famDual(FamArgs a, int koff) {
             const size_t q = fIdx(i0 + r, l);
             const double rs = a.rs[q], yc = a.yc[q];
             double py;
-            const double yn = famDualStep(a.rp[q], yc, a.yi[q], rs * s[r], st->step, st->pw, lam, py);
+            const double yn = famDualStep(a.rp[q], yc, a.yi[q], rs * s[r], step, pw, lam, py);
             a.yc[q] = yn;
             a.ys[q] = rs * yn;
             if (last) a.yh[q] = py;
@@ -524,11 +538,29 @@ __global__ void __launch_bounds__(kBlock) famRestart(FamArgs a) {
     }
 }
 
+// Lane parameters of the next cycle from the solver state (the iteration rule
+// of `active`: the cycle runs min(N, limit - done so far) iterations).
+__device__ __forceinline__ void famLaneParams(const FamArgs& a, int l, bool done) {
+    FamLane& p = *a.lanes;
+    if (done) {
+        p.allow[l] = 0;
+        return;
+    }
+    const DevState& s = a.st[l];
+    const int cur = s.phase == 0 ? s.total : s.polish_count;
+    const int lim = s.phase == 0 ? a.max_iter : a.polish_max_iter;
+    p.allow[l] = max(0, min(a.N, lim - cur));
+    p.step[l] = s.step;
+    p.pw[l] = s.pw;
+    p.inner[l] = s.inner;
+}
+
 __global__ void famFinish(FamArgs a) {
     const int l = threadIdx.x;
     const bool done = l >= a.L || a.st[l].done;
     const unsigned live = __ballot_sync(kFull, !done);
     if (l == 0) *const_cast<unsigned*>(a.live) = live;
+    famLaneParams(a, l, done);
     if (l < a.L) a.flags[l] = (done ? 1 : 0) | 2;
 }
 
@@ -639,12 +671,14 @@ __global__ void __launch_bounds__(32 * kCtlWarps) famPowerFinish2(FamArgs a) {
 // Step size from the spectral-norm estimate (0.998 / ||A_l||_2, pdlp.cpp:796-800).
 __global__ void famInitStep(FamArgs a) {
     const int l = threadIdx.x;
-    if (l >= a.L) return;
-    DevState& s = a.st[l];
-    const double step = 0.998 / sqrt(fmax(a.ps[l].s2, 1e-12));
-    s.step = step;
-    s.tau_fac = static_cast<float>(step / s.pw);
-    s.sig_fac = static_cast<float>(step * s.pw);
+    if (l < a.L) {
+        DevState& s = a.st[l];
+        const double step = 0.998 / sqrt(fmax(a.ps[l].s2, 1e-12));
+        s.step = step;
+        s.tau_fac = static_cast<float>(step / s.pw);
+        s.sig_fac = static_cast<float>(step * s.pw);
+    }
+    famLaneParams(a, l, l >= a.L || a.st[l].done);
 }
 
 // ---------------------------------------------------------------------------
@@ -656,7 +690,7 @@ struct FamPack {
     int L = 0, n = 0, mb = 0, K = 0;
     int64_t Zb = 0, Zk = 0;
     std::vector<int> qfirst;  // first appended row of each lane
-    size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane, o_kfirst, o_live;
+    size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane, o_kfirst, o_live, o_lanes;
     size_t o_ktptr, o_ktrow, o_ktlane, o_ktval, o_cp, o_cs, o_rp, o_rs, o_st, o_dc, o_ps, o_pix;
     size_t image_end;
     size_t o_xc, o_xi, o_xh, o_xs, o_yc, o_yi, o_yh, o_ys;
@@ -702,6 +736,7 @@ struct FamPack {
         o_klane = take(4 * static_cast<size_t>(K));
         o_kfirst = take(4 * (kFam + 1));
         o_live = take(4);
+        o_lanes = take(sizeof(FamLane));
         o_ktptr = take(4 * (static_cast<size_t>(n) + 1));
         o_ktrow = take(4 * static_cast<size_t>(Zk));
         o_ktlane = take(4 * static_cast<size_t>(Zk));
@@ -940,6 +975,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         a.k_lane = Pi(fp.o_klane);
         a.k_first = Pi(fp.o_kfirst);
         a.live = reinterpret_cast<const unsigned*>(d + fp.o_live);
+        a.lanes = reinterpret_cast<FamLane*>(d + fp.o_lanes);
         a.kt_ptr = Pi(fp.o_ktptr);
         a.kt_row = Pi(fp.o_ktrow);
         a.kt_lane = Pi(fp.o_ktlane);
