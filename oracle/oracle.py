@@ -24,8 +24,9 @@ _libs: dict = {}
 
 
 def build(ref: bool = True) -> None:
-    """Compile the oracle (and, when the reference tree exists, the reference shim)."""
-    targets = ["liboracle_pdlp.so"] + (["ref"] if ref else [])
+    """Compile the oracle (and, when the reference tree exists, the reference's
+    CPU and FP64 GPU PDLP behind the shim)."""
+    targets = ["liboracle_pdlp.so"] + (["ref", "ref_gpu"] if ref else [])
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 

@@ -389,3 +389,22 @@ def test_anderson_window_limit():
     s.load(F.medium_lp())
     with pytest.raises(PdlpxError):
         s.solve()
+
+
+@pytest.mark.skipif(not O.REF_GPU_LIB.exists(), reason="reference GPU build not present (built where its sources exist)")
+def test_engine_fp64_matches_reference_gpu_path():
+    """The reference's own FP64 GPU PDLP (cuSPARSE path of pdlp.cpp:1739-2792,
+    compiled from its sources) and the engine's FP64 mode on the same LP: same
+    status, objectives within 2 tol (1 + |obj|) of each other and of the
+    reference's CPU golden value."""
+    name = "rand_2000x5000"  # above the reference's GPU thresholds (512 rows, 10k nonzeros)
+    e = GC.INDEX[name]
+    lp = GC.problem(name)
+    o = GC.options(name, precision=Precision.FP64)
+    o.use_gpu = True
+    ref, _, _ = O.ref_solve(lp, o, gpu=True)
+    r, _ = solve(lp, o)
+    assert int(ref.status) == int(r.status) == e["status"] == Status.Optimal
+    tol = e["options"]["optimality_tol"]
+    assert abs(r.objective - ref.objective) <= 2 * tol * (1 + abs(ref.objective)), (r.objective, ref.objective)
+    assert abs(ref.objective - e["objective"]) <= 2 * tol * (1 + abs(e["objective"]))
