@@ -263,7 +263,8 @@ typedef struct pdlpx_server_config {
     double budget_bytes;   /* device bytes of the packs in flight; 0 = 85% of free memory */
     int32_t max_packs;     /* packs solved at the same time (streams), default 4 */
     int32_t max_pack_lps;  /* LPs per pack, default 32 */
-    int32_t prep_threads;  /* host threads copying and scaling submitted LPs, 0 = half the cores */
+    int32_t prep_threads;  /* host threads scaling submitted LPs, 0 = all cores but one (pack threads
+                              sleep while their restart cycles run) */
     int32_t queue_limit;   /* unfinished requests before submit returns PDLPX_E_BUSY, default 100000 */
     int32_t batch_window_ms; /* a pack starts when max_pack_lps requests are ready or the oldest ready
                                 request has waited this long (default 50; 0 = start at once) */

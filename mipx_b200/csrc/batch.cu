@@ -630,6 +630,23 @@ void parallelFor(int count, F&& f) {
         default: { constexpr int UU = kSellU[2]; CALL; } break;      \
     }
 
+// Host wait for the work queued on a stream, sleeping instead of spinning: a
+// restart cycle runs for milliseconds, and the host cores are wanted by the
+// request server's preparation threads meanwhile.
+struct SleepWait {
+    cudaEvent_t ev = nullptr;
+    ~SleepWait() {
+        if (ev) cudaEventDestroy(ev);
+    }
+    cudaError_t wait(cudaStream_t s) {
+        cudaError_t e = cudaSuccess;
+        if (!ev) e = cudaEventCreateWithFlags(&ev, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev);
+        return e;
+    }
+};
+
 // One launch of a step / check kernel: the tiles of one shape class, all of them
 // (list0 < 0: tiles [tile0, tile0 + count) from row `base`) or `count` live ones
 // listed from list0.
@@ -1431,6 +1448,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
         if (rc != PDLPX_OK) return rc;
     }
+    SleepWait sleeper;
     std::vector<char> keep(L, 1), collected(L, 0);
     std::vector<int> cl, rl;
     int cycles = 0, ncollected = 0;
@@ -1439,6 +1457,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         PDLPX_BCK(cudaGraphLaunch(pk.cycle, s));
         launches += pk.cycle_launches;
         ++cycles;
+        PDLPX_BCK(sleeper.wait(s));
         PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
         int done_count = 0, fp64 = 0, live_tiles = 0;

@@ -1100,6 +1100,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         int32_t rc = capture(fp.cycle, fp.cycle_launches, false);
         if (rc != PDLPX_OK) return rc;
     }
+    SleepWait sleeper;
     std::vector<char> collected(L, 0);
     int ncollected = 0, cycles = 0;
     auto collect = [&](int l, bool out_of_time, double secs, double dev_s) -> int32_t {
@@ -1127,6 +1128,7 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         PDLPX_BCK(cudaGraphLaunch(fp.cycle, s));
         launches += fp.cycle_launches;
         ++cycles;
+        PDLPX_BCK(sleeper.wait(s));
         PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
         int done_count = 0;

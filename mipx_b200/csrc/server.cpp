@@ -132,7 +132,7 @@ public:
     void start() {
         const int prep = cfg_.prep_threads > 0
                              ? cfg_.prep_threads
-                             : std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / 2);
+                             : std::max(1, static_cast<int>(std::thread::hardware_concurrency()) - 1);
         for (int k = 0; k < prep; ++k) prep_threads_.emplace_back([this] { prepLoop(); });
         dispatcher_ = std::thread([this] { dispatchLoop(); });
     }
