@@ -64,6 +64,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the 512-LP batched workload")
     p.add_argument("--batch-lps", type=int, default=512)
     p.add_argument("--no-serving", action="store_true", help="skip the node-LP serving workload")
+    p.add_argument("--no-large", action="store_true", help="skip the 500k x 2M power-law LP")
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--profile", type=int, default=0, metavar="ITERS",
                    help="profiling run: one solve of the workload capped at ITERS iterations, no JSON line")
@@ -340,6 +341,36 @@ def serving_workload(local, requests=64, rate=500.0, single_sample=4) -> dict:
             "speedup_vs_single_lp_fp64": lps / (single_sample / single), "solve_seconds_max": span}
 
 
+def large_workload(local) -> dict:
+    """The large single LP: 500,000 x 2,000,000, column lengths power-law (2 to
+    2,000, mean 10, ~20M nonzeros), values N(0,1) with 1% of the rows scaled by
+    1e3, seed 11; one mixed-precision solve to 1e-6 relative KKT with the LP
+    resident (device time), and the step kernels' bandwidth from their
+    algorithmic bytes (16 nnz + 40 (m + n) per iteration in mixed mode)."""
+    from mipx_b200 import generators as G
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver
+    lp, _ = G.powerlaw_lp(500_000, 2_000_000, 2, 2000, 10.0, 0.01, 1e3, 11)
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.matrix.numNonzeros()
+    s = PdlpSolver()
+    s.setOptions(PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local,
+                             max_solve_seconds=120.0))
+    t0 = time.perf_counter()
+    s.load(lp)
+    r = s.solve()
+    wall = time.perf_counter() - t0
+    kt = s.timeKernels(10)
+    bp = 4 * (n + 1) + 8 * nnz + 8 * m + 40 * n
+    bd = 4 * (m + 1) + 8 * nnz + 4 * n + 36 * m
+    return {"workload": f"power-law LP {m} x {n}, {nnz} nonzeros (column lengths 2-2000, mean 10; 1% of rows x1e3), "
+                        "to 1e-6 rel KKT, mixed precision",
+            "status": int(r.status), "iterations": r.iterations, "fp64_iterations": r.fp64_iterations,
+            "device_s": r.device_seconds, "wall_s": wall, "iters_per_sec": r.iterations / r.device_seconds,
+            "rel_primal": r.rel_primal_resid, "rel_dual": r.rel_dual_resid, "rel_gap": r.rel_gap,
+            "objective": r.objective,
+            "primal_step_GBps": bp / (kt["primal_ms"] * 1e-3) / 1e9,
+            "dual_step_GBps": bd / (kt["dual_ms"] * 1e-3) / 1e9}
+
+
 def run_reference(args, rank, pg):
     if rank != 0:
         return
@@ -450,6 +481,12 @@ def main():
 
     batch = None if args.no_batch else batch_workload(rank, world, local, args.batch_lps)
     serving = None if args.no_serving else serving_workload(local)
+    large = None
+    if not args.no_large:
+        try:
+            large = large_workload(local)
+        except Exception as exc:  # a report beside the headline, never a reason to lose the line
+            large = {"error": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -490,6 +527,7 @@ def main():
             "cpu_baseline": cpu,
             "batch": batch,
             "serving": serving,
+            "large": large,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
