@@ -353,8 +353,9 @@ typedef struct pdlpx_gen_lp {
     double* col_ub;
     double* row_lb;
     double* row_ub;
-    double* x0;        /* feasible point used by the construction (length n) */
+    double* x0;        /* feasible point used by the construction (length n), NULL from pdlpx_read_mps */
     int32_t* is_int;   /* integrality marks (length n) or NULL */
+    double obj_offset; /* objective constant (0 for the generators) */
 } pdlpx_gen_lp;
 
 /* Random sparse LP: columns with U{nnz_lo..nnz_hi} nonzeros at uniform rows,
@@ -370,6 +371,16 @@ int32_t pdlpx_gen_transport(int32_t s, int32_t d, uint64_t seed, pdlpx_gen_lp* o
 int32_t pdlpx_gen_powerlaw(int32_t m, int32_t n, int32_t kmin, int32_t kmax, double kmean,
                            double big_frac, double big_scale, uint64_t seed, pdlpx_gen_lp* out);
 void pdlpx_free_lp(pdlpx_gen_lp* lp);
+
+/* Read an LP from a free-format MPS file, plain or gzip-compressed, with the
+ * meaning mipx's reader gives every section (readMps, src/io/mps_reader.cpp:432-813):
+ * N/L/G/E rows, integer markers, objective constant = -(RHS of the objective
+ * row), RANGES, bounds LO/UP/FX/FR/MI/PL/BV/LI/UI/SC/SI, columns defaulting to
+ * [0, +inf), minimisation; rows' entries sorted, duplicates summed, zeros
+ * dropped.  Output allocated by the library (release with pdlpx_free_lp);
+ * is_int marks integer columns (the LP ignores them).  Errors: PDLPX_E_INVALID
+ * with the file position in pdlpx_last_error(NULL). */
+int32_t pdlpx_read_mps(const char* path, pdlpx_gen_lp* out);
 
 #ifdef __cplusplus
 }

@@ -62,7 +62,7 @@ class GenLp(C.Structure):
     _fields_ = [
         ("m", i32), ("n", i32), ("nnz", i32), ("row_ptr", P_i32), ("col_idx", P_i32), ("val", P_f64),
         ("obj", P_f64), ("col_lb", P_f64), ("col_ub", P_f64), ("row_lb", P_f64), ("row_ub", P_f64),
-        ("x0", P_f64), ("is_int", P_i32),
+        ("x0", P_f64), ("is_int", P_i32), ("obj_offset", f64),
     ]
 
 
@@ -128,6 +128,7 @@ SIGNATURES = [
     ("pdlpx_gen_transport", i32, [i32, i32, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_gen_powerlaw", i32, [i32, i32, i32, i32, f64, f64, f64, C.c_uint64, C.POINTER(GenLp)]),
     ("pdlpx_free_lp", None, [C.POINTER(GenLp)]),
+    ("pdlpx_read_mps", i32, [C.c_char_p, C.POINTER(GenLp)]),
 ]
 
 _lib = None

@@ -22,7 +22,8 @@ BUILD = PKG / "_build"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libpdlpx.so"
 
-SOURCES = ["engine.cu", "batch.cu", "residual.cu", "problem.cpp", "capi.cpp", "server.cpp", "generators.cpp"]
+SOURCES = ["engine.cu", "batch.cu", "residual.cu", "problem.cpp", "capi.cpp", "server.cpp", "generators.cpp", "mps.cpp"]
+CLI = LIBDIR / "pdlpx_cli"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,10 +41,10 @@ def _deps() -> list[Path]:
 
 
 def up_to_date() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not CLI.exists():
         return False
-    t = LIB.stat().st_mtime
-    return all(p.stat().st_mtime <= t for p in _deps())
+    t = min(LIB.stat().st_mtime, CLI.stat().st_mtime)
+    return all(p.stat().st_mtime <= t for p in _deps() + [CSRC / "cli.cpp", ROOT / "include" / "pdlpx.hpp"])
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
@@ -73,11 +74,21 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(compile_one, srcs))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [cc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+    cmd = [cc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lrt", "-lpthread", "-ldl",
+           "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    # command-line front end (mipx's `--pdlp` LP mode and its summary lines) over the library
+    cxx = shutil.which("g++") or "g++"
+    tmp = CLI.with_suffix(".tmp")
+    cmd = [cxx, "-std=c++20", "-O2", "-I", str(ROOT / "include"), str(CSRC / "cli.cpp"), "-o", str(tmp),
+           "-L", str(LIBDIR), "-lpdlpx", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"cli build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, CLI)
     return LIB
 
 

@@ -445,6 +445,32 @@ def batch_solve(problems: Sequence[LpProblem], options: PdlpOptions, warm: Seque
     return [(LpResult.from_c(res[k]), xs[k], ys[k]) for k in range(len(problems))]
 
 
+def read_mps(path) -> LpProblem:
+    """Read a free-format MPS file (plain or .gz) as mipx's ``readMps`` does
+    (src/io/mps_reader.cpp:432-813) through the engine library's reader."""
+    lib = _capi.load()
+    g = _capi.GenLp()
+    rc = lib.pdlpx_read_mps(str(path).encode(), C.byref(g))
+    if rc != 0:
+        raise _capi.PdlpxError(rc, f"{lib.pdlpx_error_string(rc).decode()}: {lib.pdlpx_last_error(None).decode()}")
+    try:
+        m, n, nnz = g.m, g.n, g.nnz
+        arr = lambda p, k, dt: (np.ctypeslib.as_array(p, shape=(k,)).astype(dt, copy=True) if k > 0
+                                else np.zeros(0, dt))
+        rp = arr(g.row_ptr, m + 1, np.int32)
+        lp = LpProblem(
+            name=str(path), sense=Sense.Minimize, num_cols=n, num_rows=m,
+            obj=arr(g.obj, n, np.float64), col_lower=arr(g.col_lb, n, np.float64),
+            col_upper=arr(g.col_ub, n, np.float64), row_lower=arr(g.row_lb, m, np.float64),
+            row_upper=arr(g.row_ub, m, np.float64), obj_offset=float(g.obj_offset),
+            matrix=SparseMatrix(m, n, values=arr(g.val, nnz, np.float64), col_indices=arr(g.col_idx, nnz, np.int32),
+                                row_starts=rp),
+            col_type=["I" if k else "C" for k in arr(g.is_int, n, np.int32)])
+    finally:
+        lib.pdlpx_free_lp(C.byref(g))
+    return lp
+
+
 class Server:
     """LP solves as they arrive (``pdlpx_server_*``): submitted LPs are packed
     with whatever else is waiting and solved several packs at a time on the
