@@ -3,9 +3,12 @@
 //                            loaded, LPs without rows: closed form on the host)
 //   pdlpx_api_test gpu    -- solves on the device
 // Prints one line per check; exits non-zero on the first failure.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "pdlpx.hpp"
@@ -80,6 +83,64 @@ static int host() {
     return fails;
 }
 
+// The concurrent-root race of mipx (mip_solver.cpp:4470-4605): arms on their
+// own threads and solvers share one stop flag; the first arm to finish sets it
+// and the other returns IterLimit at its next check (or finishes first).
+static int race() {
+    LpProblem lp;  // a 300-row random-like LP: sum_j x_j <= 10 + i per row, max sum x
+    lp.num_cols = 600;
+    lp.num_rows = 300;
+    lp.obj.assign(600, -1.0);
+    lp.col_lower.assign(600, 0.0);
+    lp.col_upper.assign(600, 5.0);
+    lp.row_lower.assign(300, -kInf);
+    lp.row_starts = {0};
+    for (int i = 0; i < 300; ++i) {
+        lp.row_upper.push_back(10.0 + i);
+        for (int k = 0; k < 7; ++k) {
+            lp.col_indices.push_back((i * 7 + k * 97) % 600);
+            lp.values.push_back(1.0 + 0.1 * k);
+        }
+        std::vector<int32_t> row(lp.col_indices.end() - 7, lp.col_indices.end());
+        std::vector<double> val(lp.values.end() - 7, lp.values.end());
+        // columns sorted and distinct within the row
+        std::vector<std::pair<int32_t, double>> e;
+        for (int k = 0; k < 7; ++k) e.emplace_back(row[k], val[k]);
+        std::sort(e.begin(), e.end());
+        for (int k = 0; k < 7; ++k) {
+            lp.col_indices[lp.col_indices.size() - 7 + k] = e[k].first;
+            lp.values[lp.values.size() - 7 + k] = e[k].second;
+        }
+        lp.row_starts.push_back(static_cast<int32_t>(lp.values.size()));
+    }
+    int32_t stop = 0;
+    pdlpx::LpResult res[2];
+    std::atomic<int> first{-1};
+    auto arm = [&](int k) {
+        PdlpSolver s;
+        pdlpx::PdlpOptions o;
+        o.verbose = 0;
+        o.max_iter = 200000;
+        o.precision = k == 0 ? PDLPX_PREC_MIXED : PDLPX_PREC_FP64;
+        o.primal_tol = o.dual_tol = o.optimality_tol = k == 0 ? 1e-4 : 1e-9;  // arm 1 needs far longer
+        s.setOptions(o);
+        s.setStopFlag(&stop);
+        s.load(lp);
+        res[k] = s.solve();
+        int expected = -1;
+        if (first.compare_exchange_strong(expected, k)) __atomic_store_n(&stop, 1, __ATOMIC_SEQ_CST);
+    };
+    std::thread a(arm, 0), b(arm, 1);
+    a.join();
+    b.join();
+    const int w = first.load(), l = 1 - w;
+    CHECK(res[w].status == Status::Optimal);
+    CHECK(res[l].status == Status::IterLimit || res[l].status == Status::Optimal);
+    std::printf("race: arm %d won, the other ended %d after %d iterations\n", w, static_cast<int>(res[l].status),
+                res[l].iterations);
+    return 0;
+}
+
 static int gpu() {
     PdlpSolver s;
     pdlpx::PdlpOptions o;
@@ -111,7 +172,7 @@ static int gpu() {
     s.setColBounds(1, 0.0, 2.0);  // y <= 2: max becomes 3
     r = s.solve();
     CHECK(r.status == Status::Optimal && std::fabs(r.objective - 3.0) <= 1e-4);
-    return fails;
+    return race() + fails;
 }
 
 int main(int argc, char** argv) {
