@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libpdlpx.so"
 
-SOURCES = ["engine.cu", "batch.cu", "residual.cu", "problem.cpp", "capi.cpp", "server.cpp", "generators.cpp", "mps.cpp"]
+SOURCES = ["engine.cu", "batch.cu", "residual.cu", "problem.cpp", "capi.cpp", "server.cpp", "generators.cpp", "mps.cpp", "scaling.cu"]
 CLI = LIBDIR / "pdlpx_cli"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

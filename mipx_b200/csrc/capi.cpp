@@ -101,6 +101,7 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->batch_pack_mb = 0;
     o->batch_compact = 1;
     o->batch_sell = 1;
+    o->scale_on_device = -1;
 }
 
 const char* pdlpx_error_string(int32_t code) {

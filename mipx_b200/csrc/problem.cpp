@@ -94,7 +94,7 @@ void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<do
     }
 }
 
-void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s) {
+void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const RuizFn& ruiz) {
     const int32_t m = lp.m, n = lp.n;
     s.obj_sign = lp.maximize ? -1.0 : 1.0;
     s.c.resize(static_cast<size_t>(n));
@@ -128,7 +128,7 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s) {
     }
 
     // Ruiz: alternate row and column infinity-norm equilibration, scale 1/sqrt(max).
-    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0) {
+    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0 && !(ruiz && ruiz(a, s.row_scale, s.col_scale, o.ruiz_iterations))) {
         std::vector<double> cmax(static_cast<size_t>(n));
         for (int32_t pass = 0; pass < o.ruiz_iterations; ++pass) {
             for (int32_t i = 0; i < m; ++i) {

@@ -11,6 +11,8 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
+#include <string>
 #include <vector>
 
 #include "pdlpx.h"
@@ -57,7 +59,16 @@ bool canonicalCsr(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const in
 
 void transposeCsr(const Csr& a, Csr& at);
 
-void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s);
+// Ruiz equilibration done elsewhere (the device): scales the matrix values and
+// multiplies the factors into row_scale / col_scale exactly as the host loop
+// would; returns false to leave the work to the host loop.
+using RuizFn = std::function<bool(Csr& a, std::vector<double>& row_scale, std::vector<double>& col_scale, int passes)>;
+
+void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const RuizFn& ruiz = {});
+
+// Ruiz passes on `device` (scaling.cu); bit-identical to the host loop.
+bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& col_scale, int passes, int device,
+                  std::string& err);
 
 // Recompute sigma/tau from the scaled matrix (pdlp.cpp:713-742).
 void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<double>& tau);

@@ -131,6 +131,7 @@ class PdlpOptions:
     batch_pack_mb: int = 0
     batch_compact: bool = True
     batch_sell: bool = True
+    scale_on_device: int = -1
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()

@@ -38,7 +38,8 @@ def quiet(**kw) -> PdlpOptions:
 TIGHT = dict(primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
 # Launch-shape and batching knobs of the device engine: no meaning for the
 # reference, left at their defaults when the cases are replayed.
-ENGINE_ONLY = {"autotune", "shape_primal", "shape_dual", "batch_pack_mb", "batch_compact", "batch_sell"}
+ENGINE_ONLY = {"autotune", "shape_primal", "shape_dual", "batch_pack_mb", "batch_compact", "batch_sell",
+               "scale_on_device"}
 
 CASES = {
     # name: (problem builder, options) -- options follow the mipx test that uses the LP

@@ -34,7 +34,7 @@ def test_defaults_match_reference_options():
     ref = PdlpOptions()  # field defaults of include/mipx/pdlp.h:19-87
     for name, _ in _capi.Options._fields_:
         if name in ("reserved", "precision", "device", "fp64_switch", "spmv_group_a", "spmv_group_at", "autotune", "shape_primal",
-                    "shape_dual", "batch_pack_mb", "batch_compact", "batch_sell"):
+                    "shape_dual", "batch_pack_mb", "batch_compact", "batch_sell", "scale_on_device"):
             continue
         assert getattr(o, name) == pytest.approx(float(getattr(ref, name))), name
 

@@ -408,3 +408,22 @@ def test_engine_fp64_matches_reference_gpu_path():
     tol = e["options"]["optimality_tol"]
     assert abs(r.objective - ref.objective) <= 2 * tol * (1 + abs(ref.objective)), (r.objective, ref.objective)
     assert abs(ref.objective - e["objective"]) <= 2 * tol * (1 + abs(e["objective"]))
+
+
+@pytest.mark.parametrize("make", [lambda: G.random_lp(2000, 5000, 4, 12, 1)[0], lambda: G.transport_lp(300, 400, 3)[0],
+                                  lambda: G.powerlaw_lp(20000, 80000, 2, 2000, 10.0, 0.01, 1e3, 11)[0]])
+def test_device_ruiz_bit_identical_to_host(make):
+    """Ruiz passes on the device (scale_on_device=1) give the host pipeline's
+    scaled problem bit for bit, so the solve that follows is identical too."""
+    lp = make()
+    out = []
+    for mode in (0, 1):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, max_iter=3000, scale_on_device=mode))
+        s.load(lp)
+        out.append((s.scaling(), s.solve(), s.getPrimalValues()))
+    (sa, ra, xa), (sb, rb, xb) = out
+    for k in sa:
+        np.testing.assert_array_equal(np.asarray(sa[k]), np.asarray(sb[k]), err_msg=k)
+    assert (ra.status, ra.iterations, ra.objective) == (rb.status, rb.iterations, rb.objective)
+    np.testing.assert_array_equal(xa, xb)
