@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <thread>
 
 namespace pdlpx {
 
@@ -57,21 +58,82 @@ bool canonicalCsr(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const in
     return true;
 }
 
+namespace {
+
+// Host threads for the O(nnz) passes of large LPs (1 below 1M entries).
+int hostThreads(size_t work) {
+    if (work < (1u << 20)) return 1;
+    return static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+}
+
+template <class F>
+void forBlocks(int nt, int64_t count, F&& f) {  // f(t, begin, end) over nt contiguous blocks
+    if (nt <= 1) {
+        f(0, int64_t{0}, count);
+        return;
+    }
+    std::vector<std::thread> ts;
+    for (int t = 0; t < nt; ++t)
+        ts.emplace_back([&, t] { f(t, count * t / nt, count * (t + 1) / nt); });
+    for (auto& th : ts) th.join();
+}
+
+}  // namespace
+
+// Counting transpose.  With T threads each takes a contiguous block of rows,
+// counts its entries per column, and scatters them after the entries of the
+// blocks before it, so every A^T row keeps ascending row order -- the output
+// does not depend on T.
 void transposeCsr(const Csr& a, Csr& at) {
     at.rows = a.cols;
     at.cols = a.rows;
-    at.ptr.assign(static_cast<size_t>(a.cols) + 1, 0);
+    const int32_t n = a.cols;
+    at.ptr.assign(static_cast<size_t>(n) + 1, 0);
     at.idx.resize(a.idx.size());
     at.val.resize(a.val.size());
-    for (int32_t c : a.idx) ++at.ptr[c + 1];
-    for (int32_t j = 0; j < a.cols; ++j) at.ptr[j + 1] += at.ptr[j];
-    std::vector<int32_t> cur(at.ptr.begin(), at.ptr.end() - 1);
-    for (int32_t i = 0; i < a.rows; ++i)
-        for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
-            const int32_t p = cur[a.idx[k]]++;
-            at.idx[p] = i;
-            at.val[p] = a.val[k];
+    const int nt = std::min<int64_t>(hostThreads(a.idx.size()), std::max<int32_t>(1, a.rows));
+    if (nt <= 1) {
+        for (int32_t c : a.idx) ++at.ptr[c + 1];
+        for (int32_t j = 0; j < n; ++j) at.ptr[j + 1] += at.ptr[j];
+        std::vector<int32_t> cur(at.ptr.begin(), at.ptr.end() - 1);
+        for (int32_t i = 0; i < a.rows; ++i)
+            for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                const int32_t p = cur[a.idx[k]]++;
+                at.idx[p] = i;
+                at.val[p] = a.val[k];
+            }
+        return;
+    }
+    std::vector<std::vector<int32_t>> cnt(nt, std::vector<int32_t>(static_cast<size_t>(n), 0));
+    forBlocks(nt, a.rows, [&](int t, int64_t r0, int64_t r1) {
+        std::vector<int32_t>& c = cnt[t];
+        for (int64_t k = a.ptr[r0]; k < a.ptr[r1]; ++k) ++c[a.idx[k]];
+    });
+    // column starts, then each block's first slot inside every column
+    for (int32_t j = 0; j < n; ++j) {
+        int32_t tot = 0;
+        for (int t = 0; t < nt; ++t) tot += cnt[t][j];
+        at.ptr[j + 1] = at.ptr[j] + tot;
+    }
+    forBlocks(nt, n, [&](int, int64_t j0, int64_t j1) {
+        for (int64_t j = j0; j < j1; ++j) {
+            int32_t pos = at.ptr[j];
+            for (int t = 0; t < nt; ++t) {
+                const int32_t c = cnt[t][j];
+                cnt[t][j] = pos;
+                pos += c;
+            }
         }
+    });
+    forBlocks(nt, a.rows, [&](int t, int64_t r0, int64_t r1) {
+        std::vector<int32_t>& cur = cnt[t];
+        for (int64_t i = r0; i < r1; ++i)
+            for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                const int32_t p = cur[a.idx[k]]++;
+                at.idx[p] = static_cast<int32_t>(i);
+                at.val[p] = a.val[k];
+            }
+    });
 }
 
 void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<double>& tau) {
@@ -82,16 +144,21 @@ void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<do
     const Csr& at = s.at;
     sigma.assign(static_cast<size_t>(a.rows), 1.0);
     tau.assign(static_cast<size_t>(a.cols), 1.0);
-    for (int32_t i = 0; i < a.rows; ++i) {
-        double acc = 0.0;
-        for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) acc += a.val[k] * a.val[k];
-        sigma[i] = 1.0 / std::max(std::sqrt(acc), 1e-8);
-    }
-    for (int32_t j = 0; j < at.rows; ++j) {
-        double acc = 0.0;
-        for (int32_t k = at.ptr[j]; k < at.ptr[j + 1]; ++k) acc += at.val[k] * at.val[k];
-        tau[j] = 1.0 / std::max(std::sqrt(acc), 1e-8);
-    }
+    const int nt = hostThreads(a.idx.size());  // rows are independent: any split gives the same sums
+    forBlocks(nt, a.rows, [&](int, int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
+            double acc = 0.0;
+            for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) acc += a.val[k] * a.val[k];
+            sigma[i] = 1.0 / std::max(std::sqrt(acc), 1e-8);
+        }
+    });
+    forBlocks(nt, at.rows, [&](int, int64_t j0, int64_t j1) {
+        for (int64_t j = j0; j < j1; ++j) {
+            double acc = 0.0;
+            for (int32_t k = at.ptr[j]; k < at.ptr[j + 1]; ++k) acc += at.val[k] * at.val[k];
+            tau[j] = 1.0 / std::max(std::sqrt(acc), 1e-8);
+        }
+    });
 }
 
 void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const RuizFn& ruiz) {

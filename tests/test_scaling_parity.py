@@ -21,6 +21,9 @@ CASES = [
     ("rand", lambda: G.random_lp(300, 700, 4, 12, 9)[0], {}),
     ("transport", lambda: G.transport_lp(30, 40, 3)[0], {}),
     ("powerlaw", lambda: G.powerlaw_lp(400, 1500, 2, 200, 10.0, 0.01, 1e3, 4)[0], {}),
+    # above 1M entries: multithreaded transpose and Pock-Chambolle norms (and the
+    # device Ruiz passes where a GPU is present)
+    ("powerlaw_large", lambda: G.powerlaw_lp(60000, 240000, 2, 2000, 10.0, 0.01, 1e3, 4)[0], {}),
 ]
 
 
