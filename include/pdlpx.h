@@ -115,7 +115,9 @@ typedef struct pdlpx_options {
     int32_t spmv_group_a;             /* 0 = autotune; else threads per row of A (1,2,4,8,16,32) */
     int32_t spmv_group_at;            /* 0 = autotune; else threads per row of A^T */
     int32_t autotune;                 /* 1: time the step kernels' launch shapes on LPs with >= 100k
-                                         nonzeros and keep the fastest; 0 (default): row-length table,
+                                         nonzeros and keep the fastest; in pdlpx_batch_solve and the
+                                         server, time each sliced-ELL class's entries-per-round variants
+                                         on the pack (identical results); 0 (default): row-length table,
                                          deterministic */
     int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step */
     int32_t shape_dual;               /* 0 = automatic; k > 0 pins launch shape k-1 of the dual step */

@@ -650,8 +650,13 @@ struct SleepWait {
 // One launch of a step / check kernel: the tiles of one shape class, all of them
 // (list0 < 0: tiles [tile0, tile0 + count) from row `base`) or `count` live ones
 // listed from list0.
+// `kern` is the shape whose kernel runs the class: the class's own shape, or
+// for a sliced-ELL class the entries-per-round variant the pack's autotuner
+// picked (all variants read the same slices and sum every row in entry order).
 struct Launch {
     int shape, tile0, base, count, list0;
+    int kern = -1;
+    int k() const { return kern >= 0 ? kern : shape; }
 };
 
 // Shapes in placement order: sliced-ELL classes first (their rows start at 0
@@ -939,7 +944,7 @@ struct Pack {
                     for (int k = 0; k < count; ++k) out.push_back(first + k);
                 }
                 const int count = static_cast<int>(out.size()) - list0;
-                if (count > 0) (side == 0 ? lc : lr).push_back(Launch{c.shape, c.tile0, c.base, count, list0});
+                if (count > 0) (side == 0 ? lc : lr).push_back(Launch{c.shape, c.tile0, c.base, count, list0, c.kern});
             }
         }
         listed = true;
@@ -951,9 +956,9 @@ struct Pack {
         const PackArgs& a = args;
         if (isSell(c.shape)) {
             if (listed) {
-                PDLPX_SELL_SWITCH(c.shape, (packPrimalSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+                PDLPX_SELL_SWITCH(c.k(), (packPrimalSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
             } else {
-                PDLPX_SELL_SWITCH(c.shape, (packPrimalSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+                PDLPX_SELL_SWITCH(c.k(), (packPrimalSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
             }
         } else if (listed) {
             PDLPX_SHAPE_SWITCH(c.shape, (packPrimal<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
@@ -966,9 +971,9 @@ struct Pack {
         const PackArgs& a = args;
         if (isSell(c.shape)) {
             if (listed) {
-                PDLPX_SELL_SWITCH(c.shape, (packDualSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
+                PDLPX_SELL_SWITCH(c.k(), (packDualSell<UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
             } else {
-                PDLPX_SELL_SWITCH(c.shape, (packDualSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
+                PDLPX_SELL_SWITCH(c.k(), (packDualSell<UU, false><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, 0, k)));
             }
         } else if (listed) {
             PDLPX_SHAPE_SWITCH(c.shape, (packDual<GG, RR, UU, true><<<c.count, kBlock, 0, s>>>(a, c.tile0, c.base, c.list0, k)));
@@ -1034,8 +1039,6 @@ struct Pack {
     }
 };
 
-// Host image of one LP's share of the pack, in the pack numbering (renumbered
-// sides, padded rows and columns included).
 // Controller constants and initial solver state of one LP (as the single-LP
 // solve sets them up); nb_rows / nb_cols are its partial counts.
 void lpState(const Item& it, const pdlpx_options& o, bool mixed, int nb_rows, int nb_cols, DevConst& dc, DevState& st) {
@@ -1087,6 +1090,8 @@ void lpState(const Item& it, const pdlpx_options& o, bool mixed, int nb_rows, in
     st.switch_total = -1;
 }
 
+// Host image of one LP's share of the pack, in the pack numbering (renumbered
+// sides, padded rows and columns included).
 void stageItem(const Pack& pk, const Item& it, const pdlpx_options& o, char* img, char* iters) {
     const ScaledLp& sc = it.sc;
     const int32_t m = it.lp.m, n = it.lp.n;
@@ -1442,6 +1447,66 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
     packInitStep<<<(L + 127) / 128, 128, 0, s>>>(pk.args);
     ++launches;
     PDLPX_BCK(cudaGetLastError());
+
+    // ---- autotuner (option autotune): per sliced-ELL class and side, time
+    // three launches of each entries-per-round variant on the pack itself and
+    // keep the fastest (a variant must beat the table's pick by 3%).  The
+    // variants give identical results, so the choice never changes an LP's
+    // solution; the timing launches' writes to the iterates are undone by
+    // re-uploading the initial iterates.
+    if (o.autotune) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        PDLPX_BCK(cudaEventCreate(&e0));
+        PDLPX_BCK(cudaEventCreate(&e1));
+        struct EvPair {
+            cudaEvent_t a, b;
+            ~EvPair() {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } evp{e0, e1};
+        for (int side = 0; side < 2; ++side)
+            for (Launch& c : side == 0 ? pk.cls_c : pk.cls_r) {
+                if (!isSell(c.shape) || c.count == 0) continue;
+                float best = 0.0f;
+                int pick = c.shape;
+                for (int cand : {c.shape, kNumShapes + 0, kNumShapes + 1, kNumShapes + 2}) {
+                    if (cand == c.shape && best > 0.0f) continue;
+                    c.kern = cand;
+                    for (int r = 0; r < 4; ++r) {  // one warm-up, three timed
+                        if (r == 1) PDLPX_BCK(cudaEventRecord(e0, s));
+                        side == 0 ? pk.launchPrimal(c, 1) : pk.launchDual(c, 1);
+                    }
+                    PDLPX_BCK(cudaEventRecord(e1, s));
+                    PDLPX_BCK(cudaGetLastError());
+                    PDLPX_BCK(cudaEventSynchronize(e1));
+                    float ms = 0.0f;
+                    PDLPX_BCK(cudaEventElapsedTime(&ms, e0, e1));
+                    launches += 4;
+                    if (best == 0.0f || ms < 0.97f * best) {
+                        best = ms;
+                        pick = cand;
+                    }
+                }
+                c.kern = pick;
+            }
+        pk.lc = pk.cls_c;
+        pk.lr = pk.cls_r;
+        if (any_warm)
+            PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.image_end, iters.get(), pk.iter_end - pk.image_end,
+                                      cudaMemcpyHostToDevice, s));
+        else
+            PDLPX_BCK(cudaMemsetAsync(pk.d + pk.image_end, 0, pk.iter_end - pk.image_end, s));
+        if (o.verbose) {
+            for (int side = 0; side < 2; ++side)
+                for (const Launch& c : side == 0 ? pk.cls_c : pk.cls_r)
+                    if (isSell(c.shape) && c.count > 0)
+                        std::printf("PDLP batch autotune: %s sliced-ELL class U%d -> U%d (%d tiles)\n",
+                                    side == 0 ? "primal" : "dual", kSellU[c.shape - kNumShapes],
+                                    kSellU[c.k() - kNumShapes], c.count);
+            std::fflush(stdout);
+        }
+    }
 
     // ---- restart cycles; finished LPs are read back after the cycle that ends them
     {

@@ -165,3 +165,18 @@ def test_fixed_column_with_negative_reduced_cost_converges():
     (q, x, _), = batch_solve([lp], o)
     assert q.status == Status.Optimal and abs(q.objective + 2.5) <= 1e-5, q
     np.testing.assert_allclose(x, [1.0, 0.5], atol=1e-5)
+
+
+def test_autotuned_pack_gives_identical_results():
+    """The pack autotuner only picks how many sliced-ELL entries a thread loads
+    per round; every variant sums a row in entry order, so results are
+    bit-identical with and without it."""
+    sizes = G.batch_sizes(24, seed=13)
+    lps = [G.random_lp(m, n, 4, 12, 300 + k)[0] for k, (m, n) in enumerate(sizes)]
+    base = dict(verbose=False, primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
+    a = batch_solve(lps, PdlpOptions(**base))
+    b = batch_solve(lps, PdlpOptions(autotune=True, **base))
+    for (r, x, y), (q, u, v) in zip(a, b):
+        assert (r.status, r.iterations, r.objective) == (q.status, q.iterations, q.objective)
+        np.testing.assert_array_equal(x, u)
+        np.testing.assert_array_equal(y, v)
