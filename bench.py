@@ -79,7 +79,9 @@ def parse():
     return p.parse_args()
 
 
-def dist_init(n):
+def dist_init(n, backend=None):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK); NCCL on
+    GPUs, gloo where none is visible (the multi-rank host logic on CPU)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -89,37 +91,51 @@ def dist_init(n):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return rank, world, local, pg
 
 
-def max_over_ranks(pg, value: float) -> float:
+def _reduce(pg, value: float, op) -> float:
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(pg, value: float) -> float:
+    return _reduce(pg, value, pg.ReduceOp.MAX if pg is not None else None)
 
 
 def sum_over_ranks(pg, value: float) -> float:
-    if pg is None:
-        return value
-    import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(pg, value, pg.ReduceOp.SUM if pg is not None else None)
+
+
+def aggregate(pg, units: float, seconds: float) -> tuple[float, float]:
+    """Whole-job throughput of a weakly scaled run: the units every rank
+    processed over the slowest rank's time (max over ranks, never wall clock)."""
+    t = max_over_ranks(pg, seconds)
+    return sum_over_ranks(pg, units) / t, t
 
 
 def barrier(pg):
     import torch
-    torch.cuda.synchronize()
+    cuda = torch.cuda.is_available()
+    if cuda:
+        torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
-    torch.cuda.synchronize()
+    if cuda:
+        torch.cuda.synchronize()
 
 
 class ClockSampler:
@@ -448,9 +464,7 @@ def main():
             kkts.append(max(r.rel_primal_resid, r.rel_dual_resid, r.rel_gap))
         barrier(pg)
         wall = time.perf_counter() - t_wall
-    t_dev = max_over_ranks(pg, sum(dev_s))
-    total_iters = sum_over_ranks(pg, float(sum(iters)))
-    value = total_iters / t_dev
+    value, t_dev = aggregate(pg, float(sum(iters)), sum(dev_s))
     lps_per_sec = sum_over_ranks(pg, float(args.steps)) / t_dev
 
     # kernel timing for the roofline (dominant kernel: fused primal step)
