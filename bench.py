@@ -495,14 +495,15 @@ def main():
     e2e_t = max_over_ranks(pg, e2e_t)
     e2e_val = sum_over_ranks(pg, float(e2e_iters)) / e2e_t
 
-    batch = None if args.no_batch else batch_workload(rank, world, local, args.batch_lps)
-    serving = None if args.no_serving else serving_workload(local)
-    large = None
-    if not args.no_large:
+    def side_line(fn, *a):  # a report beside the headline, never a reason to lose the line
         try:
-            large = large_workload(local)
-        except Exception as exc:  # a report beside the headline, never a reason to lose the line
-            large = {"error": str(exc)}
+            return fn(*a)
+        except Exception as exc:
+            return {"error": str(exc)}
+
+    batch = None if args.no_batch else side_line(batch_workload, rank, world, local, args.batch_lps)
+    serving = None if args.no_serving else side_line(serving_workload, local)
+    large = None if args.no_large else side_line(large_workload, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
