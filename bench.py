@@ -517,7 +517,7 @@ def main():
     gold = ROOT / "tests" / "golden" / "ref_pdlp.json"
     if gold.exists():
         hi = json.loads(gold.read_text()).get(f"transport_{args.supplies}x{args.demands}", {}).get("highs_objective")
-    traffic = ncu_traffic("primalStep", "transport_1000x1000")
+    traffic = ncu_traffic("primalStep", f"transport_{args.supplies}x{args.demands}")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": args.steps,
