@@ -1,10 +1,10 @@
 // Family packs: node LPs that share the leading rows of one base matrix.
 //
 // Branch-and-bound node LPs of one base LP (bound changes on integer columns
-// and a few appended cut rows) have the same
-// constraint matrix in their first m_b rows.  A family pack stores those rows
-// once and runs up to 32 node LPs over them in the same sweep: one warp per
-// matrix row or column, one lane per LP.  The warp loads a row's entries once
+// and a few appended cut rows) have the same constraint matrix in their first
+// m_b rows.  A family pack stores those rows once and runs up to 32 node LPs
+// over them in the same sweep: one lane per LP, a warp per group of adjacent
+// rows or columns.  The warp loads a row's entries once
 // (coalesced, broadcast by shuffle) and every lane gathers its own LP's value
 // of each entry; per-LP vectors are interleaved [row or column][32 lanes], so
 // each gather of the warp is one 256-byte request instead of 32 scattered
