@@ -209,3 +209,21 @@ def test_cli_solves_mps_on_device(tmp_path):
     assert s["status"] == "Optimal" and int(res.status) == 0
     assert abs(s["objective"] - res.objective) <= 2e-6 * (1 + abs(res.objective))
     assert s["iterations"] > 0 and s["work"] > 0
+
+
+def test_mps_edge_rules(tmp_path):
+    """RANGES and RHS on the objective row, unknown rows in RHS / RANGES and a
+    bound on a column that only BOUNDS names: as mipx's reader treats them
+    (objective RHS sets the constant, objective ranges and unknown rows are
+    skipped, the new column gets cost 0 and the default lower bound)."""
+    p = tmp_path / "edge.mps"
+    p.write_text("NAME e\nROWS\n N obj\n E r\nCOLUMNS\n    x obj 1.0 r 1.0\nRHS\n    rhs obj 3.0 nosuch 9.0\n"
+                 "    rhs r 2.0\nRANGES\n    rng obj 5.0 nosuch 1.0\nBOUNDS\n UP bnd y 4.0\nENDATA\n")
+    lp = read_mps(p)
+    assert lp.obj_offset == -3.0
+    assert (lp.num_rows, lp.num_cols) == (1, 2)
+    np.testing.assert_array_equal(lp.obj, [1.0, 0.0])
+    np.testing.assert_array_equal(lp.col_lower, [0.0, 0.0])
+    np.testing.assert_array_equal(lp.col_upper, [INF, 4.0])
+    np.testing.assert_array_equal(lp.row_lower, [2.0])
+    np.testing.assert_array_equal(lp.row_upper, [2.0])
