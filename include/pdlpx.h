@@ -129,8 +129,9 @@ typedef struct pdlpx_options {
     int32_t batch_sell;               /* pdlpx_batch_solve: 1 (default) stores matrix sides with mean row
                                          length <= 32 as sliced ELL (32-row slices, column-major, rows
                                          sorted by length inside each 256-row tile); 0 keeps CSR */
-    int32_t scale_on_device;          /* Ruiz passes of load / edits on the GPU (identical results):
-                                         -1 (default) for LPs with >= 1M nonzeros, 1 always, 0 never */
+    int32_t scale_on_device;          /* Ruiz passes of the scaling pipeline on the GPU (load, edits,
+                                         batch / server preparation; identical results): -1 (default)
+                                         for LPs with >= 200k nonzeros, 1 always, 0 never */
     int32_t reserved[1];
 } pdlpx_options;
 

@@ -1614,7 +1614,7 @@ int32_t prepareItem(const pdlpx_lp& in, const pdlpx_options& o, Item& it) {
     it.trivial = lp.m == 0 || lp.n == 0;
     if (it.trivial) return PDLPX_OK;
     const bool mixed = o.precision != PDLPX_PREC_FP64;
-    buildScaled(lp, o, it.sc);
+    buildScaled(lp, o, it.sc, ruizFor(o, lp.a.nnz()));
     const int64_t z = it.sc.a.nnz();
     it.shapeP = batchSideShape(o.shape_primal, o.spmv_group_at, o.batch_sell != 0, z, lp.n);
     it.shapeD = batchSideShape(o.shape_dual, o.spmv_group_a, o.batch_sell != 0, z, lp.m);

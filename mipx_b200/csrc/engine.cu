@@ -894,19 +894,10 @@ int32_t Engine::load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const
 }
 
 // Scaling pipeline; its Ruiz passes run on the device for large LPs
-// (scale_on_device: 1 always, -1 from 1M nonzeros, 0 never), with identical
+// (scale_on_device: 1 always, -1 from 200k nonzeros, 0 never), with identical
 // results, and on the host when the device is unavailable.
 void Engine::rescale() {
-    const int mode = opt_.scale_on_device;
-    RuizFn dev;
-    if (mode > 0 || (mode < 0 && lp_.a.nnz() >= 1000000))
-        dev = [this](Csr& a, std::vector<double>& rs, std::vector<double>& cs, int passes) {
-            std::string err;
-            const bool ok = ruizOnDevice(a, rs, cs, passes, opt_.device, err);
-            if (!ok) last_error = err;
-            return ok;
-        };
-    buildScaled(lp_, opt_, sc_, dev);
+    buildScaled(lp_, opt_, sc_, ruizFor(opt_, lp_.a.nnz()));
     dev_.reset();
 }
 

@@ -70,6 +70,10 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
 bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& col_scale, int passes, int device,
                   std::string& err);
 
+// The Ruiz hook the options ask for: the device for scale_on_device = 1, or for
+// -1 (auto) from 200k nonzeros; none (host loop) otherwise.
+RuizFn ruizFor(const pdlpx_options& o, int64_t nnz);
+
 // Recompute sigma/tau from the scaled matrix (pdlp.cpp:713-742).
 void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<double>& tau);
 
