@@ -20,7 +20,8 @@ def _build(tmp_path) -> Path:
     if not lib.exists():
         _capi.load()
     exe = tmp_path / "pdlpx_api_test"
-    subprocess.run(["g++", "-std=c++20", "-O1", f"-I{ROOT / 'include'}", str(SRC), "-o", str(exe),
+    subprocess.run(["g++", "-std=c++20", "-O1", "-Wall", "-Wextra", "-Werror", f"-I{ROOT / 'include'}", str(SRC),
+                    "-o", str(exe),
                     f"-L{lib.parent}", "-lpdlpx", f"-Wl,-rpath,{lib.parent}"], check=True)
     return exe
 
