@@ -19,6 +19,7 @@
  *   pdlpx_get_reduced_costs  <- getReducedCosts               src/lp/pdlp.cpp:2808-2819
  *   pdlpx_set_warm_start     <- setWarmStart/clearWarmStart   include/mipx/pdlp.h:114-120
  *   pdlpx_set_stop_flag      <- PdlpOptions::stop_flag        include/mipx/pdlp.h:86
+ *   pdlpx_set_stop_callback  <- PdlpOptions::stop_flag        include/mipx/pdlp.h:86 (any flag type)
  *   pdlpx_add_rows ...       <- addRows/removeRows/setColBounds/setObjective  src/lp/pdlp.cpp:2833-2907
  *   pdlpx_used_gpu           <- PdlpSolver::usedGpu           include/mipx/pdlp.h:124
  */
@@ -191,6 +192,15 @@ int32_t pdlpx_clear_warm_start(pdlpx_solver* h);
 /* Cooperative cancel: *flag != 0 makes the solve return ITER_LIMIT at the next
  * batch boundary (pdlp.cpp:972-976).  NULL clears.  Read with an atomic load. */
 int32_t pdlpx_set_stop_flag(pdlpx_solver* h, const int32_t* flag);
+/* Cooperative cancel through a caller function: poll(ctx) != 0 makes the solve
+ * return ITER_LIMIT at the next batch boundary, like the flag above.  This is
+ * how a caller maps a flag of its own type -- the reference's
+ * `const std::atomic<bool>* stop_flag` (pdlp.h:86) -- without a mirroring
+ * thread: poll loads the atomic.  poll runs on the thread that called
+ * pdlpx_solve, once per restart cycle; it must not call back into the same
+ * handle.  poll == NULL clears.  Flag and callback may both be set; either stops. */
+typedef int32_t (*pdlpx_stop_poll)(void* ctx);
+int32_t pdlpx_set_stop_callback(pdlpx_solver* h, pdlpx_stop_poll poll, void* ctx);
 int32_t pdlpx_solve(pdlpx_solver* h, pdlpx_result* out);
 int32_t pdlpx_get_status(const pdlpx_solver* h, int32_t* status);
 int32_t pdlpx_get_objective(const pdlpx_solver* h, double* objective);
@@ -339,8 +349,10 @@ int32_t pdlpx_row_violation(int32_t m, int32_t n, int32_t nnz, const int32_t* ro
  * 48, 32 up to 128, 64 up to 384, 128 up to 768, else 256); larger inputs return
  * PDLPX_E_INVALID with the reason in pdlpx_last_error(NULL).  The first call on
  * each device resolves the array's device address with that device current;
- * make that first call before any stream capture.  Calls share the array and
- * race if they overlap on the GPU. */
+ * make that first call before any stream capture.  The cached address belongs
+ * to the device's current context: after cudaDeviceReset on that device it is
+ * stale and the library must not be called on that device again in the same
+ * process.  Calls share the array and race if they overlap on the GPU. */
 int32_t pdlpx_row_violation_noalloc(int32_t m, int32_t n, int32_t nnz, const int32_t* d_row_ptr,
                                     const int32_t* d_col_idx, const double* d_val,
                                     const double* d_x, const double* d_row_lb,

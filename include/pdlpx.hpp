@@ -19,6 +19,7 @@
  */
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <limits>
 #include <span>
@@ -47,9 +48,14 @@ struct LpResult {
 };
 
 /* The reference's PdlpOptions fields under the same names and defaults
- * (booleans are int32 0/1), plus the engine's launch and batching knobs. */
+ * (booleans are int32 0/1), plus the engine's launch and batching knobs.
+ * stop_flag has the reference's type (pdlp.h:86): code that sets
+ * `opts.stop_flag = &flag; solver.setOptions(opts);` compiles unchanged, and
+ * the solver polls the atomic once per restart cycle through the C ABI's stop
+ * callback (no mirroring thread). */
 struct PdlpOptions : pdlpx_options {
     PdlpOptions() { pdlpx_options_default(this); }
+    const std::atomic<bool>* stop_flag = nullptr;
 };
 
 /* An LP in the reference's ranged form: row_lower <= A x <= row_upper,
@@ -163,6 +169,7 @@ public:
     void setOptions(const PdlpOptions& options) {
         options_ = options;
         if (h_) pdlpx_set_options(h_, &options_);
+        applyStopFlag();
     }
     const PdlpOptions& options() const { return options_; }
     bool usedGpu() const {
@@ -171,13 +178,28 @@ public:
         return u != 0;
     }
 
-    /* Cancellation (PdlpOptions::stop_flag of the reference): polled once per check interval. */
+    /* Cancellation (PdlpOptions::stop_flag of the reference, pdlp.h:86): polled
+     * once per restart cycle; true ends the solve with Status::IterLimit. */
+    void setStopFlag(const std::atomic<bool>* flag) {
+        options_.stop_flag = flag;
+        applyStopFlag();
+    }
+    /* The same with a plain int32 flag (read with an atomic load). */
     void setStopFlag(const int32_t* flag) {
         if (h_) pdlpx_set_stop_flag(h_, flag);
     }
     const char* lastError() const { return h_ ? pdlpx_last_error(h_) : "solver handle not created"; }
 
 private:
+    static int32_t pollAtomic(void* ctx) {
+        return static_cast<const std::atomic<bool>*>(ctx)->load(std::memory_order_relaxed) ? 1 : 0;
+    }
+    void applyStopFlag() {
+        if (!h_) return;
+        const std::atomic<bool>* f = options_.stop_flag;
+        pdlpx_set_stop_callback(h_, f != nullptr ? &PdlpSolver::pollAtomic : nullptr,
+                                const_cast<void*>(static_cast<const void*>(f)));
+    }
     std::pair<int32_t, int32_t> dims() const {
         int32_t m = 0, n = 0, z = 0;
         if (h_) pdlpx_get_dims(h_, &m, &n, &z);

@@ -17,6 +17,9 @@ i32 = C.c_int32
 f64 = C.c_double
 P_i32 = C.POINTER(C.c_int32)
 P_f64 = C.POINTER(C.c_double)
+# pdlpx_stop_poll: int32_t (*)(void* ctx); a Python function wrapped in it can be
+# passed to pdlpx_set_stop_callback (keep the wrapper alive while it is set).
+STOP_POLL = C.CFUNCTYPE(C.c_int32, C.c_void_p)
 
 
 class Options(C.Structure):
@@ -93,6 +96,7 @@ SIGNATURES = [
     ("pdlpx_set_warm_start", i32, [C.c_void_p, P_f64, i32, P_f64, i32]),
     ("pdlpx_clear_warm_start", i32, [C.c_void_p]),
     ("pdlpx_set_stop_flag", i32, [C.c_void_p, P_i32]),
+    ("pdlpx_set_stop_callback", i32, [C.c_void_p, C.c_void_p, C.c_void_p]),  # poll: STOP_POLL or None
     ("pdlpx_solve", i32, [C.c_void_p, C.POINTER(Result)]),
     ("pdlpx_get_status", i32, [C.c_void_p, P_i32]),
     ("pdlpx_get_objective", i32, [C.c_void_p, P_f64]),

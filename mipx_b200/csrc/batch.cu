@@ -575,6 +575,7 @@ struct Item {
     int64_t np = 0, mp = 0;    // columns / rows padded to whole tiles
     SideOrder cols, rows;      // renumbering of columns (A^T rows) and rows
     size_t bytes = 0;          // share of a pack's device image
+    std::string scale_note;    // why the device Ruiz passes fell back to the host (empty: they did not)
     // position within its pack
     int64_t r0 = 0, c0 = 0;    // first row, first column
     int64_t za = 0, zt = 0;    // first entry of A / of A^T
@@ -1614,7 +1615,7 @@ int32_t prepareItem(const pdlpx_lp& in, const pdlpx_options& o, Item& it) {
     it.trivial = lp.m == 0 || lp.n == 0;
     if (it.trivial) return PDLPX_OK;
     const bool mixed = o.precision != PDLPX_PREC_FP64;
-    buildScaled(lp, o, it.sc, ruizFor(o, lp.a.nnz()));
+    buildScaled(lp, o, it.sc, ruizFor(o, lp.a.nnz(), &it.scale_note));
     const int64_t z = it.sc.a.nnz();
     it.shapeP = batchSideShape(o.shape_primal, o.spmv_group_at, o.batch_sell != 0, z, lp.n);
     it.shapeD = batchSideShape(o.shape_dual, o.spmv_group_a, o.batch_sell != 0, z, lp.m);
@@ -1854,6 +1855,8 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
         }
         rc = runPack(pack, o, t0, nullptr, [&](int l, LpOutcome&& out) { deliver(index[l], out); }, err);
         if (rc != PDLPX_OK) return rc;
+        for (const Item* it : pack)
+            if (!it->scale_note.empty()) err = it->scale_note;  // solved; pdlpx_last_error says why scaling was host-side
     }
     return PDLPX_OK;
 }

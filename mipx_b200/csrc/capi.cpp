@@ -194,6 +194,12 @@ int32_t pdlpx_set_stop_flag(pdlpx_solver* h, const int32_t* flag) {
     return PDLPX_OK;
 }
 
+int32_t pdlpx_set_stop_callback(pdlpx_solver* h, pdlpx_stop_poll poll, void* ctx) {
+    if (h == nullptr) return PDLPX_E_INVALID;
+    h->engine.setStopCallback(poll, ctx);
+    return PDLPX_OK;
+}
+
 int32_t pdlpx_solve(pdlpx_solver* h, pdlpx_result* out) {
     if (h == nullptr || out == nullptr) return PDLPX_E_INVALID;
     return guarded(h, [&] { return h->engine.solve(out); });

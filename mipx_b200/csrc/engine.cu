@@ -897,7 +897,9 @@ int32_t Engine::load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const
 // (scale_on_device: 1 always, -1 from 200k nonzeros, 0 never), with identical
 // results, and on the host when the device is unavailable.
 void Engine::rescale() {
-    buildScaled(lp_, opt_, sc_, ruizFor(opt_, lp_.a.nnz()));
+    std::string note;
+    buildScaled(lp_, opt_, sc_, ruizFor(opt_, lp_.a.nnz(), &note));
+    if (!note.empty()) last_error = note;  // the solve still runs; pdlpx_last_error says why scaling was host-side
     dev_.reset();
 }
 
@@ -1291,7 +1293,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     int prec = d.mixed ? 0 : 1;
     while (true) {
         if (timeUp(t0, opt_.max_solve_seconds)) break;
-        if (stop_flag_ != nullptr && __atomic_load_n(stop_flag_, __ATOMIC_RELAXED) != 0) {
+        if (stopRequested()) {
             stopped = true;
             break;
         }

@@ -34,6 +34,14 @@ public:
     void setWarmStart(const double* x, int32_t nx, const double* y, int32_t ny);
     void clearWarmStart();
     void setStopFlag(const int32_t* f) { stop_flag_ = f; }
+    void setStopCallback(pdlpx_stop_poll poll, void* ctx) {
+        stop_poll_ = poll;
+        stop_ctx_ = poll != nullptr ? ctx : nullptr;
+    }
+    bool stopRequested() const {
+        return (stop_flag_ != nullptr && __atomic_load_n(stop_flag_, __ATOMIC_RELAXED) != 0) ||
+               (stop_poll_ != nullptr && stop_poll_(stop_ctx_) != 0);
+    }
 
     bool loaded() const { return loaded_; }
     int32_t status() const { return status_; }
@@ -70,6 +78,8 @@ private:
     std::vector<double> warm_x_, warm_y_;
     bool has_warm_ = false;
     const int32_t* stop_flag_ = nullptr;
+    pdlpx_stop_poll stop_poll_ = nullptr;
+    void* stop_ctx_ = nullptr;
 
     int32_t status_ = PDLPX_STATUS_ERROR;
     double objective_ = 0.0;

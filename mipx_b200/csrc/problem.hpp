@@ -71,8 +71,10 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
                   std::string& err);
 
 // The Ruiz hook the options ask for: the device for scale_on_device = 1, or for
-// -1 (auto) from 200k nonzeros; none (host loop) otherwise.
-RuizFn ruizFor(const pdlpx_options& o, int64_t nnz);
+// -1 (auto) from 200k nonzeros; none (host loop) otherwise.  When the device
+// passes fail (the host loop then does the work, with identical results) the
+// reason goes to *fallback_note if given.
+RuizFn ruizFor(const pdlpx_options& o, int64_t nnz, std::string* fallback_note = nullptr);
 
 // Recompute sigma/tau from the scaled matrix (pdlp.cpp:713-742).
 void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<double>& tau);

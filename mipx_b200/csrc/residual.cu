@@ -159,6 +159,7 @@ int32_t pdlpx_row_violation(int32_t m, int32_t n, int32_t nnz, const int32_t* ro
 int32_t pdlpx_row_violation_noalloc(int32_t m, int32_t n, int32_t nnz, const int32_t* d_row_ptr,
                                     const int32_t* d_col_idx, const double* d_val, const double* d_x,
                                     const double* d_row_lb, const double* d_row_ub, double* d_out, void* stream) {
+    try {
     if (m < 0 || n < 0 || nnz < 0 || d_out == nullptr ||
         (m > 0 && (d_row_ptr == nullptr || d_row_lb == nullptr || d_row_ub == nullptr)) ||
         (nnz > 0 && (d_col_idx == nullptr || d_val == nullptr)) || (n > 0 && d_x == nullptr)) {
@@ -206,6 +207,11 @@ int32_t pdlpx_row_violation_noalloc(int32_t m, int32_t n, int32_t nnz, const int
         return PDLPX_E_CUDA;
     }
     return PDLPX_OK;
+    } catch (const std::bad_alloc&) {
+        return PDLPX_E_NOMEM;  // building an error message failed; nothing was enqueued
+    } catch (...) {
+        return PDLPX_E_INVALID;
+    }
 }
 
 }  // extern "C"

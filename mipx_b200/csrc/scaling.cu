@@ -139,12 +139,14 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
     return true;
 }
 
-RuizFn ruizFor(const pdlpx_options& o, int64_t nnz) {
+RuizFn ruizFor(const pdlpx_options& o, int64_t nnz, std::string* fallback_note) {
     if (!(o.scale_on_device > 0 || (o.scale_on_device < 0 && nnz >= 200000))) return {};
     const int device = o.device;
-    return [device](Csr& a, std::vector<double>& rs, std::vector<double>& cs, int passes) {
+    return [device, fallback_note](Csr& a, std::vector<double>& rs, std::vector<double>& cs, int passes) {
         std::string err;
-        return ruizOnDevice(a, rs, cs, passes, device, err);
+        const bool ok = ruizOnDevice(a, rs, cs, passes, device, err);
+        if (!ok && fallback_note != nullptr) *fallback_note = "device Ruiz scaling fell back to the host: " + err;
+        return ok;
     };
 }
 

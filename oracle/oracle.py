@@ -10,6 +10,7 @@ module; the engine (mipx_b200/) never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -23,10 +24,24 @@ REF_GPU_LIB = HERE / "_ref" / "libmipx_pdlp_ref_gpu.so"
 _libs: dict = {}
 
 
+def reference_dir() -> Path | None:
+    """The mipx source tree the reference libraries are compiled from:
+    $MIPX_REFERENCE_DIR, else the checkout this build recipe reads
+    (/root/reference); None where neither exists (the GPU box, which uses the
+    libraries built beforehand)."""
+    for cand in (os.environ.get("MIPX_REFERENCE_DIR"), "/root/reference"):
+        if cand and (Path(cand) / "src" / "lp" / "pdlp.cpp").exists():
+            return Path(cand)
+    return None
+
+
 def build(ref: bool = True) -> None:
     """Compile the oracle (and, when the reference tree exists, the reference's
     CPU and FP64 GPU PDLP behind the shim)."""
-    targets = ["liboracle_pdlp.so"] + (["ref", "ref_gpu"] if ref else [])
+    targets = ["liboracle_pdlp.so"]
+    rd = reference_dir()
+    if ref and rd is not None:
+        targets += ["ref", "ref_gpu", f"REF={rd}"]
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 

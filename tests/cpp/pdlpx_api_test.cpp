@@ -84,8 +84,10 @@ static int host() {
 }
 
 // The concurrent-root race of mipx (mip_solver.cpp:4470-4605): arms on their
-// own threads and solvers share one stop flag; the first arm to finish sets it
-// and the other returns IterLimit at its next check (or finishes first).
+// own threads and solvers share one stop flag, a std::atomic<bool> handed over
+// through PdlpOptions::stop_flag exactly as the reference's race does; the first
+// arm to finish sets it and the other returns IterLimit at its next check (or
+// finishes first).
 static int race() {
     LpProblem lp;  // a 300-row random-like LP: sum_j x_j <= 10 + i per row, max sum x
     lp.num_cols = 600;
@@ -113,7 +115,7 @@ static int race() {
         }
         lp.row_starts.push_back(static_cast<int32_t>(lp.values.size()));
     }
-    int32_t stop = 0;
+    std::atomic<bool> stop{false};
     pdlpx::LpResult res[2];
     std::atomic<int> first{-1};
     auto arm = [&](int k) {
@@ -123,12 +125,12 @@ static int race() {
         o.max_iter = 200000;
         o.precision = k == 0 ? PDLPX_PREC_MIXED : PDLPX_PREC_FP64;
         o.primal_tol = o.dual_tol = o.optimality_tol = k == 0 ? 1e-4 : 1e-9;  // arm 1 needs far longer
+        o.stop_flag = &stop;
         s.setOptions(o);
-        s.setStopFlag(&stop);
         s.load(lp);
         res[k] = s.solve();
         int expected = -1;
-        if (first.compare_exchange_strong(expected, k)) __atomic_store_n(&stop, 1, __ATOMIC_SEQ_CST);
+        if (first.compare_exchange_strong(expected, k)) stop.store(true);
     };
     std::thread a(arm, 0), b(arm, 1);
     a.join();
@@ -172,6 +174,14 @@ static int gpu() {
     s.setColBounds(1, 0.0, 2.0);  // y <= 2: max becomes 3
     r = s.solve();
     CHECK(r.status == Status::Optimal && std::fabs(r.objective - 3.0) <= 1e-4);
+    // a flag raised before the solve stops it at the first check: IterLimit, as in the reference
+    std::atomic<bool> raised{true};
+    pdlpx::PdlpOptions so = o;
+    so.stop_flag = &raised;
+    s.setOptions(so);
+    CHECK(s.solve().status == Status::IterLimit);
+    s.setStopFlag(static_cast<const std::atomic<bool>*>(nullptr));  // cleared: solves again
+    CHECK(s.solve().status == Status::Optimal);
     return race() + fails;
 }
 

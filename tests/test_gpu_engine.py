@@ -283,7 +283,7 @@ def test_batch_solve_matches_single():
     for lp, (r, x, y) in zip(lps, out):
         single, s = solve(lp, o)
         assert r.status == single.status == Status.Optimal
-        # different kernels (cluster-sliced vs grid-wide), same algorithm: two 1e-6-KKT points
+        # packed-batch kernels (tiles, sliced ELL) vs single-LP kernels, same algorithm: two 1e-6-KKT points
         assert abs(r.objective - single.objective) <= 2e-6 * (1 + abs(single.objective))
 
 

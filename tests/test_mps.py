@@ -18,7 +18,10 @@ from mipx_b200._capi import PdlpxError
 from mipx_b200.pdlp import read_mps
 
 INF = math.inf
-REF_TINY = Path("/root/reference/tests/data/tiny.mps")
+from oracle.oracle import reference_dir
+
+_REF_DIR = reference_dir()
+REF_TINY = (_REF_DIR / "tests" / "data" / "tiny.mps") if _REF_DIR is not None else Path("tiny.mps.absent")
 
 RULES = """NAME          rules
 * comment line
