@@ -19,9 +19,11 @@ from .pdlp import (  # noqa: F401
     batch_solve,
     csr_spmv,
     kInf,
+    read_mps,
+    solve_mps,
 )
 
 __all__ = [
     "BasisStatus", "LpProblem", "LpResult", "PdlpOptimalityNorm", "PdlpOptions", "PdlpSolver", "Precision",
-    "Sense", "SparseMatrix", "Status", "StopFlag", "batch_solve", "csr_spmv", "kInf",
+    "Sense", "SparseMatrix", "Status", "StopFlag", "batch_solve", "csr_spmv", "kInf", "read_mps", "solve_mps",
 ]

@@ -1,5 +1,10 @@
 """Seeded synthetic LPs of the benchmark workloads (C generators in libpdlpx).
 
+Every generator takes ``lib``: the loaded library whose ``pdlpx_gen_*`` entry
+points build the LP (default: the engine's libpdlpx.so).  Any library built
+from the same generator source gives the same arrays, which is how a caller
+that must not load the engine (a CPU baseline) builds the identical workload.
+
 * ``random_lp``      -- random sparse LP: columns with U{lo..hi} nonzeros at
   uniform rows, N(0,1) values, x0~U[0,10], rows alternating '=' / '<=' with
   b = A x0 (+U[0,1] slack), 0 <= x <= 10, c~N(0,1).  2,000 x 5,000 with 4-12
@@ -23,7 +28,7 @@ from . import _capi
 from .pdlp import LpProblem, Sense, SparseMatrix
 
 
-def _take(g: _capi.GenLp) -> tuple[LpProblem, np.ndarray]:
+def _take(g: _capi.GenLp, lib) -> tuple[LpProblem, np.ndarray]:
     m, n, nnz = g.m, g.n, g.nnz
     arr = lambda p, k, dt: np.ctypeslib.as_array(p, shape=(k,)).astype(dt, copy=True) if k > 0 else np.zeros(0, dt)
     rp = arr(g.row_ptr, m + 1, np.int32)
@@ -35,31 +40,39 @@ def _take(g: _capi.GenLp) -> tuple[LpProblem, np.ndarray]:
         row_lower=arr(g.row_lb, m, np.float64), row_upper=arr(g.row_ub, m, np.float64),
         matrix=SparseMatrix(m, n, values=v, col_indices=ci, row_starts=rp))
     x0 = arr(g.x0, n, np.float64)
-    _capi.load().pdlpx_free_lp(C.byref(g))
+    lib.pdlpx_free_lp(C.byref(g))
     return lp, x0
 
 
-def random_lp(m: int = 2000, n: int = 5000, nnz_lo: int = 4, nnz_hi: int = 12, seed: int = 1):
+def _check(lib, code: int) -> None:
+    if code != 0:
+        raise _capi.PdlpxError(code, "generator rejected its arguments")
+
+
+def random_lp(m: int = 2000, n: int = 5000, nnz_lo: int = 4, nnz_hi: int = 12, seed: int = 1, lib=None):
+    lib = lib or _capi.load()
     g = _capi.GenLp()
-    _capi.check(_capi.load().pdlpx_gen_random(m, n, nnz_lo, nnz_hi, seed, C.byref(g)))
-    lp, x0 = _take(g)
+    _check(lib, lib.pdlpx_gen_random(m, n, nnz_lo, nnz_hi, seed, C.byref(g)))
+    lp, x0 = _take(g, lib)
     lp.name = f"random_{m}x{n}_s{seed}"
     return lp, x0
 
 
-def transport_lp(supplies: int = 1000, demands: int = 1000, seed: int = 7):
+def transport_lp(supplies: int = 1000, demands: int = 1000, seed: int = 7, lib=None):
+    lib = lib or _capi.load()
     g = _capi.GenLp()
-    _capi.check(_capi.load().pdlpx_gen_transport(supplies, demands, seed, C.byref(g)))
-    lp, x0 = _take(g)
+    _check(lib, lib.pdlpx_gen_transport(supplies, demands, seed, C.byref(g)))
+    lp, x0 = _take(g, lib)
     lp.name = f"transport_{supplies}x{demands}_s{seed}"
     return lp, x0
 
 
 def powerlaw_lp(m: int = 500_000, n: int = 2_000_000, kmin: int = 2, kmax: int = 2000, kmean: float = 10.0,
-                big_frac: float = 0.01, big_scale: float = 1e3, seed: int = 11):
+                big_frac: float = 0.01, big_scale: float = 1e3, seed: int = 11, lib=None):
+    lib = lib or _capi.load()
     g = _capi.GenLp()
-    _capi.check(_capi.load().pdlpx_gen_powerlaw(m, n, kmin, kmax, kmean, big_frac, big_scale, seed, C.byref(g)))
-    lp, x0 = _take(g)
+    _check(lib, lib.pdlpx_gen_powerlaw(m, n, kmin, kmax, kmean, big_frac, big_scale, seed, C.byref(g)))
+    lp, x0 = _take(g, lib)
     lp.name = f"powerlaw_{m}x{n}_s{seed}"
     return lp, x0
 
@@ -71,8 +84,9 @@ def batch_sizes(count: int = 512, median: float = 1500.0, sigma: float = 0.8, lo
     return [(int(m), int(round(2.5 * m))) for m in ms]
 
 
-def batch_lps(count: int = 512, seed: int = 5, **kw) -> list[LpProblem]:
-    return [random_lp(m, n, 4, 12, seed * 100003 + k)[0] for k, (m, n) in enumerate(batch_sizes(count, seed=seed, **kw))]
+def batch_lps(count: int = 512, seed: int = 5, lib=None, **kw) -> list[LpProblem]:
+    return [random_lp(m, n, 4, 12, seed * 100003 + k, lib=lib)[0]
+            for k, (m, n) in enumerate(batch_sizes(count, seed=seed, **kw))]
 
 
 def integer_marks(n: int, frac: float = 0.3, seed: int = 3) -> np.ndarray:

@@ -10,6 +10,7 @@ solve runs on the GPU through ``libpdlpx.so``; there is no CPU path here.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import enum
 import math
 from dataclasses import dataclass, field, fields
@@ -134,7 +135,9 @@ class PdlpOptions:
     scale_on_device: int = -1
 
     def to_c(self) -> _capi.Options:
-        o = _capi.default_options()
+        # every field of pdlpx_options but `reserved` (zero) is set here, so no
+        # library call is needed to build the struct
+        o = _capi.Options()
         for f in fields(self):
             if f.name == "stop_flag":
                 continue
@@ -470,6 +473,26 @@ def read_mps(path) -> LpProblem:
     finally:
         lib.pdlpx_free_lp(C.byref(g))
     return lp
+
+
+def solve_mps(filename, time_limit: float = 3600.0, verbose: bool = False,
+              options: PdlpOptions | None = None):
+    """Read an MPS file (plain or .gz) and solve it with PDLP on the GPU.
+
+    The PDLP path's counterpart of mipx's Python ``solve_mps``
+    (python/src/bindings.cpp:169-205: ``readMps`` then a solve with default
+    settings): the model is read as mipx's reader reads it and its LP -- integer
+    marks ignored, as the CLI's ``--pdlp`` LP mode does (src/cli/main.cpp:509-522)
+    -- is solved by ``PdlpSolver``.  ``time_limit`` and ``verbose`` override the
+    corresponding fields of ``options`` (default PdlpOptions()).  Returns
+    ``(LpResult, x, y)`` with x, y in the model's original space."""
+    opts = options if options is not None else PdlpOptions()
+    opts = dataclasses.replace(opts, max_solve_seconds=float(time_limit), verbose=bool(verbose))
+    s = PdlpSolver()
+    s.setOptions(opts)
+    s.load(read_mps(filename))
+    r = s.solve()
+    return r, s.getPrimalValues(), s.getDualValues()
 
 
 class Server:

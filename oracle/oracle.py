@@ -5,7 +5,9 @@ ctypes access to the CPU checkers of the PDLP path:
   * ``_ref/libmipx_pdlp_ref.so`` -- the reference's own PdlpSolver compiled from its
     sources (present only where the reference tree was available at build time).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use this
-module; the engine (mipx_b200/) never imports it.
+module; the engine (mipx_b200/) never imports it.  The oracle library also
+carries the workload generators, so the CPU-baseline legs build their inputs
+without loading the engine library.
 """
 from __future__ import annotations
 
@@ -20,6 +22,8 @@ HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liboracle_pdlp.so"
 REF_LIB = HERE / "_ref" / "libmipx_pdlp_ref.so"
 REF_GPU_LIB = HERE / "_ref" / "libmipx_pdlp_ref_gpu.so"
+# the reference's PdlpSolver with the pdlpx binding as its solveGpu body (make ref_bound)
+REF_BOUND_LIB = HERE / "_ref" / "libmipx_pdlp_bound.so"
 
 _libs: dict = {}
 
@@ -41,7 +45,7 @@ def build(ref: bool = True) -> None:
     targets = ["liboracle_pdlp.so"]
     rd = reference_dir()
     if ref and rd is not None:
-        targets += ["ref", "ref_gpu", f"REF={rd}"]
+        targets += ["ref", "ref_gpu", "ref_bound", f"REF={rd}"]
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 
@@ -61,6 +65,22 @@ def _load(path: Path):
                 getattr(lib, name).restype = C.c_int
         if hasattr(lib, "ref_pdlp_solve_rc"):
             lib.ref_pdlp_solve_rc.argtypes = sig[:3] + [_capi.P_f64]
+        for name, res, args in _capi.SIGNATURES:  # the workload generators built into the oracle library
+            if name.startswith("pdlpx_gen_") or name == "pdlpx_free_lp":
+                if hasattr(lib, name):
+                    getattr(lib, name).restype = res
+                    getattr(lib, name).argtypes = args
+        if hasattr(lib, "ref_pdlp_open"):
+            lib.ref_pdlp_open.argtypes = sig[:2]
+            lib.ref_pdlp_open.restype = C.c_void_p
+            lib.ref_pdlp_run.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(_capi.Result)]
+            lib.ref_pdlp_run.restype = C.c_int
+            lib.ref_pdlp_close.argtypes = [C.c_void_p]
+            lib.ref_pdlp_close.restype = None
+        if hasattr(lib, "ref_pdlp_race"):
+            lib.ref_pdlp_race.argtypes = [C.POINTER(_capi.Lp), C.POINTER(_capi.Options), C.POINTER(_capi.Options),
+                                          C.POINTER(_capi.Result), C.POINTER(_capi.Result), C.POINTER(C.c_int)]
+            lib.ref_pdlp_race.restype = C.c_int
         if hasattr(lib, "oracle_scaling"):
             lib.oracle_scaling.argtypes = [C.POINTER(_capi.Lp), C.POINTER(_capi.Options)] + [_capi.P_f64] * 11
             lib.oracle_spectral_norm.argtypes = [C.POINTER(_capi.Lp), C.POINTER(_capi.Options)]
@@ -74,6 +94,13 @@ def _load(path: Path):
 
 def ref_available() -> bool:
     return REF_LIB.exists()
+
+
+def gen_lib():
+    """The oracle library as a generator source for mipx_b200.generators
+    (``lib=``): the same generator code as the engine's, without loading the
+    engine library."""
+    return _load(ORACLE_LIB)
 
 
 def _solve(fn, problem, options, warm=None):
@@ -97,9 +124,64 @@ def oracle_solve(problem, options, warm=None):
     return _solve(_load(ORACLE_LIB).oracle_pdlp_solve, problem, options, warm)
 
 
-def ref_solve(problem, options, warm=None, gpu: bool = False):
-    """The reference's own PdlpSolver (compiled from source): (LpResult, x, y)."""
-    return _solve(_load(REF_GPU_LIB if gpu else REF_LIB).ref_pdlp_solve, problem, options, warm)
+def _ref_lib(gpu: bool = False, bound: bool = False):
+    return _load(REF_BOUND_LIB if bound else (REF_GPU_LIB if gpu else REF_LIB))
+
+
+def ref_solve(problem, options, warm=None, gpu: bool = False, bound: bool = False):
+    """The reference's own PdlpSolver (compiled from source): (LpResult, x, y).
+    gpu: its cuSPARSE FP64 GPU path; bound: its class with the pdlpx binding as
+    the solveGpu body (the drop-in build)."""
+    return _solve(_ref_lib(gpu, bound).ref_pdlp_solve, problem, options, warm)
+
+
+def ref_race(problem, arm0, arm1, bound: bool = False):
+    """mipx's concurrent-root race pattern over the reference's PdlpSolver: two
+    arms with a shared std::atomic<bool> stop flag.  Returns (r0, r1, winner)."""
+    from mipx_b200.pdlp import LpResult
+    from mipx_b200 import _capi
+    keep: list = []
+    lp = problem.to_c(keep)
+    r0, r1, w = _capi.Result(), _capi.Result(), C.c_int(-1)
+    rc = _ref_lib(bound=bound).ref_pdlp_race(C.byref(lp), C.byref(arm0.to_c()), C.byref(arm1.to_c()), C.byref(r0),
+                                             C.byref(r1), C.byref(w))
+    if rc != 0:
+        raise RuntimeError(f"race failed ({rc})")
+    return LpResult.from_c(r0), LpResult.from_c(r1), w.value
+
+
+class RefSession:
+    """The reference's PdlpSolver loaded once (its scaling pipeline runs in
+    load), then solved repeatedly with new caps: ``run(max_iter, sv_max_iter)``
+    returns (LpResult, wall seconds of the reference's solve()).  Used to time
+    the reference's iteration rate without paying its load for every sample."""
+
+    def __init__(self, problem, options, gpu: bool = False):
+        self._lib = _ref_lib(gpu)
+        keep: list = []
+        lp = problem.to_c(keep)
+        self._h = self._lib.ref_pdlp_open(C.byref(lp), C.byref(options.to_c()))
+        if not self._h:
+            raise RuntimeError("reference solver could not be created")
+
+    def run(self, max_iter: int, sv_max_iter: int):
+        from mipx_b200.pdlp import LpResult
+        from mipx_b200 import _capi
+        res = _capi.Result()
+        if self._lib.ref_pdlp_run(self._h, int(max_iter), int(sv_max_iter), C.byref(res)) != 0:
+            raise RuntimeError("reference run failed")
+        return LpResult.from_c(res), res.solve_seconds
+
+    def close(self):
+        if self._h:
+            self._lib.ref_pdlp_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def ref_reduced_costs(problem, options):

@@ -10,6 +10,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "mipx/pdlp.h"
@@ -136,6 +137,81 @@ int ref_pdlp_solve_rc(const pdlpx_lp* lp, const pdlpx_options* opts, pdlpx_resul
     res->work_units = r.work_units;
     auto v = solver.getReducedCosts();
     for (size_t j = 0; j < v.size(); ++j) rc[j] = v[j];
+    return PDLPX_OK;
+}
+
+// A reference solver kept across calls, for the CPU baseline timing: open
+// copies and loads the LP once (the reference's load runs its scaling
+// pipeline); every run then calls the reference's solve() with a new iteration
+// cap and power-iteration cap and reports its wall time in res->solve_seconds.
+struct RefHandle {
+    mipx::PdlpSolver solver;
+    mipx::PdlpOptions opts;
+};
+
+void* ref_pdlp_open(const pdlpx_lp* lp, const pdlpx_options* opts) {
+    if (lp == nullptr || opts == nullptr) return nullptr;
+    auto* h = new RefHandle();
+    h->opts = toRefOptions(*opts);
+    h->solver.setOptions(h->opts);
+    h->solver.load(toRefProblem(*lp));
+    return h;
+}
+
+int ref_pdlp_run(void* handle, int32_t max_iter, int32_t sv_max_iter, pdlpx_result* res) {
+    auto* h = static_cast<RefHandle*>(handle);
+    if (h == nullptr || res == nullptr) return PDLPX_E_INVALID;
+    h->opts.max_iter = max_iter;
+    h->opts.sv_max_iter = sv_max_iter;
+    h->solver.setOptions(h->opts);
+    auto t0 = std::chrono::steady_clock::now();
+    mipx::LpResult r = h->solver.solve();
+    std::memset(res, 0, sizeof(*res));
+    res->solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    res->status = static_cast<int32_t>(r.status);
+    res->objective = r.objective;
+    res->iterations = r.iterations;
+    res->work_units = r.work_units;
+    res->used_gpu = h->solver.usedGpu() ? 1 : 0;
+    return PDLPX_OK;
+}
+
+void ref_pdlp_close(void* handle) { delete static_cast<RefHandle*>(handle); }
+
+// The concurrent-root race pattern of mipx (mip_solver.cpp:4470-4605) over the
+// reference's own PdlpSolver class: two arms on their own threads, each with
+// its own solver and options, share one std::atomic<bool> through
+// PdlpOptions::stop_flag; the first arm to finish raises it and the other ends
+// at its next check with IterLimit (or finishes first).  winner = 0 or 1.
+int ref_pdlp_race(const pdlpx_lp* lp, const pdlpx_options* arm0, const pdlpx_options* arm1, pdlpx_result* r0,
+                  pdlpx_result* r1, int* winner) {
+    if (lp == nullptr || arm0 == nullptr || arm1 == nullptr || r0 == nullptr || r1 == nullptr || winner == nullptr)
+        return PDLPX_E_INVALID;
+    const mipx::LpProblem problem = toRefProblem(*lp);
+    std::atomic<bool> stop{false};
+    std::atomic<int> first{-1};
+    pdlpx_result* out[2] = {r0, r1};
+    const pdlpx_options* opts[2] = {arm0, arm1};
+    auto arm = [&](int k) {
+        mipx::PdlpSolver solver;
+        mipx::PdlpOptions o = toRefOptions(*opts[k]);
+        o.stop_flag = &stop;
+        solver.setOptions(o);
+        solver.load(problem);
+        const mipx::LpResult r = solver.solve();
+        int expected = -1;
+        if (first.compare_exchange_strong(expected, k)) stop.store(true);
+        std::memset(out[k], 0, sizeof(pdlpx_result));
+        out[k]->status = static_cast<int32_t>(r.status);
+        out[k]->objective = r.objective;
+        out[k]->iterations = r.iterations;
+        out[k]->work_units = r.work_units;
+        out[k]->used_gpu = solver.usedGpu() ? 1 : 0;
+    };
+    std::thread a(arm, 0), b(arm, 1);
+    a.join();
+    b.join();
+    *winner = first.load();
     return PDLPX_OK;
 }
 

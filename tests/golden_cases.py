@@ -62,3 +62,17 @@ def options(name: str, **over) -> PdlpOptions:
 
 NAMES = sorted(k for k in INDEX if "objective" in INDEX[k])
 HIGHS_ONLY = sorted(k for k in INDEX if "objective" not in INDEX[k])
+
+# Objective parity bound of the north-star workloads: results within 1e-6
+# relative of an FP64 oracle, relative to max(1, |oracle|) so objectives near
+# zero are held to 1e-6 absolute.
+OBJ_TOL = 1e-6
+
+
+def rel_err(value: float, oracle: float) -> float:
+    return abs(value - oracle) / max(1.0, abs(oracle))
+
+
+def config_pins() -> dict:
+    """FP64 objective pins of the benchmark configurations (tests/golden/make_config_pins.py)."""
+    return json.loads((GOLDEN / "config_pins.json").read_text())

@@ -58,3 +58,22 @@ def test_batch_sizes():
     assert len(sizes) == 512 and ms.min() >= 200 and ms.max() <= 20000
     assert 1200 < np.median(ms) < 1800
     assert all(n == round(2.5 * m) for m, n in sizes)
+
+
+def test_oracle_library_generates_the_same_workloads():
+    """The CPU-baseline legs build their inputs through the oracle library (so
+    they never load the engine); its generators must give the engine's arrays
+    exactly."""
+    from oracle import oracle
+
+    lib = oracle.gen_lib()
+    cases = [(G.random_lp, (700, 1750, 4, 12, 9)), (G.transport_lp, (60, 80, 7)),
+             (G.powerlaw_lp, (3000, 12000, 2, 2000, 10.0, 0.01, 1e3, 11))]
+    for fn, args in cases:
+        (a, xa), (b, xb) = fn(*args), fn(*args, lib=lib)
+        for f in ("obj", "col_lower", "col_upper", "row_lower", "row_upper"):
+            np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+        np.testing.assert_array_equal(a.matrix.row_starts, b.matrix.row_starts)
+        np.testing.assert_array_equal(a.matrix.col_indices, b.matrix.col_indices)
+        np.testing.assert_array_equal(a.matrix.values, b.matrix.values)
+        np.testing.assert_array_equal(xa, xb)

@@ -230,3 +230,29 @@ def test_mps_edge_rules(tmp_path):
     np.testing.assert_array_equal(lp.col_upper, [INF, 4.0])
     np.testing.assert_array_equal(lp.row_lower, [2.0])
     np.testing.assert_array_equal(lp.row_upper, [2.0])
+
+
+@pytest.mark.gpu
+def test_solve_mps_entry_point(tmp_path):
+    """mipx_b200.solve_mps: read + PDLP solve in one call, as mipx's Python
+    solve_mps does for its models; same result as reading and solving through
+    PdlpSolver, and time_limit / verbose reach the options."""
+    from mipx_b200 import solve_mps
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver
+    lp, _ = G.random_lp(300, 750, 4, 12, 8)
+    p = tmp_path / "r.mps"
+    _write_mps(lp, p)
+    tight = PdlpOptions(primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6)
+    r, x, y = solve_mps(p, time_limit=300.0, options=tight)
+    q = PdlpSolver()
+    q.setOptions(PdlpOptions(verbose=False, primal_tol=1e-6, dual_tol=1e-6, optimality_tol=1e-6,
+                             max_solve_seconds=300.0))
+    q.load(read_mps(p))
+    res = q.solve()
+    assert int(r.status) == int(res.status) == 0
+    assert r.objective == res.objective and r.iterations == res.iterations
+    np.testing.assert_array_equal(x, q.getPrimalValues())
+    np.testing.assert_array_equal(y, q.getDualValues())
+    assert x.size == 750 and y.size == 300
+    r0, _, _ = solve_mps(p, time_limit=0.0, options=tight)
+    assert int(r0.status) == 4  # TimeLimit: the limit reached the solver
