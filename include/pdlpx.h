@@ -133,6 +133,15 @@ typedef struct pdlpx_options {
     int32_t scale_on_device;          /* Ruiz passes of the scaling pipeline on the GPU (load, edits,
                                          batch / server preparation; identical results): -1 (default)
                                          for LPs with >= 200k nonzeros, 1 always, 0 never */
+    int32_t sell;                     /* single-LP engine: store the short rows of a matrix side (rows
+                                         longer than max(64, 8 x mean) excepted) as sliced ELL, 32-row
+                                         slices, when their mean length is <= 64: -1 (default)
+                                         automatic, 1 whenever the side has short rows, 0 never (CSR) */
+    int32_t reference_fixed_columns;  /* 1: a fixed column (lb == ub) contributes to the dual residual
+                                         exactly as in the reference's check (pdlp.cpp:1134-1140, lower
+                                         bound tested first, so a negative reduced cost counts and
+                                         such LPs may not converge, as there); 0 (default): a fixed
+                                         column adds no dual residual */
     int32_t reserved[1];
 } pdlpx_options;
 
@@ -227,15 +236,29 @@ int32_t pdlpx_get_scaling(const pdlpx_solver* h, double* col_scale, double* csca
                           double* col_ub_scaled, double* objective_scale,
                           double* constraint_scale);
 
-/* Average device time in milliseconds of one launch of the fused primal step,
- * the fused dual step and the FP64 check pass (both kernels) on the loaded
- * problem, each launched `reps` times back to back on the engine's stream
- * between CUDA events.  Needs a completed pdlpx_solve on this handle; leaves
- * the returned solution untouched.  Any output pointer may be NULL. */
-int32_t pdlpx_time_kernels(pdlpx_solver* h, int32_t reps, double* ms_primal, double* ms_dual,
-                           double* ms_check);
-/* Threads per row chosen for A (dual step) and A^T (primal step), and the grid
- * sizes of the two step kernels. */
+/* Average device time in milliseconds of one launch of the fused primal step
+ * and the fused dual step (each with its long- and short-row launches) in the
+ * given precision (PDLPX_PREC_MIXED: the FP32 kernels, PDLPX_PREC_FP64: the
+ * FP64 kernels; -1: the precision the last solve ended in), run as `reps`
+ * PDHG iterations -- primal, dual, primal, ... as in the solve loop -- with a
+ * CUDA event between every two launches on the engine's stream, after a write
+ * of flush_bytes bytes to a scratch buffer (0: none) that evicts the L2; and
+ * of one FP64 check pass.  Needs a completed pdlpx_solve on this handle and, for
+ * PDLPX_PREC_MIXED, a mixed-precision image; leaves the returned solution
+ * untouched.  Any output pointer may be NULL. */
+int32_t pdlpx_time_kernels(pdlpx_solver* h, int32_t precision, int32_t reps, int64_t flush_bytes,
+                           double* ms_primal, double* ms_dual, double* ms_check);
+/* Device time of the step kernels measured inside the last solve itself: the
+ * restart-cycle graph records CUDA events around the primal and the dual step
+ * of one iteration of every cycle, and the host reads them after the cycle.
+ * For precision p (PDLPX_PREC_MIXED: FP32 kernels, PDLPX_PREC_FP64: FP64
+ * kernels) returns the mean ms per launch of each step and the number of
+ * cycles sampled (0: none ran in that precision). */
+int32_t pdlpx_get_step_times(const pdlpx_solver* h, int32_t precision, double* ms_primal, double* ms_dual,
+                             int32_t* samples);
+/* Threads per row chosen for A (dual step) and A^T (primal step) -- 1 for a
+ * side stored as sliced ELL -- and the grid sizes of the two step kernels'
+ * short-row launches. */
 int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t* group_at,
                                 int32_t* blocks_primal, int32_t* blocks_dual);
 

@@ -39,7 +39,8 @@ class Options(C.Structure):
         ("use_gpu", i32), ("gpu_min_rows", i32), ("gpu_min_nnz", i32), ("verbose", i32),
         ("precision", i32), ("device", i32), ("fp64_switch", i32), ("spmv_group_a", i32),
         ("spmv_group_at", i32), ("autotune", i32), ("shape_primal", i32), ("shape_dual", i32), ("batch_pack_mb", i32),
-        ("batch_compact", i32), ("batch_sell", i32), ("scale_on_device", i32), ("reserved", i32 * 1),
+        ("batch_compact", i32), ("batch_sell", i32), ("scale_on_device", i32), ("sell", i32),
+        ("reference_fixed_columns", i32), ("reserved", i32 * 1),
     ]
 
 
@@ -110,7 +111,8 @@ SIGNATURES = [
     ("pdlpx_set_col_bounds", i32, [C.c_void_p, i32, f64, f64]),
     ("pdlpx_set_objective", i32, [C.c_void_p, P_f64, i32]),
     ("pdlpx_get_scaling", i32, [C.c_void_p] + [P_f64] * 11),
-    ("pdlpx_time_kernels", i32, [C.c_void_p, i32, P_f64, P_f64, P_f64]),
+    ("pdlpx_time_kernels", i32, [C.c_void_p, i32, i32, C.c_int64, P_f64, P_f64, P_f64]),
+    ("pdlpx_get_step_times", i32, [C.c_void_p, i32, P_f64, P_f64, P_i32]),
     ("pdlpx_get_launch_config", i32, [C.c_void_p, P_i32, P_i32, P_i32, P_i32]),
     ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),
                                 C.POINTER(P_f64), C.POINTER(P_f64)]),

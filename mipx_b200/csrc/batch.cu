@@ -59,12 +59,8 @@ namespace {
 constexpr int kModeFp32 = 0, kModeFp64 = 1, kModeIdle = 2;
 
 // Sliced-ELL launch shapes follow the kNumShapes CSR shapes: entries per lane
-// per round U, one row per thread, kBlock rows per tile.
-constexpr int kSellU[] = {4, 8, 16};
-constexpr int kNumSell = 3;
-constexpr int kSlice = 32;  // rows per slice (one warp)
+// per round kSellU[k], one row per thread, kBlock rows per tile.
 
-__host__ __device__ constexpr bool isSell(int shape) { return shape >= kNumShapes; }
 // Rows one tile of a launch shape covers.
 inline int tileRows(int shape) { return isSell(shape) ? kBlock : rowsPerBlock(shape); }
 // Lanes per row of the CSR check and power kernels on that shape's tiles.
@@ -193,66 +189,7 @@ __global__ void __launch_bounds__(kBlock, PDLPX_PACK_MIN_BLOCKS)
     }
 }
 
-// ---- PDHG step over one sliced-ELL tile -------------------------------------
-// Dot product of this thread's row with x: entry k of the row sits at
-// hdr.x + k * 32 + lane; U entries are loaded per round, then their U gathers,
-// then the products are summed in entry order.
-// Entries past the row's end hold index 0 and value 0 (index 0 always exists).
-template <int U, class V, class X>
-__device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* __restrict__ val, int2 h, int lane,
-                                          const X* __restrict__ x) {
-    const int* ip = idx + h.x + lane;
-    const V* vp = val + h.x + lane;
-    double acc = 0.0;
-    for (int k0 = 0; k0 < h.y; k0 += U) {
-        int c[U];
-        V v[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int k = k0 + u;
-            const bool ok = k < h.y;
-            c[u] = ok ? __ldg(ip + k * kSlice) : 0;
-            v[u] = ok ? __ldg(vp + k * kSlice) : V(0);
-        }
-        X g[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) g[u] = __ldg(x + c[u]);
-#pragma unroll
-        for (int u = 0; u < U; ++u) acc += static_cast<double>(v[u]) * static_cast<double>(g[u]);
-    }
-    return acc;
-}
-
-template <int U, class T>
-__device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
-                                               int koff) {
-    const ColPack<T> q = p.cp[j];
-    const double xc = p.xc[j];
-    const double xi = static_cast<double>(p.xi[j]);
-    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
-    bool last = false;
-    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
-    const double step = p.st->step, pw = p.st->pw;
-    const int k = p.st->inner + koff;
-    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
-    primalUpdate<T>(p, j, q, xc, xi, s, step, pw, lam, last);
-}
-
-template <int U, class T>
-__device__ __forceinline__ void dualSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int i, int2 h,
-                                             int koff) {
-    const RowPack<T> q = p.rp[i];
-    const double yc = p.yc[i];
-    const double yi = static_cast<double>(p.yi[i]);
-    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
-    bool last = false;
-    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
-    const double step = p.st->step, pw = p.st->pw;
-    const int k = p.st->inner + koff;
-    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
-    dualUpdate<T>(p, i, q, yc, yi, s, step, pw, lam, last);
-}
-
+// ---- PDHG step over one sliced-ELL tile (sellDot / primalSellFrom / dualSellFrom in kernels.cuh) ----
 template <int U, bool IND>
 __global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packPrimalSell(PackArgs a, int tile0, int base, int list0, int koff) {
     const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
@@ -623,13 +560,6 @@ void parallelFor(int count, F&& f) {
             return e_ == cudaErrorMemoryAllocation ? PDLPX_E_NOMEM : PDLPX_E_CUDA;   \
         }                                                                            \
     } while (0)
-
-#define PDLPX_SELL_SWITCH(S, CALL)                                   \
-    switch (S - kNumShapes) {                                        \
-        case 0: { constexpr int UU = kSellU[0]; CALL; } break;       \
-        case 1: { constexpr int UU = kSellU[1]; CALL; } break;       \
-        default: { constexpr int UU = kSellU[2]; CALL; } break;      \
-    }
 
 // Host wait for the work queued on a stream, sleeping instead of spinning: a
 // restart cycle runs for milliseconds, and the host cores are wanted by the
@@ -1060,6 +990,7 @@ void lpState(const Item& it, const pdlpx_options& o, bool mixed, int nb_rows, in
     dc.nb_rows = nb_rows;
     dc.nb_cols = nb_cols;
     dc.stall_limit = 10;
+    dc.ref_fixed = o.reference_fixed_columns != 0;
     dc.primal_tol = o.primal_tol;
     dc.dual_tol = o.dual_tol;
     dc.opt_tol = o.optimality_tol;

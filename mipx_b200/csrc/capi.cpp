@@ -102,6 +102,8 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->batch_compact = 1;
     o->batch_sell = 1;
     o->scale_on_device = -1;
+    o->sell = -1;
+    o->reference_fixed_columns = 0;
 }
 
 const char* pdlpx_error_string(int32_t code) {
@@ -319,9 +321,19 @@ int32_t pdlpx_get_scaling(const pdlpx_solver* h, double* col_scale, double* csca
     return PDLPX_OK;
 }
 
-int32_t pdlpx_time_kernels(pdlpx_solver* h, int32_t reps, double* ms_primal, double* ms_dual, double* ms_check) {
+int32_t pdlpx_time_kernels(pdlpx_solver* h, int32_t precision, int32_t reps, int64_t flush_bytes, double* ms_primal,
+                           double* ms_dual, double* ms_check) {
     if (h == nullptr) return PDLPX_E_INVALID;
-    return guarded(h, [&] { return h->engine.timeKernels(reps, ms_primal, ms_dual, ms_check); });
+    return guarded(h, [&] {
+        return h->engine.timeKernels(precision, reps, flush_bytes, ms_primal, ms_dual, ms_check);
+    });
+}
+
+int32_t pdlpx_get_step_times(const pdlpx_solver* h, int32_t precision, double* ms_primal, double* ms_dual,
+                             int32_t* samples) {
+    if (h == nullptr || (precision != PDLPX_PREC_MIXED && precision != PDLPX_PREC_FP64)) return PDLPX_E_INVALID;
+    h->engine.stepTimes(precision, ms_primal, ms_dual, samples);
+    return PDLPX_OK;
 }
 
 int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t* group_at, int32_t* blocks_primal,

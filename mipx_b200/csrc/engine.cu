@@ -127,6 +127,29 @@ __global__ void __launch_bounds__(kBlock) powerFinish2(PowerArgs a) {
     }
 }
 
+// ---- sliced-ELL step launches ------------------------------------------------
+// The short rows [begin, end) of a matrix side stored as sliced ELL (slice s of
+// the range described by hdr[s]); one thread per row, the fused step of
+// kernels.cuh.  Compiled for 8 resident blocks (32 registers), the occupancy
+// at which the packed batch's sliced-ELL kernels measured fastest.
+template <int U, class T>
+__global__ void __launch_bounds__(kBlock, 8) primalSellStep(IterArgs<T> p, const int2* __restrict__ hdr,
+                                                            const int* __restrict__ idx, const T* __restrict__ val,
+                                                            int koff, int begin, int end) {
+    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    primalSellFrom<U, T>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+}
+
+template <int U, class T>
+__global__ void __launch_bounds__(kBlock, 8) dualSellStep(IterArgs<T> p, const int2* __restrict__ hdr,
+                                                          const int* __restrict__ idx, const T* __restrict__ val,
+                                                          int koff, int begin, int end) {
+    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    dualSellFrom<U, T>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+}
+
 static int gridFor(int64_t rows, int G) {
     const int64_t threads = rows * G;
     return static_cast<int>(std::max<int64_t>(1, (threads + kBlock - 1) / kBlock));
@@ -165,8 +188,24 @@ struct DeviceLp {
     // the device numbering and get their own launches: lane counts gLA / gLAT,
     // step shapes shapeLD / shapeLP; the other rows use gA / gAT, shapeD / shapeP.
     int nlD = 0, nlP = 0, gLA = 1, gLAT = 1, shapeLD = 0, shapeLP = 0;
+    int64_t zlD = 0, zlP = 0;  // entries of the long rows
     int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
     std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
+    // Sides stored as sliced ELL (shapeP / shapeD >= kNumShapes): their short
+    // rows [nl, rows) in 32-row slices; the CSR arrays stay for the long rows,
+    // the check pass and the power iteration.
+    int2* sp_hdr = nullptr;  // A^T short rows (primal step)
+    int* sp_idx = nullptr;
+    float* sp_v32 = nullptr;
+    double* sp_v64 = nullptr;
+    int2* sd_hdr = nullptr;  // A short rows (dual step)
+    int* sd_idx = nullptr;
+    float* sd_v32 = nullptr;
+    double* sd_v64 = nullptr;
+    // CUDA events recorded inside the cycle graphs around the primal and dual
+    // step of iteration kev_iter of every cycle: [FP32 / FP64 graph][3]
+    cudaEvent_t kev[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int kev_iter = 1;
 
     int *a_ptr = nullptr, *a_idx = nullptr, *at_ptr = nullptr, *at_idx = nullptr;
     float *a_v32 = nullptr, *at_v32 = nullptr;
@@ -206,6 +245,9 @@ struct DeviceLp {
     ~DeviceLp() {
         for (auto& g : cycle)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& row : kev)
+            for (auto& e : row)
+                if (e) cudaEventDestroy(e);
         if (power) cudaGraphExecDestroy(power);
         if (arena) cudaFree(arena);
         if (h_st) cudaFreeHost(h_st);
@@ -330,6 +372,42 @@ IterArgs<double> iterArgs<double>(const DeviceLp& d, const pdlpx_options& o) {
     return d.iter64(o);
 }
 
+// Sliced-ELL values of a side in storage type T.
+template <class T>
+const T* sellVals(const DeviceLp& d, bool primal);
+template <>
+const float* sellVals<float>(const DeviceLp& d, bool primal) {
+    return primal ? d.sp_v32 : d.sd_v32;
+}
+template <>
+const double* sellVals<double>(const DeviceLp& d, bool primal) {
+    return primal ? d.sp_v64 : d.sd_v64;
+}
+
+static int sellGrid(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kBlock - 1) / kBlock)); }
+
+// Short-row launch of one side in `shape` (CSR, or sliced ELL when isSell).
+template <class T>
+void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
+    if (isSell(shape)) {
+        PDLPX_SELL_SWITCH(shape, (primalSellStep<UU, T><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
+                                     ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n)));
+    } else {
+        PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<gridForShape(d.n - d.nlP, shape), kBlock, 0, s>>>(
+                                      ia, k, d.nlP, d.n)));
+    }
+}
+template <class T>
+void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
+    if (isSell(shape)) {
+        PDLPX_SELL_SWITCH(shape, (dualSellStep<UU, T><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
+                                     ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
+    } else {
+        PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<gridForShape(d.m - d.nlD, shape), kBlock, 0, s>>>(
+                                      ia, k, d.nlD, d.m)));
+    }
+}
+
 // Step launches of one iteration on each side: the long rows (if any), then the rest.
 template <class T>
 int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s) {
@@ -340,8 +418,7 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
         ++n;
     }
     if (d.n > d.nlP) {
-        PDLPX_SHAPE_SWITCH(d.shapeP, (primalStep<GG, RR, UU, T><<<gridForShape(d.n - d.nlP, d.shapeP), kBlock, 0, s>>>(
-                                         ia, k, d.nlP, d.n)));
+        launchPrimalShort<T>(d, ia, d.shapeP, k, s);
         ++n;
     }
     return n;
@@ -355,8 +432,7 @@ int launchDual(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s) 
         ++n;
     }
     if (d.m > d.nlD) {
-        PDLPX_SHAPE_SWITCH(d.shapeD, (dualStep<GG, RR, UU, T><<<gridForShape(d.m - d.nlD, d.shapeD), kBlock, 0, s>>>(
-                                         ia, k, d.nlD, d.m)));
+        launchDualShort<T>(d, ia, d.shapeD, k, s);
         ++n;
     }
     return n;
@@ -385,9 +461,18 @@ int launchCycle(DeviceLp& d, const pdlpx_options& o) {
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
     int launches = 0;
+    const int p = sizeof(T) == 8 ? 1 : 0;
+    // Live step timing: under capture, an event recorded with the External flag
+    // becomes an event-record node of the graph (a plain record would only
+    // mark a dependency), so every replay records it on the device.
+    auto mark = [&](cudaEvent_t e) { cudaEventRecordWithFlags(e, s, cudaEventRecordExternal); };
     for (int k = 1; k <= o.termination_eval_frequency; ++k) {
+        const bool timed = k == d.kev_iter && d.kev[p][0] != nullptr;
+        if (timed) mark(d.kev[p][0]);
         launches += launchPrimal<T>(d, ia, k, s);
+        if (timed) mark(d.kev[p][1]);
         launches += launchDual<T>(d, ia, k, s);
+        if (timed) mark(d.kev[p][2]);
     }
     launches += launchChecks<T>(d, ca, s) - 2;
     controller<<<1, kBlock, 0, s>>>(d.st, d.dc, d.part_rows, d.part_cols, sizeof(T) == 8 ? 1 : 0);
@@ -477,24 +562,100 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
 
 }  // namespace
 
-// Rows of one matrix side far longer than the rest (more entries than
-// max(64, 8 x the mean)): the renumbering that puts them first, longest first,
-// the other rows after them in their original order.  Returns their count
-// (0 and an empty order: no such rows, identity).
-static int32_t longRowsFirst(const Csr& a, std::vector<int32_t>& order) {
+// Rows per window inside which a sliced-ELL side's short rows are sorted by
+// length: slices of 32 rows then hold rows of nearly equal length (on the
+// 500k x 2M power-law LP 5% padding, against 100% for 256-row windows), while
+// every row stays within 4096 places of where it was, so whatever locality
+// the other side's gathers had survives the renumbering.
+constexpr int32_t kSellWindow = 4096;
+
+// Device numbering of one matrix side's rows.  Rows far longer than the rest
+// (more entries than max(64, 8 x the mean)) come first, longest first; the
+// other rows follow -- sorted by length (longest first, stable) inside windows
+// of kSellWindow rows when the side is stored as sliced ELL, else in their
+// original order.  `sell_opt` is the option (-1 automatic: sliced ELL when the
+// short rows' mean length is at most 64; 1 whenever there are short rows;
+// 0 never); `sell` receives the decision.  Returns the number of long rows;
+// `order` stays empty for the identity.
+static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int32_t>& order) {
     order.clear();
+    sell = false;
     const int32_t rows = a.rows;
     if (rows == 0) return 0;
     const double mean = static_cast<double>(a.nnz()) / rows;
     const int32_t thr = std::max<int32_t>(64, static_cast<int32_t>(8.0 * mean));
     std::vector<int32_t> lng, sht;
-    for (int32_t i = 0; i < rows; ++i) (a.ptr[i + 1] - a.ptr[i] > thr ? lng : sht).push_back(i);
-    if (lng.empty()) return 0;
-    std::stable_sort(lng.begin(), lng.end(),
-                     [&](int32_t x, int32_t y) { return a.ptr[x + 1] - a.ptr[x] > a.ptr[y + 1] - a.ptr[y]; });
+    int64_t zs = 0;
+    for (int32_t i = 0; i < rows; ++i) {
+        const int32_t len = a.ptr[i + 1] - a.ptr[i];
+        if (len > thr) {
+            lng.push_back(i);
+        } else {
+            sht.push_back(i);
+            zs += len;
+        }
+    }
+    auto len = [&](int32_t x) { return a.ptr[x + 1] - a.ptr[x]; };
+    if (!sht.empty())
+        sell = sell_opt > 0 || (sell_opt < 0 && static_cast<double>(zs) <= 64.0 * static_cast<double>(sht.size()));
+    if (sell) {
+        for (size_t w0 = 0; w0 < sht.size(); w0 += kSellWindow) {
+            const size_t w1 = std::min(sht.size(), w0 + kSellWindow);
+            std::stable_sort(sht.begin() + w0, sht.begin() + w1, [&](int32_t x, int32_t y) { return len(x) > len(y); });
+        }
+    }
+    std::stable_sort(lng.begin(), lng.end(), [&](int32_t x, int32_t y) { return len(x) > len(y); });
+    bool identity = true;
+    for (size_t k = 0; k < sht.size() && identity; ++k) identity = sht[k] == static_cast<int32_t>(lng.size() + k);
+    if (lng.empty() && identity) return 0;
     order = lng;
     order.insert(order.end(), sht.begin(), sht.end());
     return static_cast<int32_t>(lng.size());
+}
+
+// Sliced ELL of rows [r0, a.rows) of a (device numbering): slice s holds rows
+// r0 + 32 s .. r0 + 32 s + 31, entry k of lane l at hdr[s].x + 32 k + l, padded
+// with index 0 / value 0 to the slice's longest row (hdr[s].y).  False when the
+// padded entries would not fit 32-bit offsets (the side then keeps CSR).
+struct SellHost {
+    std::vector<int2> hdr;
+    std::vector<int32_t> idx;
+    std::vector<double> val;
+};
+static bool buildSell(const Csr& a, int32_t r0, SellHost& h) {
+    const int64_t rows = static_cast<int64_t>(a.rows) - r0;
+    const int64_t slices = (rows + kSlice - 1) / kSlice;
+    h.hdr.resize(static_cast<size_t>(slices));
+    int64_t e = 0;
+    for (int64_t s = 0; s < slices; ++s) {
+        int32_t w = 0;
+        for (int64_t r = s * kSlice; r < std::min<int64_t>(rows, (s + 1) * kSlice); ++r)
+            w = std::max(w, a.ptr[r0 + r + 1] - a.ptr[r0 + r]);
+        h.hdr[static_cast<size_t>(s)] = make_int2(static_cast<int>(e), w);
+        e += static_cast<int64_t>(w) * kSlice;
+        if (e > std::numeric_limits<int32_t>::max()) return false;
+    }
+    h.idx.assign(static_cast<size_t>(e), 0);
+    h.val.assign(static_cast<size_t>(e), 0.0);
+    for (int64_t r = 0; r < rows; ++r) {
+        const int64_t first = h.hdr[static_cast<size_t>(r / kSlice)].x + (r % kSlice);
+        const int32_t b = a.ptr[r0 + r], cnt = a.ptr[r0 + r + 1] - b;
+        for (int32_t k = 0; k < cnt; ++k) {
+            const size_t at = static_cast<size_t>(first + static_cast<int64_t>(k) * kSlice);
+            h.idx[at] = a.idx[b + k];
+            h.val[at] = a.val[b + k];
+        }
+    }
+    return true;
+}
+
+// Sliced-ELL shape of a side from the options: a pinned sliced-ELL shape
+// (kNumShapes + 1 .. kNumShapes + kNumSell), else 4 entries per round for mean
+// lengths up to 12 and 8 above (the packed batch's measured picks).
+static int sellShape(int pinned, int64_t nnz, int32_t rows) {
+    if (pinned > kNumShapes && pinned <= kNumShapes + kNumSell) return pinned - 1;
+    const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
+    return kNumShapes + (mean <= 12.0 ? 0 : 1);
 }
 
 // The scaled LP with its rows in order `ro` and columns in order `co` (new
@@ -581,26 +742,42 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.device = dev;
     PDLPX_CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
     PDLPX_CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
-    // Skewed sides: long rows first in the device numbering (identity otherwise).
+    // Device numbering: long rows first, sliced-ELL sides' short rows sorted by
+    // length (identity where neither applies).  A side whose shape or lane
+    // count is pinned to CSR keeps CSR.
     std::vector<int32_t> ro, co;
-    d.nlD = longRowsFirst(sc_in.a, ro);
-    d.nlP = longRowsFirst(sc_in.at, co);
+    const int sellD_opt = (o.spmv_group_a > 0 || (o.shape_dual > 0 && o.shape_dual <= kNumShapes)) ? 0
+                          : o.shape_dual > kNumShapes                                         ? 1
+                                                                                               : o.sell;
+    const int sellP_opt = (o.spmv_group_at > 0 || (o.shape_primal > 0 && o.shape_primal <= kNumShapes)) ? 0
+                          : o.shape_primal > kNumShapes                                           ? 1
+                                                                                                   : o.sell;
+    bool sellD = false, sellP = false;
+    d.nlD = sideOrder(sc_in.a, sellD_opt, sellD, ro);
+    d.nlP = sideOrder(sc_in.at, sellP_opt, sellP, co);
+    const bool perm = !ro.empty() || !co.empty();
     ScaledLp permuted;
-    if (d.nlD > 0 || d.nlP > 0) permuteScaled(sc_in, ro, co, permuted, d.rpos, d.cpos);
-    const ScaledLp& sc = (d.nlD > 0 || d.nlP > 0) ? permuted : sc_in;
-    if (d.nlD == 0) d.rpos.clear();
-    if (d.nlP == 0) d.cpos.clear();
+    if (perm) permuteScaled(sc_in, ro, co, permuted, d.rpos, d.cpos);
+    const ScaledLp& sc = perm ? permuted : sc_in;
+    if (ro.empty()) d.rpos.clear();
+    if (co.empty()) d.cpos.clear();
+    SellHost hsP, hsD;
+    if (sellP && !buildSell(sc.at, d.nlP, hsP)) sellP = false;
+    if (sellD && !buildSell(sc.a, d.nlD, hsD)) sellD = false;
     d.m = sc.a.rows;
     d.n = sc.a.cols;
     d.nnz = sc.a.nnz();
     d.mixed = o.precision != PDLPX_PREC_FP64;
     const int64_t m = d.m, n = d.n, nnz = d.nnz;
     const int64_t zlD = d.nlD > 0 ? sc.a.ptr[d.nlD] : 0, zlP = d.nlP > 0 ? sc.at.ptr[d.nlP] : 0;
+    d.zlD = zlD;
+    d.zlP = zlP;
     const int32_t msD = d.m - d.nlD, msP = d.n - d.nlP;  // short rows
     d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz - zlD, msD);
     d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz - zlP, msP);
-    d.shapeD = chooseShape(o.shape_dual, o.spmv_group_a, nnz - zlD, msD);
-    d.shapeP = chooseShape(o.shape_primal, o.spmv_group_at, nnz - zlP, msP);
+    d.shapeD = sellD ? sellShape(o.shape_dual, nnz - zlD, msD) : chooseShape(o.shape_dual, o.spmv_group_a, nnz - zlD, msD);
+    d.shapeP = sellP ? sellShape(o.shape_primal, nnz - zlP, msP)
+                     : chooseShape(o.shape_primal, o.spmv_group_at, nnz - zlP, msP);
     d.gLA = d.nlD > 0 ? std::min(256, pickGroup(zlD, d.nlD)) : 1;
     d.gLAT = d.nlP > 0 ? std::min(256, pickGroup(zlP, d.nlP)) : 1;
     d.shapeLD = longShape(zlD, d.nlD);
@@ -643,6 +820,12 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     const size_t o_pi_x = take(8 * n), o_pi_y = take(8 * m), o_pi_xn = take(8 * n),
                  o_pi_part = take(8 * 2 * d.nb_pi);
     const size_t o_prow = take(8 * kRowSlots * d.nb_rows), o_pcol = take(8 * kColSlots * d.nb_cols);
+    // sliced-ELL sides: slice headers, indices, FP64 values, FP32 values (mixed)
+    const size_t eP = hsP.idx.size(), eD = hsD.idx.size();
+    const size_t o_sp_hdr = sellP ? take(8 * hsP.hdr.size()) : 0, o_sp_idx = sellP ? take(4 * eP) : 0,
+                 o_sp_v64 = sellP ? take(8 * eP) : 0, o_sp_v32 = sellP && mixed ? take(4 * eP) : 0;
+    const size_t o_sd_hdr = sellD ? take(8 * hsD.hdr.size()) : 0, o_sd_idx = sellD ? take(4 * eD) : 0,
+                 o_sd_v64 = sellD ? take(8 * eD) : 0, o_sd_v32 = sellD && mixed ? take(4 * eD) : 0;
     // Anderson ring (2 w (n + m) doubles), extrapolation scratch, partials, Gram matrix.
     d.aa_w = o.anderson_acceleration && o.anderson_window_size >= 2 ? o.anderson_window_size : 0;
     const size_t dim = static_cast<size_t>(n) + static_cast<size_t>(m);
@@ -710,6 +893,21 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.pi_part = reinterpret_cast<double*>(b + o_pi_part);
     d.part_rows = reinterpret_cast<double*>(b + o_prow);
     d.part_cols = reinterpret_cast<double*>(b + o_pcol);
+    if (sellP) {
+        d.sp_hdr = reinterpret_cast<int2*>(b + o_sp_hdr);
+        d.sp_idx = reinterpret_cast<int*>(b + o_sp_idx);
+        d.sp_v64 = reinterpret_cast<double*>(b + o_sp_v64);
+        if (mixed) d.sp_v32 = reinterpret_cast<float*>(b + o_sp_v32);
+    }
+    if (sellD) {
+        d.sd_hdr = reinterpret_cast<int2*>(b + o_sd_hdr);
+        d.sd_idx = reinterpret_cast<int*>(b + o_sd_idx);
+        d.sd_v64 = reinterpret_cast<double*>(b + o_sd_v64);
+        if (mixed) d.sd_v32 = reinterpret_cast<float*>(b + o_sd_v32);
+    }
+    d.kev_iter = o.termination_eval_frequency >= 2 ? 2 : 1;
+    for (auto& row : d.kev)
+        for (auto& e : row) PDLPX_CK(cudaEventCreate(&e));
     if (d.aa_w > 0) {
         d.aa_X = reinterpret_cast<double*>(b + o_aa[0]);
         d.aa_R = reinterpret_cast<double*>(b + o_aa[1]);
@@ -750,6 +948,23 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         PDLPX_CK(up(d.rp32, rp.data(), 16 * m));
         PDLPX_CK(cudaStreamSynchronize(s));
     }
+    // sliced-ELL sides (each host buffer is released once its copy is done)
+    auto upSell = [&](SellHost& h, int2* hdr, int* idx, double* v64, float* v32) -> cudaError_t {
+        cudaError_t e;
+        if ((e = up(hdr, h.hdr.data(), 8 * h.hdr.size())) != cudaSuccess) return e;
+        if ((e = up(idx, h.idx.data(), 4 * h.idx.size())) != cudaSuccess) return e;
+        if ((e = up(v64, h.val.data(), 8 * h.val.size())) != cudaSuccess) return e;
+        if (v32 != nullptr) {
+            std::vector<float> f(h.val.begin(), h.val.end());
+            if ((e = up(v32, f.data(), 4 * f.size())) != cudaSuccess) return e;
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        h = SellHost{};
+        return cudaSuccess;
+    };
+    if (sellP) PDLPX_CK(upSell(hsP, d.sp_hdr, d.sp_idx, d.sp_v64, d.sp_v32));
+    if (sellD) PDLPX_CK(upSell(hsD, d.sd_hdr, d.sd_idx, d.sd_v64, d.sd_v32));
     {
         std::vector<ColPack<double>> cp;
         std::vector<RowPack<double>> rp;
@@ -807,15 +1022,21 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
             cudaEventDestroy(b);
         }
     } guard{e0, e1};
-    auto timeShape = [&](bool primal, int shape, float& ms) -> int32_t {
-        const int grid = primal ? gridForShape(d.n - d.nlP, shape) : gridForShape(d.m - d.nlD, shape);
+    // which: 0 primal short rows, 1 dual short rows, 2 primal long rows, 3 dual long rows
+    auto timeShape = [&](int which, int shape, float& ms) -> int32_t {
         constexpr int reps = 5;
         for (int r = 0; r <= reps; ++r) {
             if (r == 1) PDLPX_CK(cudaEventRecord(e0, s));
-            if (primal) {
-                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1, d.nlP, d.n)));
+            if (which == 0) {
+                launchPrimalShort<T>(d, ia, shape, 1, s);
+            } else if (which == 1) {
+                launchDualShort<T>(d, ia, shape, 1, s);
+            } else if (which == 2) {
+                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<gridForShape(d.nlP, shape), kBlock, 0, s>>>(
+                                              ia, 1, 0, d.nlP)));
             } else {
-                PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<grid, kBlock, 0, s>>>(ia, 1, d.nlD, d.m)));
+                PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<gridForShape(d.nlD, shape), kBlock, 0, s>>>(
+                                              ia, 1, 0, d.nlD)));
             }
         }
         PDLPX_CK(cudaEventRecord(e1, s));
@@ -828,14 +1049,41 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
         const bool primal = pass == 0;
         if ((primal && !tune_p) || (!primal && !tune_d)) continue;
         int& pick = primal ? d.shapeP : d.shapeD;
-        const int g0 = kShapes[pick].G;
+        const int which = primal ? 0 : 1;
+        // candidates: the sliced-ELL variants where the side has them, and the
+        // CSR shapes within 4x of the row-length table's lane count (the CSR
+        // arrays cover the same rows in the same numbering)
+        const bool has_sell = primal ? d.sp_hdr != nullptr : d.sd_hdr != nullptr;
+        const int64_t rows = primal ? d.n - d.nlP : d.m - d.nlD;
+        const int64_t zshort = primal ? d.nnz - d.zlP : d.nnz - d.zlD;
+        const int g0 = kShapes[defaultShape(zshort, static_cast<int32_t>(rows))].G;
         float best = 0.0f;
-        int32_t rc = timeShape(primal, pick, best);
+        int32_t rc = timeShape(which, pick, best);
+        if (rc != PDLPX_OK) return rc;
+        for (int c = 0; c < kNumShapes + (has_sell ? kNumSell : 0); ++c) {
+            if (c == pick || (!isSell(c) && (kShapes[c].G * 4 < g0 || kShapes[c].G > g0 * 4))) continue;
+            float ms = 0.0f;
+            rc = timeShape(which, c, ms);
+            if (rc != PDLPX_OK) return rc;
+            if (ms < 0.97f * best) {
+                best = ms;
+                pick = c;
+            }
+        }
+    }
+    // long rows (their own launches): the CSR shapes with 8 or more lanes per row
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool primal = pass == 0;
+        if ((primal && (!tune_p || d.nlP == 0)) || (!primal && (!tune_d || d.nlD == 0))) continue;
+        int& pick = primal ? d.shapeLP : d.shapeLD;
+        const int which = primal ? 2 : 3;
+        float best = 0.0f;
+        int32_t rc = timeShape(which, pick, best);
         if (rc != PDLPX_OK) return rc;
         for (int c = 0; c < kNumShapes; ++c) {
-            if (c == pick || kShapes[c].G * 4 < g0 || kShapes[c].G > g0 * 4) continue;
+            if (c == pick || kShapes[c].G < 8) continue;
             float ms = 0.0f;
-            rc = timeShape(primal, c, ms);
+            rc = timeShape(which, c, ms);
             if (rc != PDLPX_OK) return rc;
             if (ms < 0.97f * best) {
                 best = ms;
@@ -1184,6 +1432,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     dc.nb_rows = d.nb_rows;
     dc.nb_cols = d.nb_cols;
     dc.stall_limit = 10;
+    dc.ref_fixed = opt_.reference_fixed_columns != 0;
     dc.primal_tol = opt_.primal_tol;
     dc.dual_tol = opt_.dual_tol;
     dc.opt_tol = opt_.optimality_tol;
@@ -1291,6 +1540,11 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     bool stopped = false;
     int switch_total = -1;
     int prec = d.mixed ? 0 : 1;
+    int prev_total = 0;
+    for (int p = 0; p < 2; ++p) {
+        step_ms_[p][0] = step_ms_[p][1] = 0.0;
+        step_samples_[p] = 0;
+    }
     while (true) {
         if (timeUp(t0, opt_.max_solve_seconds)) break;
         if (stopRequested()) {
@@ -1304,6 +1558,19 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
         PDLPX_CK(cudaMemcpyAsync(d.h_st, d.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
         PDLPX_CK(cudaStreamSynchronize(s));
         const DevState& h = *d.h_st;
+        if (h.total - prev_total >= d.kev_iter) {
+            // the timed iteration ran in full: read the step kernels' events of this cycle
+            float a = 0.0f, b = 0.0f;
+            if (cudaEventElapsedTime(&a, d.kev[prec][0], d.kev[prec][1]) == cudaSuccess &&
+                cudaEventElapsedTime(&b, d.kev[prec][1], d.kev[prec][2]) == cudaSuccess) {
+                step_ms_[prec][0] += a;
+                step_ms_[prec][1] += b;
+                ++step_samples_[prec];
+            } else {
+                (void)cudaGetLastError();
+            }
+        }
+        prev_total = h.total;
         if (opt_.verbose && (h.total <= N || h.total % (10 * N) == 0)) {
             std::printf("PDLP %7d  pobj=% .8e  pinf=% .2e  dinf=% .2e  gap=% .2e  fpe=% .2e  pw=% .2e  step=% .2e  [B200%s]\n",
                         h.total, h.pobj, h.pterm, h.dterm, h.gap, h.fpe, h.pw, h.step,
@@ -1401,43 +1668,84 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
 }
 
 // ---------------------------------------------------------------------------
-// Kernel timing (roofline numerator): eager launches between CUDA events on the
-// engine's stream, on a scratch copy of the solver state so that the step
-// kernels are active; the saved state is restored afterwards.
+// Kernel timing (roofline numerator): eager launches on the engine's stream, on
+// a scratch copy of the solver state so that the step kernels of precision T
+// are active; the saved state is restored afterwards.  The steps run as PDHG
+// iterations (primal, dual, primal, ...) with an event between every two
+// launches, so each kernel sees the cache state of the solve loop; with
+// flush_bytes > 0 a write of that many bytes precedes every iteration (outside
+// the timed intervals) and each iteration starts from an evicted L2.
 // ---------------------------------------------------------------------------
 namespace {
 template <class T>
-int32_t timeStepKernels(DeviceLp& d, const pdlpx_options& o, int reps, float ms[3], std::string& err) {
+int32_t timeStepKernels(DeviceLp& d, const pdlpx_options& o, int reps, int64_t flush_bytes, double ms[3],
+                        std::string& err) {
     const IterArgs<T> ia = iterArgs<T>(d, o);
     const CheckArgs<T> ca = d.check<T>(ia.xh, ia.xi, ia.yh, ia.yi);
     cudaStream_t s = d.stream;
-    cudaEvent_t ev[4];
+    std::vector<cudaEvent_t> ev(3 * static_cast<size_t>(reps) + 2, nullptr);
+    struct Guard {
+        std::vector<cudaEvent_t>& e;
+        void* flush = nullptr;
+        cudaStream_t s = nullptr;
+        ~Guard() {
+            for (auto x : e)
+                if (x) cudaEventDestroy(x);
+            if (flush) cudaFreeAsync(flush, s);
+        }
+    } guard{ev, nullptr, s};
     for (auto& e : ev) PDLPX_CK(cudaEventCreate(&e));
-    // warm-up launch of each; a step's time covers its long- and short-row launches
+    if (flush_bytes > 0) PDLPX_CK(cudaMallocAsync(&guard.flush, static_cast<size_t>(flush_bytes), s));
+    // warm-up iteration; a step's time covers its long- and short-row launches
     launchPrimal<T>(d, ia, 1, s);
     launchDual<T>(d, ia, 1, s);
-    PDLPX_CK(cudaEventRecord(ev[0], s));
-    for (int r = 0; r < reps; ++r) launchPrimal<T>(d, ia, 1, s);
-    PDLPX_CK(cudaEventRecord(ev[1], s));
-    for (int r = 0; r < reps; ++r) launchDual<T>(d, ia, 1, s);
-    PDLPX_CK(cudaEventRecord(ev[2], s));
-    for (int r = 0; r < reps; ++r) launchChecks<T>(d, ca, s);
-    PDLPX_CK(cudaEventRecord(ev[3], s));
+    for (int r = 0; r < reps; ++r) {
+        if (guard.flush) PDLPX_CK(cudaMemsetAsync(guard.flush, r & 0xff, static_cast<size_t>(flush_bytes), s));
+        PDLPX_CK(cudaEventRecord(ev[3 * r], s));
+        launchPrimal<T>(d, ia, 1, s);
+        PDLPX_CK(cudaEventRecord(ev[3 * r + 1], s));
+        launchDual<T>(d, ia, 1, s);
+        PDLPX_CK(cudaEventRecord(ev[3 * r + 2], s));
+    }
+    const size_t c0 = 3 * static_cast<size_t>(reps);
+    PDLPX_CK(cudaEventRecord(ev[c0], s));
+    launchChecks<T>(d, ca, s);
+    PDLPX_CK(cudaEventRecord(ev[c0 + 1], s));
     PDLPX_CK(cudaGetLastError());
-    PDLPX_CK(cudaEventSynchronize(ev[3]));
-    for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
-    for (auto& e : ev) cudaEventDestroy(e);
+    PDLPX_CK(cudaEventSynchronize(ev[c0 + 1]));
+    ms[0] = ms[1] = ms[2] = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        float a = 0.0f, b = 0.0f;
+        PDLPX_CK(cudaEventElapsedTime(&a, ev[3 * r], ev[3 * r + 1]));
+        PDLPX_CK(cudaEventElapsedTime(&b, ev[3 * r + 1], ev[3 * r + 2]));
+        ms[0] += a;
+        ms[1] += b;
+    }
+    float c = 0.0f;
+    PDLPX_CK(cudaEventElapsedTime(&c, ev[c0], ev[c0 + 1]));
+    ms[0] /= reps;
+    ms[1] /= reps;
+    ms[2] = c;
     return PDLPX_OK;
 }
 }  // namespace
 
-int32_t Engine::timeKernels(int32_t reps, double* ms_primal, double* ms_dual, double* ms_check) {
+int32_t Engine::timeKernels(int32_t precision, int32_t reps, int64_t flush_bytes, double* ms_primal, double* ms_dual,
+                            double* ms_check) {
     std::string& err = last_error;
     if (!dev_ || !used_gpu_) {
         err = "time_kernels needs a completed device solve";
         return PDLPX_E_NOT_LOADED;
     }
     if (reps <= 0) reps = 1;
+    if (precision != -1 && precision != PDLPX_PREC_MIXED && precision != PDLPX_PREC_FP64) {
+        err = "time_kernels: precision must be PDLPX_PREC_MIXED, PDLPX_PREC_FP64 or -1";
+        return PDLPX_E_INVALID;
+    }
+    if (precision == PDLPX_PREC_MIXED && !dev_->mixed) {
+        err = "time_kernels: the FP32 kernels need a mixed-precision solve";
+        return PDLPX_E_INVALID;
+    }
     DeviceLp& d = *dev_;
     PDLPX_CK(cudaSetDevice(d.device));
     cudaStream_t s = d.stream;
@@ -1449,27 +1757,29 @@ int32_t Engine::timeKernels(int32_t reps, double* ms_primal, double* ms_dual, do
     t.phase = 0;
     t.total = 0;
     t.inner = 0;
+    if (precision != -1) t.prec = precision == PDLPX_PREC_FP64 ? 1 : 0;
     *d.h_st = t;
     PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
-    float ms[3] = {0, 0, 0};
-    const int32_t rc = t.prec == 0 ? timeStepKernels<float>(d, opt_, reps, ms, err)
-                                   : timeStepKernels<double>(d, opt_, reps, ms, err);
+    double ms[3] = {0, 0, 0};
+    const int32_t rc = t.prec == 0 ? timeStepKernels<float>(d, opt_, reps, flush_bytes, ms, err)
+                                   : timeStepKernels<double>(d, opt_, reps, flush_bytes, ms, err);
     *d.h_st = saved;
     PDLPX_CK(cudaMemcpyAsync(d.st, d.h_st, sizeof(DevState), cudaMemcpyHostToDevice, s));
     PDLPX_CK(cudaStreamSynchronize(s));
     if (rc != PDLPX_OK) return rc;
-    if (ms_primal) *ms_primal = ms[0] / reps;
-    if (ms_dual) *ms_dual = ms[1] / reps;
-    if (ms_check) *ms_check = ms[2] / reps;
+    if (ms_primal) *ms_primal = ms[0];
+    if (ms_dual) *ms_dual = ms[1];
+    if (ms_check) *ms_check = ms[2];
     return PDLPX_OK;
 }
 
 int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const {
     if (!dev_) return PDLPX_E_NOT_LOADED;
-    if (ga) *ga = kShapes[dev_->shapeD].G;
-    if (gat) *gat = kShapes[dev_->shapeP].G;
-    if (bp) *bp = gridForShape(dev_->n - dev_->nlP, dev_->shapeP);
-    if (bd) *bd = gridForShape(dev_->m - dev_->nlD, dev_->shapeD);
+    const DeviceLp& d = *dev_;
+    if (ga) *ga = isSell(d.shapeD) ? 1 : kShapes[d.shapeD].G;
+    if (gat) *gat = isSell(d.shapeP) ? 1 : kShapes[d.shapeP].G;
+    if (bp) *bp = isSell(d.shapeP) ? sellGrid(d.n - d.nlP) : gridForShape(d.n - d.nlP, d.shapeP);
+    if (bd) *bd = isSell(d.shapeD) ? sellGrid(d.m - d.nlD) : gridForShape(d.m - d.nlD, d.shapeD);
     return PDLPX_OK;
 }
 

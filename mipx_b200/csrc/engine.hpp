@@ -60,8 +60,18 @@ public:
     void setColBounds(int32_t col, double lo, double up);
     void setObjective(const double* obj, int32_t n);
 
-    // Kernel timing for the roofline report (pdlpx_time_kernels).
-    int32_t timeKernels(int32_t reps, double* ms_primal, double* ms_dual, double* ms_check);
+    // Kernel timing for the roofline report (pdlpx_time_kernels): precision
+    // PDLPX_PREC_MIXED / PDLPX_PREC_FP64 / -1 (the last solve's final one).
+    int32_t timeKernels(int32_t precision, int32_t reps, int64_t flush_bytes, double* ms_primal, double* ms_dual,
+                        double* ms_check);
+    // Step-kernel times sampled inside the last solve (pdlpx_get_step_times).
+    void stepTimes(int32_t precision, double* ms_primal, double* ms_dual, int32_t* samples) const {
+        const int p = precision == PDLPX_PREC_FP64 ? 1 : 0;
+        const int k = step_samples_[p];
+        if (ms_primal) *ms_primal = k > 0 ? step_ms_[p][0] / k : 0.0;
+        if (ms_dual) *ms_dual = k > 0 ? step_ms_[p][1] / k : 0.0;
+        if (samples) *samples = k;
+    }
     int32_t launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const;
 
     std::string last_error;
@@ -86,6 +96,8 @@ private:
     int32_t iterations_ = 0;
     bool used_gpu_ = false;
     std::vector<double> x_orig_, y_orig_;
+    double step_ms_[2][2] = {{0, 0}, {0, 0}};  // [FP32 / FP64 kernels][primal / dual] sums of the last solve
+    int step_samples_[2] = {0, 0};
 
     std::unique_ptr<DeviceLp> dev_;
 };

@@ -65,6 +65,7 @@ struct DevConst {
     int linf, update_pw, enable_polish, mixed, fp64_switch, adaptive, precond_refresh;
     int nb_rows, nb_cols;  // number of check partial blocks
     int stall_limit;
+    int ref_fixed;         // 1: a fixed column's dual residual as in the reference's check
     double primal_tol, dual_tol, opt_tol, polish_ptol, polish_dtol;
     double kp, ki, kd, ismooth, suff, nec, art;
     double c_norm, b_norm, obj_sign, obj_scale, con_scale, offset;
@@ -525,6 +526,76 @@ __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff, int 
                          koff);
 }
 
+// ---- sliced ELL (SELL-32) step ----------------------------------------------
+// A matrix side stored as 32-row slices: entry k of the slice's row `lane` sits
+// at hdr.x + k * 32 + lane, hdr.y is the slice's longest row, and shorter rows
+// are padded with index 0 / value 0 (index 0 exists whenever the side has a
+// column).  One thread owns one row, so a warp's load of its rows' k-th entries
+// is one coalesced request.  Used by the single-LP engine for its short rows
+// and by the packed batch for whole tiles.
+constexpr int kSlice = 32;           // rows per slice (one warp)
+constexpr int kSellU[] = {4, 8, 16};  // entries per thread per round of the variants
+constexpr int kNumSell = 3;
+
+// Dot product of this thread's row with x: entry k of the row sits at
+// hdr.x + k * 32 + lane; U entries are loaded per round, then their U gathers,
+// then the products are summed in entry order.
+// Entries past the row's end hold index 0 and value 0 (index 0 always exists).
+template <int U, class V, class X>
+__device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* __restrict__ val, int2 h, int lane,
+                                          const X* __restrict__ x) {
+    const int* ip = idx + h.x + lane;
+    const V* vp = val + h.x + lane;
+    double acc = 0.0;
+    for (int k0 = 0; k0 < h.y; k0 += U) {
+        int c[U];
+        V v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            const bool ok = k < h.y;
+            c[u] = ok ? __ldg(ip + k * kSlice) : 0;
+            v[u] = ok ? __ldg(vp + k * kSlice) : V(0);
+        }
+        X g[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) g[u] = __ldg(x + c[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc += static_cast<double>(v[u]) * static_cast<double>(g[u]);
+    }
+    return acc;
+}
+
+template <int U, class T>
+__device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
+                                               int koff) {
+    const ColPack<T> q = p.cp[j];
+    const double xc = p.xc[j];
+    const double xi = static_cast<double>(p.xi[j]);
+    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+    primalUpdate<T>(p, j, q, xc, xi, s, step, pw, lam, last);
+}
+
+template <int U, class T>
+__device__ __forceinline__ void dualSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int i, int2 h,
+                                             int koff) {
+    const RowPack<T> q = p.rp[i];
+    const double yc = p.yc[i];
+    const double yi = static_cast<double>(p.yi[i]);
+    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
+    bool last = false;
+    if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+    dualUpdate<T>(p, i, q, yc, yi, s, step, pw, lam, last);
+}
+
 // ---- block reduction of NS slots with per-slot operators -------------------
 template <int NS>
 __device__ __forceinline__ void blockReduceSlots(double (&acc)[NS], const int (&ops)[NS], double* out) {
@@ -613,9 +684,9 @@ __device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const De
     // no dual residual.  (The reference tests the lower bound first,
     // pdlp.cpp:1134-1140, and counts a negative reduced cost of a fixed column,
     // which never vanishes: LPs with fixed columns whose reduced cost is negative
-    // cannot reach its tolerance.)
+    // cannot reach its tolerance.  dc.ref_fixed = 1 restores that behaviour.)
     double dr;
-    if (hl && hu && lb == ub)
+    if (hl && hu && lb == ub && !dc.ref_fixed)
         dr = 0.0;
     else if (xh <= lbT + 1e-12 && hl)
         dr = fmin(g, 0.0);

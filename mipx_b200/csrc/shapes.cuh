@@ -42,6 +42,17 @@ namespace pdlpx {
     }
 static_assert(kNumShapes == 16, "shape switch covers 16 shapes");
 
+// Shape indices kNumShapes .. kNumShapes + kNumSell - 1 are the sliced-ELL
+// variants (one row per thread, kSellU entries per round).
+__host__ __device__ constexpr bool isSell(int shape) { return shape >= kNumShapes; }
+
+#define PDLPX_SELL_SWITCH(S, CALL)                                   \
+    switch (S - kNumShapes) {                                        \
+        case 0: { constexpr int UU = kSellU[0]; CALL; } break;       \
+        case 1: { constexpr int UU = kSellU[1]; CALL; } break;       \
+        default: { constexpr int UU = kSellU[2]; CALL; } break;      \
+    }
+
 // Rows one block of shape `shape` covers.
 inline int rowsPerBlock(int shape) { return (kBlock / kShapes[shape].G) * kShapes[shape].R; }
 

@@ -133,6 +133,8 @@ class PdlpOptions:
     batch_compact: bool = True
     batch_sell: bool = True
     scale_on_device: int = -1
+    sell: int = -1
+    reference_fixed_columns: bool = False
 
     def to_c(self) -> _capi.Options:
         # every field of pdlpx_options but `reserved` (zero) is set here, so no
@@ -405,11 +407,24 @@ class PdlpSolver:
         _capi.check(self._lib.pdlpx_used_gpu(self._h, C.byref(u)), self._h)
         return bool(u.value)
 
-    def timeKernels(self, reps: int = 20) -> dict:
-        """Average device ms per launch of the primal step, dual step and check pass."""
+    def timeKernels(self, reps: int = 20, precision: int = -1, flush_bytes: int = 0) -> dict:
+        """Average device ms per launch of the primal step, dual step (run as
+        `reps` interleaved PDHG iterations in `precision`: Precision.Mixed = the
+        FP32 kernels, Precision.FP64, -1 = the precision the solve ended in,
+        after an L2-evicting write of flush_bytes) and check pass."""
         a, b, c = C.c_double(), C.c_double(), C.c_double()
-        _capi.check(self._lib.pdlpx_time_kernels(self._h, int(reps), C.byref(a), C.byref(b), C.byref(c)), self._h)
+        _capi.check(self._lib.pdlpx_time_kernels(self._h, int(precision), int(reps), int(flush_bytes), C.byref(a),
+                                                 C.byref(b), C.byref(c)), self._h)
         return {"primal_ms": a.value, "dual_ms": b.value, "check_ms": c.value}
+
+    def stepTimes(self, precision: int) -> dict:
+        """Mean device ms of the primal and dual step measured inside the last
+        solve (one iteration per restart cycle), for Precision.Mixed (FP32
+        kernels) or Precision.FP64; samples = cycles measured."""
+        a, b, k = C.c_double(), C.c_double(), C.c_int32()
+        _capi.check(self._lib.pdlpx_get_step_times(self._h, int(precision), C.byref(a), C.byref(b), C.byref(k)),
+                    self._h)
+        return {"primal_ms": a.value, "dual_ms": b.value, "samples": k.value}
 
     def launchConfig(self) -> dict:
         ga, gat, bp, bd = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
