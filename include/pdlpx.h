@@ -178,6 +178,11 @@ const char* pdlpx_last_error(const pdlpx_solver* h);
 int32_t pdlpx_device_count(void);
 /* Library version string. */
 const char* pdlpx_version(void);
+/* Writes sizes[0..6) = sizeof of the ABI structures as compiled into the
+ * library, in the order pdlpx_options, pdlpx_result, pdlpx_lp, pdlpx_gen_lp,
+ * pdlpx_server_config, pdlpx_server_stats; bindings compare their own layouts
+ * against these. */
+void pdlpx_struct_sizes(int32_t* sizes);
 
 /* ---- single-LP solver (PdlpSolver : LpSolver) ---- */
 int32_t pdlpx_create(const pdlpx_options* opts, pdlpx_solver** out);
@@ -284,6 +289,24 @@ typedef struct pdlpx_lp {
 int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts,
                           pdlpx_result* results, double* const* x_out, double* const* y_out);
 
+/* ---- several GPUs: independent LPs sharded across devices ----
+ * No counterpart in the reference.  pdlpx_shard_lps assigns count LPs of the
+ * given non-negative weights to ndev devices by longest-processing-time bin
+ * packing: heaviest first, each onto the device with the least weight so far
+ * (ties to the lower device index, equal weights in input order), so the
+ * assignment is deterministic and balanced to within one LP's weight.
+ * device_of[count] receives indices in [0, ndev). */
+int32_t pdlpx_shard_lps(int32_t count, const int64_t* weights, int32_t ndev, int32_t* device_of);
+/* pdlpx_batch_solve over the CUDA devices devices[0..ndev): the LPs are
+ * sharded by per-iteration work (nnz + m + n) with pdlpx_shard_lps and each
+ * device solves its share with its own host thread, stream and packs; no data
+ * moves between devices and no collective runs.  Repeated ordinals are allowed
+ * (the shares then run side by side on one device).  Results as
+ * pdlpx_batch_solve, each identical to that LP's single-device result. */
+int32_t pdlpx_batch_solve_devices(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts,
+                                  const int32_t* devices, int32_t ndev, pdlpx_result* results,
+                                  double* const* x_out, double* const* y_out);
+
 /* ---- request server: LP solves as they arrive, continuously batched ----
  * No counterpart in the reference (the MIP search there calls PdlpSolver::solve
  * once per LP).  Submitted LPs are copied and scaled by a pool of host threads,
@@ -310,7 +333,12 @@ typedef struct pdlpx_server_config {
                               with the ticket's rows unchanged (a branch-and-bound node: new bounds,
                               appended rows) is solved in a family pack with the other nodes of that
                               ticket -- the shared rows stored once, FP64 iterates; 0: regular packs */
-    int32_t reserved[2];
+    int32_t num_devices;   /* 0 or 1: packs run on opts->device; k in 2..16: packs are placed on the
+                              CUDA devices devices[0..k), each pack on the listed device with a free
+                              stream and the fewest bytes in flight (max_packs streams and its own
+                              budget per device; no data moves between devices) */
+    int32_t reserved;
+    int32_t devices[16];
 } pdlpx_server_config;
 
 typedef struct pdlpx_server_stats {

@@ -20,10 +20,12 @@ from .pdlp import (  # noqa: F401
     csr_spmv,
     kInf,
     read_mps,
+    shard_lps,
     solve_mps,
 )
 
 __all__ = [
     "BasisStatus", "LpProblem", "LpResult", "PdlpOptimalityNorm", "PdlpOptions", "PdlpSolver", "Precision",
-    "Sense", "SparseMatrix", "Status", "StopFlag", "batch_solve", "csr_spmv", "kInf", "read_mps", "solve_mps",
+    "Sense", "SparseMatrix", "Status", "StopFlag", "batch_solve", "csr_spmv", "kInf", "read_mps", "shard_lps",
+    "solve_mps",
 ]

@@ -1,7 +1,8 @@
 """ctypes binding of ``include/pdlpx.h`` (the engine's C ABI).
 
 The structure layouts below mirror the header field for field; ``check_layout``
-compares their sizes with what the library reports through its own calls.
+compares their sizes with the sizes the library was compiled with
+(pdlpx_struct_sizes).
 Loading fails loudly when the library is missing: there is no Python or CPU
 stand-in for the device engine.
 """
@@ -73,7 +74,8 @@ class GenLp(C.Structure):
 # (name, restype, argtypes) of every entry point declared in include/pdlpx.h
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", f64), ("max_packs", i32), ("max_pack_lps", i32), ("prep_threads", i32),
-                ("queue_limit", i32), ("batch_window_ms", i32), ("families", i32), ("reserved", i32 * 2)]
+                ("queue_limit", i32), ("batch_window_ms", i32), ("families", i32), ("num_devices", i32),
+                ("reserved", i32), ("devices", i32 * 16)]
 
 
 class ServerStats(C.Structure):
@@ -88,6 +90,7 @@ SIGNATURES = [
     ("pdlpx_last_error", C.c_char_p, [C.c_void_p]),
     ("pdlpx_device_count", i32, []),
     ("pdlpx_version", C.c_char_p, []),
+    ("pdlpx_struct_sizes", None, [P_i32]),
     ("pdlpx_create", i32, [C.POINTER(Options), C.POINTER(C.c_void_p)]),
     ("pdlpx_destroy", i32, [C.c_void_p]),
     ("pdlpx_set_options", i32, [C.c_void_p, C.POINTER(Options)]),
@@ -114,6 +117,9 @@ SIGNATURES = [
     ("pdlpx_time_kernels", i32, [C.c_void_p, i32, i32, C.c_int64, P_f64, P_f64, P_f64]),
     ("pdlpx_get_step_times", i32, [C.c_void_p, i32, P_f64, P_f64, P_i32]),
     ("pdlpx_get_launch_config", i32, [C.c_void_p, P_i32, P_i32, P_i32, P_i32]),
+    ("pdlpx_shard_lps", i32, [i32, C.POINTER(C.c_int64), i32, P_i32]),
+    ("pdlpx_batch_solve_devices", i32, [i32, C.POINTER(Lp), C.POINTER(Options), P_i32, i32, C.POINTER(Result),
+                                        C.POINTER(P_f64), C.POINTER(P_f64)]),
     ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),
                                 C.POINTER(P_f64), C.POINTER(P_f64)]),
     ("pdlpx_server_config_default", None, [C.POINTER(ServerConfig)]),
@@ -160,7 +166,17 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         fn.restype = res
         fn.argtypes = args
     _lib = lib
+    check_layout()
     return lib
+
+
+def check_layout() -> None:
+    """Raise when a ctypes structure here differs in size from the library's."""
+    sizes = (C.c_int32 * 6)()
+    load().pdlpx_struct_sizes(sizes)
+    ours = [C.sizeof(t) for t in (Options, Result, Lp, GenLp, ServerConfig, ServerStats)]
+    if list(sizes) != ours:
+        raise RuntimeError(f"ABI structure sizes differ: library {list(sizes)}, binding {ours}")
 
 
 def default_options() -> Options:

@@ -1793,3 +1793,88 @@ int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, p
 }
 
 }  // namespace pdlpx
+
+namespace pdlpx {
+
+// Longest-processing-time sharding of independent LPs over ndev devices: the
+// heaviest LP first, each onto the device with the least weight assigned so far
+// (ties to the lower device index; equal weights keep input order), so the
+// assignment is deterministic and no device ends more than one LP's weight
+// above the least-loaded one.
+void shardLps(int32_t count, const int64_t* weights, int32_t ndev, int32_t* device_of) {
+    std::vector<int32_t> order(static_cast<size_t>(count));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return weights[a] > weights[b]; });
+    std::vector<int64_t> load(static_cast<size_t>(ndev), 0);
+    for (const int32_t k : order) {
+        const int32_t d = static_cast<int32_t>(std::min_element(load.begin(), load.end()) - load.begin());
+        device_of[k] = d;
+        load[static_cast<size_t>(d)] += weights[k];
+    }
+}
+
+// pdlpx_batch_solve over several devices: shard by per-iteration work (nonzeros
+// + rows + columns), one host thread per device solving its share with the
+// single-device batch path (its own stream, packs and budget).  No data moves
+// between devices; batch invariance makes every result identical to a
+// single-device solve of the same LP.
+int32_t batchSolveDevices(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, const int32_t* devices,
+                          int32_t ndev, pdlpx_result* results, double* const* x_out, double* const* y_out,
+                          std::string& err) {
+    std::vector<int64_t> w(static_cast<size_t>(count));
+    for (int32_t k = 0; k < count; ++k)
+        w[static_cast<size_t>(k)] = static_cast<int64_t>(lps[k].nnz) + lps[k].m + lps[k].n;
+    std::vector<int32_t> dev_of(static_cast<size_t>(count), 0);
+    shardLps(count, w.data(), ndev, dev_of.data());
+    struct Share {
+        std::vector<int32_t> index;
+        std::vector<pdlpx_lp> lps;
+        std::vector<pdlpx_result> res;
+        std::vector<double*> x, y;
+        int32_t rc = PDLPX_OK;
+        std::string err;
+    };
+    std::vector<Share> sh(static_cast<size_t>(ndev));
+    for (int32_t k = 0; k < count; ++k) {
+        Share& s = sh[static_cast<size_t>(dev_of[static_cast<size_t>(k)])];
+        s.index.push_back(k);
+        s.lps.push_back(lps[k]);
+        s.x.push_back(x_out ? x_out[k] : nullptr);
+        s.y.push_back(y_out ? y_out[k] : nullptr);
+    }
+    std::vector<std::thread> th;
+    for (int32_t d = 0; d < ndev; ++d) {
+        Share& s = sh[static_cast<size_t>(d)];
+        if (s.index.empty()) continue;
+        s.res.resize(s.index.size());
+        th.emplace_back([&s, &o, d, devices] {
+            pdlpx_options od = o;
+            od.device = devices[d];
+            try {
+                s.rc = batchSolve(static_cast<int32_t>(s.index.size()), s.lps.data(), od, s.res.data(), s.x.data(),
+                                  s.y.data(), s.err);
+            } catch (const std::bad_alloc&) {
+                s.rc = PDLPX_E_NOMEM;
+                s.err = "host allocation failed";
+            } catch (const std::exception& e) {
+                s.rc = PDLPX_E_INVALID;
+                s.err = e.what();
+            }
+        });
+    }
+    for (auto& t : th) t.join();
+    int32_t rc = PDLPX_OK;
+    for (int32_t d = 0; d < ndev; ++d) {
+        Share& s = sh[static_cast<size_t>(d)];
+        for (size_t i = 0; i < s.index.size() && s.rc == PDLPX_OK; ++i) results[s.index[i]] = s.res[i];
+        if (s.rc != PDLPX_OK && rc == PDLPX_OK) {
+            rc = s.rc;
+            err = "device " + std::to_string(devices[d]) + ": " + s.err;
+        } else if (s.rc == PDLPX_OK && !s.err.empty() && err.empty()) {
+            err = s.err;  // a note (host-side scaling fallback), not an error
+        }
+    }
+    return rc;
+}
+
+}  // namespace pdlpx

@@ -137,6 +137,16 @@ int32_t pdlpx_device_count(void) {
 
 const char* pdlpx_version(void) { return "pdlpx 0.1 (sm_100a)"; }
 
+void pdlpx_struct_sizes(int32_t* sizes) {
+    if (sizes == nullptr) return;
+    sizes[0] = static_cast<int32_t>(sizeof(pdlpx_options));
+    sizes[1] = static_cast<int32_t>(sizeof(pdlpx_result));
+    sizes[2] = static_cast<int32_t>(sizeof(pdlpx_lp));
+    sizes[3] = static_cast<int32_t>(sizeof(pdlpx_gen_lp));
+    sizes[4] = static_cast<int32_t>(sizeof(pdlpx_server_config));
+    sizes[5] = static_cast<int32_t>(sizeof(pdlpx_server_stats));
+}
+
 int32_t pdlpx_create(const pdlpx_options* opts, pdlpx_solver** out) {
     if (out == nullptr) return PDLPX_E_INVALID;
     *out = nullptr;
@@ -353,6 +363,51 @@ int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_option
         pdlpx_options_default(&o);
     try {
         return pdlpx::batchSolve(count, lps, o, results, x_out, y_out, g_last_error);
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return PDLPX_E_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return PDLPX_E_INVALID;
+    }
+}
+
+int32_t pdlpx_shard_lps(int32_t count, const int64_t* weights, int32_t ndev, int32_t* device_of) {
+    if (count < 0 || ndev <= 0 || (count > 0 && (weights == nullptr || device_of == nullptr))) return PDLPX_E_INVALID;
+    for (int32_t k = 0; k < count; ++k)
+        if (weights[k] < 0) return PDLPX_E_INVALID;
+    try {
+        pdlpx::shardLps(count, weights, ndev, device_of);
+    } catch (const std::bad_alloc&) {
+        return PDLPX_E_NOMEM;
+    }
+    return PDLPX_OK;
+}
+
+int32_t pdlpx_batch_solve_devices(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts,
+                                  const int32_t* devices, int32_t ndev, pdlpx_result* results,
+                                  double* const* x_out, double* const* y_out) {
+    if (count < 0 || (count > 0 && (lps == nullptr || results == nullptr)) || ndev <= 0 || devices == nullptr)
+        return PDLPX_E_INVALID;
+    int devcount = 0;
+    if (cudaGetDeviceCount(&devcount) != cudaSuccess || devcount <= 0) {
+        cudaGetLastError();
+        g_last_error = "no CUDA device visible";
+        return PDLPX_E_NO_DEVICE;
+    }
+    for (int32_t d = 0; d < ndev; ++d)
+        if (devices[d] < 0 || devices[d] >= devcount) {
+            g_last_error = "device ordinal " + std::to_string(devices[d]) + " out of range";
+            return PDLPX_E_INVALID;
+        }
+    if (count == 0) return PDLPX_OK;
+    pdlpx_options o;
+    if (opts)
+        o = *opts;
+    else
+        pdlpx_options_default(&o);
+    try {
+        return pdlpx::batchSolveDevices(count, lps, o, devices, ndev, results, x_out, y_out, g_last_error);
     } catch (const std::bad_alloc&) {
         g_last_error = "host allocation failed";
         return PDLPX_E_NOMEM;

@@ -109,6 +109,13 @@ int32_t pickGroup(int64_t nnz, int32_t rows);
 int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,
                    double* const* x_out, double* const* y_out, std::string& err);
 
+// Independent LPs over several devices (batch.cu): deterministic
+// longest-processing-time sharding, and the batch solved per device.
+void shardLps(int32_t count, const int64_t* weights, int32_t ndev, int32_t* device_of);
+int32_t batchSolveDevices(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, const int32_t* devices,
+                          int32_t ndev, pdlpx_result* results, double* const* x_out, double* const* y_out,
+                          std::string& err);
+
 // Message returned by pdlpx_last_error(NULL) on this thread (calls without a handle).
 void setGlobalError(const std::string& msg);
 

@@ -125,7 +125,10 @@ double quantile(std::vector<double> v, double q) {
 
 class Server {
 public:
-    Server(const pdlpx_options& o, const pdlpx_server_config& c, size_t budget) : opt_(o), cfg_(c), budget_(budget) {}
+    // devices[k] is a CUDA ordinal, budget[k] its device-byte budget for packs in flight.
+    Server(const pdlpx_options& o, const pdlpx_server_config& c, std::vector<int> devices, std::vector<size_t> budget)
+        : opt_(o), cfg_(c), devices_(std::move(devices)), budget_(std::move(budget)),
+          bytes_in_flight_(devices_.size(), 0), packs_on_(devices_.size(), 0) {}
 
     ~Server() { shutdown(); }
 
@@ -278,6 +281,8 @@ public:
         s->waiting = waiting;
         s->running = running;
         s->packs_running = packs_running_;
+        size_t inflight = 0;
+        for (size_t b : bytes_in_flight_) inflight += b;
         s->p50_latency_s = quantile(latencies_, 0.50);
         s->p99_latency_s = quantile(latencies_, 0.99);
         double sum = 0.0, mx = 0.0;
@@ -289,7 +294,7 @@ public:
         s->max_latency_s = mx;
         const double span = completed_ > 0 ? std::chrono::duration<double>(last_complete_ - first_submit_).count() : 0.0;
         s->lps_per_sec = span > 0.0 ? static_cast<double>(completed_) / span : 0.0;
-        s->bytes_in_flight = static_cast<double>(bytes_in_flight_);
+        s->bytes_in_flight = static_cast<double>(inflight);
     }
 
 private:
@@ -340,25 +345,41 @@ private:
         }
     }
 
+    // The device a pack of `head` would start on now (mu_ held): among the
+    // devices with a free stream whose budget admits the head request (or that
+    // run nothing), the one with the fewest bytes in flight, ties to the lower
+    // index; -1 when none.
+    int pickDevice(const Request& head, int max_packs) const {
+        int best = -1;
+        for (size_t d = 0; d < devices_.size(); ++d) {
+            if (packs_on_[d] >= max_packs) continue;
+            if (bytes_in_flight_[d] != 0 && bytes_in_flight_[d] + head.bytes > budget_[d]) continue;
+            if (best < 0 || bytes_in_flight_[d] < bytes_in_flight_[static_cast<size_t>(best)]) best = static_cast<int>(d);
+        }
+        return best;
+    }
+
     void dispatchLoop() {
         const int max_packs = std::max(1, cfg_.max_packs);
         const size_t max_lps = static_cast<size_t>(std::max(1, cfg_.max_pack_lps));
         while (true) {
             std::vector<Request*> pack;
             size_t bytes = 0;
+            int dev = -1;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                // A pack starts when a stream and memory are free and either a full
-                // pack is ready or the oldest ready request has waited the batching
-                // window (a pack runs for many restart cycles, so a short wait that
-                // fills it costs less latency than it saves).
+                // A pack starts when a stream and memory are free on some device and
+                // either a full pack is ready or the oldest ready request has waited
+                // the batching window (a pack runs for many restart cycles, so a
+                // short wait that fills it costs less latency than it saves).
                 const auto window = std::chrono::milliseconds(std::max(0, cfg_.batch_window_ms));
                 while (true) {
                     if (closed_) return;
-                    bool can = !ready_q_.empty() && packs_running_ < max_packs;
+                    bool can = !ready_q_.empty();
                     if (can) {
                         const Request& head = *reqs_.at(ready_q_.front());
-                        can = bytes_in_flight_ == 0 || bytes_in_flight_ + head.bytes <= budget_;
+                        dev = pickDevice(head, max_packs);
+                        can = dev >= 0;
                         if (can && ready_q_.size() < max_lps) {
                             const auto due = head.ready + window;
                             if (Clock::now() < due) {
@@ -374,11 +395,12 @@ private:
                 // in arrival order
                 const FamilyPtr fam = reqs_.at(ready_q_.front())->family;
                 const size_t cap = fam ? std::min<size_t>(max_lps, kFamilyLanes) : max_lps;
+                const size_t du = static_cast<size_t>(dev);
                 std::deque<int64_t> rest;
                 while (!ready_q_.empty()) {
                     Request* r = reqs_.at(ready_q_.front()).get();
                     const bool take = r->family == fam && pack.size() < cap &&
-                                      (pack.empty() || bytes_in_flight_ + bytes + r->bytes <= budget_);
+                                      (pack.empty() || bytes_in_flight_[du] + bytes + r->bytes <= budget_[du]);
                     if (take) {
                         bytes += r->bytes;
                         r->state = kRunning;
@@ -389,10 +411,11 @@ private:
                     ready_q_.pop_front();
                 }
                 ready_q_.swap(rest);
-                bytes_in_flight_ += bytes;
+                bytes_in_flight_[du] += bytes;
+                ++packs_on_[du];
                 ++packs_running_;
             }
-            std::thread([this, pack, bytes] { runPack(pack, bytes); }).detach();
+            std::thread([this, pack, bytes, dev] { runPack(pack, bytes, dev); }).detach();
             pack.clear();
         }
     }
@@ -401,7 +424,7 @@ private:
     // LP of the pack until the last one finishes), and a finished request may be
     // released by its client at once, so completion is tracked here, never by
     // reading a request after it was completed.
-    void runPack(std::vector<Request*> pack, size_t bytes) {
+    void runPack(std::vector<Request*> pack, size_t bytes, int dev) {
         std::vector<PreparedPtr> preps;
         std::vector<PreparedLp*> lps;
         FamilyPtr fam;
@@ -423,8 +446,9 @@ private:
             finishLocked(r);
             cv_done_.notify_all();
         };
-        const int32_t rc = fam ? solveFamily(*fam, lps, opt_, &stop_, done, err)
-                               : solvePrepared(lps, opt_, &stop_, done, err);
+        pdlpx_options o = opt_;
+        o.device = devices_[static_cast<size_t>(dev)];
+        const int32_t rc = fam ? solveFamily(*fam, lps, o, &stop_, done, err) : solvePrepared(lps, o, &stop_, done, err);
         std::lock_guard<std::mutex> g(mu_);
         for (size_t k = 0; k < pack.size(); ++k) {
             if (finished[k]) continue;
@@ -433,7 +457,8 @@ private:
             r->err = rc != PDLPX_OK ? err : "pack ended without a result";
             finishLocked(*r);
         }
-        bytes_in_flight_ -= bytes;
+        bytes_in_flight_[static_cast<size_t>(dev)] -= bytes;
+        --packs_on_[static_cast<size_t>(dev)];
         --packs_running_;
         cv_done_.notify_all();
         cv_dispatch_.notify_all();
@@ -442,7 +467,8 @@ private:
 
     const pdlpx_options opt_;
     const pdlpx_server_config cfg_;
-    const size_t budget_;
+    const std::vector<int> devices_;     // CUDA ordinals the packs run on
+    const std::vector<size_t> budget_;   // per device
     mutable std::mutex mu_;
     std::condition_variable cv_prep_, cv_dispatch_, cv_done_, cv_packs_;
     std::unordered_map<int64_t, std::unique_ptr<Request>> reqs_;
@@ -451,8 +477,9 @@ private:
     std::thread dispatcher_;
     std::atomic<int> stop_{0};
     bool closed_ = false;
-    int packs_running_ = 0;
-    size_t bytes_in_flight_ = 0;
+    int packs_running_ = 0;               // all devices
+    std::vector<size_t> bytes_in_flight_;  // per device
+    std::vector<int> packs_on_;            // per device
     int64_t next_ticket_ = 1, submitted_ = 0, completed_ = 0;
     Clock::time_point first_submit_, last_complete_;
     std::vector<double> latencies_;
@@ -501,18 +528,41 @@ int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config
             pdlpx::setGlobalError("no CUDA device visible");
             return PDLPX_E_NO_DEVICE;
         }
-        cudaSetDevice((o.device >= 0 && o.device < devcount) ? o.device : 0);
-        size_t budget = static_cast<size_t>(c.budget_bytes > 0.0 ? c.budget_bytes : 0.0);
-        if (budget == 0) {
-            size_t free_b = 0, total_b = 0;
-            if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-                pdlpx::setGlobalError("cudaMemGetInfo failed");
-                return PDLPX_E_CUDA;
+        std::vector<int> devices;
+        if (c.num_devices > 1) {
+            if (c.num_devices > static_cast<int32_t>(sizeof(c.devices) / sizeof(c.devices[0]))) {
+                pdlpx::setGlobalError("num_devices exceeds the devices array");
+                return PDLPX_E_INVALID;
             }
-            budget = static_cast<size_t>(0.85 * static_cast<double>(free_b));
+            for (int32_t k = 0; k < c.num_devices; ++k) {
+                if (c.devices[k] < 0 || c.devices[k] >= devcount) {
+                    pdlpx::setGlobalError("device ordinal " + std::to_string(c.devices[k]) + " out of range");
+                    return PDLPX_E_INVALID;
+                }
+                devices.push_back(c.devices[k]);
+            }
+        } else {
+            devices.push_back((o.device >= 0 && o.device < devcount) ? o.device : 0);
         }
+        std::vector<size_t> budget;
+        for (int dev : devices) {
+            size_t b = static_cast<size_t>(c.budget_bytes > 0.0 ? c.budget_bytes : 0.0);
+            if (b == 0) {
+                size_t free_b = 0, total_b = 0;
+                if (cudaSetDevice(dev) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+                    cudaGetLastError();
+                    pdlpx::setGlobalError("cudaMemGetInfo failed");
+                    return PDLPX_E_CUDA;
+                }
+                // a device listed twice shares its memory between its entries
+                const auto copies = std::count(devices.begin(), devices.end(), dev);
+                b = static_cast<size_t>(0.85 * static_cast<double>(free_b) / static_cast<double>(copies));
+            }
+            budget.push_back(b);
+        }
+        cudaSetDevice(devices.front());
         auto* s = new pdlpx_server();
-        s->impl = std::make_unique<pdlpx::Server>(o, c, budget);
+        s->impl = std::make_unique<pdlpx::Server>(o, c, devices, budget);
         s->impl->start();
         *out = s;
         return PDLPX_OK;

@@ -447,8 +447,11 @@ class PdlpSolver:
         return out
 
 
-def batch_solve(problems: Sequence[LpProblem], options: PdlpOptions, warm: Sequence | None = None):
-    """Solve many independent LPs in one call; returns [(LpResult, x, y)]."""
+def batch_solve(problems: Sequence[LpProblem], options: PdlpOptions, warm: Sequence | None = None,
+                devices: Sequence[int] | None = None):
+    """Solve many independent LPs in one call; returns [(LpResult, x, y)].
+    ``devices``: CUDA ordinals to shard the LPs over (pdlpx_batch_solve_devices;
+    one host thread per device, no data between devices); None = options.device."""
     lib = _capi.load()
     keep: list = []
     arr = (_capi.Lp * len(problems))()
@@ -460,8 +463,23 @@ def batch_solve(problems: Sequence[LpProblem], options: PdlpOptions, warm: Seque
     ys = [np.zeros(p.num_rows) for p in problems]
     xp = (_capi.P_f64 * len(problems))(*[_pd(x) for x in xs])
     yp = (_capi.P_f64 * len(problems))(*[_pd(y) for y in ys])
-    _capi.check(lib.pdlpx_batch_solve(len(problems), arr, C.byref(options.to_c()), res, xp, yp))
+    if devices is None:
+        _capi.check(lib.pdlpx_batch_solve(len(problems), arr, C.byref(options.to_c()), res, xp, yp))
+    else:
+        dv = np.ascontiguousarray(devices, dtype=np.int32)
+        _capi.check(lib.pdlpx_batch_solve_devices(len(problems), arr, C.byref(options.to_c()), _pi(dv), int(dv.size),
+                                                  res, xp, yp))
     return [(LpResult.from_c(res[k]), xs[k], ys[k]) for k in range(len(problems))]
+
+
+def shard_lps(weights: Sequence[int], ndev: int) -> np.ndarray:
+    """Device index of each LP under the engine's deterministic
+    longest-processing-time sharding (pdlpx_shard_lps)."""
+    lib = _capi.load()
+    w = np.ascontiguousarray(weights, dtype=np.int64)
+    out = np.zeros(w.size, dtype=np.int32)
+    _capi.check(lib.pdlpx_shard_lps(int(w.size), w.ctypes.data_as(C.POINTER(C.c_int64)), int(ndev), _pi(out)))
+    return out
 
 
 def read_mps(path) -> LpProblem:
@@ -515,6 +533,8 @@ class Server:
     with whatever else is waiting and solved several packs at a time on the
     device; each result is available as soon as it is finished.
 
+    ``devices``: CUDA ordinals the packs are placed on (the listed device with
+    a free stream and the fewest bytes in flight); None = options.device.
     ``submit(lp, warm=None)`` returns a ticket; ``warm`` is an ``(x, y)`` pair or
     the ticket of a finished request.  ``wait(ticket)`` returns
     ``(LpResult, x, y)``.  ``stats()`` reports p50/p99 latency and LPs/s.
@@ -523,7 +543,7 @@ class Server:
 
     def __init__(self, options: PdlpOptions, budget_bytes: float = 0.0, max_packs: int = 4,
                  max_pack_lps: int = 32, prep_threads: int = 0, queue_limit: int = 100000,
-                 batch_window_ms: int = 50, families: bool = True):
+                 batch_window_ms: int = 50, families: bool = True, devices: Sequence[int] | None = None):
         self._lib = _capi.load()
         cfg = _capi.ServerConfig()
         self._lib.pdlpx_server_config_default(C.byref(cfg))
@@ -534,6 +554,12 @@ class Server:
         cfg.queue_limit = int(queue_limit)
         cfg.batch_window_ms = int(batch_window_ms)
         cfg.families = int(bool(families))
+        if devices is not None and len(devices) > 1:
+            if len(devices) > len(cfg.devices):
+                raise ValueError(f"at most {len(cfg.devices)} devices")
+            cfg.num_devices = len(devices)
+            for k, d in enumerate(devices):
+                cfg.devices[k] = int(d)
         self._h = C.c_void_p()
         _capi.check(self._lib.pdlpx_server_create(C.byref(options.to_c()), C.byref(cfg), C.byref(self._h)))
         self._dims: dict[int, tuple[int, int]] = {}

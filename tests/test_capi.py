@@ -107,3 +107,8 @@ def test_struct_layout_is_consistent():
         if name != "reserved":
             assert getattr(back, name) == getattr(o, name), name
     lib.pdlpx_destroy(h)
+
+
+def test_struct_layouts_match_the_library():
+    _capi.check_layout()
+    assert C.sizeof(_capi.ServerConfig) == 8 + 4 * (6 + 2 + 16)

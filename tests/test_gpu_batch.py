@@ -180,3 +180,50 @@ def test_autotuned_pack_gives_identical_results():
         assert (r.status, r.iterations, r.objective) == (q.status, q.iterations, q.objective)
         np.testing.assert_array_equal(x, u)
         np.testing.assert_array_equal(y, v)
+
+
+def test_batch_over_devices_identical_to_one_device():
+    """pdlpx_batch_solve_devices: the LPs sharded over a device list (here GPU 0
+    twice: two host threads with their own streams and packs side by side) give
+    results bit-identical to one pdlpx_batch_solve call (batch invariance), and
+    the sharding splits the LPs between both entries of the list."""
+    from mipx_b200.pdlp import shard_lps
+    lps = _mix(900, [250, 1800, 600, 3200, 400, 1100, 750, 2400, 520, 1500])
+    o = PdlpOptions(verbose=False, **TIGHT)
+    one = batch_solve(lps, o)
+    two = batch_solve(lps, o, devices=[0, 0])
+    _same(one, two)
+    d = shard_lps([lp.matrix.numNonzeros() + lp.num_rows + lp.num_cols for lp in lps], 2)
+    assert set(d.tolist()) == {0, 1}
+
+
+def test_device_ruiz_in_batch_and_server_is_bit_identical():
+    """scale_on_device = 1 runs the Ruiz passes of every LP's preparation on the
+    GPU (scaling.cu); the scaled data equal the host loop's to the last bit, so
+    the batch and server results are identical with 1 and with 0."""
+    from mipx_b200.pdlp import Server
+    lps = _mix(1300, [400, 1500, 900])
+    res = {}
+    for dev in (0, 1):
+        o = PdlpOptions(verbose=False, scale_on_device=dev, **TIGHT)
+        res[("batch", dev)] = batch_solve(lps, o)
+        with Server(o, max_packs=2, max_pack_lps=8, batch_window_ms=0) as srv:
+            tickets = [srv.submit(lp) for lp in lps]
+            res[("server", dev)] = [srv.wait(t) for t in tickets]
+    _same(res[("batch", 0)], res[("batch", 1)])
+    _same(res[("server", 0)], res[("server", 1)])
+    assert all(r.status == Status.Optimal for r, _, _ in res[("batch", 1)])
+
+
+def test_server_over_device_list():
+    """A server over the device list [0, 0] places its packs on both entries and
+    returns the results a one-device server gives."""
+    from mipx_b200.pdlp import Server
+    lps = _mix(1400, [300, 900, 1200, 500])
+    o = PdlpOptions(verbose=False, **TIGHT)
+    out = {}
+    for devs in (None, [0, 0]):
+        with Server(o, max_packs=1, max_pack_lps=1, batch_window_ms=0, devices=devs) as srv:
+            tickets = [srv.submit(lp) for lp in lps]
+            out[str(devs)] = [srv.wait(t) for t in tickets]
+    _same(out["None"], out["[0, 0]"])
