@@ -194,7 +194,7 @@ def test_cli_summary_lines_without_rows(tmp_path):
 @pytest.mark.gpu
 def test_cli_solves_mps_on_device(tmp_path):
     """CLI solve of a generated LP written as MPS against the Python API on the
-    same LP: same status, objectives within 2e-6 (1 + |obj|) at 1e-6 KKT."""
+    same LP: same status, objectives within 1e-6 relative at 1e-6 KKT."""
     from mipx_b200.pdlp import PdlpOptions, PdlpSolver
     lp, _ = G.random_lp(500, 1250, 4, 12, 5)
     p = tmp_path / "r.mps.gz"
@@ -210,7 +210,7 @@ def test_cli_solves_mps_on_device(tmp_path):
     q.load(read_mps(p))
     res = q.solve()
     assert s["status"] == "Optimal" and int(res.status) == 0
-    assert abs(s["objective"] - res.objective) <= 2e-6 * (1 + abs(res.objective))
+    assert abs(s["objective"] - res.objective) <= 1e-6 * max(1.0, abs(res.objective))
     assert s["iterations"] > 0 and s["work"] > 0
 
 
