@@ -337,7 +337,10 @@ typedef struct pdlpx_server_config {
                               CUDA devices devices[0..k), each pack on the listed device with a free
                               stream and the fewest bytes in flight (max_packs streams and its own
                               budget per device; no data moves between devices) */
-    int32_t reserved;
+    int32_t lane_admission; /* 1 (default): a family member that arrives while a family pack of its
+                               family runs takes a free lane of that pack between restart cycles
+                               (the lane of a finished member, or an unused one); 0: it waits for
+                               a new pack */
     int32_t devices[16];
 } pdlpx_server_config;
 
@@ -349,6 +352,7 @@ typedef struct pdlpx_server_stats {
     double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s; /* submit -> result */
     double lps_per_sec;           /* completed / (last completion - first submission) */
     double bytes_in_flight;       /* device bytes of the running packs */
+    int64_t admitted;             /* requests that joined a running family pack in a free lane */
 } pdlpx_server_stats;
 
 void pdlpx_server_config_default(pdlpx_server_config* c);

@@ -75,13 +75,14 @@ class GenLp(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", f64), ("max_packs", i32), ("max_pack_lps", i32), ("prep_threads", i32),
                 ("queue_limit", i32), ("batch_window_ms", i32), ("families", i32), ("num_devices", i32),
-                ("reserved", i32), ("devices", i32 * 16)]
+                ("lane_admission", i32), ("devices", i32 * 16)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("waiting", C.c_int64), ("running", C.c_int64),
                 ("packs_running", i32), ("reserved0", i32), ("p50_latency_s", f64), ("p99_latency_s", f64),
-                ("mean_latency_s", f64), ("max_latency_s", f64), ("lps_per_sec", f64), ("bytes_in_flight", f64)]
+                ("mean_latency_s", f64), ("max_latency_s", f64), ("lps_per_sec", f64), ("bytes_in_flight", f64),
+                ("admitted", C.c_int64)]
 
 
 SIGNATURES = [

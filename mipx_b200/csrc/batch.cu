@@ -1700,7 +1700,7 @@ size_t familyMemberBytes(const PreparedLp& p, const FamilyBase& f) {
 }
 
 int32_t solveFamily(const FamilyBase& f, const std::vector<PreparedLp*>& lps, const pdlpx_options& o,
-                    const std::atomic<int>* stop, const LpDone& done, std::string& err) {
+                    const std::atomic<int>* stop, const LpDone& done, std::string& err, const FamilyAdmit& admit) {
     const auto t0 = std::chrono::steady_clock::now();
     if (!optionsSupported(o, err)) return PDLPX_E_INVALID;
     if (lps.empty()) return PDLPX_OK;
@@ -1722,7 +1722,16 @@ int32_t solveFamily(const FamilyBase& f, const std::vector<PreparedLp*>& lps, co
     fp.L = static_cast<int>(fp.items.size());
     int32_t rc = selectDevice(o, err);
     if (rc != PDLPX_OK) return rc;
-    return solveFamilyPack(fp, o, t0, stop, done, err);
+    FamAdmit fam_admit;
+    if (admit) {
+        fam_admit = [&admit](const std::function<bool(const Item&)>& fits, Item*& item, int& id) {
+            PreparedLp* p = nullptr;
+            if (!admit([&fits](const PreparedLp& q) { return fits(q.item); }, p, id) || p == nullptr) return false;
+            item = &p->item;
+            return true;
+        };
+    }
+    return solveFamilyPack(fp, o, t0, stop, done, err, fam_admit);
 }
 
 int32_t batchSolve(int32_t count, const pdlpx_lp* lps, const pdlpx_options& o, pdlpx_result* results,

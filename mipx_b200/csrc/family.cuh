@@ -684,12 +684,19 @@ __global__ void famInitStep(FamArgs a) {
 // ---------------------------------------------------------------------------
 // Host side of a family pack
 // ---------------------------------------------------------------------------
+// Offered between restart cycles when a lane is free: return a prepared
+// member of the family for which fits(item) holds (its appended rows fit the
+// pack's reserved room) and the caller's id for it, or false when none is
+// waiting.  The pack reports that member through `done(id, outcome)`.
+using FamAdmit = std::function<bool(const std::function<bool(const Item&)>& fits, Item*& item, int& id)>;
+
 struct FamPack {
     const FamilyBase* base = nullptr;
-    std::vector<Item*> items;
+    std::vector<Item*> items;   // by lane (kFam entries; null for a lane never used)
     int L = 0, n = 0, mb = 0, K = 0;
-    int64_t Zb = 0, Zk = 0;
-    std::vector<int> qfirst;  // first appended row of each lane
+    int Kcap = 0;               // appended rows the arrays hold (room for admitted members)
+    int64_t Zb = 0, Zk = 0, Zkcap = 0;
+    std::vector<int> qfirst;    // first appended row of each lane (kFam + 1 entries)
     size_t o_aptr, o_aidx, o_aval, o_atptr, o_atidx, o_atval, o_kptr, o_kidx, o_kval, o_klane, o_kfirst, o_live, o_lanes;
     size_t o_ktptr, o_ktrow, o_ktlane, o_ktval, o_cp, o_cs, o_rp, o_rs, o_st, o_dc, o_ps, o_pix;
     size_t image_end;
@@ -713,10 +720,10 @@ struct FamPack {
         }
     }
 
-    size_t rowsAll() const { return static_cast<size_t>(mb) * kFam + static_cast<size_t>(K); }
+    size_t rowsAll() const { return static_cast<size_t>(mb) * kFam + static_cast<size_t>(Kcap); }
     size_t colsAll() const { return static_cast<size_t>(n) * kFam; }
 
-    void layout(int nbr, int nbk, int nbc) {
+    void layout(int nbr, int nbc) {
         size_t off = 0;
         auto take = [&](size_t bytes) {
             const size_t at = off;
@@ -730,17 +737,17 @@ struct FamPack {
         o_atptr = take(4 * (static_cast<size_t>(n) + 1));
         o_atidx = take(4 * static_cast<size_t>(Zb));
         o_atval = take(8 * static_cast<size_t>(Zb));
-        o_kptr = take(4 * (static_cast<size_t>(K) + 1));
-        o_kidx = take(4 * static_cast<size_t>(Zk));
-        o_kval = take(8 * static_cast<size_t>(Zk));
-        o_klane = take(4 * static_cast<size_t>(K));
+        o_kptr = take(4 * (static_cast<size_t>(Kcap) + 1));
+        o_kidx = take(4 * static_cast<size_t>(Zkcap));
+        o_kval = take(8 * static_cast<size_t>(Zkcap));
+        o_klane = take(4 * static_cast<size_t>(Kcap));
         o_kfirst = take(4 * (kFam + 1));
         o_live = take(4);
         o_lanes = take(sizeof(FamLane));
         o_ktptr = take(4 * (static_cast<size_t>(n) + 1));
-        o_ktrow = take(4 * static_cast<size_t>(Zk));
-        o_ktlane = take(4 * static_cast<size_t>(Zk));
-        o_ktval = take(8 * static_cast<size_t>(Zk));
+        o_ktrow = take(4 * static_cast<size_t>(Zkcap));
+        o_ktlane = take(4 * static_cast<size_t>(Zkcap));
+        o_ktval = take(8 * static_cast<size_t>(Zkcap));
         o_cp = take(32 * C);
         o_cs = take(8 * C);
         o_rp = take(32 * R);
@@ -762,7 +769,8 @@ struct FamPack {
         o_piy = take(8 * R);
         o_pixn = take(8 * C);
         o_pipart = take(8 * 2 * kFam * static_cast<size_t>(nbc));
-        o_prows = take(8 * kRowSlots * kFam * static_cast<size_t>(nbr + nbk));
+        // appended rows are checked in one block per lane: room for every lane
+        o_prows = take(8 * kRowSlots * kFam * static_cast<size_t>(nbr + kFam));
         o_pcols = take(8 * kColSlots * kFam * static_cast<size_t>(nbc));
         o_flags = take(4 * kFam);
         o_counters = take(16);
@@ -782,11 +790,108 @@ size_t familyPackBytes(int64_t n, int64_t mb, int64_t zb, int64_t K, int64_t zk,
 
 int famBlocks(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kWarps - 1) / kWarps)); }
 
+// Appended rows a lane's member brings (rows after the base rows) and their entries.
+int famCuts(const Item& it, int mb) { return it.lp.m - mb; }
+int64_t famCutEntries(const Item& it, int mb) { return it.lp.a.ptr[it.lp.m] - it.lp.a.ptr[mb]; }
+
+// Per-lane data of one member in its own (contiguous) order: the scaled
+// column constants, column scales, starting x (warm start scaled like the
+// reference, pdlp.cpp:1812-1827, else 0) and its column-scaled copy; the same
+// for every row of the member (base rows, then its appended rows).
+struct FamLaneData {
+    std::vector<ColPack<double>> cp;
+    std::vector<double> cs, x, xs;
+    std::vector<RowPack<double>> rp;
+    std::vector<double> rs, y, ys;
+};
+
+void famLaneData(const Item& it, int n, FamLaneData& q) {
+    const ScaledLp& sc = it.sc;
+    const int32_t m = it.lp.m;
+    q.cp.resize(n);
+    q.cs.resize(n);
+    q.x.assign(n, 0.0);
+    q.xs.resize(n);
+    q.rp.resize(m);
+    q.rs.resize(m);
+    q.y.assign(m, 0.0);
+    q.ys.resize(m);
+    if (!it.warm_x.empty()) {
+        for (int32_t j = 0; j < n; ++j) q.x[j] = it.warm_x[j] / sc.col_scale[j] * sc.con_scale;
+        for (int32_t i = 0; i < m; ++i) q.y[i] = it.warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
+    }
+    for (int32_t j = 0; j < n; ++j) {
+        q.cp[j] = ColPack<double>{sc.c[j], sc.cl[j], sc.cu[j], sc.tau[j]};
+        q.cs[j] = sc.col_scale[j];
+        q.xs[j] = sc.col_scale[j] * q.x[j];
+    }
+    for (int32_t i = 0; i < m; ++i) {
+        q.rp[i] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
+        q.rs[i] = sc.row_scale[i];
+        q.ys[i] = sc.row_scale[i] * q.y[i];
+    }
+}
+
+// The appended rows of the lanes in use (lane order; a lane without a member
+// contributes none): row pointers, entries, lanes, per-lane first row, and the
+// same entries by column (row order inside a column).
+struct FamCuts {
+    std::vector<int32_t> kp, ki, kl, kf, ktp, ktr, ktl;
+    std::vector<double> kv, ktv;
+    int K = 0;
+    int64_t Zk = 0;
+};
+
+void famBuildCuts(const FamPack& fp, const std::vector<char>& in_use, FamCuts& c) {
+    const int n = fp.n, mb = fp.mb;
+    c.kp.clear();
+    c.ki.clear();
+    c.kv.clear();
+    c.kl.clear();
+    c.kf.assign(kFam + 1, 0);
+    std::vector<int32_t> colcnt(static_cast<size_t>(n) + 1, 0);
+    int q = 0;
+    for (int l = 0; l < kFam; ++l) {
+        c.kf[l] = q;
+        if (!in_use[l] || fp.items[l] == nullptr) continue;
+        const Csr& a = fp.items[l]->lp.a;
+        for (int32_t i = mb; i < a.rows; ++i, ++q) {
+            c.kp.push_back(static_cast<int32_t>(c.ki.size()));
+            c.kl.push_back(l);
+            for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                c.ki.push_back(a.idx[k]);
+                c.kv.push_back(a.val[k]);
+                ++colcnt[a.idx[k] + 1];
+            }
+        }
+    }
+    c.kf[kFam] = q;
+    c.K = q;
+    c.Zk = static_cast<int64_t>(c.ki.size());
+    c.kp.push_back(static_cast<int32_t>(c.Zk));
+    for (int32_t j = 0; j < n; ++j) colcnt[j + 1] += colcnt[j];
+    c.ktp = colcnt;
+    c.ktr.resize(static_cast<size_t>(c.Zk));
+    c.ktl.resize(static_cast<size_t>(c.Zk));
+    c.ktv.resize(static_cast<size_t>(c.Zk));
+    for (int qq = 0; qq < c.K; ++qq)
+        for (int32_t k = c.kp[qq]; k < c.kp[qq + 1]; ++k) {
+            const int32_t at = colcnt[c.ki[k]]++;
+            c.ktr[at] = qq;
+            c.ktl[at] = c.kl[qq];
+            c.ktv[at] = c.kv[k];
+        }
+}
+
 // Build the image, run the power iteration and the restart cycles of one family
-// pack; `done(l, outcome)` as for a regular pack.
+// pack; `done(id, outcome)` as for a regular pack, with id = the member's
+// position in fp.items for the initial members and the id `admit` returned for
+// members admitted later (admit may be empty: no admission).
 int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady_clock::time_point t0,
-                        const std::atomic<int>* stop, const LpDone& done, std::string& err) {
-    const int L = fp.L, n = fp.n, mb = fp.mb;
+                        const std::atomic<int>* stop, const LpDone& done, std::string& err,
+                        const FamAdmit& admit) {
+    const int n = fp.n, mb = fp.mb;
+    int L = fp.L;
     const FamilyBase& fb = *fp.base;
     int sms = 148;
     {
@@ -794,25 +899,29 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    // appended rows of every lane, in lane order
-    fp.qfirst.assign(L + 1, 0);
-    fp.K = 0;
-    fp.Zk = 0;
+    fp.items.resize(kFam, nullptr);
+    std::vector<char> in_use(kFam, 0);  // lane holds a member that is not yet reported
+    std::vector<int> lane_id(kFam, -1);
     for (int l = 0; l < L; ++l) {
-        const Item& it = *fp.items[l];
-        fp.qfirst[l] = fp.K;
-        fp.K += it.lp.m - mb;
-        fp.Zk += it.lp.a.ptr[it.lp.m] - it.lp.a.ptr[mb];
+        in_use[l] = 1;
+        lane_id[l] = l;
     }
-    fp.qfirst[L] = fp.K;
+    FamCuts cuts;
+    famBuildCuts(fp, in_use, cuts);
+    fp.K = cuts.K;
+    fp.Zk = cuts.Zk;
+    fp.qfirst.assign(cuts.kf.begin(), cuts.kf.end());
+    // room for the appended rows of members admitted later: at least 64 rows of
+    // 256 entries per lane, and twice what the first members bring
+    fp.Kcap = std::max(2 * cuts.K, kFam * 64);
+    fp.Zkcap = std::max<int64_t>(2 * cuts.Zk, static_cast<int64_t>(kFam) * 64 * 256);
     fp.Zb = fb.ptr[mb];
-    const int K = fp.K;
-    const int gb = famBlocks(mb), gk = K > 0 ? famBlocks(K) : 0;
+    const int gb = famBlocks(mb);
     const int gp = famBlocks((static_cast<int64_t>(n) + kFamColsPerWarp - 1) / kFamColsPerWarp);
     const int gd = famBlocks((static_cast<int64_t>(mb) + kFamRowsPerWarp - 1) / kFamRowsPerWarp);
     const int cap = 4 * sms;
-    const int nbr = std::min(gb, cap), nbk = K > 0 ? L : 0, nbc = std::min(famBlocks(n), cap);
-    fp.layout(nbr, nbk, nbc);
+    const int nbr = std::min(gb, cap), nbc = std::min(famBlocks(n), cap);
+    fp.layout(nbr, nbc);
 
     // ---- host image
     std::unique_ptr<char[]> img(new char[fp.image_end]);
@@ -837,45 +946,16 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         for (int64_t k = 0; k < fp.Zb; ++k) I(fp.o_atidx)[k] = at.idx[k] * kFam;
         std::memcpy(D(fp.o_atval), at.val.data(), 8 * static_cast<size_t>(fp.Zb));
     }
-    {
-        // appended rows, then their entries by column (row order inside a column)
-        int32_t* kp = I(fp.o_kptr);
-        int32_t* ki = I(fp.o_kidx);
-        double* kv = D(fp.o_kval);
-        int32_t* kl = I(fp.o_klane);
-        std::vector<int32_t> colcnt(static_cast<size_t>(n) + 1, 0);
-        int64_t z = 0;
-        int q = 0;
-        for (int l = 0; l < L; ++l) {
-            const Csr& a = fp.items[l]->lp.a;
-            for (int32_t i = mb; i < a.rows; ++i, ++q) {
-                kp[q] = static_cast<int32_t>(z);
-                kl[q] = l;
-                for (int32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k, ++z) {
-                    ki[z] = a.idx[k];
-                    kv[z] = a.val[k];
-                    ++colcnt[a.idx[k] + 1];
-                }
-            }
-        }
-        kp[K] = static_cast<int32_t>(z);
-        int32_t* kf = I(fp.o_kfirst);
-        for (int l = 0; l <= kFam; ++l) kf[l] = fp.qfirst[std::min(l, L)];
-        *reinterpret_cast<uint32_t*>(H + fp.o_live) = L >= kFam ? ~0u : ((1u << L) - 1u);
-        int32_t* ktp = I(fp.o_ktptr);
-        for (int32_t j = 0; j < n; ++j) colcnt[j + 1] += colcnt[j];
-        std::memcpy(ktp, colcnt.data(), 4 * (static_cast<size_t>(n) + 1));
-        int32_t* ktr = I(fp.o_ktrow);
-        int32_t* ktl = I(fp.o_ktlane);
-        double* ktv = D(fp.o_ktval);
-        for (int qq = 0; qq < K; ++qq)
-            for (int32_t k = kp[qq]; k < kp[qq + 1]; ++k) {
-                const int32_t at = colcnt[ki[k]]++;
-                ktr[at] = qq;
-                ktl[at] = kl[qq];
-                ktv[at] = kv[k];
-            }
-    }
+    std::memcpy(I(fp.o_kptr), cuts.kp.data(), 4 * cuts.kp.size());
+    std::memcpy(I(fp.o_kidx), cuts.ki.data(), 4 * cuts.ki.size());
+    std::memcpy(D(fp.o_kval), cuts.kv.data(), 8 * cuts.kv.size());
+    std::memcpy(I(fp.o_klane), cuts.kl.data(), 4 * cuts.kl.size());
+    std::memcpy(I(fp.o_kfirst), cuts.kf.data(), 4 * cuts.kf.size());
+    *reinterpret_cast<uint32_t*>(H + fp.o_live) = L >= kFam ? ~0u : ((1u << L) - 1u);
+    std::memcpy(I(fp.o_ktptr), cuts.ktp.data(), 4 * cuts.ktp.size());
+    std::memcpy(I(fp.o_ktrow), cuts.ktr.data(), 4 * cuts.ktr.size());
+    std::memcpy(I(fp.o_ktlane), cuts.ktl.data(), 4 * cuts.ktl.size());
+    std::memcpy(D(fp.o_ktval), cuts.ktv.data(), 8 * cuts.ktv.size());
     // per-lane constants, state, power start vector and iterates
     const double inf = std::numeric_limits<double>::infinity();
     std::vector<double> g(n);
@@ -893,10 +973,17 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
     }
     ColPack<double>* cp = reinterpret_cast<ColPack<double>*>(H + fp.o_cp);
     RowPack<double>* rp = reinterpret_cast<RowPack<double>*>(H + fp.o_rp);
-    double *cs = D(fp.o_cs), *rs = D(fp.o_rs), *pix = D(fp.o_pix);
+    double *cs = D(fp.o_cs), *pix = D(fp.o_pix);
+    double* rs = D(fp.o_rs);
     double *xc = ID(fp.o_xc), *xi = ID(fp.o_xi), *xh = ID(fp.o_xh), *xsv = ID(fp.o_xs);
     double *yc = ID(fp.o_yc), *yi = ID(fp.o_yi), *yh = ID(fp.o_yh), *ysv = ID(fp.o_ys);
     const size_t Rb = static_cast<size_t>(mb) * kFam;
+    // appended-row slots no member uses yet: empty, free rows
+    for (size_t r = Rb; r < fp.rowsAll(); ++r) {
+        rp[r] = RowPack<double>{1.0, -inf, inf, static_cast<double>(kRowRanged)};
+        rs[r] = 1.0;
+        yc[r] = yi[r] = yh[r] = ysv[r] = 0.0;
+    }
     parallelFor(kFam, [&](int l) {
         if (l >= L) {
             for (int32_t j = 0; j < n; ++j) {
@@ -914,31 +1001,26 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
             return;
         }
         const Item& it = *fp.items[l];
-        const ScaledLp& sc = it.sc;
-        const int32_t m = it.lp.m;
-        std::vector<double> wx(n, 0.0), wy(m, 0.0);
-        if (!it.warm_x.empty()) {
-            for (int32_t j = 0; j < n; ++j) wx[j] = it.warm_x[j] / sc.col_scale[j] * sc.con_scale;
-            for (int32_t i = 0; i < m; ++i) wy[i] = it.warm_y[i] * sc.obj_scale / (sc.obj_sign * sc.row_scale[i]);
-        }
+        FamLaneData q;
+        famLaneData(it, n, q);
         for (int32_t j = 0; j < n; ++j) {
             const size_t c = static_cast<size_t>(j) * kFam + l;
-            cp[c] = ColPack<double>{sc.c[j], sc.cl[j], sc.cu[j], sc.tau[j]};
-            cs[c] = sc.col_scale[j];
+            cp[c] = q.cp[j];
+            cs[c] = q.cs[j];
             pix[c] = g[j];
-            xc[c] = xi[c] = xh[c] = wx[j];
-            xsv[c] = sc.col_scale[j] * wx[j];
+            xc[c] = xi[c] = xh[c] = q.x[j];
+            xsv[c] = q.xs[j];
         }
-        for (int32_t i = 0; i < m; ++i) {
+        for (int32_t i = 0; i < it.lp.m; ++i) {
             const size_t r = i < mb ? static_cast<size_t>(i) * kFam + l : Rb + static_cast<size_t>(fp.qfirst[l] + i - mb);
-            rp[r] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
-            rs[r] = sc.row_scale[i];
-            yc[r] = yi[r] = yh[r] = wy[i];
-            ysv[r] = sc.row_scale[i] * wy[i];
+            rp[r] = q.rp[i];
+            rs[r] = q.rs[i];
+            yc[r] = yi[r] = yh[r] = q.y[i];
+            ysv[r] = q.ys[i];
         }
         DevConst dc{};
         DevState st{};
-        lpState(it, o, false, nbr + nbk, nbc, dc, st);
+        lpState(it, o, false, nbr + L, nbc, dc, st);
         reinterpret_cast<DevConst*>(H + fp.o_dc)[l] = dc;
         reinterpret_cast<DevState*>(H + fp.o_st)[l] = st;
         reinterpret_cast<PowerState*>(H + fp.o_ps)[l] = PowerState{1.0, 0.0, 0.0, 0, o.sv_max_iter <= 0 ? 1 : 0};
@@ -1005,14 +1087,10 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         a.pi_part = Pd(fp.o_pipart);
         a.n = n;
         a.mb = mb;
-        a.K = K;
-        a.L = L;
         a.gb = gb;
         a.gp = gp;
         a.gd = gd;
-        a.gk = gk;
         a.nbr = nbr;
-        a.nbk = nbk;
         a.nbc = nbc;
         a.max_iter = o.max_iter;
         a.polish_max_iter = o.polish_max_iter;
@@ -1020,7 +1098,14 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         a.sv_max_iter = o.sv_max_iter;
         a.sv_tol = o.sv_tol;
     }
-    const FamArgs args = fp.args;
+    // the parts of the arguments that admission changes
+    auto setShape = [&](FamArgs& a) {
+        a.K = fp.K;
+        a.L = L;
+        a.gk = fp.K > 0 ? famBlocks(fp.K) : 0;
+        a.nbk = L;  // one check block per lane for its appended rows (identity partials when it has none)
+    };
+    setShape(fp.args);
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     PDLPX_BCK(cudaEventCreate(&ev0));
@@ -1043,30 +1128,36 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
     auto hostSeconds = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
     auto stopped = [&]() { return stop != nullptr && stop->load(std::memory_order_relaxed) != 0; };
     std::vector<int> h_flags(kFam);
-    const int stepRows = gb + gk;
-    const int ctl = (L + kCtlWarps - 1) / kCtlWarps;
-    const int nrs = std::max(1, std::min<int>(static_cast<int>((fp.colsAll() + fp.rowsAll() + kBlock - 1) / kBlock), 8 * sms));
     auto capture = [&](cudaGraphExec_t& gx, int& count, bool power) -> int32_t {
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+        const FamArgs args = fp.args;
+        const int stepRows = args.gb + args.gk;
+        const int ctl = (args.L + kCtlWarps - 1) / kCtlWarps;
+        const int nrs = std::max(1, std::min<int>(static_cast<int>((fp.colsAll() + fp.rowsAll() + kBlock - 1) / kBlock),
+                                                  8 * sms));
         cudaGraph_t graph = nullptr;
         PDLPX_BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         count = 0;
         if (power) {
             for (int r = 0; r < 8; ++r) {
                 famPowerA<<<stepRows, kBlock, 0, s>>>(args);
-                famPowerAt<<<nbc, kBlock, 0, s>>>(args);
+                famPowerAt<<<args.nbc, kBlock, 0, s>>>(args);
                 famPowerFinish1<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
-                famPowerNormalize<<<nbc, kBlock, 0, s>>>(args);
+                famPowerNormalize<<<args.nbc, kBlock, 0, s>>>(args);
                 famPowerFinish2<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
                 count += 5;
             }
         } else {
             for (int k = 1; k <= o.termination_eval_frequency; ++k) {
-                famPrimal<<<gp, kBlock, 0, s>>>(args, k);
-                famDual<<<gd + gk, kBlock, 0, s>>>(args, k);
+                famPrimal<<<args.gp, kBlock, 0, s>>>(args, k);
+                famDual<<<args.gd + args.gk, kBlock, 0, s>>>(args, k);
                 count += 2;
             }
-            famCheckRows<<<nbr + nbk, kBlock, 0, s>>>(args);
-            famCheckCols<<<nbc, kBlock, 0, s>>>(args);
+            famCheckRows<<<args.nbr + args.nbk, kBlock, 0, s>>>(args);
+            famCheckCols<<<args.nbc, kBlock, 0, s>>>(args);
             famController<<<ctl, 32 * kCtlWarps, 0, s>>>(args);
             famRestart<<<nrs, kBlock, 0, s>>>(args);
             famFinish<<<1, kFam, 0, s>>>(args);
@@ -1078,85 +1169,235 @@ int32_t solveFamilyPack(FamPack& fp, const pdlpx_options& o, std::chrono::steady
         PDLPX_BCK(ie);
         return PDLPX_OK;
     };
-
-    // ---- power iteration of every lane
-    if (o.sv_max_iter > 0) {
-        int32_t rc = capture(fp.power, fp.power_launches, true);
-        if (rc != PDLPX_OK) return rc;
-        for (int guard = 0; guard < 2 + o.sv_max_iter / 8; ++guard) {
-            PDLPX_BCK(cudaGraphLaunch(fp.power, s));
-            launches += fp.power_launches;
-            PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), args.counters, 4, cudaMemcpyDeviceToHost, s));
-            PDLPX_BCK(cudaStreamSynchronize(s));
-            if (h_flags[0] >= L || stopped()) break;
+    // power iteration of every lane whose PowerState is not done, then the step sizes
+    auto powerPhase = [&]() -> int32_t {
+        if (o.sv_max_iter > 0) {
+            int32_t rc = capture(fp.power, fp.power_launches, true);
+            if (rc != PDLPX_OK) return rc;
+            for (int guard = 0; guard < 2 + o.sv_max_iter / 8; ++guard) {
+                PDLPX_BCK(cudaGraphLaunch(fp.power, s));
+                launches += fp.power_launches;
+                PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), fp.args.counters, 4, cudaMemcpyDeviceToHost, s));
+                PDLPX_BCK(cudaStreamSynchronize(s));
+                if (h_flags[0] >= L || stopped()) break;
+            }
         }
+        // the step of every lane from its power result; a lane already iterating
+        // gets the value it has (its power state is unchanged) and its lane
+        // parameters as the end of a cycle writes them
+        famInitStep<<<1, kFam, 0, s>>>(fp.args);
+        ++launches;
+        PDLPX_BCK(cudaGetLastError());
+        return PDLPX_OK;
+    };
+    {
+        int32_t rc = powerPhase();
+        if (rc != PDLPX_OK) return rc;
+        rc = capture(fp.cycle, fp.cycle_launches, false);
+        if (rc != PDLPX_OK) return rc;
     }
-    famInitStep<<<1, kFam, 0, s>>>(args);
-    ++launches;
-    PDLPX_BCK(cudaGetLastError());
+
+    // ---- admission: members that arrive while the pack runs take free lanes
+    // between cycles.  The appended rows of all lanes are rebuilt (the members
+    // still running keep their appended rows' iterates), the new member's
+    // columns and base rows are written into its lane, its state starts fresh,
+    // its power iteration runs (the others' power state is done, so the power
+    // kernels skip them) and the graphs are captured again for the new shape.
+    std::vector<double> lane_dev0(kFam, 0.0), lane_t0(kFam, 0.0);
+    auto admitMembers = [&](std::vector<int>& fresh_lanes) -> int32_t {
+        fresh_lanes.clear();
+        if (!admit) return PDLPX_OK;
+        int K_run = 0;
+        int64_t Z_run = 0;
+        for (int l = 0; l < kFam; ++l)
+            if (in_use[l] && fp.items[l]) {
+                K_run += famCuts(*fp.items[l], mb);
+                Z_run += famCutEntries(*fp.items[l], mb);
+            }
+        for (int l = 0; l < kFam; ++l) {
+            if (in_use[l]) continue;
+            Item* it = nullptr;
+            int id = -1;
+            auto fits = [&](const Item& c) {
+                return K_run + famCuts(c, mb) <= fp.Kcap && Z_run + famCutEntries(c, mb) <= fp.Zkcap;
+            };
+            if (!admit(fits, it, id) || it == nullptr) break;
+            K_run += famCuts(*it, mb);
+            Z_run += famCutEntries(*it, mb);
+            fp.items[l] = it;
+            in_use[l] = 1;
+            lane_id[l] = id;
+            fresh_lanes.push_back(l);
+        }
+        if (fresh_lanes.empty()) return PDLPX_OK;
+        const int L_new = std::max(L, fresh_lanes.back() + 1);
+        // appended rows: keep the running members' iterates of their rows
+        const size_t Kold = static_cast<size_t>(fp.K);
+        std::vector<double> ov[4];
+        double* const drow[4] = {fp.args.yc, fp.args.yi, fp.args.yh, fp.args.ys};
+        for (int k = 0; k < 4; ++k) {
+            ov[k].resize(Kold);
+            if (Kold > 0)
+                PDLPX_BCK(cudaMemcpyAsync(ov[k].data(), drow[k] + Rb, 8 * Kold, cudaMemcpyDeviceToHost, s));
+        }
+        PDLPX_BCK(cudaStreamSynchronize(s));
+        const std::vector<int> old_first = fp.qfirst;
+        FamCuts c;
+        famBuildCuts(fp, in_use, c);
+        const size_t Kn = static_cast<size_t>(c.K);
+        std::vector<RowPack<double>> krp(Kn);
+        std::vector<double> krs(Kn), kv[4];
+        for (auto& v : kv) v.assign(Kn, 0.0);
+        std::vector<FamLaneData> fresh(fresh_lanes.size());
+        for (size_t f = 0; f < fresh_lanes.size(); ++f) famLaneData(*fp.items[fresh_lanes[f]], n, fresh[f]);
+        for (int l = 0; l < kFam; ++l) {
+            if (!in_use[l]) continue;
+            const Item& it = *fp.items[l];
+            const auto fi = std::find(fresh_lanes.begin(), fresh_lanes.end(), l);
+            const bool is_new = fi != fresh_lanes.end();
+            const ScaledLp& sc = it.sc;
+            for (int i = mb; i < it.lp.m; ++i) {
+                const size_t r = static_cast<size_t>(c.kf[l] + i - mb);
+                krp[r] = RowPack<double>{sc.sigma[i], sc.rl[i], sc.ru[i], static_cast<double>(sc.row_type[i])};
+                krs[r] = sc.row_scale[i];
+                if (is_new) {
+                    const FamLaneData& q = fresh[static_cast<size_t>(fi - fresh_lanes.begin())];
+                    kv[0][r] = kv[1][r] = kv[2][r] = q.y[i];
+                    kv[3][r] = q.ys[i];
+                } else {
+                    const size_t o_r = static_cast<size_t>(old_first[l] + i - mb);
+                    for (int k = 0; k < 4; ++k) kv[k][r] = ov[k][o_r];
+                }
+            }
+        }
+        auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+            return bytes == 0 ? cudaSuccess : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        char* d = fp.d;
+        PDLPX_BCK(up(d + fp.o_kptr, c.kp.data(), 4 * c.kp.size()));
+        PDLPX_BCK(up(d + fp.o_kidx, c.ki.data(), 4 * c.ki.size()));
+        PDLPX_BCK(up(d + fp.o_kval, c.kv.data(), 8 * c.kv.size()));
+        PDLPX_BCK(up(d + fp.o_klane, c.kl.data(), 4 * c.kl.size()));
+        PDLPX_BCK(up(d + fp.o_kfirst, c.kf.data(), 4 * c.kf.size()));
+        PDLPX_BCK(up(d + fp.o_ktptr, c.ktp.data(), 4 * c.ktp.size()));
+        PDLPX_BCK(up(d + fp.o_ktrow, c.ktr.data(), 4 * c.ktr.size()));
+        PDLPX_BCK(up(d + fp.o_ktlane, c.ktl.data(), 4 * c.ktl.size()));
+        PDLPX_BCK(up(d + fp.o_ktval, c.ktv.data(), 8 * c.ktv.size()));
+        PDLPX_BCK(up(d + fp.o_rp + 32 * Rb, krp.data(), 32 * Kn));
+        PDLPX_BCK(up(d + fp.o_rs + 8 * Rb, krs.data(), 8 * Kn));
+        for (int k = 0; k < 4; ++k) PDLPX_BCK(up(drow[k] + Rb, kv[k].data(), 8 * Kn));
+        // the new members' lanes: columns and base rows are interleaved by lane
+        auto lane2d = [&](size_t base_off, int l, const void* src, size_t elem, size_t rows) -> cudaError_t {
+            if (rows == 0) return cudaSuccess;
+            return cudaMemcpy2DAsync(d + base_off + elem * static_cast<size_t>(l), elem * kFam, src, elem, elem, rows,
+                                     cudaMemcpyHostToDevice, s);
+        };
+        std::vector<DevConst> hdc(fresh_lanes.size());
+        std::vector<DevState> hst(fresh_lanes.size());
+        std::vector<PowerState> hps(fresh_lanes.size());
+        const double now_dev = deviceSeconds(), now_host = hostSeconds();
+        for (size_t f = 0; f < fresh_lanes.size(); ++f) {
+            const int l = fresh_lanes[f];
+            const FamLaneData& q = fresh[f];
+            const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(mb);
+            PDLPX_BCK(lane2d(fp.o_cp, l, q.cp.data(), sizeof(ColPack<double>), nn));
+            PDLPX_BCK(lane2d(fp.o_cs, l, q.cs.data(), 8, nn));
+            PDLPX_BCK(lane2d(fp.o_pix, l, g.data(), 8, nn));
+            for (size_t off : {fp.o_xc, fp.o_xi, fp.o_xh}) PDLPX_BCK(lane2d(off, l, q.x.data(), 8, nn));
+            PDLPX_BCK(lane2d(fp.o_xs, l, q.xs.data(), 8, nn));
+            PDLPX_BCK(lane2d(fp.o_rp, l, q.rp.data(), sizeof(RowPack<double>), mm));
+            PDLPX_BCK(lane2d(fp.o_rs, l, q.rs.data(), 8, mm));
+            for (size_t off : {fp.o_yc, fp.o_yi, fp.o_yh}) PDLPX_BCK(lane2d(off, l, q.y.data(), 8, mm));
+            PDLPX_BCK(lane2d(fp.o_ys, l, q.ys.data(), 8, mm));
+            lpState(*fp.items[l], o, false, nbr + L_new, nbc, hdc[f], hst[f]);
+            hps[f] = PowerState{1.0, 0.0, 0.0, 0, o.sv_max_iter <= 0 ? 1 : 0};
+            PDLPX_BCK(up(d + fp.o_dc + sizeof(DevConst) * l, &hdc[f], sizeof(DevConst)));
+            PDLPX_BCK(up(d + fp.o_st + sizeof(DevState) * l, &hst[f], sizeof(DevState)));
+            PDLPX_BCK(up(d + fp.o_ps + sizeof(PowerState) * l, &hps[f], sizeof(PowerState)));
+            PDLPX_BCK(cudaMemsetAsync(d + fp.o_flags + 4 * static_cast<size_t>(l), 0, 4, s));
+            lane_dev0[l] = now_dev;
+            lane_t0[l] = now_host;
+        }
+        uint32_t live = 0;
+        for (int l = 0; l < kFam; ++l)
+            if (in_use[l]) live |= 1u << l;
+        int32_t powered = L_new - static_cast<int32_t>(o.sv_max_iter > 0 ? fresh_lanes.size() : 0);
+        PDLPX_BCK(up(d + fp.o_live, &live, 4));
+        PDLPX_BCK(up(d + fp.o_counters, &powered, 4));
+        PDLPX_BCK(cudaStreamSynchronize(s));  // the host buffers above go out of scope
+        fp.K = c.K;
+        fp.Zk = c.Zk;
+        fp.qfirst = c.kf;
+        L = L_new;
+        setShape(fp.args);
+        int32_t rc = powerPhase();
+        if (rc != PDLPX_OK) return rc;
+        return capture(fp.cycle, fp.cycle_launches, false);
+    };
 
     // ---- restart cycles
-    {
-        int32_t rc = capture(fp.cycle, fp.cycle_launches, false);
-        if (rc != PDLPX_OK) return rc;
-    }
     SleepWait sleeper;
-    std::vector<char> collected(L, 0);
-    int ncollected = 0, cycles = 0;
+    std::vector<char> collected(kFam, 0);
+    int cycles = 0;
     auto collect = [&](int l, bool out_of_time, double secs, double dev_s) -> int32_t {
         const Item& it = *fp.items[l];
         const int32_t m = it.lp.m;
         DevState f{};
         std::vector<double> xv(n), yv(m);
-        PDLPX_BCK(cudaMemcpyAsync(&f, args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-        PDLPX_BCK(cudaMemcpy2DAsync(xv.data(), 8, args.xh + l, 8 * kFam, 8, n, cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(&f, fp.args.st + l, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpy2DAsync(xv.data(), 8, fp.args.xh + l, 8 * kFam, 8, n, cudaMemcpyDeviceToHost, s));
         if (mb > 0)
-            PDLPX_BCK(cudaMemcpy2DAsync(yv.data(), 8, args.yh + l, 8 * kFam, 8, mb, cudaMemcpyDeviceToHost, s));
+            PDLPX_BCK(cudaMemcpy2DAsync(yv.data(), 8, fp.args.yh + l, 8 * kFam, 8, mb, cudaMemcpyDeviceToHost, s));
         if (m > mb)
-            PDLPX_BCK(cudaMemcpyAsync(yv.data() + mb, args.yh + Rb + fp.qfirst[l], 8 * static_cast<size_t>(m - mb),
+            PDLPX_BCK(cudaMemcpyAsync(yv.data() + mb, fp.args.yh + Rb + fp.qfirst[l], 8 * static_cast<size_t>(m - mb),
                                       cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
         LpOutcome out;
-        finishOutcome(it, f, xv, yv, false, out_of_time, secs, dev_s, launches, out);
+        finishOutcome(it, f, xv, yv, false, out_of_time, secs - lane_t0[l], dev_s - lane_dev0[l], launches, out);
         collected[l] = 1;
-        ++ncollected;
-        done(l, std::move(out));
+        in_use[l] = 0;
+        done(lane_id[l], std::move(out));
         return PDLPX_OK;
     };
-    while (ncollected < L) {
+    auto running = [&]() {
+        int k = 0;
+        for (int l = 0; l < kFam; ++l) k += in_use[l];
+        return k;
+    };
+    std::vector<int> fresh_lanes;
+    while (running() > 0) {
         if (timeUp(t0, o.max_solve_seconds) || stopped()) break;
         PDLPX_BCK(cudaGraphLaunch(fp.cycle, s));
         launches += fp.cycle_launches;
         ++cycles;
         PDLPX_BCK(sleeper.wait(s));
-        PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
+        PDLPX_BCK(cudaMemcpyAsync(h_flags.data(), fp.args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
-        int done_count = 0;
         bool fresh = false;
-        for (int l = 0; l < L; ++l) {
-            done_count += h_flags[l] & 1;
-            fresh |= (h_flags[l] & 1) && !collected[l];
-        }
+        for (int l = 0; l < L; ++l) fresh |= in_use[l] && (h_flags[l] & 1);
         if (fresh) {
             const double dev_s = deviceSeconds(), secs = hostSeconds();
             for (int l = 0; l < L; ++l) {
-                if (!(h_flags[l] & 1) || collected[l]) continue;
+                if (!in_use[l] || !(h_flags[l] & 1)) continue;
                 const int32_t rc = collect(l, false, secs, dev_s);
                 if (rc != PDLPX_OK) return rc;
             }
         }
         if (o.verbose && cycles % 10 == 0) {
-            std::printf("PDLP family %7d iterations per LP  %d/%d LPs done  %d shared rows  %d appended rows  %.3fs  [B200]\n",
-                        cycles * o.termination_eval_frequency, done_count, L, mb, K, hostSeconds());
+            std::printf("PDLP family %7d cycles  %d LPs running  %d shared rows  %d appended rows  %.3fs  [B200]\n",
+                        cycles, running(), mb, fp.K, hostSeconds());
             std::fflush(stdout);
         }
-        if (done_count >= L) break;
+        if (!stopped() && running() < kFam) {
+            const int32_t rc = admitMembers(fresh_lanes);
+            if (rc != PDLPX_OK) return rc;
+        }
     }
-    if (ncollected < L) {
+    if (running() > 0) {
         const double dev_s = deviceSeconds(), secs = hostSeconds();
         const bool out_of_time = timeUp(t0, o.max_solve_seconds);
         for (int l = 0; l < L; ++l) {
-            if (collected[l]) continue;
+            if (!in_use[l]) continue;
             const int32_t rc = collect(l, out_of_time, secs, dev_s);
             if (rc != PDLPX_OK) return rc;
         }

@@ -73,9 +73,21 @@ FamilyPtr makeFamilyBase(const pdlpx_lp& base);
 bool familyMember(const PreparedLp& p, const FamilyBase& f, const pdlpx_options& o);
 // Device bytes a member adds to a family pack (its lane plus its share of the base rows).
 size_t familyMemberBytes(const PreparedLp& p, const FamilyBase& f);
+// Offered between restart cycles while a family pack has a free lane: return a
+// prepared member of the same family for which fits(lp) holds (its appended
+// rows fit the room the pack reserved) and an id under which the pack reports
+// it through `done`, or false when no member is waiting.  The caller keeps the
+// returned LP alive until it is reported.
+using FamilyAdmit =
+    std::function<bool(const std::function<bool(const PreparedLp&)>& fits, PreparedLp*& lp, int& id)>;
+
 // Solve up to kFamilyLanes members of one family as one pack on the current
-// device (FP64 iterates, per-LP scaling and state); `done` as for solvePrepared.
+// device (FP64 iterates, per-LP scaling and state); `done` as for solvePrepared
+// (ids 0..lps.size()-1 for the initial members).  With `admit`, members that
+// arrive while the pack runs take the lanes of finished ones (or unused lanes)
+// between restart cycles, and the pack runs until no lane is busy.
 int32_t solveFamily(const FamilyBase& f, const std::vector<PreparedLp*>& lps, const pdlpx_options& o,
-                    const std::atomic<int>* stop, const LpDone& done, std::string& err);
+                    const std::atomic<int>* stop, const LpDone& done, std::string& err,
+                    const FamilyAdmit& admit = {});
 
 }  // namespace pdlpx

@@ -295,6 +295,7 @@ public:
         const double span = completed_ > 0 ? std::chrono::duration<double>(last_complete_ - first_submit_).count() : 0.0;
         s->lps_per_sec = span > 0.0 ? static_cast<double>(completed_) / span : 0.0;
         s->bytes_in_flight = static_cast<double>(inflight);
+        s->admitted = admitted_;
     }
 
 private:
@@ -448,7 +449,37 @@ private:
         };
         pdlpx_options o = opt_;
         o.device = devices_[static_cast<size_t>(dev)];
-        const int32_t rc = fam ? solveFamily(*fam, lps, o, &stop_, done, err) : solvePrepared(lps, o, &stop_, done, err);
+        const size_t du = static_cast<size_t>(dev);
+        // Continuous admission into a family pack: between restart cycles the pack
+        // offers its free lanes, and a waiting member of its family whose
+        // appended rows fit takes one (within this device's budget) instead of
+        // waiting for a new pack.
+        FamilyAdmit admit;
+        if (fam && cfg_.lane_admission) {
+            admit = [&](const std::function<bool(const PreparedLp&)>& fits, PreparedLp*& lp, int& id) -> bool {
+                std::lock_guard<std::mutex> g(mu_);
+                if (closed_) return false;
+                for (auto it = ready_q_.begin(); it != ready_q_.end(); ++it) {
+                    Request* r = reqs_.at(*it).get();
+                    if (r->family != fam || !fits(*r->prep)) continue;
+                    if (bytes_in_flight_[du] + r->bytes > budget_[du]) return false;
+                    r->state = kRunning;
+                    bytes += r->bytes;
+                    bytes_in_flight_[du] += r->bytes;
+                    pack.push_back(r);
+                    finished.push_back(0);
+                    preps.push_back(std::move(r->prep));
+                    lp = preps.back().get();
+                    id = static_cast<int>(pack.size()) - 1;
+                    ready_q_.erase(it);
+                    ++admitted_;
+                    return true;
+                }
+                return false;
+            };
+        }
+        const int32_t rc =
+            fam ? solveFamily(*fam, lps, o, &stop_, done, err, admit) : solvePrepared(lps, o, &stop_, done, err);
         std::lock_guard<std::mutex> g(mu_);
         for (size_t k = 0; k < pack.size(); ++k) {
             if (finished[k]) continue;
@@ -481,6 +512,7 @@ private:
     std::vector<size_t> bytes_in_flight_;  // per device
     std::vector<int> packs_on_;            // per device
     int64_t next_ticket_ = 1, submitted_ = 0, completed_ = 0;
+    int64_t admitted_ = 0;  // requests that joined a running family pack
     Clock::time_point first_submit_, last_complete_;
     std::vector<double> latencies_;
 };
@@ -509,6 +541,7 @@ void pdlpx_server_config_default(pdlpx_server_config* c) {
     c->queue_limit = 100000;
     c->batch_window_ms = 50;
     c->families = 1;
+    c->lane_admission = 1;
 }
 
 int32_t pdlpx_server_create(const pdlpx_options* opts, const pdlpx_server_config* cfg, pdlpx_server** out) {

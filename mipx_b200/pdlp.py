@@ -543,7 +543,8 @@ class Server:
 
     def __init__(self, options: PdlpOptions, budget_bytes: float = 0.0, max_packs: int = 4,
                  max_pack_lps: int = 32, prep_threads: int = 0, queue_limit: int = 100000,
-                 batch_window_ms: int = 50, families: bool = True, devices: Sequence[int] | None = None):
+                 batch_window_ms: int = 50, families: bool = True, devices: Sequence[int] | None = None,
+                 lane_admission: bool = True):
         self._lib = _capi.load()
         cfg = _capi.ServerConfig()
         self._lib.pdlpx_server_config_default(C.byref(cfg))
@@ -554,6 +555,7 @@ class Server:
         cfg.queue_limit = int(queue_limit)
         cfg.batch_window_ms = int(batch_window_ms)
         cfg.families = int(bool(families))
+        cfg.lane_admission = int(bool(lane_admission))
         if devices is not None and len(devices) > 1:
             if len(devices) > len(cfg.devices):
                 raise ValueError(f"at most {len(cfg.devices)} devices")

@@ -229,3 +229,29 @@ def test_family_off_uses_regular_packs():
     for r, _, _ in res:
         assert r.status == Status.Optimal
         assert r.fp64_iterations < r.iterations
+
+
+def test_family_lane_admission_joins_running_pack():
+    """Continuous admission at lane granularity: with one pack stream, nodes that
+    arrive while a family pack runs take its free lanes between restart cycles
+    instead of waiting for it to end; each admitted node's result is
+    bit-identical to the same node solved in a family of one (a lane's
+    arithmetic depends on its LP alone, whenever it joins)."""
+    base, nodes = _family(seed=61, count=5, m=20000, n=50000)
+    o = PdlpOptions(**TIGHT)
+    with Server(o, max_packs=1, max_pack_lps=32, batch_window_ms=0) as srv:
+        tb = srv.submit(base)
+        srv.wait(tb, timeout=300)
+        first = srv.submit(nodes[0], warm=tb)  # starts a pack of one at once
+        time.sleep(0.05)
+        later = [srv.submit(nd, warm=tb) for nd in nodes[1:]]
+        res = [srv.wait(t, timeout=300) for t in [first] + later]
+        st = srv.stats()
+    assert st["admitted"] >= 1, st
+    for k in (0, 1, len(nodes) - 1):
+        alone = _solve_nodes(base, [nodes[k]], o, max_packs=1, lane_admission=False)[0]
+        (r, x, y), (q, u, v) = res[k], alone
+        assert r.status == q.status == Status.Optimal
+        assert r.iterations == q.iterations and r.objective == q.objective
+        np.testing.assert_array_equal(x, u)
+        np.testing.assert_array_equal(y, v)
