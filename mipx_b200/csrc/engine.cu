@@ -1456,6 +1456,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     dc.step_up = opt_.adaptive_step_up;
     dc.precond_ratio = opt_.preconditioner_refresh_ratio;
     dc.switch_score = 30.0;
+    dc.noise_factor = 10.0;
     PDLPX_CK(cudaMemcpyAsync(d.dc, &dc, sizeof(DevConst), cudaMemcpyHostToDevice, s));
 
     DevState st0{};

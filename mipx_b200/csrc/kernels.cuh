@@ -72,6 +72,7 @@ struct DevConst {
     double step_lb, step_ub, step_down, step_up;
     double precond_ratio;
     double switch_score;
+    double noise_factor;  // hand-over only when a residual is within this factor of its FP32 noise floor
 };
 
 // Packed per-column / per-row constants of the step kernels (one vector load each).
@@ -136,6 +137,7 @@ enum RowSlot {
     R_UB_LE,        // max  Ax/r over '<=' rows                 certificate
     R_UB_GE,        // min  Ax/r over '>=' rows                 certificate
     R_ADAPT,        // sum  sigma_i (Ax - prev Ax)^2           adaptive step
+    R_NOISE_SQ,     // sum  (sum_j |a_ij x_j|)^2 (original units)  FP32 noise floor of the primal residual
     kRowSlots
 };
 enum ColSlot {
@@ -152,6 +154,7 @@ enum ColSlot {
     C_MAX_GUB,    // max over finite-ub columns                  certificate
     C_COLSUP,     // sum column support of the dual ray         certificate
     C_ADAPT,      // sum (x_hat - prev x_hat)^2 / tau        adaptive step
+    C_NOISE_SQ,   // sum (sum_i |a_ij y_i|)^2 (original units)   FP32 noise floor of the dual residual
     kColSlots
 };
 enum SlotOp { OP_SUM = 0, OP_MIN = 1, OP_MAX = 2 };
@@ -262,12 +265,49 @@ __device__ __forceinline__ Acc rowDot(int b, int e, int lane, const int* __restr
     return rowDotU<G, 4, Acc>(b, e, lane, idx, val, x);
 }
 
-// Two dot products of one row (A^T y and A^T (y - y0)) in one pass.
+// rowDot (same loads, same accumulation order for the dot product) that also
+// sums |a_k x_k|: the scale of the rounding an FP32 product of this row carries.
+template <int G, class V, class X>
+__device__ __forceinline__ double rowDotAbs(int b, int e, int lane, const int* __restrict__ idx,
+                                            const V* __restrict__ val, const X* __restrict__ x, double& sa) {
+    constexpr int U = 4;
+    double s[U], a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) s[u] = a[u] = 0.0;
+    for (int k0 = b + lane; k0 < e; k0 += U * G) {
+        int c[U];
+        V v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u * G;
+            const bool ok = k < e;
+            c[u] = ok ? __ldg(idx + k) : 0;
+            v[u] = ok ? __ldg(val + k) : V(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double p = static_cast<double>(v[u]) * static_cast<double>(__ldg(x + c[u]));
+            s[u] += p;
+            a[u] += fabs(p);
+        }
+    }
+    double t = s[0];
+    sa = a[0];
+#pragma unroll
+    for (int u = 1; u < U; ++u) {
+        t += s[u];
+        sa += a[u];
+    }
+    return t;
+}
+
+// Two dot products of one row (A^T y and A^T (y - y0)) in one pass, and the
+// sum of |a_k y_k| (the scale of the rounding an FP32 product of the row carries).
 template <int G>
 __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __restrict__ idx,
                                         const double* __restrict__ val, const float* y,
-                                        const float* y0, double& s, double& d) {
-    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+                                        const float* y0, double& s, double& d, double& sa) {
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0, z0 = 0, z1 = 0;
     int k = b + lane;
     for (; k + G < e; k += 2 * G) {
         const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G);
@@ -275,6 +315,8 @@ __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __res
         const double y0v = y[c0], y1v = y[c1];
         a0 += v0 * y0v;
         a1 += v1 * y1v;
+        z0 += fabs(v0 * y0v);
+        z1 += fabs(v1 * y1v);
         b0 += v0 * (y0v - static_cast<double>(y0[c0]));
         b1 += v1 * (y1v - static_cast<double>(y0[c1]));
     }
@@ -282,16 +324,18 @@ __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __res
         const int c = __ldg(idx + k);
         const double v = __ldg(val + k), yv = y[c];
         a0 += v * yv;
+        z0 += fabs(v * yv);
         b0 += v * (yv - static_cast<double>(y0[c]));
     }
     s = a0 + a1;
     d = b0 + b1;
+    sa = z0 + z1;
 }
 template <int G>
 __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __restrict__ idx,
                                         const double* __restrict__ val, const double* y,
-                                        const double* y0, double& s, double& d) {
-    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+                                        const double* y0, double& s, double& d, double& sa) {
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0, z0 = 0, z1 = 0;
     int k = b + lane;
     for (; k + G < e; k += 2 * G) {
         const int c0 = __ldg(idx + k), c1 = __ldg(idx + k + G);
@@ -299,6 +343,8 @@ __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __res
         const double y0v = y[c0], y1v = y[c1];
         a0 += v0 * y0v;
         a1 += v1 * y1v;
+        z0 += fabs(v0 * y0v);
+        z1 += fabs(v1 * y1v);
         b0 += v0 * (y0v - y0[c0]);
         b1 += v1 * (y1v - y0[c1]);
     }
@@ -306,10 +352,12 @@ __device__ __forceinline__ void rowDot2(int b, int e, int lane, const int* __res
         const int c = __ldg(idx + k);
         const double v = __ldg(val + k), yv = y[c];
         a0 += v * yv;
+        z0 += fabs(v * yv);
         b0 += v * (yv - y0[c]);
     }
     s = a0 + a1;
     d = b0 + b1;
+    sa = z0 + z1;
 }
 
 __device__ __forceinline__ bool active(const DevState* st, int prec, int koff, int max_iter,
@@ -629,10 +677,12 @@ __device__ __forceinline__ double slotInit(int op) {
 // movement, and the Farkas / primal-ray certificate terms of pdlp.cpp:119-284
 // in scaled space.
 __device__ __forceinline__ void accRowMetrics(double (&acc)[kRowSlots], const DevConst& dc, double ax, double rl,
-                                              double ru, double r, double y, double yi) {
+                                              double ru, double r, double y, double yi, double axabs = 0.0) {
     const double cl = ax < rl ? rl : (ru < ax ? ru : ax);
     const double v = (ax - cl) / (dc.con_scale * r);
     acc[R_PRES_SQ] += v * v;
+    const double nz = axabs / (dc.con_scale * r);
+    acc[R_NOISE_SQ] += nz * nz;
     acc[R_PRES_MAX] = fmax(acc[R_PRES_MAX], fabs(v));
     const double dy = y - yi;
     const bool hl = isfinite(rl), hu = isfinite(ru);
@@ -673,7 +723,8 @@ __device__ __forceinline__ void accRowMetrics(double (&acc)[kRowSlots], const De
 // on float(ub) < ub is at its bound, not interior.
 template <class T>
 __device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const DevConst& dc, double xh, double xi,
-                                              double c, double lb, double ub, double cs, double aty, double atdy) {
+                                              double c, double lb, double ub, double cs, double aty, double atdy,
+                                              double atyabs = 0.0) {
     const double dx = xh - xi;
     const bool hl = isfinite(lb), hu = isfinite(ub);
     acc[C_POBJ] += c * xh;
@@ -696,6 +747,8 @@ __device__ __forceinline__ void accColMetrics(double (&acc)[kColSlots], const De
         dr = g;
     const double d = dr / (dc.obj_scale * cs);
     acc[C_DRES_SQ] += d * d;
+    const double nd = atyabs / (dc.obj_scale * cs);
+    acc[C_NOISE_SQ] += nd * nd;
     acc[C_DRES_MAX] = fmax(acc[C_DRES_MAX], fabs(d));
     double gp = g;
     if (!hl) gp = fmin(gp, 0.0);
@@ -738,12 +791,13 @@ __device__ __forceinline__ void checkRowsRange(const CheckArgs<T>& p, const DevC
     for (int base = lo; base < hi; base += stride) {
         const int i = base + threadIdx.x / G;
         const bool valid = i < hi;
-        double ax = 0.0;
-        if (valid) ax = rowDot<G, double>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh);
+        double ax = 0.0, axa = 0.0;
+        if (valid) ax = rowDotAbs<G>(p.a_ptr[i], p.a_ptr[i + 1], lane, p.a_idx, p.a_val, p.xh, axa);
         ax = groupSum<G>(ax);
+        axa = groupSum<G>(axa);
         if (valid && lane == 0) {
             accRowMetrics(acc, dc, ax, p.rl64[i], p.ru64[i], p.rs64[i], static_cast<double>(p.yh[i]),
-                          static_cast<double>(p.yi[i]));
+                          static_cast<double>(p.yi[i]), axa);
             if (adapt) {
                 const double d = ax - p.prev_ax[i];
                 acc[R_ADAPT] += p.sig64[i] * d * d;
@@ -781,14 +835,15 @@ __device__ __forceinline__ void checkColsRange(const CheckArgs<T>& p, const DevC
     for (int base = lo; base < hi; base += stride) {
         const int j = base + threadIdx.x / G;
         const bool valid = j < hi;
-        double aty = 0.0, atdy = 0.0;
-        if (valid) rowDot2<G>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yh, p.yi, aty, atdy);
+        double aty = 0.0, atdy = 0.0, atya = 0.0;
+        if (valid) rowDot2<G>(p.at_ptr[j], p.at_ptr[j + 1], lane, p.at_idx, p.at_val, p.yh, p.yi, aty, atdy, atya);
         aty = groupSum<G>(aty);
         atdy = groupSum<G>(atdy);
+        atya = groupSum<G>(atya);
         if (valid && lane == 0) {
             const double xh = static_cast<double>(p.xh[j]);
             accColMetrics<T>(acc, dc, xh, static_cast<double>(p.xi[j]), p.c64[j], p.lb64[j], p.ub64[j], p.cs64[j],
-                             aty, atdy);
+                             aty, atdy, atya);
             if (adapt) {
                 const double dd = xh - p.prev_xh[j];
                 acc[C_ADAPT] += dd * dd / p.tau64[j];
