@@ -120,7 +120,11 @@ typedef struct pdlpx_options {
                                          server, time each sliced-ELL class's entries-per-round variants
                                          on the pack (identical results); 0 (default): row-length table,
                                          deterministic */
-    int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step */
+    int32_t shape_primal;             /* 0 = automatic; k > 0 pins launch shape k-1 of the primal step's
+                                         short rows: 1..16 the CSR shapes (lanes x rows x loads), 17..19
+                                         sliced ELL with 4 / 8 / 16 entries per round, 20..22 the same
+                                         with streaming loads of the matrix (no L1 allocation,
+                                         evict-first in L2; single-LP engine only) */
     int32_t shape_dual;               /* 0 = automatic; k > 0 pins launch shape k-1 of the dual step */
     int32_t batch_pack_mb;            /* pdlpx_batch_solve: device megabytes per pack of LPs solved
                                          together (0 = 85% of free device memory); larger batches are

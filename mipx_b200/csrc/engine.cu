@@ -130,25 +130,45 @@ __global__ void __launch_bounds__(kBlock) powerFinish2(PowerArgs a) {
 // ---- sliced-ELL step launches ------------------------------------------------
 // The short rows [begin, end) of a matrix side stored as sliced ELL (slice s of
 // the range described by hdr[s]); one thread per row, the fused step of
-// kernels.cuh.  Compiled for 8 resident blocks (32 registers), the occupancy
-// at which the packed batch's sliced-ELL kernels measured fastest.
-template <int U, class T>
-__global__ void __launch_bounds__(kBlock, 8) primalSellStep(IterArgs<T> p, const int2* __restrict__ hdr,
-                                                            const int* __restrict__ idx, const T* __restrict__ val,
-                                                            int koff, int begin, int end) {
-    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
-    if (begin + r >= end) return;
-    primalSellFrom<U, T>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+// kernels.cuh.  FP32 kernels are compiled for 8 resident blocks (32
+// registers), the occupancy at which the packed batch's sliced-ELL kernels
+// measured fastest; the FP64 kernels, whose values and gathers take register
+// pairs, for 5 (51 registers: at 32 they spilled 130-400 bytes per thread).
+template <class T>
+constexpr int sellMinBlocks() {
+    return sizeof(T) == 8 ? 5 : 8;
 }
 
-template <int U, class T>
-__global__ void __launch_bounds__(kBlock, 8) dualSellStep(IterArgs<T> p, const int2* __restrict__ hdr,
-                                                          const int* __restrict__ idx, const T* __restrict__ val,
-                                                          int koff, int begin, int end) {
+template <int U, class T, bool ST>
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
+    primalSellStep(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
+                   const T* __restrict__ val, int koff, int begin, int end) {
     const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
     if (begin + r >= end) return;
-    dualSellFrom<U, T>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+    primalSellFrom<U, T, ST>(p, idx, val, begin + r, hdr[r / kSlice], koff);
 }
+
+template <int U, class T, bool ST>
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
+    dualSellStep(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
+                 const T* __restrict__ val, int koff, int begin, int end) {
+    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    dualSellFrom<U, T, ST>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+}
+
+// Sliced-ELL shapes of the single-LP engine: kNumShapes + k for k < kEngSell,
+// U = kSellU[k % kNumSell], streaming loads for k >= kNumSell.
+constexpr int kEngSell = 2 * kNumSell;
+#define PDLPX_ENG_SELL_SWITCH(S, CALL)                                              \
+    switch (S - kNumShapes) {                                                       \
+        case 0: { constexpr int UU = kSellU[0]; constexpr bool SS = false; CALL; } break; \
+        case 1: { constexpr int UU = kSellU[1]; constexpr bool SS = false; CALL; } break; \
+        case 2: { constexpr int UU = kSellU[2]; constexpr bool SS = false; CALL; } break; \
+        case 3: { constexpr int UU = kSellU[0]; constexpr bool SS = true; CALL; } break;  \
+        case 4: { constexpr int UU = kSellU[1]; constexpr bool SS = true; CALL; } break;  \
+        default: { constexpr int UU = kSellU[2]; constexpr bool SS = true; CALL; } break; \
+    }
 
 static int gridFor(int64_t rows, int G) {
     const int64_t threads = rows * G;
@@ -390,8 +410,8 @@ static int sellGrid(int64_t rows) { return static_cast<int>(std::max<int64_t>(1,
 template <class T>
 void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
     if (isSell(shape)) {
-        PDLPX_SELL_SWITCH(shape, (primalSellStep<UU, T><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
-                                     ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n)));
+        PDLPX_ENG_SELL_SWITCH(shape, (primalSellStep<UU, T, SS><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
+                                         ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n)));
     } else {
         PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<gridForShape(d.n - d.nlP, shape), kBlock, 0, s>>>(
                                       ia, k, d.nlP, d.n)));
@@ -400,8 +420,8 @@ void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int 
 template <class T>
 void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
     if (isSell(shape)) {
-        PDLPX_SELL_SWITCH(shape, (dualSellStep<UU, T><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
-                                     ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
+        PDLPX_ENG_SELL_SWITCH(shape, (dualSellStep<UU, T, SS><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
+                                         ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
     } else {
         PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<gridForShape(d.m - d.nlD, shape), kBlock, 0, s>>>(
                                       ia, k, d.nlD, d.m)));
@@ -653,7 +673,7 @@ static bool buildSell(const Csr& a, int32_t r0, SellHost& h) {
 // (kNumShapes + 1 .. kNumShapes + kNumSell), else 4 entries per round for mean
 // lengths up to 12 and 8 above (the packed batch's measured picks).
 static int sellShape(int pinned, int64_t nnz, int32_t rows) {
-    if (pinned > kNumShapes && pinned <= kNumShapes + kNumSell) return pinned - 1;
+    if (pinned > kNumShapes && pinned <= kNumShapes + kEngSell) return pinned - 1;
     const double mean = rows > 0 ? static_cast<double>(nnz) / rows : 0.0;
     return kNumShapes + (mean <= 12.0 ? 0 : 1);
 }
@@ -1060,7 +1080,7 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
         float best = 0.0f;
         int32_t rc = timeShape(which, pick, best);
         if (rc != PDLPX_OK) return rc;
-        for (int c = 0; c < kNumShapes + (has_sell ? kNumSell : 0); ++c) {
+        for (int c = 0; c < kNumShapes + (has_sell ? kEngSell : 0); ++c) {
             if (c == pick || (!isSell(c) && (kShapes[c].G * 4 < g0 || kShapes[c].G > g0 * 4))) continue;
             float ms = 0.0f;
             rc = timeShape(which, c, ms);

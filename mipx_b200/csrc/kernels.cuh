@@ -585,16 +585,44 @@ constexpr int kSlice = 32;           // rows per slice (one warp)
 constexpr int kSellU[] = {4, 8, 16};  // entries per thread per round of the variants
 constexpr int kNumSell = 3;
 
+// Loads of the matrix stream (indices and values, read once per step) that
+// neither allocate in L1 nor stay in L2 ahead of other lines (evict-first L2
+// policy), so L1 and L2 keep the gathered iterate vectors.
+__device__ __forceinline__ unsigned long long evictFirstPolicy() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ int ldStream(const int* a, unsigned long long pol) {
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ldStream(const float* a, unsigned long long pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ldStream(const double* a, unsigned long long pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+
 // Dot product of this thread's row with x: entry k of the row sits at
 // hdr.x + k * 32 + lane; U entries are loaded per round, then their U gathers,
-// then the products are summed in entry order.
-// Entries past the row's end hold index 0 and value 0 (index 0 always exists).
-template <int U, class V, class X>
+// then the products are summed in entry order (so every U, and either kind of
+// load, gives the same bits).  ST: the index / value loads use the streaming
+// hints above.  Entries past the row's end hold index 0 and value 0 (index 0
+// always exists).
+template <int U, class V, class X, bool ST = false>
 __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* __restrict__ val, int2 h, int lane,
                                           const X* __restrict__ x) {
     const int* ip = idx + h.x + lane;
     const V* vp = val + h.x + lane;
     double acc = 0.0;
+    unsigned long long pol = 0;
+    if constexpr (ST) pol = evictFirstPolicy();
     for (int k0 = 0; k0 < h.y; k0 += U) {
         int c[U];
         V v[U];
@@ -602,8 +630,13 @@ __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* 
         for (int u = 0; u < U; ++u) {
             const int k = k0 + u;
             const bool ok = k < h.y;
-            c[u] = ok ? __ldg(ip + k * kSlice) : 0;
-            v[u] = ok ? __ldg(vp + k * kSlice) : V(0);
+            if constexpr (ST) {
+                c[u] = ok ? ldStream(ip + k * kSlice, pol) : 0;
+                v[u] = ok ? ldStream(vp + k * kSlice, pol) : V(0);
+            } else {
+                c[u] = ok ? __ldg(ip + k * kSlice) : 0;
+                v[u] = ok ? __ldg(vp + k * kSlice) : V(0);
+            }
         }
         X g[U];
 #pragma unroll
@@ -614,13 +647,13 @@ __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* 
     return acc;
 }
 
-template <int U, class T>
+template <int U, class T, bool ST = false>
 __device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
                                                int koff) {
     const ColPack<T> q = p.cp[j];
     const double xc = p.xc[j];
     const double xi = static_cast<double>(p.xi[j]);
-    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
+    const double s = sellDot<U, T, double, ST>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     const double step = p.st->step, pw = p.st->pw;
@@ -629,13 +662,13 @@ __device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* 
     primalUpdate<T>(p, j, q, xc, xi, s, step, pw, lam, last);
 }
 
-template <int U, class T>
+template <int U, class T, bool ST = false>
 __device__ __forceinline__ void dualSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int i, int2 h,
                                              int koff) {
     const RowPack<T> q = p.rp[i];
     const double yc = p.yc[i];
     const double yi = static_cast<double>(p.yi[i]);
-    const double s = sellDot<U>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
+    const double s = sellDot<U, T, T, ST>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     const double step = p.st->step, pw = p.st->pw;
