@@ -98,6 +98,8 @@ def parse():
                    help="profiling run: LPS node LPs of the serving workload's base LP as one family pack")
     p.add_argument("--profile-iters", type=int, default=2000,
                    help="iteration cap of the --profile-* runs")
+    p.add_argument("--profile-fp64", action="store_true",
+                   help="profiling run of the single-LP cases in FP64 (the iterations after the hand-over)")
     return p.parse_args()
 
 
@@ -592,7 +594,7 @@ def serving_line(local, requests: int, rates) -> dict:
 def profile_run(args, local) -> None:
     """Capped runs for ncu (no JSON line)."""
     from mipx_b200 import generators as G
-    from mipx_b200.pdlp import PdlpOptions, PdlpSolver, batch_solve
+    from mipx_b200.pdlp import PdlpOptions, PdlpSolver, Precision, batch_solve
     o = PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local,
                     max_iter=args.profile_iters)
     if args.profile_batch:
@@ -619,6 +621,8 @@ def profile_run(args, local) -> None:
         lps.append(G.powerlaw_lp(args.profile_large, 4 * args.profile_large, 2, 2000, 10.0, 0.01, 1e3, 11)[0])
     if args.profile_transport:
         lps.append(G.transport_lp(1000, 1000, 7)[0])
+    if args.profile_fp64:
+        o.precision = Precision.FP64
     for lp in lps:
         s = PdlpSolver()
         s.setOptions(o)

@@ -210,10 +210,11 @@ __device__ inline void controlStep(DevState& s, const DevConst& c, const double*
 
     // Mixed precision: hand the iterates to FP64 when the FP32 phase stalls close
     // to the tolerance (score = worst KKT term / its tolerance <= switch_score)
-    // while a residual sits near its FP32 noise floor: the rounding of an FP32
-    // product of row i is of order 2^-24 sum_j |a_ij x_j|, so the primal (dual)
-    // residual cannot fall much below 2^-24 || sum_j |a_ij x_j| || (the same
-    // with |a_ij y_i|), in the units of the relative residual.  A plateau far
+    // while a residual that misses its tolerance sits near its FP32 noise floor:
+    // the rounding of an FP32 product of row i is of order 2^-24 sum_j |a_ij x_j|,
+    // so the primal (dual) residual cannot fall much below
+    // 2^-24 || sum_j |a_ij x_j| || (the same with |a_ij y_i|), in the units of
+    // the relative residual.  A plateau far
     // above that floor is ordinary PDHG behaviour and stays in FP32 (measured on
     // the 500k x 2M power-law LP: FP32 alone converges in the same iteration
     // count as the mixed solve that handed over at a quarter of it).
@@ -225,7 +226,13 @@ __device__ inline void controlStep(DevState& s, const DevConst& c, const double*
         constexpr double kU32 = 5.9604644775390625e-08;  // 2^-24
         const double noise_p = kU32 * sqrt(rows[R_NOISE_SQ]) / (1.0 + c.b_norm);
         const double noise_d = kU32 * sqrt(cols[C_NOISE_SQ]) / (1.0 + c.c_norm);
-        const bool near_floor = pterm <= c.noise_factor * noise_p || dterm <= c.noise_factor * noise_d;
+        // only a term that still misses its tolerance can be held up by the floor;
+        // a gap-limited stall counts when either residual sits at its floor
+        const bool p_floor = pterm <= c.noise_factor * noise_p;
+        const bool d_floor = dterm <= c.noise_factor * noise_d;
+        const bool gap_open = s.phase == 0 && gap > c.opt_tol;
+        const bool near_floor = (pterm > pt && p_floor) || (dterm > dt && d_floor) ||
+                                (gap_open && pterm <= pt && dterm <= dt && (p_floor || d_floor));
         if (score <= c.switch_score) {
             if (score < 0.7 * s.best_kkt) {
                 s.best_kkt = score;

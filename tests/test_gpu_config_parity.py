@@ -7,9 +7,11 @@ and every relative KKT term <= 1e-6.
 * 16 LPs of the batched workload (one pdlpx_batch_solve call): the reference's
   own CPU PdlpSolver at 1e-6 relative KKT and the HiGHS optimum;
 * 8 node LPs of the serving workload (1-5% of the integer columns fixed, 0-50
-  cuts), warm-started through the request server: the HiGHS optimum;
+  cuts), warm-started through the request server: the reference's CPU
+  PdlpSolver at 1e-8 relative KKT on the node LP with its fixed columns
+  substituted out;
 * the power-law LP at a fifth of the headline size (100,000 x 400,000, 4M
-  nonzeros): the HiGHS optimum;
+  nonzeros): the reference's CPU PdlpSolver at 1e-7 relative KKT;
 the latter three from tests/golden/config_pins.json
 (tests/golden/make_config_pins.py).
 
@@ -55,13 +57,14 @@ def test_batch_sample_against_reference_and_highs():
     for p, (r, _, _) in zip(pins, out):
         assert p["reference_status"] == 0 and r.status == Status.Optimal and _kkt_ok(r), (p["k"], r)
         assert GC.rel_err(r.objective, p["reference_objective"]) <= GC.OBJ_TOL, (p, r.objective)
-        assert GC.rel_err(r.objective, p["highs_objective"]) <= GC.OBJ_TOL, (p, r.objective)
+        if p["highs_objective"] is not None:
+            assert GC.rel_err(r.objective, p["highs_objective"]) <= GC.OBJ_TOL, (p, r.objective)
 
 
-def test_serving_nodes_against_highs():
+def test_serving_nodes_against_reference():
     """Node LPs carry fixed columns (lb == ub), which the engine's check treats as
-    free of dual residual (the reference's check cannot converge on them); HiGHS
-    is the FP64 oracle for these LPs."""
+    free of dual residual; the reference's check cannot converge on them, so its
+    pin solves the same LP with the fixed columns substituted out."""
     pins = GC.config_pins()["nodes"]
     base, x0 = G.random_lp(20000, 50000, 4, 12, 101)
     ints = G.integer_marks(base.num_cols)
@@ -71,13 +74,13 @@ def test_serving_nodes_against_highs():
         tickets = [srv.submit(G.node_lp(base, x0, ints, p["seed"]), warm=tb) for p in pins]
         res = [srv.wait(t)[0] for t in tickets]
     for p, r in zip(pins, res):
-        assert p["fixed_columns"] > 0
+        assert p["fixed_columns"] > 0 and p["reference_status"] == 0
         assert r.status == Status.Optimal and _kkt_ok(r), (p["k"], r)
-        assert GC.rel_err(r.objective, p["highs_objective"]) <= GC.OBJ_TOL, (p, r.objective)
+        assert GC.rel_err(r.objective, p["reference_objective"]) <= GC.OBJ_TOL, (p, r.objective)
 
 
 @pytest.mark.parametrize("precision", [Precision.Mixed, Precision.FP64])
-def test_powerlaw_fifth_scale_against_highs(precision):
+def test_powerlaw_fifth_scale_against_reference(precision):
     p = GC.config_pins()["powerlaw_100000x400000"]
     lp, _ = G.powerlaw_lp(p["m"], p["n"], 2, 2000, 10.0, 0.01, 1e3, p["seed"])
     assert lp.matrix.numNonzeros() == p["nnz"]
@@ -85,8 +88,9 @@ def test_powerlaw_fifth_scale_against_highs(precision):
     s.setOptions(PdlpOptions(verbose=False, precision=precision, max_solve_seconds=300, **TIGHT))
     s.load(lp)
     r = s.solve()
+    assert p["reference_status"] == 0
     assert r.status == Status.Optimal and _kkt_ok(r), r
-    assert GC.rel_err(r.objective, p["highs_objective"]) <= GC.OBJ_TOL, (r.objective, p["highs_objective"])
+    assert GC.rel_err(r.objective, p["reference_objective"]) <= GC.OBJ_TOL, (r.objective, p["reference_objective"])
 
 
 @pytest.mark.parametrize("name", ["medium", "rand_500x1250", "rand_2000x5000"])
