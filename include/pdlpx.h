@@ -146,7 +146,12 @@ typedef struct pdlpx_options {
                                          bound tested first, so a negative reduced cost counts and
                                          such LPs may not converge, as there); 0 (default): a fixed
                                          column adds no dual residual */
-    int32_t reserved[1];
+    int32_t hot_cache;                /* single-LP engine, sliced-ELL sides: serve the step's gathers of
+                                         the other side's longest rows (first in the device numbering)
+                                         from a shared-memory copy of that prefix, in persistent
+                                         blocks: -1 (default) when those rows hold >= 10 % of the
+                                         nonzeros, 1 whenever the other side has long rows, 0 never;
+                                         identical results either way */
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

@@ -1010,7 +1010,7 @@ void lpState(const Item& it, const pdlpx_options& o, bool mixed, int nb_rows, in
     dc.offset = it.lp.offset;
     dc.precond_ratio = o.preconditioner_refresh_ratio;
     dc.switch_score = 30.0;
-    dc.noise_factor = 10.0;
+    dc.noise_factor = 1.0;
     st.step = 1.0;
     st.pw = o.primal_weight;
     st.prec = mixed ? 0 : 1;

@@ -157,6 +157,65 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
     dualSellFrom<U, T, ST>(p, idx, val, begin + r, hdr[r / kSlice], koff);
 }
 
+// ---- sliced-ELL steps with the hot prefix of the gathered vector in shared memory
+// The device numbering puts each side's long rows first, so the entries of the
+// vector a step gathers that belong to the other side's longest rows form a
+// prefix [0, H).  On power-law LPs that prefix takes a large share of the
+// gathers (the 31,442 columns longer than 80 of the 500k x 2M power-law LP
+// hold 41 % of its nonzeros).  These kernels are persistent (hotMinBlocks
+// blocks of kHotBlock threads per SM, warps striding over the slices); each
+// block first copies the prefix into shared memory with 16-byte loads, then
+// runs the same per-row step as above with those gathers served from shared
+// memory.  Same arithmetic and order as the plain kernels, so the same bits.
+constexpr int kHotBlock = 1024;
+template <class T>
+constexpr int hotMinBlocks() {
+    return sizeof(T) == 8 ? 1 : 2;
+}
+
+template <class X>
+__device__ __forceinline__ void fillHot(X* xs, const X* x, int H) {
+    const int nv = static_cast<int>((static_cast<int64_t>(H) * static_cast<int64_t>(sizeof(X))) / 16);
+    const int4* src = reinterpret_cast<const int4*>(x);
+    int4* dst = reinterpret_cast<int4*>(xs);
+    for (int k = static_cast<int>(threadIdx.x); k < nv; k += kHotBlock) dst[k] = __ldg(src + k);
+    for (int k = nv * static_cast<int>(16 / sizeof(X)) + static_cast<int>(threadIdx.x); k < H; k += kHotBlock)
+        xs[k] = x[k];
+    __syncthreads();
+}
+
+template <int U, class T, bool ST>
+__global__ void __launch_bounds__(kHotBlock, hotMinBlocks<T>())
+    primalSellHot(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
+                  const T* __restrict__ val, int koff, int begin, int end, int H) {
+    extern __shared__ int4 hot_smem[];
+    double* ys = reinterpret_cast<double*>(hot_smem);
+    fillHot(ys, p.yc, H);
+    const int lane = static_cast<int>(threadIdx.x) & 31, wpb = kHotBlock / 32;
+    const int slices = (end - begin + kSlice - 1) / kSlice;
+    for (int sl = static_cast<int>(blockIdx.x) * wpb + (static_cast<int>(threadIdx.x) >> 5); sl < slices;
+         sl += static_cast<int>(gridDim.x) * wpb) {
+        const int j = begin + sl * kSlice + lane;
+        if (j < end) primalSellFrom<U, T, ST, true>(p, idx, val, j, hdr[sl], koff, ys, H);
+    }
+}
+
+template <int U, class T, bool ST>
+__global__ void __launch_bounds__(kHotBlock, hotMinBlocks<T>())
+    dualSellHot(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
+                const T* __restrict__ val, int koff, int begin, int end, int H) {
+    extern __shared__ int4 hot_smem[];
+    T* xs = reinterpret_cast<T*>(hot_smem);
+    fillHot(xs, p.xr, H);
+    const int lane = static_cast<int>(threadIdx.x) & 31, wpb = kHotBlock / 32;
+    const int slices = (end - begin + kSlice - 1) / kSlice;
+    for (int sl = static_cast<int>(blockIdx.x) * wpb + (static_cast<int>(threadIdx.x) >> 5); sl < slices;
+         sl += static_cast<int>(gridDim.x) * wpb) {
+        const int i = begin + sl * kSlice + lane;
+        if (i < end) dualSellFrom<U, T, ST, true>(p, idx, val, i, hdr[sl], koff, xs, H);
+    }
+}
+
 // Sliced-ELL shapes of the single-LP engine: kNumShapes + k for k < kEngSell,
 // U = kSellU[k % kNumSell], streaming loads for k >= kNumSell.
 constexpr int kEngSell = 2 * kNumSell;
@@ -209,6 +268,11 @@ struct DeviceLp {
     // step shapes shapeLD / shapeLP; the other rows use gA / gAT, shapeD / shapeP.
     int nlD = 0, nlP = 0, gLA = 1, gLAT = 1, shapeLD = 0, shapeLP = 0;
     int64_t zlD = 0, zlP = 0;  // entries of the long rows
+    // hot prefixes: the primal step's gathers of y[0, hotP) and the dual step's
+    // of x[0, hotD) are served from shared memory (0: off); the launch caps
+    // them at what one block's shared memory holds
+    int32_t hotP = 0, hotD = 0;
+    int hot_smem_sm = 0, hot_smem_block = 0;  // shared memory per SM / per block (opt-in)
     int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
     std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
     // Sides stored as sliced ELL (shapeP / shapeD >= kNumShapes): their short
@@ -406,10 +470,53 @@ const double* sellVals<double>(const DeviceLp& d, bool primal) {
 
 static int sellGrid(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kBlock - 1) / kBlock)); }
 
+// Entries of gathered type X that one block of a hot kernel running `minb`
+// blocks per SM holds in shared memory (1 KB of each block's share is the
+// runtime's).
+template <class X>
+static int hotCap(const DeviceLp& d, int minb) {
+    const int per_block = std::min(d.hot_smem_block, d.hot_smem_sm / minb - 1024);
+    return per_block > 0 ? per_block / static_cast<int>(sizeof(X)) : 0;
+}
+// Hot prefix length of the primal (y, double) / dual (x_refl, T) gathers at
+// precision T; 0 when the side does not use a hot kernel.
+template <class T>
+static int hotPrimal(const DeviceLp& d) {
+    return d.hotP > 0 ? std::min(d.hotP, hotCap<double>(d, hotMinBlocks<T>())) : 0;
+}
+template <class T>
+static int hotDual(const DeviceLp& d) {
+    return d.hotD > 0 ? std::min(d.hotD, hotCap<T>(d, hotMinBlocks<T>())) : 0;
+}
+static int hotGrid(const DeviceLp& d, int minb, int64_t rows) {
+    const int64_t warps = (rows + kSlice - 1) / kSlice;
+    const int64_t need = (warps + kHotBlock / 32 - 1) / (kHotBlock / 32);
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(d.sms) * minb)));
+}
+
+// Dynamic shared memory limits of every hot kernel (set once per load).
+template <class T>
+static void setHotAttrs(const DeviceLp& d) {
+    const int bytes = std::min(d.hot_smem_block, d.hot_smem_sm / hotMinBlocks<T>() - 1024);
+    for (int k = 0; k < kEngSell; ++k) {
+        const int shape = kNumShapes + k;
+        PDLPX_ENG_SELL_SWITCH(shape, {
+            cudaFuncSetAttribute(primalSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            cudaFuncSetAttribute(dualSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        });
+    }
+}
+
 // Short-row launch of one side in `shape` (CSR, or sliced ELL when isSell).
 template <class T>
 void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
-    if (isSell(shape)) {
+    const int H = isSell(shape) ? hotPrimal<T>(d) : 0;
+    if (H > 0) {
+        const size_t bytes = static_cast<size_t>(H) * sizeof(double);
+        PDLPX_ENG_SELL_SWITCH(shape, (primalSellHot<UU, T, SS>
+                                      <<<hotGrid(d, hotMinBlocks<T>(), d.n - d.nlP), kHotBlock, bytes, s>>>(
+                                          ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n, H)));
+    } else if (isSell(shape)) {
         PDLPX_ENG_SELL_SWITCH(shape, (primalSellStep<UU, T, SS><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
                                          ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n)));
     } else {
@@ -419,7 +526,13 @@ void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int 
 }
 template <class T>
 void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
-    if (isSell(shape)) {
+    const int H = isSell(shape) ? hotDual<T>(d) : 0;
+    if (H > 0) {
+        const size_t bytes = static_cast<size_t>(H) * sizeof(T);
+        PDLPX_ENG_SELL_SWITCH(shape, (dualSellHot<UU, T, SS>
+                                      <<<hotGrid(d, hotMinBlocks<T>(), d.m - d.nlD), kHotBlock, bytes, s>>>(
+                                          ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m, H)));
+    } else if (isSell(shape)) {
         PDLPX_ENG_SELL_SWITCH(shape, (dualSellStep<UU, T, SS><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
                                          ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
     } else {
@@ -802,6 +915,20 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.gLAT = d.nlP > 0 ? std::min(256, pickGroup(zlP, d.nlP)) : 1;
     d.shapeLD = longShape(zlD, d.nlD);
     d.shapeLP = longShape(zlP, d.nlP);
+    // Hot prefixes: the dual step gathers x, whose long columns [0, nlP) hold
+    // zlP of the entries; the primal step gathers y, whose long rows [0, nlD)
+    // hold zlD.
+    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    auto hotOn = [&](int64_t zl_other) {
+        return o.hot_cache > 0 || (o.hot_cache < 0 && nnz > 0 && 10 * zl_other >= nnz);
+    };
+    d.hotD = (sellD && d.nlP > 0 && hotOn(zlP)) ? d.nlP : 0;
+    d.hotP = (sellP && d.nlD > 0 && hotOn(zlD)) ? d.nlD : 0;
+    if (d.hotD > 0 || d.hotP > 0) {
+        setHotAttrs<float>(d);
+        setHotAttrs<double>(d);
+    }
     const int cap = 4 * d.sms;
     d.nb_rows_s = std::max(1, std::min(gridFor(msD, d.gA), cap));
     d.nb_cols_s = std::max(1, std::min(gridFor(msP, d.gAT), cap));
@@ -1476,7 +1603,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
     dc.step_up = opt_.adaptive_step_up;
     dc.precond_ratio = opt_.preconditioner_refresh_ratio;
     dc.switch_score = 30.0;
-    dc.noise_factor = 10.0;
+    dc.noise_factor = 1.0;
     PDLPX_CK(cudaMemcpyAsync(d.dc, &dc, sizeof(DevConst), cudaMemcpyHostToDevice, s));
 
     DevState st0{};
@@ -1799,8 +1926,19 @@ int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd
     const DeviceLp& d = *dev_;
     if (ga) *ga = isSell(d.shapeD) ? 1 : kShapes[d.shapeD].G;
     if (gat) *gat = isSell(d.shapeP) ? 1 : kShapes[d.shapeP].G;
-    if (bp) *bp = isSell(d.shapeP) ? sellGrid(d.n - d.nlP) : gridForShape(d.n - d.nlP, d.shapeP);
-    if (bd) *bd = isSell(d.shapeD) ? sellGrid(d.m - d.nlD) : gridForShape(d.m - d.nlD, d.shapeD);
+    // blocks of the short-row launches at the starting precision (persistent
+    // blocks when the side runs a hot kernel)
+    const int hp = d.mixed ? hotPrimal<float>(d) : hotPrimal<double>(d);
+    const int hd = d.mixed ? hotDual<float>(d) : hotDual<double>(d);
+    const int minb = d.mixed ? hotMinBlocks<float>() : hotMinBlocks<double>();
+    if (bp)
+        *bp = !isSell(d.shapeP) ? gridForShape(d.n - d.nlP, d.shapeP)
+              : hp > 0          ? hotGrid(d, minb, d.n - d.nlP)
+                                : sellGrid(d.n - d.nlP);
+    if (bd)
+        *bd = !isSell(d.shapeD) ? gridForShape(d.m - d.nlD, d.shapeD)
+              : hd > 0          ? hotGrid(d, minb, d.m - d.nlD)
+                                : sellGrid(d.m - d.nlD);
     return PDLPX_OK;
 }
 

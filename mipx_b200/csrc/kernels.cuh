@@ -611,13 +611,17 @@ __device__ __forceinline__ double ldStream(const double* a, unsigned long long p
 
 // Dot product of this thread's row with x: entry k of the row sits at
 // hdr.x + k * 32 + lane; U entries are loaded per round, then their U gathers,
-// then the products are summed in entry order (so every U, and either kind of
-// load, gives the same bits).  ST: the index / value loads use the streaming
-// hints above.  Entries past the row's end hold index 0 and value 0 (index 0
-// always exists).
-template <int U, class V, class X, bool ST = false>
+// then the products are summed in entry order (so every U, either kind of
+// load, and either source of a gathered value give the same bits).  ST: the
+// index / value loads use the streaming hints above.  HOT: x[0, H) -- the
+// other side's longest rows, which the device numbering puts first -- is also
+// held in shared memory at xs, and gathers of those entries read it there
+// instead of through L1 (whose tag stage serves one sector of a scattered
+// gather per clock).  Entries past the row's end hold index 0 and value 0
+// (index 0 always exists).
+template <int U, class V, class X, bool ST = false, bool HOT = false>
 __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* __restrict__ val, int2 h, int lane,
-                                          const X* __restrict__ x) {
+                                          const X* __restrict__ x, const X* xs = nullptr, int H = 0) {
     const int* ip = idx + h.x + lane;
     const V* vp = val + h.x + lane;
     double acc = 0.0;
@@ -640,20 +644,25 @@ __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* 
         }
         X g[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) g[u] = __ldg(x + c[u]);
+        for (int u = 0; u < U; ++u) {
+            if constexpr (HOT)
+                g[u] = c[u] < H ? xs[c[u]] : __ldg(x + c[u]);
+            else
+                g[u] = __ldg(x + c[u]);
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) acc += static_cast<double>(v[u]) * static_cast<double>(g[u]);
     }
     return acc;
 }
 
-template <int U, class T, bool ST = false>
+template <int U, class T, bool ST = false, bool HOT = false>
 __device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
-                                               int koff) {
+                                               int koff, const double* ys = nullptr, int H = 0) {
     const ColPack<T> q = p.cp[j];
     const double xc = p.xc[j];
     const double xi = static_cast<double>(p.xi[j]);
-    const double s = sellDot<U, T, double, ST>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
+    const double s = sellDot<U, T, double, ST, HOT>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc, ys, H);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     const double step = p.st->step, pw = p.st->pw;
@@ -662,13 +671,13 @@ __device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* 
     primalUpdate<T>(p, j, q, xc, xi, s, step, pw, lam, last);
 }
 
-template <int U, class T, bool ST = false>
+template <int U, class T, bool ST = false, bool HOT = false>
 __device__ __forceinline__ void dualSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int i, int2 h,
-                                             int koff) {
+                                             int koff, const T* xs = nullptr, int H = 0) {
     const RowPack<T> q = p.rp[i];
     const double yc = p.yc[i];
     const double yi = static_cast<double>(p.yi[i]);
-    const double s = sellDot<U, T, T, ST>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr);
+    const double s = sellDot<U, T, T, ST, HOT>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.xr, xs, H);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     const double step = p.st->step, pw = p.st->pw;

@@ -44,3 +44,52 @@ def test_powerlaw_lp_single_and_batch_agree():
     (q, u, _), = batch_solve([lp], o)
     assert q.status == Status.Optimal
     assert GC.rel_err(r.objective, q.objective) <= GC.OBJ_TOL, (r.objective, q.objective)
+
+
+def _transposed(lp, seed):
+    """An LP over A^T of `lp` (its long columns become long rows): columns in
+    [0, 10], rows within 1 of A^T x0 for a random x0 in the box, so it has an
+    optimum."""
+    from scipy.sparse import csr_matrix
+    from mipx_b200.pdlp import LpProblem, SparseMatrix
+    a = csr_matrix((lp.matrix.values, lp.matrix.col_indices, lp.matrix.row_starts), shape=(lp.num_rows, lp.num_cols))
+    t = a.T.tocsr()
+    t.sort_indices()
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(0, 10, lp.num_rows)
+    ax = t @ x0
+    return LpProblem(num_cols=lp.num_rows, obj=rng.normal(size=lp.num_rows), col_lower=np.zeros(lp.num_rows),
+                     col_upper=np.full(lp.num_rows, 10.0), num_rows=lp.num_cols, row_lower=ax - 1.0,
+                     row_upper=ax + 1.0,
+                     matrix=SparseMatrix(lp.num_cols, lp.num_rows, values=t.data.astype(np.float64),
+                                         col_indices=t.indices.astype(np.int32),
+                                         row_starts=t.indptr.astype(np.int32)))
+
+
+@pytest.mark.parametrize("side", ["dual", "primal"])
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_hot_prefix_in_shared_memory_gives_same_bits(side, precision):
+    """The hot-prefix kernels (gathers of the other side's longest rows served
+    from shared memory, persistent blocks) compute what the plain sliced-ELL
+    kernels compute, bit for bit: same iterations, objective, x and y.  'dual':
+    power-law columns (the dual step's x gathers); 'primal': the transposed LP,
+    whose long rows are the primal step's y gathers."""
+    from mipx_b200.pdlp import Precision
+    lp, _ = G.powerlaw_lp(20000, 80000, 2, 2000, 10.0, 0.01, 1e3, 5)
+    if side == "primal":
+        lp = _transposed(lp, 9)
+    prec = Precision.Mixed if precision == "mixed" else Precision.FP64
+    out = []
+    for hot in (0, 1):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, precision=prec, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL,
+                                 max_iter=4000, hot_cache=hot))
+        s.load(lp)
+        r = s.solve()
+        out.append((r, s.getPrimalValues(), s.getDualValues(), s.launchConfig()))
+    (r0, x0, y0, c0), (r1, x1, y1, c1) = out
+    key = "blocks_dual" if side == "dual" else "blocks_primal"
+    assert c1[key] < c0[key], (c0, c1)  # persistent blocks: the hot kernel ran
+    assert r0.iterations == r1.iterations and r0.objective == r1.objective
+    np.testing.assert_array_equal(x0, x1)
+    np.testing.assert_array_equal(y0, y1)
