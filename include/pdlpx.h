@@ -150,8 +150,9 @@ typedef struct pdlpx_options {
                                          the other side's longest rows (first in the device numbering)
                                          from a shared-memory copy of that prefix, in persistent
                                          blocks: -1 (default) when those rows hold >= 10 % of the
-                                         nonzeros, 1 whenever the other side has long rows, 0 never;
-                                         identical results either way */
+                                         nonzeros, with 64 KB of shared memory per SM; k > 0 whenever
+                                         the other side has long rows, with k KB per SM (capped at the
+                                         device's limit); 0 never.  Identical results either way */
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

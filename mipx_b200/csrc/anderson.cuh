@@ -226,7 +226,7 @@ __global__ void aaDecide(AaArgs a) {
 // Accepted extrapolation: x (clamped to the scaled bounds) and y become both
 // the anchor and the current iterate (pdlp.cpp:2437-2456).
 template <class T>
-__global__ void __launch_bounds__(kBlock) aaApply(AaArgs a, T* xi, T* yi, double* xc, double* yc) {
+__global__ void __launch_bounds__(kBlock) aaApply(AaArgs a, T* xi, T* yi, double* xc, double* yc, T* yg) {
     if (!a.as->accepted || a.st->prec != precTag<T>()) return;
     const int n = a.n, m = a.m;
     const int total = n > m ? n : m;
@@ -240,6 +240,9 @@ __global__ void __launch_bounds__(kBlock) aaApply(AaArgs a, T* xi, T* yi, double
             const T v = static_cast<T>(a.out[n + k]);
             yi[k] = v;
             yc[k] = static_cast<double>(v);
+            if constexpr (sizeof(T) == 4) {
+                if (yg != nullptr) yg[k] = v;
+            }
         }
     }
 }

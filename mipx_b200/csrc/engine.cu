@@ -130,22 +130,24 @@ __global__ void __launch_bounds__(kBlock) powerFinish2(PowerArgs a) {
 // ---- sliced-ELL step launches ------------------------------------------------
 // The short rows [begin, end) of a matrix side stored as sliced ELL (slice s of
 // the range described by hdr[s]); one thread per row, the fused step of
-// kernels.cuh.  FP32 kernels are compiled for 8 resident blocks (32
+// kernels.cuh.  FP32 dual kernels are compiled for 8 resident blocks (32
 // registers), the occupancy at which the packed batch's sliced-ELL kernels
-// measured fastest; the FP64 kernels, whose values and gathers take register
-// pairs, for 5 (51 registers: at 32 they spilled 130-400 bytes per thread).
-template <class T>
+// measured fastest; the FP32 primal kernels, which spilled 16-40 bytes per
+// thread at 32 registers, for 6 (40 registers); the FP64 kernels, whose
+// values and gathers take register pairs, for 5 (48 registers: at 32 they
+// spilled 130-400 bytes per thread).
+template <class T, bool PRIMAL = false>
 constexpr int sellMinBlocks() {
-    return sizeof(T) == 8 ? 5 : 8;
+    return sizeof(T) == 8 ? 5 : (PRIMAL ? 6 : 8);
 }
 
 template <int U, class T, bool ST>
-__global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<T, true>())
     primalSellStep(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                    const T* __restrict__ val, int koff, int begin, int end) {
     const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
     if (begin + r >= end) return;
-    primalSellFrom<U, T, ST>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+    primalSellFrom<U, T, ST, false, true>(p, idx, val, begin + r, hdr[r / kSlice], koff);
 }
 
 template <int U, class T, bool ST>
@@ -168,6 +170,7 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
 // runs the same per-row step as above with those gathers served from shared
 // memory.  Same arithmetic and order as the plain kernels, so the same bits.
 constexpr int kHotBlock = 1024;
+constexpr int kHotDefaultKb = 64;  // shared memory per SM for the prefix unless pinned
 template <class T>
 constexpr int hotMinBlocks() {
     return sizeof(T) == 8 ? 1 : 2;
@@ -189,14 +192,14 @@ __global__ void __launch_bounds__(kHotBlock, hotMinBlocks<T>())
     primalSellHot(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                   const T* __restrict__ val, int koff, int begin, int end, int H) {
     extern __shared__ int4 hot_smem[];
-    double* ys = reinterpret_cast<double*>(hot_smem);
-    fillHot(ys, p.yc, H);
+    T* ys = reinterpret_cast<T*>(hot_smem);
+    fillHot(ys, p.yg, H);
     const int lane = static_cast<int>(threadIdx.x) & 31, wpb = kHotBlock / 32;
     const int slices = (end - begin + kSlice - 1) / kSlice;
     for (int sl = static_cast<int>(blockIdx.x) * wpb + (static_cast<int>(threadIdx.x) >> 5); sl < slices;
          sl += static_cast<int>(gridDim.x) * wpb) {
         const int j = begin + sl * kSlice + lane;
-        if (j < end) primalSellFrom<U, T, ST, true>(p, idx, val, j, hdr[sl], koff, ys, H);
+        if (j < end) primalSellFrom<U, T, ST, true, true>(p, idx, val, j, hdr[sl], koff, ys, H);
     }
 }
 
@@ -273,6 +276,7 @@ struct DeviceLp {
     // them at what one block's shared memory holds
     int32_t hotP = 0, hotD = 0;
     int hot_smem_sm = 0, hot_smem_block = 0;  // shared memory per SM / per block (opt-in)
+    int hot_bytes_sm = 0;                      // shared memory per SM given to the hot prefix
     int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
     std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
     // Sides stored as sliced ELL (shapeP / shapeD >= kNumShapes): their short
@@ -304,6 +308,7 @@ struct DeviceLp {
     float *yi32 = nullptr, *yh32 = nullptr;
     double *xc64 = nullptr, *xi64 = nullptr, *xr64 = nullptr, *xh64 = nullptr;
     double *yc64 = nullptr, *yi64 = nullptr, *yh64 = nullptr;
+    float* yg32 = nullptr;  // FP32 copy of yc, gathered by the mixed-mode primal step
     double *prev_ax = nullptr, *prev_xh = nullptr;
     double *pi_x = nullptr, *pi_y = nullptr, *pi_xn = nullptr, *pi_part = nullptr;
     double *part_rows = nullptr, *part_cols = nullptr;
@@ -354,6 +359,7 @@ struct DeviceLp {
         a.xr = xr32;
         a.xh = xh32;
         a.yc = yc64;
+        a.yg = yg32;
         a.yi = yi32;
         a.yh = yh32;
         a.st = st;
@@ -379,6 +385,7 @@ struct DeviceLp {
         a.xr = xr64;
         a.xh = xh64;
         a.yc = yc64;
+        a.yg = yc64;
         a.yi = yi64;
         a.yh = yh64;
         a.st = st;
@@ -456,6 +463,13 @@ IterArgs<double> iterArgs<double>(const DeviceLp& d, const pdlpx_options& o) {
     return d.iter64(o);
 }
 
+// The FP32 copy of y that writers of yc keep (mixed mode), else null (in FP64
+// mode the primal step gathers yc itself).
+template <class T>
+T* ygCopy(const IterArgs<T>& ia) {
+    return sizeof(T) == 4 ? ia.yg : nullptr;
+}
+
 // Sliced-ELL values of a side in storage type T.
 template <class T>
 const T* sellVals(const DeviceLp& d, bool primal);
@@ -470,19 +484,24 @@ const double* sellVals<double>(const DeviceLp& d, bool primal) {
 
 static int sellGrid(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kBlock - 1) / kBlock)); }
 
-// Entries of gathered type X that one block of a hot kernel running `minb`
-// blocks per SM holds in shared memory (1 KB of each block's share is the
-// runtime's).
+// Shared memory per block of a hot kernel running `minb` blocks per SM: the
+// prefix's share of the SM, within the device limits (1 KB of each block's
+// share is the runtime's).  Shared memory is carved out of the SM's L1, which
+// also holds the sectors of the loads in flight, so the prefix's share is a
+// trade between gathers served from shared memory and L1 room for the rest.
+static int hotBlockBytes(const DeviceLp& d, int minb) {
+    const int b = std::min({d.hot_smem_block, d.hot_smem_sm / minb - 1024, d.hot_bytes_sm / minb});
+    return std::max(0, b & ~15);
+}
 template <class X>
 static int hotCap(const DeviceLp& d, int minb) {
-    const int per_block = std::min(d.hot_smem_block, d.hot_smem_sm / minb - 1024);
-    return per_block > 0 ? per_block / static_cast<int>(sizeof(X)) : 0;
+    return hotBlockBytes(d, minb) / static_cast<int>(sizeof(X));
 }
 // Hot prefix length of the primal (y, double) / dual (x_refl, T) gathers at
 // precision T; 0 when the side does not use a hot kernel.
 template <class T>
 static int hotPrimal(const DeviceLp& d) {
-    return d.hotP > 0 ? std::min(d.hotP, hotCap<double>(d, hotMinBlocks<T>())) : 0;
+    return d.hotP > 0 ? std::min(d.hotP, hotCap<T>(d, hotMinBlocks<T>())) : 0;
 }
 template <class T>
 static int hotDual(const DeviceLp& d) {
@@ -497,7 +516,7 @@ static int hotGrid(const DeviceLp& d, int minb, int64_t rows) {
 // Dynamic shared memory limits of every hot kernel (set once per load).
 template <class T>
 static void setHotAttrs(const DeviceLp& d) {
-    const int bytes = std::min(d.hot_smem_block, d.hot_smem_sm / hotMinBlocks<T>() - 1024);
+    const int bytes = hotBlockBytes(d, hotMinBlocks<T>());
     for (int k = 0; k < kEngSell; ++k) {
         const int shape = kNumShapes + k;
         PDLPX_ENG_SELL_SWITCH(shape, {
@@ -512,7 +531,7 @@ template <class T>
 void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k, cudaStream_t s) {
     const int H = isSell(shape) ? hotPrimal<T>(d) : 0;
     if (H > 0) {
-        const size_t bytes = static_cast<size_t>(H) * sizeof(double);
+        const size_t bytes = static_cast<size_t>(H) * sizeof(T);
         PDLPX_ENG_SELL_SWITCH(shape, (primalSellHot<UU, T, SS>
                                       <<<hotGrid(d, hotMinBlocks<T>(), d.n - d.nlP), kHotBlock, bytes, s>>>(
                                           ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n, H)));
@@ -520,7 +539,7 @@ void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int 
         PDLPX_ENG_SELL_SWITCH(shape, (primalSellStep<UU, T, SS><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
                                          ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n)));
     } else {
-        PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<gridForShape(d.n - d.nlP, shape), kBlock, 0, s>>>(
+        PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T, true><<<gridForShape(d.n - d.nlP, shape), kBlock, 0, s>>>(
                                       ia, k, d.nlP, d.n)));
     }
 }
@@ -547,7 +566,7 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
     int n = 0;
     if (d.nlP > 0) {
         PDLPX_SHAPE_SWITCH(d.shapeLP,
-                           (primalStep<GG, RR, UU, T><<<gridForShape(d.nlP, d.shapeLP), kBlock, 0, s>>>(ia, k, 0, d.nlP)));
+                           (primalStep<GG, RR, UU, T, true><<<gridForShape(d.nlP, d.shapeLP), kBlock, 0, s>>>(ia, k, 0, d.nlP)));
         ++n;
     }
     if (d.n > d.nlP) {
@@ -619,9 +638,9 @@ int launchCycle(DeviceLp& d, const pdlpx_options& o) {
         launches += 4;
     }
     restartCopy<T><<<nb, kBlock, 0, s>>>(d.st, d.n, d.m, ia.xh, ia.yh, ia.xi, ia.yi, ia.xc, ia.yc,
-                                         d.aa_w > 0 ? &d.aa_st->accepted : nullptr);
+                                         d.aa_w > 0 ? &d.aa_st->accepted : nullptr, ygCopy(ia));
     if (d.aa_w > 0) {
-        aaApply<T><<<nb, kBlock, 0, s>>>(aa, ia.xi, ia.yi, ia.xc, ia.yc);
+        aaApply<T><<<nb, kBlock, 0, s>>>(aa, ia.xi, ia.yi, ia.xc, ia.yc, ygCopy(ia));
         ++launches;
     }
     launches += 4;
@@ -923,6 +942,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     auto hotOn = [&](int64_t zl_other) {
         return o.hot_cache > 0 || (o.hot_cache < 0 && nnz > 0 && 10 * zl_other >= nnz);
     };
+    d.hot_bytes_sm = 1024 * (o.hot_cache > 0 ? o.hot_cache : kHotDefaultKb);
     d.hotD = (sellD && d.nlP > 0 && hotOn(zlP)) ? d.nlP : 0;
     d.hotP = (sellP && d.nlD > 0 && hotOn(zlD)) ? d.nlD : 0;
     if (d.hotD > 0 || d.hotP > 0) {
@@ -954,7 +974,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     const size_t o_c64 = take(8 * n), o_lb64 = take(8 * n), o_ub64 = take(8 * n), o_cs64 = take(8 * n),
                  o_tau64 = take(8 * n);
     const size_t o_rl64 = take(8 * m), o_ru64 = take(8 * m), o_rs64 = take(8 * m), o_sig64 = take(8 * m);
-    size_t o_x32[3] = {0, 0, 0}, o_y32[2] = {0, 0};
+    size_t o_x32[3] = {0, 0, 0}, o_y32[3] = {0, 0, 0};
     if (mixed) {
         for (auto& v : o_x32) v = take(4 * n);
         for (auto& v : o_y32) v = take(4 * m);
@@ -1011,6 +1031,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         d.xh32 = reinterpret_cast<float*>(b + o_x32[2]);
         d.yi32 = reinterpret_cast<float*>(b + o_y32[0]);
         d.yh32 = reinterpret_cast<float*>(b + o_y32[1]);
+        d.yg32 = reinterpret_cast<float*>(b + o_y32[2]);
     }
     d.cp64 = reinterpret_cast<ColPack<double>*>(b + o_cp64);
     d.rp64 = reinterpret_cast<RowPack<double>*>(b + o_rp64);
@@ -1159,6 +1180,7 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
     for (int k = 0; k < 2; ++k) PDLPX_CK(cudaMemsetAsync(ys[k], 0, sizeof(T) * static_cast<size_t>(d.m), s));
     PDLPX_CK(cudaMemsetAsync(ia.xc, 0, 8 * static_cast<size_t>(d.n), s));
     PDLPX_CK(cudaMemsetAsync(ia.yc, 0, 8 * static_cast<size_t>(d.m), s));
+    if (ygCopy(ia) != nullptr) PDLPX_CK(cudaMemsetAsync(ygCopy(ia), 0, sizeof(T) * static_cast<size_t>(d.m), s));
     cudaEvent_t e0, e1;
     PDLPX_CK(cudaEventCreate(&e0));
     PDLPX_CK(cudaEventCreate(&e1));
@@ -1179,7 +1201,7 @@ static int32_t autotuneShapes(DeviceLp& d, const pdlpx_options& o, bool tune_p, 
             } else if (which == 1) {
                 launchDualShort<T>(d, ia, shape, 1, s);
             } else if (which == 2) {
-                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T><<<gridForShape(d.nlP, shape), kBlock, 0, s>>>(
+                PDLPX_SHAPE_SWITCH(shape, (primalStep<GG, RR, UU, T, true><<<gridForShape(d.nlP, shape), kBlock, 0, s>>>(
                                               ia, 1, 0, d.nlP)));
             } else {
                 PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<gridForShape(d.nlD, shape), kBlock, 0, s>>>(
@@ -1648,6 +1670,7 @@ int32_t Engine::solveDevice(pdlpx_result* out) {
         std::vector<double> dx(fx.begin(), fx.end()), dy(fy.begin(), fy.end());
         PDLPX_CK(cudaMemcpyAsync(d.xc64, dx.data(), 8 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s));
         PDLPX_CK(cudaMemcpyAsync(d.yc64, dy.data(), 8 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
+        PDLPX_CK(cudaMemcpyAsync(d.yg32, fy.data(), 4 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s));
         PDLPX_CK(cudaStreamSynchronize(s));
     } else {
         if (!warm) {

@@ -115,12 +115,18 @@ struct IterArgs {
     T* xi;       // initial (anchor) x
     T* xr;       // reflected x (gathered by the dual SpMV)
     T* xh;       // pdhg x (written on the last iteration of a batch)
-    double* yc;  // current y (gathered by the primal SpMV)
+    double* yc;  // current y
     T* yi;
     T* yh;
     DevState* st;
     int m, n;
     int max_iter, polish_max_iter, N;
+    // y as the single-LP engine's primal SpMV gathers it (kernels with YG):
+    // an FP32 copy of yc kept by every writer of yc in mixed mode -- its
+    // rounding is of the order of the FP32 matrix values' own, and a 4-byte
+    // gather costs the L1 tag stage half of an 8-byte one -- and yc itself in
+    // FP64 mode.  Null elsewhere (the packed batch gathers yc).
+    T* yg = nullptr;
 };
 
 // Row / column metric slots of the check pass.
@@ -431,7 +437,11 @@ __device__ __forceinline__ void dualUpdate(const IterArgs<T>& p, int i, const Ro
             py = 0.0;
     }
     const double yr = 2.0 * py - ycd;
-    p.yc[i] = lam * yr + (1.0 - lam) * yid;
+    const double yn = lam * yr + (1.0 - lam) * yid;
+    p.yc[i] = yn;
+    if constexpr (sizeof(T) == 4) {
+        if (p.yg != nullptr) p.yg[i] = static_cast<float>(yn);
+    }
     if (last) p.yh[i] = static_cast<T>(py);
 }
 
@@ -459,7 +469,7 @@ __device__ __forceinline__ void rowBounds(const int* __restrict__ ptr, int j0, i
 // before the solver state is consulted, so their latencies overlap.  The step
 // arithmetic is FP64 whatever the storage type (same association as the
 // reference: tau = step * tau_base / omega), results are rounded once on store.
-template <int G, int R, int U, class T>
+template <int G, int R, int U, class T, bool YG = false>
 __device__ __forceinline__ void primalRowsFrom(const IterArgs<T>& p, int j0, int jend, const int (&b)[R],
                                                const int (&e)[R], int koff) {
     constexpr int slab = kBlock / G;
@@ -484,7 +494,12 @@ __device__ __forceinline__ void primalRowsFrom(const IterArgs<T>& p, int j0, int
     }
     double s[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[r] = rowDotU<G, U, double>(b[r], e[r], lane, p.at_idx, p.at_val, p.yc);
+    for (int r = 0; r < R; ++r) {
+        if constexpr (YG)
+            s[r] = rowDotU<G, U, double>(b[r], e[r], lane, p.at_idx, p.at_val, p.yg);
+        else
+            s[r] = rowDotU<G, U, double>(b[r], e[r], lane, p.at_idx, p.at_val, p.yc);
+    }
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
 #pragma unroll
@@ -502,19 +517,19 @@ __device__ __forceinline__ void primalRowsFrom(const IterArgs<T>& p, int j0, int
 
 // primalRows handles the columns j0 + r * slab (r < R) below jend; the
 // single-LP kernel covers [0, n), the batched kernel one tile of one LP.
-template <int G, int R, int U, class T>
+template <int G, int R, int U, class T, bool YG = false>
 __device__ __forceinline__ void primalRows(const IterArgs<T>& p, int j0, int jend, int koff) {
     int b[R], e[R];
     rowBounds<G, R>(p.at_ptr, j0, jend, b, e);
-    primalRowsFrom<G, R, U, T>(p, j0, jend, b, e, koff);
+    primalRowsFrom<G, R, U, T, YG>(p, j0, jend, b, e, koff);
 }
 
 // Columns [begin, end) of A^T (the engine launches long and short columns
 // separately when their lengths are far apart).
-template <int G, int R, int U, class T>
+template <int G, int R, int U, class T, bool YG = false>
 __global__ void __launch_bounds__(kBlock) primalStep(IterArgs<T> p, int koff, int begin, int end) {
     constexpr int slab = kBlock / G;
-    primalRows<G, R, U, T>(p, begin + static_cast<int>(blockIdx.x) * (slab * R) + static_cast<int>(threadIdx.x) / G, end,
+    primalRows<G, R, U, T, YG>(p, begin + static_cast<int>(blockIdx.x) * (slab * R) + static_cast<int>(threadIdx.x) / G, end,
                            koff);
 }
 
@@ -656,13 +671,17 @@ __device__ __forceinline__ double sellDot(const int* __restrict__ idx, const V* 
     return acc;
 }
 
-template <int U, class T, bool ST = false, bool HOT = false>
+template <int U, class T, bool ST = false, bool HOT = false, bool YG = false>
 __device__ __forceinline__ void primalSellFrom(const IterArgs<T>& p, const int* idx, const T* val, int j, int2 h,
-                                               int koff, const double* ys = nullptr, int H = 0) {
+                                               int koff, const T* ys = nullptr, int H = 0) {
     const ColPack<T> q = p.cp[j];
     const double xc = p.xc[j];
     const double xi = static_cast<double>(p.xi[j]);
-    const double s = sellDot<U, T, double, ST, HOT>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc, ys, H);
+    double s;
+    if constexpr (YG)
+        s = sellDot<U, T, T, ST, HOT>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yg, ys, H);
+    else
+        s = sellDot<U, T, double, ST>(idx, val, h, static_cast<int>(threadIdx.x) & 31, p.yc);
     bool last = false;
     if (!active(p.st, precTag<T>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     const double step = p.st->step, pw = p.st->pw;
@@ -912,7 +931,7 @@ __global__ void __launch_bounds__(kBlock) checkCols(CheckArgs<T> p, int begin, i
 template <class T>
 __global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n, int m, const T* xh,
                                                      const T* yh, T* xi, T* yi, double* xc, double* yc,
-                                                     const int* skip) {
+                                                     const int* skip, T* yg) {
     if (st->done || st->prec != precTag<T>() || !st->restart) return;
     if (skip != nullptr && *skip) return;
     for (int k = blockIdx.x * kBlock + threadIdx.x; k < (n > m ? n : m); k += gridDim.x * kBlock) {
@@ -925,6 +944,9 @@ __global__ void __launch_bounds__(kBlock) restartCopy(const DevState* st, int n,
             const T v = yh[k];
             yi[k] = v;
             yc[k] = v;
+            if constexpr (sizeof(T) == 4) {
+                if (yg != nullptr) yg[k] = v;
+            }
         }
     }
 }
