@@ -148,9 +148,9 @@ typedef struct pdlpx_options {
                                          column adds no dual residual */
     int32_t hot_cache;                /* single-LP engine, sliced-ELL sides: serve the step's gathers of
                                          the other side's longest rows (first in the device numbering)
-                                         from a shared-memory copy of that prefix, in persistent
-                                         blocks: -1 (default) when those rows hold >= 10 % of the
-                                         nonzeros, with 64 KB of shared memory per SM; k > 0 whenever
+                                         from a shared-memory copy of that prefix held by every
+                                         block: -1 (default) when those rows hold >= 10 % of the
+                                         nonzeros, with 128 KB of shared memory per SM; k > 0 whenever
                                          the other side has long rows, with k KB per SM (capped at the
                                          device's limit); 0 never.  Identical results either way */
 } pdlpx_options;
@@ -276,6 +276,11 @@ int32_t pdlpx_get_step_times(const pdlpx_solver* h, int32_t precision, double* m
  * short-row launches. */
 int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t* group_at,
                                 int32_t* blocks_primal, int32_t* blocks_dual);
+/* Length of the hot prefix (option hot_cache) that the primal step's gathers
+ * of y and the dual step's gathers of x serve from shared memory, at the
+ * given precision (PDLPX_PREC_MIXED: the FP32 kernels; PDLPX_PREC_FP64);
+ * 0 where that step runs without one. */
+int32_t pdlpx_get_hot_prefix(const pdlpx_solver* h, int32_t precision, int32_t* primal, int32_t* dual);
 
 /* ---- batched solve: many independent LPs in one persistent launch ---- */
 typedef struct pdlpx_lp {

@@ -353,6 +353,11 @@ int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t
     return h->engine.launchConfig(group_a, group_at, blocks_primal, blocks_dual);
 }
 
+int32_t pdlpx_get_hot_prefix(const pdlpx_solver* h, int32_t precision, int32_t* primal, int32_t* dual) {
+    if (h == nullptr) return PDLPX_E_INVALID;
+    return h->engine.hotPrefix(precision, primal, dual);
+}
+
 int32_t pdlpx_batch_solve(int32_t count, const pdlpx_lp* lps, const pdlpx_options* opts, pdlpx_result* results,
                           double* const* x_out, double* const* y_out) {
     if (count < 0 || (count > 0 && (lps == nullptr || results == nullptr))) return PDLPX_E_INVALID;

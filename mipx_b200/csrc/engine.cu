@@ -162,61 +162,48 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
 // ---- sliced-ELL steps with the hot prefix of the gathered vector in shared memory
 // The device numbering puts each side's long rows first, so the entries of the
 // vector a step gathers that belong to the other side's longest rows form a
-// prefix [0, H).  On power-law LPs that prefix takes a large share of the
-// gathers (the 31,442 columns longer than 80 of the 500k x 2M power-law LP
-// hold 41 % of its nonzeros).  These kernels are persistent (hotMinBlocks
-// blocks of kHotBlock threads per SM, warps striding over the slices); each
-// block first copies the prefix into shared memory with 16-byte loads, then
-// runs the same per-row step as above with those gathers served from shared
-// memory.  Same arithmetic and order as the plain kernels, so the same bits.
-constexpr int kHotBlock = 1024;
-constexpr int kHotDefaultKb = 64;  // shared memory per SM for the prefix unless pinned
-template <class T>
-constexpr int hotMinBlocks() {
-    return sizeof(T) == 8 ? 1 : 2;
-}
+// prefix [0, H).  On power-law LPs a short prefix takes a large share of the
+// gathers (on the 500k x 2M power-law LP the 4,096 longest columns hold 18 %
+// of the nonzeros).  Each block first copies the prefix into shared memory
+// with 16-byte loads, then runs the same per-row step as the kernels above
+// with those gathers served from shared memory (same arithmetic and order, so
+// the same bits).  Persistent blocks holding a larger prefix measured slower
+// on that LP (warps with one or two slices each, no block refill).
+constexpr int kHotDefaultKb = 128;  // shared memory per SM for the prefix unless pinned
 
 template <class X>
 __device__ __forceinline__ void fillHot(X* xs, const X* x, int H) {
     const int nv = static_cast<int>((static_cast<int64_t>(H) * static_cast<int64_t>(sizeof(X))) / 16);
     const int4* src = reinterpret_cast<const int4*>(x);
     int4* dst = reinterpret_cast<int4*>(xs);
-    for (int k = static_cast<int>(threadIdx.x); k < nv; k += kHotBlock) dst[k] = __ldg(src + k);
-    for (int k = nv * static_cast<int>(16 / sizeof(X)) + static_cast<int>(threadIdx.x); k < H; k += kHotBlock)
+    for (int k = static_cast<int>(threadIdx.x); k < nv; k += kBlock) dst[k] = __ldg(src + k);
+    for (int k = nv * static_cast<int>(16 / sizeof(X)) + static_cast<int>(threadIdx.x); k < H; k += kBlock)
         xs[k] = x[k];
     __syncthreads();
 }
 
 template <int U, class T, bool ST>
-__global__ void __launch_bounds__(kHotBlock, hotMinBlocks<T>())
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<T, true>())
     primalSellHot(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                   const T* __restrict__ val, int koff, int begin, int end, int H) {
     extern __shared__ int4 hot_smem[];
     T* ys = reinterpret_cast<T*>(hot_smem);
     fillHot(ys, p.yg, H);
-    const int lane = static_cast<int>(threadIdx.x) & 31, wpb = kHotBlock / 32;
-    const int slices = (end - begin + kSlice - 1) / kSlice;
-    for (int sl = static_cast<int>(blockIdx.x) * wpb + (static_cast<int>(threadIdx.x) >> 5); sl < slices;
-         sl += static_cast<int>(gridDim.x) * wpb) {
-        const int j = begin + sl * kSlice + lane;
-        if (j < end) primalSellFrom<U, T, ST, true, true>(p, idx, val, j, hdr[sl], koff, ys, H);
-    }
+    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    primalSellFrom<U, T, ST, true, true>(p, idx, val, begin + r, hdr[r / kSlice], koff, ys, H);
 }
 
 template <int U, class T, bool ST>
-__global__ void __launch_bounds__(kHotBlock, hotMinBlocks<T>())
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
     dualSellHot(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                 const T* __restrict__ val, int koff, int begin, int end, int H) {
     extern __shared__ int4 hot_smem[];
     T* xs = reinterpret_cast<T*>(hot_smem);
     fillHot(xs, p.xr, H);
-    const int lane = static_cast<int>(threadIdx.x) & 31, wpb = kHotBlock / 32;
-    const int slices = (end - begin + kSlice - 1) / kSlice;
-    for (int sl = static_cast<int>(blockIdx.x) * wpb + (static_cast<int>(threadIdx.x) >> 5); sl < slices;
-         sl += static_cast<int>(gridDim.x) * wpb) {
-        const int i = begin + sl * kSlice + lane;
-        if (i < end) dualSellFrom<U, T, ST, true>(p, idx, val, i, hdr[sl], koff, xs, H);
-    }
+    const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    dualSellFrom<U, T, ST, true>(p, idx, val, begin + r, hdr[r / kSlice], koff, xs, H);
 }
 
 // Sliced-ELL shapes of the single-LP engine: kNumShapes + k for k < kEngSell,
@@ -497,31 +484,26 @@ template <class X>
 static int hotCap(const DeviceLp& d, int minb) {
     return hotBlockBytes(d, minb) / static_cast<int>(sizeof(X));
 }
-// Hot prefix length of the primal (y, double) / dual (x_refl, T) gathers at
-// precision T; 0 when the side does not use a hot kernel.
+// Hot prefix length of the primal (y) / dual (x_refl) gathers at precision T
+// (both gathered as T); 0 when the side does not use a hot kernel.
 template <class T>
 static int hotPrimal(const DeviceLp& d) {
-    return d.hotP > 0 ? std::min(d.hotP, hotCap<T>(d, hotMinBlocks<T>())) : 0;
+    return d.hotP > 0 ? std::min(d.hotP, hotCap<T>(d, sellMinBlocks<T, true>())) : 0;
 }
 template <class T>
 static int hotDual(const DeviceLp& d) {
-    return d.hotD > 0 ? std::min(d.hotD, hotCap<T>(d, hotMinBlocks<T>())) : 0;
-}
-static int hotGrid(const DeviceLp& d, int minb, int64_t rows) {
-    const int64_t warps = (rows + kSlice - 1) / kSlice;
-    const int64_t need = (warps + kHotBlock / 32 - 1) / (kHotBlock / 32);
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(d.sms) * minb)));
+    return d.hotD > 0 ? std::min(d.hotD, hotCap<T>(d, sellMinBlocks<T>())) : 0;
 }
 
 // Dynamic shared memory limits of every hot kernel (set once per load).
 template <class T>
 static void setHotAttrs(const DeviceLp& d) {
-    const int bytes = hotBlockBytes(d, hotMinBlocks<T>());
+    const int bp = hotBlockBytes(d, sellMinBlocks<T, true>()), bd = hotBlockBytes(d, sellMinBlocks<T>());
     for (int k = 0; k < kEngSell; ++k) {
         const int shape = kNumShapes + k;
         PDLPX_ENG_SELL_SWITCH(shape, {
-            cudaFuncSetAttribute(primalSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            cudaFuncSetAttribute(dualSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            cudaFuncSetAttribute(primalSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bp);
+            cudaFuncSetAttribute(dualSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
         });
     }
 }
@@ -533,7 +515,7 @@ void launchPrimalShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int 
     if (H > 0) {
         const size_t bytes = static_cast<size_t>(H) * sizeof(T);
         PDLPX_ENG_SELL_SWITCH(shape, (primalSellHot<UU, T, SS>
-                                      <<<hotGrid(d, hotMinBlocks<T>(), d.n - d.nlP), kHotBlock, bytes, s>>>(
+                                      <<<sellGrid(d.n - d.nlP), kBlock, bytes, s>>>(
                                           ia, d.sp_hdr, d.sp_idx, sellVals<T>(d, true), k, d.nlP, d.n, H)));
     } else if (isSell(shape)) {
         PDLPX_ENG_SELL_SWITCH(shape, (primalSellStep<UU, T, SS><<<sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
@@ -549,7 +531,7 @@ void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k,
     if (H > 0) {
         const size_t bytes = static_cast<size_t>(H) * sizeof(T);
         PDLPX_ENG_SELL_SWITCH(shape, (dualSellHot<UU, T, SS>
-                                      <<<hotGrid(d, hotMinBlocks<T>(), d.m - d.nlD), kHotBlock, bytes, s>>>(
+                                      <<<sellGrid(d.m - d.nlD), kBlock, bytes, s>>>(
                                           ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m, H)));
     } else if (isSell(shape)) {
         PDLPX_ENG_SELL_SWITCH(shape, (dualSellStep<UU, T, SS><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
@@ -1944,24 +1926,24 @@ int32_t Engine::timeKernels(int32_t precision, int32_t reps, int64_t flush_bytes
     return PDLPX_OK;
 }
 
+int32_t Engine::hotPrefix(int32_t precision, int32_t* primal, int32_t* dual) const {
+    if (!dev_) return PDLPX_E_NOT_LOADED;
+    const DeviceLp& d = *dev_;
+    const bool fp64 = precision == PDLPX_PREC_FP64;
+    if (!fp64 && !d.mixed) return PDLPX_E_INVALID;
+    if (primal)
+        *primal = !isSell(d.shapeP) ? 0 : fp64 ? hotPrimal<double>(d) : hotPrimal<float>(d);
+    if (dual) *dual = !isSell(d.shapeD) ? 0 : fp64 ? hotDual<double>(d) : hotDual<float>(d);
+    return PDLPX_OK;
+}
+
 int32_t Engine::launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const {
     if (!dev_) return PDLPX_E_NOT_LOADED;
     const DeviceLp& d = *dev_;
     if (ga) *ga = isSell(d.shapeD) ? 1 : kShapes[d.shapeD].G;
     if (gat) *gat = isSell(d.shapeP) ? 1 : kShapes[d.shapeP].G;
-    // blocks of the short-row launches at the starting precision (persistent
-    // blocks when the side runs a hot kernel)
-    const int hp = d.mixed ? hotPrimal<float>(d) : hotPrimal<double>(d);
-    const int hd = d.mixed ? hotDual<float>(d) : hotDual<double>(d);
-    const int minb = d.mixed ? hotMinBlocks<float>() : hotMinBlocks<double>();
-    if (bp)
-        *bp = !isSell(d.shapeP) ? gridForShape(d.n - d.nlP, d.shapeP)
-              : hp > 0          ? hotGrid(d, minb, d.n - d.nlP)
-                                : sellGrid(d.n - d.nlP);
-    if (bd)
-        *bd = !isSell(d.shapeD) ? gridForShape(d.m - d.nlD, d.shapeD)
-              : hd > 0          ? hotGrid(d, minb, d.m - d.nlD)
-                                : sellGrid(d.m - d.nlD);
+    if (bp) *bp = isSell(d.shapeP) ? sellGrid(d.n - d.nlP) : gridForShape(d.n - d.nlP, d.shapeP);
+    if (bd) *bd = isSell(d.shapeD) ? sellGrid(d.m - d.nlD) : gridForShape(d.m - d.nlD, d.shapeD);
     return PDLPX_OK;
 }
 

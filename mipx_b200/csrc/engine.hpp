@@ -73,6 +73,7 @@ public:
         if (samples) *samples = k;
     }
     int32_t launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const;
+    int32_t hotPrefix(int32_t precision, int32_t* primal, int32_t* dual) const;
 
     std::string last_error;
 

@@ -433,6 +433,15 @@ class PdlpSolver:
                     self._h)
         return {"group_a": ga.value, "group_at": gat.value, "blocks_primal": bp.value, "blocks_dual": bd.value}
 
+    def hotPrefix(self, precision: "Precision" = None) -> dict:
+        """Hot-prefix lengths (option hot_cache) of the primal / dual step's
+        gathers at `precision` (default: the loaded starting precision)."""
+        if precision is None:
+            precision = Precision.FP64 if self._options.precision == Precision.FP64 else Precision.Mixed
+        p, d = C.c_int32(), C.c_int32()
+        _capi.check(self._lib.pdlpx_get_hot_prefix(self._h, int(precision), C.byref(p), C.byref(d)), self._h)
+        return {"primal": p.value, "dual": d.value}
+
     def scaling(self) -> dict:
         """Scaled-problem arrays of the last load (parity of pdlp.cpp:469-669)."""
         m, n = self._dims()

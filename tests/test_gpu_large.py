@@ -70,8 +70,8 @@ def _transposed(lp, seed):
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_hot_prefix_in_shared_memory_gives_same_bits(side, precision):
     """The hot-prefix kernels (gathers of the other side's longest rows served
-    from shared memory, persistent blocks) compute what the plain sliced-ELL
-    kernels compute, bit for bit: same iterations, objective, x and y.  'dual':
+    from a shared-memory copy) compute what the plain sliced-ELL kernels
+    compute, bit for bit: same iterations, objective, x and y.  'dual':
     power-law columns (the dual step's x gathers); 'primal': the transposed LP,
     whose long rows are the primal step's y gathers."""
     from mipx_b200.pdlp import Precision
@@ -86,10 +86,10 @@ def test_hot_prefix_in_shared_memory_gives_same_bits(side, precision):
                                  max_iter=4000, hot_cache=hot))
         s.load(lp)
         r = s.solve()
-        out.append((r, s.getPrimalValues(), s.getDualValues(), s.launchConfig()))
-    (r0, x0, y0, c0), (r1, x1, y1, c1) = out
-    key = "blocks_dual" if side == "dual" else "blocks_primal"
-    assert c1[key] < c0[key], (c0, c1)  # persistent blocks: the hot kernel ran
+        out.append((r, s.getPrimalValues(), s.getDualValues(), s.hotPrefix(prec)))
+    (r0, x0, y0, h0), (r1, x1, y1, h1) = out
+    assert h0 == {"primal": 0, "dual": 0}
+    assert h1[side] > 0 and h1["primal" if side == "dual" else "dual"] == 0, h1  # the hot kernel ran
     assert r0.iterations == r1.iterations and r0.objective == r1.objective
     np.testing.assert_array_equal(x0, x1)
     np.testing.assert_array_equal(y0, y1)
