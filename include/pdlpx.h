@@ -146,13 +146,13 @@ typedef struct pdlpx_options {
                                          bound tested first, so a negative reduced cost counts and
                                          such LPs may not converge, as there); 0 (default): a fixed
                                          column adds no dual residual */
-    int32_t hot_cache;                /* single-LP engine, sliced-ELL sides: serve the step's gathers of
-                                         the other side's longest rows (first in the device numbering)
-                                         from a shared-memory copy of that prefix held by every
-                                         block: -1 (default) when those rows hold >= 10 % of the
-                                         nonzeros, with 128 KB of shared memory per SM; k > 0 whenever
-                                         the other side has long rows, with k KB per SM (capped at the
-                                         device's limit); 0 never.  Identical results either way */
+    int32_t hot_cache;                /* single-LP engine, sliced-ELL sides: k > 0 serves the step's
+                                         gathers of the other side's longest rows (first in the device
+                                         numbering) from a shared-memory copy of that prefix held by
+                                         every block, with k KB of shared memory per SM (capped at the
+                                         device's limit); 0 (default) never.  Identical results either
+                                         way; measured slower on the 500k x 2M power-law LP, whose
+                                         popular columns L1 already caches */
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

@@ -104,7 +104,7 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->scale_on_device = -1;
     o->sell = -1;
     o->reference_fixed_columns = 0;
-    o->hot_cache = -1;
+    o->hot_cache = 0;
 }
 
 const char* pdlpx_error_string(int32_t code) {

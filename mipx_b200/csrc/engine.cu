@@ -167,9 +167,12 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
 // of the nonzeros).  Each block first copies the prefix into shared memory
 // with 16-byte loads, then runs the same per-row step as the kernels above
 // with those gathers served from shared memory (same arithmetic and order, so
-// the same bits).  Persistent blocks holding a larger prefix measured slower
-// on that LP (warps with one or two slices each, no block refill).
-constexpr int kHotDefaultKb = 128;  // shared memory per SM for the prefix unless pinned
+// the same bits).  Off unless the option asks for it: on that LP the dual step
+// measured 78.6 us without the prefix and 91.7 / 100 / 226 us with 64 / 128 /
+// 192 KB of shared memory per SM for it (B200, FP32): the shared memory is
+// carved out of the L1 that already caches the popular columns and holds the
+// sectors of the loads in flight.  (Persistent blocks holding a 110 KB prefix
+// measured ~100 us too.)
 
 template <class X>
 __device__ __forceinline__ void fillHot(X* xs, const X* x, int H) {
@@ -504,6 +507,26 @@ static void setHotAttrs(const DeviceLp& d) {
         PDLPX_ENG_SELL_SWITCH(shape, {
             cudaFuncSetAttribute(primalSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bp);
             cudaFuncSetAttribute(dualSellHot<UU, T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
+        });
+    }
+}
+
+// The step kernels use no shared memory; their scattered gathers lean on L1
+// (the power-law LPs' popular columns hit there), so they ask for the largest
+// L1 carve-out.
+template <class T>
+static void preferL1() {
+    for (int k = 0; k < kEngSell; ++k) {
+        const int shape = kNumShapes + k;
+        PDLPX_ENG_SELL_SWITCH(shape, {
+            cudaFuncSetAttribute(primalSellStep<UU, T, SS>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+            cudaFuncSetAttribute(dualSellStep<UU, T, SS>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        });
+    }
+    for (int shape = 0; shape < kNumShapes; ++shape) {
+        PDLPX_SHAPE_SWITCH(shape, {
+            cudaFuncSetAttribute(primalStep<GG, RR, UU, T, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+            cudaFuncSetAttribute(dualStep<GG, RR, UU, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
         });
     }
 }
@@ -916,21 +939,20 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.gLAT = d.nlP > 0 ? std::min(256, pickGroup(zlP, d.nlP)) : 1;
     d.shapeLD = longShape(zlD, d.nlD);
     d.shapeLP = longShape(zlP, d.nlP);
-    // Hot prefixes: the dual step gathers x, whose long columns [0, nlP) hold
-    // zlP of the entries; the primal step gathers y, whose long rows [0, nlD)
-    // hold zlD.
+    // Hot prefixes (option): the dual step gathers x, whose long columns
+    // [0, nlP) come first; the primal step gathers y, long rows [0, nlD).
     PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    auto hotOn = [&](int64_t zl_other) {
-        return o.hot_cache > 0 || (o.hot_cache < 0 && nnz > 0 && 10 * zl_other >= nnz);
-    };
-    d.hot_bytes_sm = 1024 * (o.hot_cache > 0 ? o.hot_cache : kHotDefaultKb);
-    d.hotD = (sellD && d.nlP > 0 && hotOn(zlP)) ? d.nlP : 0;
-    d.hotP = (sellP && d.nlD > 0 && hotOn(zlD)) ? d.nlD : 0;
+    const bool hot = o.hot_cache > 0;
+    d.hot_bytes_sm = hot ? 1024 * o.hot_cache : 0;
+    d.hotD = (hot && sellD && d.nlP > 0) ? d.nlP : 0;
+    d.hotP = (hot && sellP && d.nlD > 0) ? d.nlD : 0;
     if (d.hotD > 0 || d.hotP > 0) {
         setHotAttrs<float>(d);
         setHotAttrs<double>(d);
     }
+    preferL1<float>();
+    preferL1<double>();
     const int cap = 4 * d.sms;
     d.nb_rows_s = std::max(1, std::min(gridFor(msD, d.gA), cap));
     d.nb_cols_s = std::max(1, std::min(gridFor(msP, d.gAT), cap));

@@ -135,7 +135,7 @@ class PdlpOptions:
     scale_on_device: int = -1
     sell: int = -1
     reference_fixed_columns: bool = False
-    hot_cache: int = -1
+    hot_cache: int = 0
 
     def to_c(self) -> _capi.Options:
         # every field of pdlpx_options is set here, so no library call is
