@@ -253,14 +253,17 @@ def step_bytes(m: int, n: int, nnz: int) -> dict:
     """Bytes a CSR implementation of each fused step must move once per launch.
 
     FP32 kernels (mixed phase): matrix values + indices 8 B/nnz, row pointers;
-    primal: y_cur gathered once (FP64, 8 m), per column the packed constants
-    (16 B), x_cur read + write (FP64, 16 B), x_init (4 B), x_refl write (4 B);
-    dual: x_refl gathered once (4 n), per row the packed constants (16 B),
-    y_cur read + write (16 B), y_init (4 B).  FP64 kernels: 12 B/nnz, 32 B
-    packs, FP64 anchors and reflections."""
+    primal: the FP32 copy of y_cur gathered once (4 m), per column the packed
+    constants (16 B), x_cur read + write (FP64, 16 B), x_init (4 B), x_refl
+    write (4 B); dual: x_refl gathered once (4 n), per row the packed
+    constants (16 B), y_cur read + write (16 B), y_init (4 B), the FP32 copy of
+    y_cur written (4 B).  (The tiled long-column launch stores its entries in
+    6 B and adds per-chunk partial sums; the CSR figure is kept as the
+    algorithmic one.)  FP64 kernels: 12 B/nnz, 32 B packs, FP64 anchors and
+    reflections, y_cur gathered in FP64."""
     return {
-        "primal_fp32": 4 * (n + 1) + 8 * nnz + 8 * m + 40 * n,
-        "dual_fp32": 4 * (m + 1) + 8 * nnz + 4 * n + 36 * m,
+        "primal_fp32": 4 * (n + 1) + 8 * nnz + 4 * m + 40 * n,
+        "dual_fp32": 4 * (m + 1) + 8 * nnz + 4 * n + 40 * m,
         "primal_fp64": 4 * (n + 1) + 12 * nnz + 8 * m + 64 * n,
         "dual_fp64": 4 * (m + 1) + 12 * nnz + 8 * n + 56 * m,
     }

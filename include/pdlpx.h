@@ -153,6 +153,11 @@ typedef struct pdlpx_options {
                                          device's limit); 0 (default) never.  Identical results either
                                          way; measured slower on the 500k x 2M power-law LP, whose
                                          popular columns L1 already caches */
+    int32_t long_tiles;               /* single-LP engine, mixed mode: run the primal step of the long
+                                         columns (> max(64, 8 x mean) entries) in row chunks whose FP32
+                                         y sits in shared memory: -1 (default) when those columns hold
+                                         >= 1M entries, 1 whenever there are long columns, 0 never */
+    int32_t reserved[1];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

@@ -174,13 +174,15 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
 // sectors of the loads in flight.  (Persistent blocks holding a 110 KB prefix
 // measured ~100 us too.)
 
+// xs[0, H) = x[0, H) by the whole block (x 16-byte aligned), then a barrier.
 template <class X>
 __device__ __forceinline__ void fillHot(X* xs, const X* x, int H) {
     const int nv = static_cast<int>((static_cast<int64_t>(H) * static_cast<int64_t>(sizeof(X))) / 16);
     const int4* src = reinterpret_cast<const int4*>(x);
     int4* dst = reinterpret_cast<int4*>(xs);
-    for (int k = static_cast<int>(threadIdx.x); k < nv; k += kBlock) dst[k] = __ldg(src + k);
-    for (int k = nv * static_cast<int>(16 / sizeof(X)) + static_cast<int>(threadIdx.x); k < H; k += kBlock)
+    const int step = static_cast<int>(blockDim.x);
+    for (int k = static_cast<int>(threadIdx.x); k < nv; k += step) dst[k] = __ldg(src + k);
+    for (int k = nv * static_cast<int>(16 / sizeof(X)) + static_cast<int>(threadIdx.x); k < H; k += step)
         xs[k] = x[k];
     __syncthreads();
 }
@@ -207,6 +209,80 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
     const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
     if (begin + r >= end) return;
     dualSellFrom<U, T, ST, true>(p, idx, val, begin + r, hdr[r / kSlice], koff, xs, H);
+}
+
+// ---- long columns of the primal step in row chunks (mixed mode) ------------
+// Every long column's gathers of y are scattered over all of y, and a gather
+// through L1 costs its tag stage one sector whatever its size.  Cut into row
+// chunks of R rows (R * 4 bytes of shared memory), each (chunk, column group)
+// tile copies its chunk of the FP32 y into shared memory with 16-byte loads
+// and serves every gather of its columns from there; 4 lanes per column sum
+// the column's entries in the chunk (lane-strided, then a fixed shuffle tree)
+// into part[j * C + c].  A second launch sums the C partials of each column
+// in chunk order and runs the column's Halpern primal step.  The matrix copy
+// stores rows as 16-bit offsets into the chunk (6 bytes per entry).
+struct LongTileArgs {
+    const int* off;        // [c * nl + j] .. [c * nl + j + 1]: entries of column j in chunk c
+    const int* gb;         // G + 1 column-group bounds
+    const uint16_t* row;   // row - c * R
+    const float* val;
+    double* part;          // [j * C + c]
+    int R, C, G, nl;
+};
+constexpr int kTileBlock = 1024;
+constexpr int kTileLanes = 4;
+constexpr int kTileMaxRows = 28672;          // 112 KB of FP32 y per block
+constexpr int64_t kTileMinEntries = 1 << 20;  // long-column entries below which the CSR launch is kept
+
+__global__ void __launch_bounds__(kTileBlock, 1) primalLongTiles(IterArgs<float> p, LongTileArgs t, int koff) {
+    bool last = false;
+    if (!active(p.st, precTag<float>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    extern __shared__ int4 tile_smem[];
+    float* ys = reinterpret_cast<float*>(tile_smem);
+    const int c = static_cast<int>(blockIdx.x) / t.G, g = static_cast<int>(blockIdx.x) % t.G;
+    const int r0 = c * t.R;
+    fillHot(ys, p.yg + r0, min(t.R, p.m - r0));
+    const int lane = static_cast<int>(threadIdx.x) % kTileLanes;
+    const int grp = static_cast<int>(threadIdx.x) / kTileLanes;
+    constexpr int groups = kTileBlock / kTileLanes;
+    // the 4 lanes of a group take the same columns, so their shuffles name
+    // only themselves (groups of one warp may run different column counts)
+    const unsigned mask = 0xFu << ((threadIdx.x & 31u) & ~3u);
+    const int* __restrict__ off = t.off + static_cast<size_t>(c) * t.nl;
+    const uint16_t* __restrict__ row = t.row;
+    const float* __restrict__ val = t.val;
+    for (int j = t.gb[g] + grp; j < t.gb[g + 1]; j += groups) {
+        const int b = off[j], e = off[j + 1];
+        double s0 = 0.0, s1 = 0.0;
+        int k = b + lane;
+        for (; k + kTileLanes < e; k += 2 * kTileLanes) {
+            s0 += static_cast<double>(__ldg(val + k)) * static_cast<double>(ys[__ldg(row + k)]);
+            s1 += static_cast<double>(__ldg(val + k + kTileLanes)) *
+                  static_cast<double>(ys[__ldg(row + k + kTileLanes)]);
+        }
+        if (k < e) s0 += static_cast<double>(__ldg(val + k)) * static_cast<double>(ys[__ldg(row + k)]);
+        double s = s0 + s1;
+        s += __shfl_xor_sync(mask, s, 1);
+        s += __shfl_xor_sync(mask, s, 2);
+        if (lane == 0) t.part[static_cast<size_t>(j) * t.C + c] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) primalLongFinish(IterArgs<float> p, LongTileArgs t, int koff) {
+    const int j = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    if (j >= t.nl) return;
+    const ColPack<float> q = p.cp[j];
+    const double xc = p.xc[j];
+    const double xi = static_cast<double>(p.xi[j]);
+    const double* __restrict__ pj = t.part + static_cast<size_t>(j) * t.C;
+    double s = 0.0;
+    for (int c = 0; c < t.C; ++c) s += pj[c];
+    bool last = false;
+    if (!active(p.st, precTag<float>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
+    const double step = p.st->step, pw = p.st->pw;
+    const int k = p.st->inner + koff;
+    const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
+    primalUpdate<float>(p, j, q, xc, xi, s, step, pw, lam, last);
 }
 
 // Sliced-ELL shapes of the single-LP engine: kNumShapes + k for k < kEngSell,
@@ -267,6 +343,14 @@ struct DeviceLp {
     int32_t hotP = 0, hotD = 0;
     int hot_smem_sm = 0, hot_smem_block = 0;  // shared memory per SM / per block (opt-in)
     int hot_bytes_sm = 0;                      // shared memory per SM given to the hot prefix
+    // long columns in row chunks for the mixed-mode primal step (0 chunks: the
+    // CSR launch runs instead); see buildLongTiles
+    int lt_R = 0, lt_C = 0, lt_G = 0;
+    int32_t *lt_off = nullptr, *lt_gb = nullptr;
+    uint16_t* lt_row = nullptr;
+    float* lt_val = nullptr;
+    double* lt_part = nullptr;
+    LongTileArgs tiles() const { return LongTileArgs{lt_off, lt_gb, lt_row, lt_val, lt_part, lt_R, lt_C, lt_G, nlP}; }
     int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
     std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
     // Sides stored as sliced ELL (shapeP / shapeD >= kNumShapes): their short
@@ -569,6 +653,19 @@ void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k,
 template <class T>
 int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s) {
     int n = 0;
+    if constexpr (sizeof(T) == 4) {
+        if (d.lt_C > 0) {
+            const LongTileArgs t = d.tiles();
+            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, 4 * static_cast<size_t>(d.lt_R), s>>>(ia, t, k);
+            primalLongFinish<<<sellGrid(d.nlP), kBlock, 0, s>>>(ia, t, k);
+            n += 2;
+            if (d.n > d.nlP) {
+                launchPrimalShort<T>(d, ia, d.shapeP, k, s);
+                ++n;
+            }
+            return n;
+        }
+    }
     if (d.nlP > 0) {
         PDLPX_SHAPE_SWITCH(d.shapeLP,
                            (primalStep<GG, RR, UU, T, true><<<gridForShape(d.nlP, d.shapeLP), kBlock, 0, s>>>(ia, k, 0, d.nlP)));
@@ -806,6 +903,55 @@ static bool buildSell(const Csr& a, int32_t r0, SellHost& h) {
     return true;
 }
 
+// Long columns [0, nl) of A^T (device numbering) in row chunks for the tiled
+// primal step (primalLongTiles): chunk c holds rows [c R, (c + 1) R), R a
+// multiple of 16 (so each chunk of y starts on a 16-byte boundary) and at most
+// max_rows; entries of column j in chunk c keep their CSR order; G column
+// groups per chunk (as many tiles as SMs, at least one group), cut at equal
+// shares of the entries.  False when a chunk offset would not fit 16 bits.
+struct LongTilesHost {
+    int R = 0, C = 0, G = 0;
+    std::vector<int32_t> off, gb;
+    std::vector<uint16_t> row;
+    std::vector<float> val;
+};
+static bool buildLongTiles(const Csr& at, int32_t nl, int32_t m, int sms, int max_rows, LongTilesHost& t) {
+    if (nl <= 0 || m <= 0) return false;
+    int C = (m + max_rows - 1) / max_rows;
+    const int R = (((m + C - 1) / C) + 15) & ~15;
+    C = (m + R - 1) / R;
+    if (R > 65536) return false;
+    t.R = R;
+    t.C = C;
+    t.G = std::max(1, std::min(nl, sms / C));
+    const size_t cells = static_cast<size_t>(C) * static_cast<size_t>(nl);
+    t.off.assign(cells + 1, 0);
+    for (int32_t j = 0; j < nl; ++j)
+        for (int32_t k = at.ptr[j]; k < at.ptr[j + 1]; ++k)
+            ++t.off[static_cast<size_t>(at.idx[k] / R) * nl + j + 1];
+    for (size_t q = 0; q < cells; ++q) t.off[q + 1] += t.off[q];
+    const int64_t z = at.ptr[nl];
+    t.row.resize(static_cast<size_t>(z));
+    t.val.resize(static_cast<size_t>(z));
+    std::vector<int32_t> pos(t.off.begin(), t.off.end() - 1);
+    for (int32_t j = 0; j < nl; ++j)
+        for (int32_t k = at.ptr[j]; k < at.ptr[j + 1]; ++k) {
+            const int32_t c = at.idx[k] / R;
+            const int32_t p = pos[static_cast<size_t>(c) * nl + j]++;
+            t.row[p] = static_cast<uint16_t>(at.idx[k] - c * R);
+            t.val[p] = static_cast<float>(at.val[k]);
+        }
+    t.gb.assign(static_cast<size_t>(t.G) + 1, nl);
+    t.gb[0] = 0;
+    int32_t j = 0;
+    for (int g = 1; g < t.G; ++g) {
+        const int64_t target = z * g / t.G;
+        while (j < nl && at.ptr[j] < target) ++j;
+        t.gb[g] = std::max(j, t.gb[g - 1]);
+    }
+    return true;
+}
+
 // Sliced-ELL shape of a side from the options: a pinned sliced-ELL shape
 // (kNumShapes + 1 .. kNumShapes + kNumSell), else 4 entries per round for mean
 // lengths up to 12 and 8 above (the packed batch's measured picks).
@@ -929,6 +1075,13 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     const int64_t zlD = d.nlD > 0 ? sc.a.ptr[d.nlD] : 0, zlP = d.nlP > 0 ? sc.at.ptr[d.nlP] : 0;
     d.zlD = zlD;
     d.zlP = zlP;
+    LongTilesHost ltH;
+    const bool want_tiles = o.long_tiles > 0 || (o.long_tiles < 0 && zlP >= kTileMinEntries);
+    if (d.mixed && want_tiles && buildLongTiles(sc.at, d.nlP, d.m, d.sms, kTileMaxRows, ltH)) {
+        d.lt_R = ltH.R;
+        d.lt_C = ltH.C;
+        d.lt_G = ltH.G;
+    }
     const int32_t msD = d.m - d.nlD, msP = d.n - d.nlP;  // short rows
     d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz - zlD, msD);
     d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz - zlP, msP);
@@ -997,6 +1150,12 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
                  o_sp_v64 = sellP ? take(8 * eP) : 0, o_sp_v32 = sellP && mixed ? take(4 * eP) : 0;
     const size_t o_sd_hdr = sellD ? take(8 * hsD.hdr.size()) : 0, o_sd_idx = sellD ? take(4 * eD) : 0,
                  o_sd_v64 = sellD ? take(8 * eD) : 0, o_sd_v32 = sellD && mixed ? take(4 * eD) : 0;
+    // long columns in row chunks: offsets, group bounds, rows, FP32 values, partials
+    const bool lt = d.lt_C > 0;
+    const size_t zt = ltH.row.size();
+    const size_t o_lt_off = lt ? take(4 * ltH.off.size()) : 0, o_lt_gb = lt ? take(4 * ltH.gb.size()) : 0,
+                 o_lt_row = lt ? take(2 * zt) : 0, o_lt_val = lt ? take(4 * zt) : 0,
+                 o_lt_part = lt ? take(8 * static_cast<size_t>(d.nlP) * static_cast<size_t>(d.lt_C)) : 0;
     // Anderson ring (2 w (n + m) doubles), extrapolation scratch, partials, Gram matrix.
     d.aa_w = o.anderson_acceleration && o.anderson_window_size >= 2 ? o.anderson_window_size : 0;
     const size_t dim = static_cast<size_t>(n) + static_cast<size_t>(m);
@@ -1077,6 +1236,13 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         d.sd_v64 = reinterpret_cast<double*>(b + o_sd_v64);
         if (mixed) d.sd_v32 = reinterpret_cast<float*>(b + o_sd_v32);
     }
+    if (lt) {
+        d.lt_off = reinterpret_cast<int32_t*>(b + o_lt_off);
+        d.lt_gb = reinterpret_cast<int32_t*>(b + o_lt_gb);
+        d.lt_row = reinterpret_cast<uint16_t*>(b + o_lt_row);
+        d.lt_val = reinterpret_cast<float*>(b + o_lt_val);
+        d.lt_part = reinterpret_cast<double*>(b + o_lt_part);
+    }
     d.kev_iter = o.termination_eval_frequency >= 2 ? 2 : 1;
     for (auto& row : d.kev)
         for (auto& e : row) PDLPX_CK(cudaEventCreate(&e));
@@ -1137,6 +1303,16 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     };
     if (sellP) PDLPX_CK(upSell(hsP, d.sp_hdr, d.sp_idx, d.sp_v64, d.sp_v32));
     if (sellD) PDLPX_CK(upSell(hsD, d.sd_hdr, d.sd_idx, d.sd_v64, d.sd_v32));
+    if (lt) {
+        PDLPX_CK(up(d.lt_off, ltH.off.data(), 4 * ltH.off.size()));
+        PDLPX_CK(up(d.lt_gb, ltH.gb.data(), 4 * ltH.gb.size()));
+        PDLPX_CK(up(d.lt_row, ltH.row.data(), 2 * zt));
+        PDLPX_CK(up(d.lt_val, ltH.val.data(), 4 * zt));
+        PDLPX_CK(cudaStreamSynchronize(s));
+        ltH = LongTilesHost{};
+        PDLPX_CK(cudaFuncSetAttribute(primalLongTiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      4 * d.lt_R));
+    }
     {
         std::vector<ColPack<double>> cp;
         std::vector<RowPack<double>> rp;

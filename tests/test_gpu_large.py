@@ -93,3 +93,33 @@ def test_hot_prefix_in_shared_memory_gives_same_bits(side, precision):
     assert r0.iterations == r1.iterations and r0.objective == r1.objective
     np.testing.assert_array_equal(x0, x1)
     np.testing.assert_array_equal(y0, y1)
+
+
+def test_long_column_tiles_match_csr_launch():
+    """The mixed-mode primal step of the long columns in row chunks (FP32 y in
+    shared memory, per-chunk partial sums added in chunk order) against the
+    CSR launch of the same columns: the sums differ only in FP64 association,
+    so after 400 iterations (two restart cycles) the iterates agree to 1e-9
+    relative, and full solves reach the same optimum to 1e-6."""
+    lp, _ = G.powerlaw_lp(100000, 400000, 2, 2000, 10.0, 0.01, 1e3, 11)
+    out = []
+    for tiles in (0, 1):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, max_iter=400,
+                                 long_tiles=tiles))
+        s.load(lp)
+        r = s.solve()
+        out.append((r, s.getPrimalValues(), s.getDualValues()))
+    (r0, x0, y0), (r1, x1, y1) = out
+    assert r0.iterations == r1.iterations == 400
+    np.testing.assert_allclose(x1, x0, rtol=1e-9, atol=1e-9 * max(1.0, np.abs(x0).max()))
+    np.testing.assert_allclose(y1, y0, rtol=1e-9, atol=1e-9 * max(1.0, np.abs(y0).max()))
+    full = []
+    for tiles in (0, 1):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL,
+                                 max_solve_seconds=120, long_tiles=tiles))
+        s.load(lp)
+        full.append(s.solve())
+    assert full[0].status == full[1].status == Status.Optimal
+    assert GC.rel_err(full[1].objective, full[0].objective) <= GC.OBJ_TOL
