@@ -61,7 +61,9 @@ enum { PDLPX_MINIMIZE = 0, PDLPX_MAXIMIZE = 1 };
 
 /* Precision modes of the engine (no counterpart in the reference, which is FP64 only). */
 enum {
-    PDLPX_PREC_MIXED = 0, /* FP32 matrix/iterates/SpMV, FP64 checks, PI, objective, FP64 polish */
+    PDLPX_PREC_MIXED = 0, /* FP32 matrix/iterates/SpMV, FP64 checks, PI, objective, FP64 polish;
+                             an LP whose FP64 working set per iteration is under 16 MB (L2-resident:
+                             FP32 storage saves no time there) runs FP64 kernels unless fp64_switch = 0 */
     PDLPX_PREC_FP64 = 1   /* FP64 throughout ("plain FP64 GPU" mode) */
 };
 
