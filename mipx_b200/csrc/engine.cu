@@ -232,39 +232,52 @@ struct LongTileArgs {
 constexpr int kTileBlock = 1024;
 constexpr int kTileLanes = 4;
 constexpr int kTileMaxRows = 28672;          // 112 KB of FP32 y per block
+constexpr int kTileMaxCols = 8192;           // columns per group (their offsets: 32 KB of shared memory)
 constexpr int64_t kTileMinEntries = 1 << 20;  // long-column entries below which the CSR launch is kept
+
+// shared memory of a tile: the chunk of y, then its group's kTileMaxCols + 1 offsets
+static size_t tileSmemBytes(int R) { return 4 * static_cast<size_t>(R) + 4 * static_cast<size_t>(kTileMaxCols + 1); }
 
 __global__ void __launch_bounds__(kTileBlock, 1) primalLongTiles(IterArgs<float> p, LongTileArgs t, int koff) {
     bool last = false;
     if (!active(p.st, precTag<float>(), koff, p.max_iter, p.polish_max_iter, last, p.N)) return;
     extern __shared__ int4 tile_smem[];
     float* ys = reinterpret_cast<float*>(tile_smem);
+    int* so = reinterpret_cast<int*>(ys + t.R);  // the group's entry offsets in this chunk
     const int c = static_cast<int>(blockIdx.x) / t.G, g = static_cast<int>(blockIdx.x) % t.G;
+    const int j0 = t.gb[g], ncol = t.gb[g + 1] - j0;
+    const int* __restrict__ off = t.off + static_cast<size_t>(c) * t.nl + j0;
+    for (int q = static_cast<int>(threadIdx.x); q <= ncol; q += kTileBlock) so[q] = __ldg(off + q);
     const int r0 = c * t.R;
-    fillHot(ys, p.yg + r0, min(t.R, p.m - r0));
+    fillHot(ys, p.yg + r0, min(t.R, p.m - r0));  // ends with the block barrier
     const int lane = static_cast<int>(threadIdx.x) % kTileLanes;
     const int grp = static_cast<int>(threadIdx.x) / kTileLanes;
     constexpr int groups = kTileBlock / kTileLanes;
     // the 4 lanes of a group take the same columns, so their shuffles name
     // only themselves (groups of one warp may run different column counts)
     const unsigned mask = 0xFu << ((threadIdx.x & 31u) & ~3u);
-    const int* __restrict__ off = t.off + static_cast<size_t>(c) * t.nl;
     const uint16_t* __restrict__ row = t.row;
     const float* __restrict__ val = t.val;
-    for (int j = t.gb[g] + grp; j < t.gb[g + 1]; j += groups) {
-        const int b = off[j], e = off[j + 1];
+    // two columns per pass, so two independent load chains are in flight
+    for (int q = grp; q < ncol; q += 2 * groups) {
+        const int q1 = q + groups;
+        const int b0 = so[q], n0 = so[q + 1] - b0;
+        const int b1 = q1 < ncol ? so[q1] : 0, n1 = q1 < ncol ? so[q1 + 1] - b1 : 0;
         double s0 = 0.0, s1 = 0.0;
-        int k = b + lane;
-        for (; k + kTileLanes < e; k += 2 * kTileLanes) {
-            s0 += static_cast<double>(__ldg(val + k)) * static_cast<double>(ys[__ldg(row + k)]);
-            s1 += static_cast<double>(__ldg(val + k + kTileLanes)) *
-                  static_cast<double>(ys[__ldg(row + k + kTileLanes)]);
+        const int nmax = max(n0, n1);
+#pragma unroll 2
+        for (int r = lane; r < nmax; r += kTileLanes) {
+            if (r < n0) s0 += static_cast<double>(__ldg(val + b0 + r)) * static_cast<double>(ys[__ldg(row + b0 + r)]);
+            if (r < n1) s1 += static_cast<double>(__ldg(val + b1 + r)) * static_cast<double>(ys[__ldg(row + b1 + r)]);
         }
-        if (k < e) s0 += static_cast<double>(__ldg(val + k)) * static_cast<double>(ys[__ldg(row + k)]);
-        double s = s0 + s1;
-        s += __shfl_xor_sync(mask, s, 1);
-        s += __shfl_xor_sync(mask, s, 2);
-        if (lane == 0) t.part[static_cast<size_t>(j) * t.C + c] = s;
+        s0 += __shfl_xor_sync(mask, s0, 1);
+        s0 += __shfl_xor_sync(mask, s0, 2);
+        s1 += __shfl_xor_sync(mask, s1, 1);
+        s1 += __shfl_xor_sync(mask, s1, 2);
+        if (lane == 0) {
+            t.part[static_cast<size_t>(j0 + q) * t.C + c] = s0;
+            if (q1 < ncol) t.part[static_cast<size_t>(j0 + q1) * t.C + c] = s1;
+        }
     }
 }
 
@@ -656,7 +669,7 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
     if constexpr (sizeof(T) == 4) {
         if (d.lt_C > 0) {
             const LongTileArgs t = d.tiles();
-            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, 4 * static_cast<size_t>(d.lt_R), s>>>(ia, t, k);
+            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R), s>>>(ia, t, k);
             primalLongFinish<<<sellGrid(d.nlP), kBlock, 0, s>>>(ia, t, k);
             n += 2;
             if (d.n > d.nlP) {
@@ -941,14 +954,22 @@ static bool buildLongTiles(const Csr& at, int32_t nl, int32_t m, int sms, int ma
             t.row[p] = static_cast<uint16_t>(at.idx[k] - c * R);
             t.val[p] = static_cast<float>(at.val[k]);
         }
-    t.gb.assign(static_cast<size_t>(t.G) + 1, nl);
-    t.gb[0] = 0;
-    int32_t j = 0;
-    for (int g = 1; g < t.G; ++g) {
-        const int64_t target = z * g / t.G;
-        while (j < nl && at.ptr[j] < target) ++j;
-        t.gb[g] = std::max(j, t.gb[g - 1]);
+    // groups of equal weight (entries + 8 per column, the per-column work of a
+    // lane group in entries), at most kTileMaxCols columns each
+    const int64_t wtot = z + 8 * static_cast<int64_t>(nl);
+    t.gb.assign(1, 0);
+    int64_t w = 0;
+    int32_t start = 0;
+    for (int32_t j = 0; j < nl; ++j) {
+        w += (at.ptr[j + 1] - at.ptr[j]) + 8;
+        const int64_t target = wtot * static_cast<int64_t>(t.gb.size()) / t.G;
+        if (j + 1 < nl && (w >= target || j + 1 - start >= kTileMaxCols)) {
+            t.gb.push_back(j + 1);
+            start = j + 1;
+        }
     }
+    t.gb.push_back(nl);
+    t.G = static_cast<int>(t.gb.size()) - 1;
     return true;
 }
 
@@ -1325,7 +1346,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         PDLPX_CK(cudaStreamSynchronize(s));
         ltH = LongTilesHost{};
         PDLPX_CK(cudaFuncSetAttribute(primalLongTiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      4 * d.lt_R));
+                                      static_cast<int>(tileSmemBytes(d.lt_R))));
     }
     {
         std::vector<ColPack<double>> cp;
