@@ -228,15 +228,17 @@ struct LongTileArgs {
     const float* val;
     double* part;          // [j * C + c]
     int R, C, G, nl;
+    int maxcols;           // most columns in one group
 };
 constexpr int kTileBlock = 1024;
 constexpr int kTileLanes = 4;
 constexpr int kTileMaxRows = 28672;          // 112 KB of FP32 y per block
-constexpr int kTileMaxCols = 8192;           // columns per group (their offsets: 32 KB of shared memory)
 constexpr int64_t kTileMinEntries = 1 << 20;  // long-column entries below which the CSR launch is kept
 
-// shared memory of a tile: the chunk of y, then its group's kTileMaxCols + 1 offsets
-static size_t tileSmemBytes(int R) { return 4 * static_cast<size_t>(R) + 4 * static_cast<size_t>(kTileMaxCols + 1); }
+// shared memory of a tile: the chunk of y, then its group's offsets
+static size_t tileSmemBytes(int R, int maxcols) {
+    return 4 * static_cast<size_t>(R) + ((4 * static_cast<size_t>(maxcols + 1) + 15) & ~static_cast<size_t>(15));
+}
 
 __global__ void __launch_bounds__(kTileBlock, 1) primalLongTiles(IterArgs<float> p, LongTileArgs t, int koff) {
     bool last = false;
@@ -358,12 +360,14 @@ struct DeviceLp {
     int hot_bytes_sm = 0;                      // shared memory per SM given to the hot prefix
     // long columns in row chunks for the mixed-mode primal step (0 chunks: the
     // CSR launch runs instead); see buildLongTiles
-    int lt_R = 0, lt_C = 0, lt_G = 0;
+    int lt_R = 0, lt_C = 0, lt_G = 0, lt_maxcols = 0;
     int32_t *lt_off = nullptr, *lt_gb = nullptr;
     uint16_t* lt_row = nullptr;
     float* lt_val = nullptr;
     double* lt_part = nullptr;
-    LongTileArgs tiles() const { return LongTileArgs{lt_off, lt_gb, lt_row, lt_val, lt_part, lt_R, lt_C, lt_G, nlP}; }
+    LongTileArgs tiles() const {
+        return LongTileArgs{lt_off, lt_gb, lt_row, lt_val, lt_part, lt_R, lt_C, lt_G, nlP, lt_maxcols};
+    }
     int nb_rows_s = 1, nb_cols_s = 1, nb_pi_s = 1;  // partial blocks of the short-row launches
     std::vector<int32_t> rpos, cpos;  // original row / column -> device position (empty: identity)
     // Sides stored as sliced ELL (shapeP / shapeD >= kNumShapes): their short
@@ -669,7 +673,7 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
     if constexpr (sizeof(T) == 4) {
         if (d.lt_C > 0) {
             const LongTileArgs t = d.tiles();
-            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R), s>>>(ia, t, k);
+            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R, d.lt_maxcols), s>>>(ia, t, k);
             primalLongFinish<<<sellGrid(d.nlP), kBlock, 0, s>>>(ia, t, k);
             n += 2;
             if (d.n > d.nlP) {
@@ -920,15 +924,18 @@ static bool buildSell(const Csr& a, int32_t r0, SellHost& h) {
 // primal step (primalLongTiles): chunk c holds rows [c R, (c + 1) R), R a
 // multiple of 16 (so each chunk of y starts on a 16-byte boundary) and at most
 // max_rows; entries of column j in chunk c keep their CSR order; G column
-// groups per chunk (as many tiles as SMs, at least one group), cut at equal
-// shares of the entries.  False when a chunk offset would not fit 16 bits.
+// groups per chunk (as many tiles as SMs, so the tiles run in one wave of one
+// block per SM; at least one group), cut at equal weights (entries + 8 per
+// column).  False when a chunk offset would not fit 16 bits or a tile's shared
+// memory would exceed smem_max.
 struct LongTilesHost {
-    int R = 0, C = 0, G = 0;
+    int R = 0, C = 0, G = 0, maxcols = 0;
     std::vector<int32_t> off, gb;
     std::vector<uint16_t> row;
     std::vector<float> val;
 };
-static bool buildLongTiles(const Csr& at, int32_t nl, int32_t m, int sms, int max_rows, LongTilesHost& t) {
+static bool buildLongTiles(const Csr& at, int32_t nl, int32_t m, int sms, int max_rows, size_t smem_max,
+                           LongTilesHost& t) {
     if (nl <= 0 || m <= 0) return false;
     int C = (m + max_rows - 1) / max_rows;
     const int R = (((m + C - 1) / C) + 15) & ~15;
@@ -955,22 +962,20 @@ static bool buildLongTiles(const Csr& at, int32_t nl, int32_t m, int sms, int ma
             t.val[p] = static_cast<float>(at.val[k]);
         }
     // groups of equal weight (entries + 8 per column, the per-column work of a
-    // lane group in entries), at most kTileMaxCols columns each
+    // lane group in entries)
     const int64_t wtot = z + 8 * static_cast<int64_t>(nl);
     t.gb.assign(1, 0);
     int64_t w = 0;
-    int32_t start = 0;
     for (int32_t j = 0; j < nl; ++j) {
         w += (at.ptr[j + 1] - at.ptr[j]) + 8;
         const int64_t target = wtot * static_cast<int64_t>(t.gb.size()) / t.G;
-        if (j + 1 < nl && (w >= target || j + 1 - start >= kTileMaxCols)) {
-            t.gb.push_back(j + 1);
-            start = j + 1;
-        }
+        if (j + 1 < nl && static_cast<int>(t.gb.size()) < t.G && w >= target) t.gb.push_back(j + 1);
     }
     t.gb.push_back(nl);
     t.G = static_cast<int>(t.gb.size()) - 1;
-    return true;
+    t.maxcols = 0;
+    for (int g = 0; g < t.G; ++g) t.maxcols = std::max(t.maxcols, t.gb[g + 1] - t.gb[g]);
+    return tileSmemBytes(t.R, t.maxcols) <= smem_max;
 }
 
 // Sliced-ELL shape of a side from the options: a pinned sliced-ELL shape
@@ -1079,6 +1084,8 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     DeviceLp& d = *dp;
     d.device = dev;
     PDLPX_CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     PDLPX_CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
     // Device numbering: long rows first, sliced-ELL sides' short rows sorted by
     // length (identity where neither applies).  A side whose shape or lane
@@ -1112,10 +1119,12 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.zlP = zlP;
     LongTilesHost ltH;
     const bool want_tiles = o.long_tiles > 0 || (o.long_tiles < 0 && zlP >= kTileMinEntries);
-    if (d.mixed && want_tiles && buildLongTiles(sc.at, d.nlP, d.m, d.sms, kTileMaxRows, ltH)) {
+    if (d.mixed && want_tiles &&
+        buildLongTiles(sc.at, d.nlP, d.m, d.sms, kTileMaxRows, static_cast<size_t>(d.hot_smem_block), ltH)) {
         d.lt_R = ltH.R;
         d.lt_C = ltH.C;
         d.lt_G = ltH.G;
+        d.lt_maxcols = ltH.maxcols;
     }
     const int32_t msD = d.m - d.nlD, msP = d.n - d.nlP;  // short rows
     d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz - zlD, msD);
@@ -1129,8 +1138,6 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.shapeLP = longShape(zlP, d.nlP);
     // Hot prefixes (option): the dual step gathers x, whose long columns
     // [0, nlP) come first; the primal step gathers y, long rows [0, nlD).
-    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    PDLPX_CK(cudaDeviceGetAttribute(&d.hot_smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const bool hot = o.hot_cache > 0;
     d.hot_bytes_sm = hot ? 1024 * o.hot_cache : 0;
     d.hotD = (hot && sellD && d.nlP > 0) ? d.nlP : 0;
@@ -1346,7 +1353,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         PDLPX_CK(cudaStreamSynchronize(s));
         ltH = LongTilesHost{};
         PDLPX_CK(cudaFuncSetAttribute(primalLongTiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(tileSmemBytes(d.lt_R))));
+                                      static_cast<int>(tileSmemBytes(d.lt_R, d.lt_maxcols))));
     }
     {
         std::vector<ColPack<double>> cp;
