@@ -158,8 +158,14 @@ typedef struct pdlpx_options {
     int32_t long_tiles;               /* single-LP engine, mixed mode: run the primal step of the long
                                          columns (> max(64, 8 x mean) entries) in row chunks whose FP32
                                          y sits in shared memory: -1 (default) when those columns hold
-                                         >= 1M entries, 1 whenever there are long columns, 0 never */
-    int32_t reserved[1];
+                                         at least 2 x SMs x chunk rows entries (a chunk: up to 28,672
+                                         rows), 1 whenever there are long columns, 0 never */
+    int32_t batch_persistent;         /* pdlpx_batch_solve: run the N PDHG iterations of each restart
+                                         cycle as one cooperative launch over every sliced-ELL tile (a
+                                         grid barrier between the primal and the dual step) instead of
+                                         a graph of per-class launches: 1 on, 0 (default) off.  Packs
+                                         with CSR tiles or 16-entry rounds, and the request server's
+                                         packs, keep the graph.  Identical results either way */
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

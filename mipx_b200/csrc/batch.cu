@@ -190,10 +190,9 @@ __global__ void __launch_bounds__(kBlock, PDLPX_PACK_MIN_BLOCKS)
 }
 
 // ---- PDHG step over one sliced-ELL tile (sellDot / primalSellFrom / dualSellFrom in kernels.cuh) ----
-template <int U, bool IND>
-__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packPrimalSell(PackArgs a, int tile0, int base, int list0, int koff) {
-    const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
-    const int j = base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x);
+// Column j of column tile `tile` (the thread's row of the tile's slices).
+template <int U>
+__device__ __forceinline__ void primalSellTile(const PackArgs& a, int tile, int j, int koff) {
     const int2 h = a.cs.hdr[j / kSlice];
     const int4 info = a.ctinfo[tile];
     if (info.y == kModeIdle) return;
@@ -209,10 +208,8 @@ __global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packPrimalSell(
     }
 }
 
-template <int U, bool IND>
-__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packDualSell(PackArgs a, int tile0, int base, int list0, int koff) {
-    const int tile = IND ? a.rlist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
-    const int i = base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x);
+template <int U>
+__device__ __forceinline__ void dualSellTile(const PackArgs& a, int tile, int i, int koff) {
     const int2 h = a.rs.hdr[i / kSlice];
     const int4 info = a.rtinfo[tile];
     if (info.y == kModeIdle) return;
@@ -225,6 +222,84 @@ __global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packDualSell(Pa
         IterArgs<double> p = a.it64;
         p.st = st;
         dualSellFrom<U, double>(p, a.rs.idx, a.rs.v64, i, h, koff);
+    }
+}
+
+template <int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packPrimalSell(PackArgs a, int tile0, int base, int list0, int koff) {
+    const int tile = IND ? a.clist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    primalSellTile<U>(a, tile, base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x), koff);
+}
+
+template <int U, bool IND>
+__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packDualSell(PackArgs a, int tile0, int base, int list0, int koff) {
+    const int tile = IND ? a.rlist[list0 + blockIdx.x] : tile0 + static_cast<int>(blockIdx.x);
+    dualSellTile<U>(a, tile, base + (tile - tile0) * kBlock + static_cast<int>(threadIdx.x), koff);
+}
+
+// ---- persistent restart cycle (option batch_persistent) ---------------------
+// One cooperative launch runs the N PDHG iterations of a cycle over the pack's
+// sliced-ELL tiles: block b takes entries b, b + grid, ... of the primal tile
+// list, every block meets the others at a grid barrier, then the dual list and
+// a barrier again.  Each thread's work and order are those of packPrimalSell /
+// packDualSell (the same tile functions), so results are the same bits.  The
+// barrier waits on a generation word with a limit on its polls; a block that
+// runs out sets the error word, which the host reads after the cycle, and
+// every block leaves at its next barrier.
+struct PersistArgs {
+    const int4* ptiles;  // (tile, first column, entries-per-round variant, 0)
+    const int4* dtiles;  // (tile, first row, variant, 0)
+    int np, nd, N;
+    unsigned* bar;       // [0] arrivals, [1] generation
+    int* err;
+};
+constexpr long long kBarrierPolls = 1ll << 22;  // ~0.3-1 s of 64 ns sleeps
+
+__device__ __forceinline__ bool gridBarrier(unsigned* bar, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long polls = 0;
+            while (*gen == g) {
+                if (++polls > kBarrierPolls) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *reinterpret_cast<volatile int*>(err) == 0;
+}
+
+__global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packCycleSell(PackArgs a, PersistArgs q) {
+    const int t = static_cast<int>(threadIdx.x);
+    for (int k = 1; k <= q.N; ++k) {
+        for (int b = static_cast<int>(blockIdx.x); b < q.np; b += static_cast<int>(gridDim.x)) {
+            const int4 e = q.ptiles[b];
+            if (e.z == 0)
+                primalSellTile<kSellU[0]>(a, e.x, e.y + t, k);
+            else
+                primalSellTile<kSellU[1]>(a, e.x, e.y + t, k);
+        }
+        if (!gridBarrier(q.bar, q.err)) return;
+        for (int b = static_cast<int>(blockIdx.x); b < q.nd; b += static_cast<int>(gridDim.x)) {
+            const int4 e = q.dtiles[b];
+            if (e.z == 0)
+                dualSellTile<kSellU[0]>(a, e.x, e.y + t, k);
+            else
+                dualSellTile<kSellU[1]>(a, e.x, e.y + t, k);
+        }
+        if (!gridBarrier(q.bar, q.err)) return;
     }
 }
 
@@ -626,13 +701,21 @@ struct Pack {
     std::vector<Launch> lc, lr;        // launches of the current cycle graph
     bool listed = false;               // lc / lr run over the live-tile lists
     int live_ct = 0, live_rt = 0;      // tiles in the current launches
+    std::vector<int> h_cl, h_rl;       // host copies of the live-tile lists
     PackArgs args{};
+    // persistent cycle (option batch_persistent): tile lists, barrier words
+    // [arrivals, generation, error, -], cooperative grid
+    bool persist = false;
+    int persist_grid = 0;
+    char* pd = nullptr;
+    std::vector<int4> h_ptiles, h_dtiles;
 
     // Stream-ordered allocation: packs of a request server come and go while
     // other packs run, and a plain free would wait for the whole device.
     ~Pack() {
         if (cycle) cudaGraphExecDestroy(cycle);
         if (power) cudaGraphExecDestroy(power);
+        if (pd) cudaFreeAsync(pd, s);
         if (d) cudaFreeAsync(d, s);
         if (s) {
             cudaStreamSynchronize(s);
@@ -881,6 +964,54 @@ struct Pack {
         listed = true;
         live_ct = static_cast<int>(cl.size());
         live_rt = static_cast<int>(rl.size());
+        h_cl = cl;
+        h_rl = rl;
+    }
+
+    // Whether the current launches can run as one persistent cycle: every
+    // class sliced ELL with 4 or 8 entries per round.
+    bool persistable() const {
+        for (const auto* v : {&lc, &lr})
+            for (const Launch& c : *v)
+                if (!isSell(c.shape) || c.k() - kNumShapes > 1) return false;
+        return true;
+    }
+
+    // Tile lists of the persistent cycle for the current launches (the same
+    // tiles and first rows the per-class launches cover), uploaded on the
+    // pack's stream.
+    cudaError_t uploadPersistTiles() {
+        h_ptiles.clear();
+        h_dtiles.clear();
+        for (int side = 0; side < 2; ++side) {
+            std::vector<int4>& out = side == 0 ? h_ptiles : h_dtiles;
+            const std::vector<int>& list = side == 0 ? h_cl : h_rl;
+            for (const Launch& c : side == 0 ? lc : lr)
+                for (int b = 0; b < c.count; ++b) {
+                    const int tile = listed ? list[c.list0 + b] : c.tile0 + b;
+                    out.push_back(make_int4(tile, c.base + (tile - c.tile0) * kBlock, c.k() - kNumShapes, 0));
+                }
+        }
+        cudaError_t e = cudaSuccess;
+        if (!h_ptiles.empty())
+            e = cudaMemcpyAsync(pd + 16, h_ptiles.data(), sizeof(int4) * h_ptiles.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && !h_dtiles.empty())
+            e = cudaMemcpyAsync(pd + 16 + sizeof(int4) * static_cast<size_t>(nct), h_dtiles.data(),
+                                sizeof(int4) * h_dtiles.size(), cudaMemcpyHostToDevice, s);
+        return e;
+    }
+
+    // One persistent cycle of N iterations (barrier words cleared first).
+    cudaError_t launchPersistent(int N) {
+        PersistArgs q{reinterpret_cast<const int4*>(pd + 16),
+                      reinterpret_cast<const int4*>(pd + 16 + sizeof(int4) * static_cast<size_t>(nct)),
+                      static_cast<int>(h_ptiles.size()), static_cast<int>(h_dtiles.size()), N,
+                      reinterpret_cast<unsigned*>(pd), reinterpret_cast<int*>(pd + 8)};
+        cudaError_t e = cudaMemsetAsync(pd, 0, 16, s);
+        if (e != cudaSuccess) return e;
+        void* kargs[] = {&args, &q};
+        return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&packCycleSell), dim3(persist_grid),
+                                           dim3(kBlock), kargs, 0, s);
     }
 
     void launchPrimal(const Launch& c, int k) {
@@ -913,10 +1044,10 @@ struct Pack {
         }
     }
 
-    int launchCycle(int N) {
+    int launchCycle(int N, bool steps = true) {
         int n = 0;
         const PackArgs& a = args;
-        for (int k = 1; k <= N; ++k) {
+        for (int k = 1; k <= (steps ? N : 0); ++k) {
             for (const Launch& c : lc) {
                 launchPrimal(c, k);
                 ++n;
@@ -1356,7 +1487,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         }
         cudaGraph_t graph = nullptr;
         PDLPX_BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        count = power ? pk.launchPower(8) : pk.launchCycle(o.termination_eval_frequency);
+        count = power ? pk.launchPower(8) : pk.launchCycle(o.termination_eval_frequency, !pk.persist);
         PDLPX_BCK(cudaStreamEndCapture(s, &graph));
         const cudaError_t ie = cudaGraphInstantiate(&g, graph, 0);
         cudaGraphDestroy(graph);
@@ -1441,23 +1572,51 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
         }
     }
 
+    // ---- persistent cycle (option batch_persistent): the steps of a cycle as
+    // one cooperative launch ahead of the graph of its check, controller and
+    // restart launches
+    if (o.batch_persistent && pk.persistable()) {
+        int nb = 0, dev = 0, sms = 0, coop = 0;
+        PDLPX_BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, packCycleSell, kBlock, 0));
+        PDLPX_BCK(cudaGetDevice(&dev));
+        PDLPX_BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PDLPX_BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        if (nb > 0 && coop) {
+            pk.persist_grid = std::max(1, std::min(nb * sms, std::max(pk.nct, pk.nrt)));
+            PDLPX_BCK(cudaMallocAsync(reinterpret_cast<void**>(&pk.pd),
+                                      16 + sizeof(int4) * static_cast<size_t>(pk.nct + pk.nrt), s));
+            pk.persist = true;
+            PDLPX_BCK(pk.uploadPersistTiles());
+        }
+    }
+
     // ---- restart cycles; finished LPs are read back after the cycle that ends them
     {
         int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
         if (rc != PDLPX_OK) return rc;
     }
+    int perr = 0;
     SleepWait sleeper;
     std::vector<char> keep(L, 1), collected(L, 0);
     std::vector<int> cl, rl;
     int cycles = 0, ncollected = 0;
     while (ncollected < L) {
         if (timeUp(t0, o.max_solve_seconds) || stopped()) break;
+        if (pk.persist) {
+            PDLPX_BCK(pk.launchPersistent(o.termination_eval_frequency));
+            ++launches;
+        }
         PDLPX_BCK(cudaGraphLaunch(pk.cycle, s));
         launches += pk.cycle_launches;
         ++cycles;
         PDLPX_BCK(sleeper.wait(s));
         PDLPX_BCK(cudaMemcpyAsync(h_small, pk.args.flags, 4 * static_cast<size_t>(L), cudaMemcpyDeviceToHost, s));
+        if (pk.persist) PDLPX_BCK(cudaMemcpyAsync(&perr, pk.pd + 8, 4, cudaMemcpyDeviceToHost, s));
         PDLPX_BCK(cudaStreamSynchronize(s));
+        if (perr != 0) {
+            err = "persistent cycle: a grid barrier ran out of polls";
+            return PDLPX_E_TIMEOUT;
+        }
         int done_count = 0, fp64 = 0, live_tiles = 0;
         bool fresh = false;
         for (int l = 0; l < L; ++l) {
@@ -1491,6 +1650,7 @@ int32_t solvePack(Pack& pk, const pdlpx_options& o, std::chrono::steady_clock::t
                 PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_clist, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice, s));
             if (!rl.empty())
                 PDLPX_BCK(cudaMemcpyAsync(pk.d + pk.o_rlist, rl.data(), 4 * rl.size(), cudaMemcpyHostToDevice, s));
+            if (pk.persist) PDLPX_BCK(pk.uploadPersistTiles());
             int32_t rc = capture(pk.cycle, pk.cycle_launches, false);
             if (rc != PDLPX_OK) return rc;
         }
@@ -1664,7 +1824,10 @@ int32_t solvePrepared(const std::vector<PreparedLp*>& lps, const pdlpx_options& 
     if (items.empty()) return PDLPX_OK;
     int32_t rc = selectDevice(o, err);
     if (rc != PDLPX_OK) return rc;
-    return runPack(items, o, t0, stop, done, err);
+    // the server's packs share the device with each other: no cooperative cycle
+    pdlpx_options os = o;
+    os.batch_persistent = 0;
+    return runPack(items, os, t0, stop, done, err);
 }
 
 FamilyPtr makeFamilyBase(const pdlpx_lp& base) {

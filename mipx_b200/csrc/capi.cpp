@@ -106,6 +106,7 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->reference_fixed_columns = 0;
     o->hot_cache = 0;
     o->long_tiles = -1;
+    o->batch_persistent = 0;
 }
 
 const char* pdlpx_error_string(int32_t code) {

@@ -233,7 +233,6 @@ struct LongTileArgs {
 constexpr int kTileBlock = 1024;
 constexpr int kTileLanes = 4;
 constexpr int kTileMaxRows = 28672;          // 112 KB of FP32 y per block
-constexpr int64_t kTileMinEntries = 1 << 20;  // long-column entries below which the CSR launch is kept
 
 // shared memory of a tile: the chunk of y, then its group's offsets
 static size_t tileSmemBytes(int R, int maxcols) {
@@ -1118,7 +1117,14 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.zlD = zlD;
     d.zlP = zlP;
     LongTilesHost ltH;
-    const bool want_tiles = o.long_tiles > 0 || (o.long_tiles < 0 && zlP >= kTileMinEntries);
+    // automatic: when the long columns hold at least twice as many entries per
+    // SM as a chunk has rows (each tile's copy of y then serves >= 2 gathers
+    // per row it copies).  Measured on B200: the 500k x 2M power-law LP's
+    // primal step 125.0 -> 117.5 us (58k entries per tile, 27.8k rows per
+    // chunk); the 100k x 400k one 45.9 -> 66.0 us (11k entries per tile).
+    const int64_t chunk_rows = std::min<int64_t>(d.m, kTileMaxRows);
+    const bool want_tiles =
+        o.long_tiles > 0 || (o.long_tiles < 0 && zlP >= 2 * static_cast<int64_t>(d.sms) * chunk_rows);
     if (d.mixed && want_tiles &&
         buildLongTiles(sc.at, d.nlP, d.m, d.sms, kTileMaxRows, static_cast<size_t>(d.hot_smem_block), ltH)) {
         d.lt_R = ltH.R;

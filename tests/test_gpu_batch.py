@@ -227,3 +227,22 @@ def test_server_over_device_list():
             tickets = [srv.submit(lp) for lp in lps]
             out[str(devs)] = [srv.wait(t) for t in tickets]
     _same(out["None"], out["[0, 0]"])
+
+
+def test_persistent_cycle_gives_identical_results():
+    """batch_persistent runs the N steps of each restart cycle as one cooperative
+    launch over every sliced-ELL tile (grid barriers between the steps) with the
+    same per-thread work as the per-class launches: every LP's result, with and
+    without the compaction of finished LPs, is bit-identical to the graph's."""
+    lps = [G.random_lp(m, int(2.5 * m), 4, 12, 3100 + k)[0] for k, m in enumerate((300, 1800, 700, 2600, 450, 1200))]
+    for compact in (True, False):
+        o = dict(verbose=False, batch_compact=compact, **TIGHT)
+        graph = batch_solve(lps, PdlpOptions(**o))
+        pers = batch_solve(lps, PdlpOptions(batch_persistent=True, **o))
+        for (r, x, y), (q, u, v) in zip(graph, pers):
+            assert r.status == q.status == Status.Optimal
+            assert r.iterations == q.iterations and r.objective == q.objective
+            np.testing.assert_array_equal(x, u)
+            np.testing.assert_array_equal(y, v)
+        # the persistent launch replaces the per-class step launches of every cycle
+        assert pers[0][0].kernel_launches < graph[0][0].kernel_launches

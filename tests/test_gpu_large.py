@@ -123,3 +123,44 @@ def test_long_column_tiles_match_csr_launch():
         full.append(s.solve())
     assert full[0].status == full[1].status == Status.Optimal
     assert GC.rel_err(full[1].objective, full[0].objective) <= GC.OBJ_TOL
+
+
+def _duality_certificate(lp, x, y):
+    """Independent FP64 optimality certificate of (x, y) for a minimisation LP
+    with boxed columns.  The returned duals price A x the other way round (a
+    '<=' row's dual is >= 0), so u = -y; u projected onto the sign its rows
+    allow is dual feasible, and b-support(u) + bound-support(c - A^T u) is a
+    lower bound on the optimum (weak duality).  Returns (relative primal
+    residual, |c x - that bound| / max(1, |c x|))."""
+    a = lp.matrix
+    rows = np.repeat(np.arange(lp.num_rows), np.diff(a.row_starts))
+    u = -np.asarray(y, dtype=np.float64)
+    yp = np.where(np.isfinite(lp.row_lower), u, np.minimum(u, 0.0))
+    yp = np.where(np.isfinite(lp.row_upper), yp, np.maximum(yp, 0.0))
+    aty = np.bincount(a.col_indices, weights=a.values * yp[rows], minlength=lp.num_cols)
+    rc = lp.obj - aty
+    assert np.all(np.isfinite(lp.col_lower)) and np.all(np.isfinite(lp.col_upper))
+    row_part = np.where(yp > 0, lp.row_lower, lp.row_upper) * yp
+    row_part = np.where(yp == 0, 0.0, row_part)
+    dual_bound = row_part.sum() + np.where(rc > 0, lp.col_lower, lp.col_upper) @ rc + lp.obj_offset
+    primal = lp.obj @ x + lp.obj_offset
+    return _feasibility(lp, x), abs(primal - dual_bound) / max(1.0, abs(primal))
+
+
+def test_powerlaw_full_size_certificate():
+    """The 500,000 x 2,000,000 power-law LP (20.1M nonzeros), mixed precision,
+    to 1e-6 relative KKT: no FP64 oracle finishes it here, so the returned
+    (x, y) is checked by an independent numpy certificate -- primal residual
+    <= 1e-6 and the objective within 2e-6 relative of a weak-duality lower
+    bound, hence of the optimum."""
+    lp, _ = G.powerlaw_lp(500000, 2000000, 2, 2000, 10.0, 0.01, 1e3, 11)
+    s = PdlpSolver()
+    s.setOptions(PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL,
+                             max_solve_seconds=120))
+    s.load(lp)
+    r = s.solve()
+    assert r.status == Status.Optimal, r
+    x, y = s.getPrimalValues(), s.getDualValues()
+    assert np.all(x >= lp.col_lower - 1e-9) and np.all(x <= lp.col_upper + 1e-9)
+    rp, gap = _duality_certificate(lp, x, y)
+    assert rp <= 1e-6 and gap <= 2e-6, (rp, gap, r.objective)
