@@ -38,7 +38,7 @@ sys.path.insert(0, str(ROOT / "tests"))
 BATCH_SAMPLE = 16
 NODES = 8
 POWERLAW_ROWS = 100_000
-WORKERS = 6
+WORKERS = 5
 
 
 def _highs(lp, time_limit: float = 900.0):
