@@ -14,12 +14,14 @@ per-iteration working set (~420 MB) is far larger than the 126 MB L2.
 * ``e2e``: the same metric through the public API with host buffers -- load
   (host scaling with device Ruiz passes, H2D copies inside the solve), solve,
   copy x and y back -- per step.
-* ``roofline``: the dominant kernel -- the fused primal step (A^T y_cur + the
-  Halpern primal step; long columns CSR, short columns sliced ELL) -- timed live
-  inside the timed solves: the restart-cycle graph records CUDA events around
-  one primal and one dual step of every cycle.  Algorithmic bytes per launch
-  are in ``step_kernels.bytes`` (``step_bytes``); ``traffic`` is ncu's
-  dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/).
+* ``roofline``: the dominant kernel -- the fused primal step (A^T y + the
+  Halpern primal step; long columns in row chunks with y in shared memory,
+  short columns sliced ELL) -- timed live inside the timed solves: the
+  restart-cycle graph records CUDA events around one primal and one dual step
+  of every cycle (a step's time covers all of its launches).  Algorithmic
+  bytes per step are in ``step_kernels.bytes`` (``step_bytes``); ``traffic``
+  is ncu's dram__bytes_read.sum + dram__bytes_write.sum of the step's launches
+  (profiles/).
 * ``cpu_baseline`` and ``--impl reference``: the reference's own CPU
   PdlpSolver (compiled from its sources into oracle/_ref) on one host core --
   the reference PDLP is single-threaded per LP -- timed as the marginal rate
@@ -416,7 +418,8 @@ def large_headline(args, rank, world, local, pg, flush) -> dict:
         except Exception as exc:  # the baseline is a report, never a reason to lose the line
             cpu = {"value": None, "error": str(exc)}
     return {"m": m, "n": n, "nnz": nnz, "res": res, "value": value, "t_dev": t_dev, "lps": lps, "wall": wall,
-            "clk": clk.summary(), "peak": peak, "peak_kind": peak_kind, "kern": kern, "cfg": solver.launchConfig(),
+            "clk": clk.summary(), "peak": peak, "peak_kind": peak_kind, "kern": kern,
+            "cfg": dict(solver.launchConfig(), long_tiles=solver.longTiles()),
             "e2e": e2e_val, "e2e_steps": max(1, args.e2e_steps), "cpu": cpu, "load_s": load_s,
             "h2d": int(sum(a.nbytes for a in lp.arrays())), "d2h": 8 * (n + m)}
 
@@ -740,8 +743,9 @@ def main():
                     "d2h_bytes_per_step": H["d2h"], "steps": H["e2e_steps"]},
             "gpu_launches": int(sum(res["launches"])),
             "roofline": {"bound": "hbm",
-                         "kernel": f"primal step, {tag.upper()} kernels (A^T y_cur + Halpern step; long columns CSR, "
-                                   "short columns sliced ELL)",
+                         "kernel": f"primal step, {tag.upper()} kernels (A^T y + Halpern step; long columns "
+                                   + ("in row chunks with y in shared memory" if H["cfg"]["long_tiles"]["chunks"] else "CSR")
+                                   + ", short columns sliced ELL)",
                          "achieved": k["primal_GBps"], "peak": H["peak"], "peak_kind": H["peak_kind"], "unit": "GB/s",
                          "frac": k["primal_frac"], "traffic": traffic, "algorithmic_bytes": b[f"primal_{tag}"],
                          "timing": "live: CUDA events around one primal and one dual step of every restart cycle of "

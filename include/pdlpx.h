@@ -158,8 +158,8 @@ typedef struct pdlpx_options {
     int32_t long_tiles;               /* single-LP engine, mixed mode: run the primal step of the long
                                          columns (> max(64, 8 x mean) entries) in row chunks whose FP32
                                          y sits in shared memory: -1 (default) when those columns hold
-                                         at least 2 x SMs x chunk rows entries (a chunk: up to 28,672
-                                         rows), 1 whenever there are long columns, 0 never */
+                                         at least 1.5 x SMs x chunk rows entries (a chunk: up to
+                                         28,672 rows), 1 whenever there are long columns, 0 never */
     int32_t batch_persistent;         /* pdlpx_batch_solve: run the N PDHG iterations of each restart
                                          cycle as one cooperative launch over every sliced-ELL tile (a
                                          grid barrier between the primal and the dual step) instead of
@@ -294,6 +294,9 @@ int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t
  * given precision (PDLPX_PREC_MIXED: the FP32 kernels; PDLPX_PREC_FP64);
  * 0 where that step runs without one. */
 int32_t pdlpx_get_hot_prefix(const pdlpx_solver* h, int32_t precision, int32_t* primal, int32_t* dual);
+/* Row chunks and column groups of the tiled long-column primal step (option
+ * long_tiles) of the loaded LP; 0 chunks where the CSR launch runs. */
+int32_t pdlpx_get_long_tiles(const pdlpx_solver* h, int32_t* chunks, int32_t* groups);
 
 /* ---- batched solve: many independent LPs in one persistent launch ---- */
 typedef struct pdlpx_lp {

@@ -355,6 +355,11 @@ int32_t pdlpx_get_launch_config(const pdlpx_solver* h, int32_t* group_a, int32_t
     return h->engine.launchConfig(group_a, group_at, blocks_primal, blocks_dual);
 }
 
+int32_t pdlpx_get_long_tiles(const pdlpx_solver* h, int32_t* chunks, int32_t* groups) {
+    if (h == nullptr) return PDLPX_E_INVALID;
+    return h->engine.longTiles(chunks, groups);
+}
+
 int32_t pdlpx_get_hot_prefix(const pdlpx_solver* h, int32_t precision, int32_t* primal, int32_t* dual) {
     if (h == nullptr) return PDLPX_E_INVALID;
     return h->engine.hotPrefix(precision, primal, dual);

@@ -1117,14 +1117,16 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     d.zlD = zlD;
     d.zlP = zlP;
     LongTilesHost ltH;
-    // automatic: when the long columns hold at least twice as many entries per
-    // SM as a chunk has rows (each tile's copy of y then serves >= 2 gathers
-    // per row it copies).  Measured on B200: the 500k x 2M power-law LP's
-    // primal step 125.0 -> 117.5 us (58k entries per tile, 27.8k rows per
-    // chunk); the 100k x 400k one 45.9 -> 66.0 us (11k entries per tile).
-    const int64_t chunk_rows = std::min<int64_t>(d.m, kTileMaxRows);
+    // automatic: when the long columns hold at least 1.5 times as many entries
+    // per SM as a chunk has rows (each tile's copy of y then serves >= 1.5
+    // gathers per row it copies).  Measured on B200: the 500k x 2M power-law
+    // LP's primal step 125.0 -> 117.5 us (58k entries per tile, 27.8k rows per
+    // chunk: 2.1); the 100k x 400k one 45.9 -> 66.0 us (11k entries per tile,
+    // 25k rows: 0.44).
+    const int64_t chunks = d.m > 0 ? (d.m + kTileMaxRows - 1) / kTileMaxRows : 1;
+    const int64_t chunk_rows = (((d.m + chunks - 1) / chunks) + 15) & ~int64_t(15);
     const bool want_tiles =
-        o.long_tiles > 0 || (o.long_tiles < 0 && zlP >= 2 * static_cast<int64_t>(d.sms) * chunk_rows);
+        o.long_tiles > 0 || (o.long_tiles < 0 && 2 * zlP >= 3 * static_cast<int64_t>(d.sms) * chunk_rows);
     if (d.mixed && want_tiles &&
         buildLongTiles(sc.at, d.nlP, d.m, d.sms, kTileMaxRows, static_cast<size_t>(d.hot_smem_block), ltH)) {
         d.lt_R = ltH.R;
@@ -2169,6 +2171,13 @@ int32_t Engine::timeKernels(int32_t precision, int32_t reps, int64_t flush_bytes
     if (ms_primal) *ms_primal = ms[0];
     if (ms_dual) *ms_dual = ms[1];
     if (ms_check) *ms_check = ms[2];
+    return PDLPX_OK;
+}
+
+int32_t Engine::longTiles(int32_t* chunks, int32_t* groups) const {
+    if (!dev_) return PDLPX_E_NOT_LOADED;
+    if (chunks) *chunks = dev_->lt_C;
+    if (groups) *groups = dev_->lt_G;
     return PDLPX_OK;
 }
 

@@ -74,6 +74,7 @@ public:
     }
     int32_t launchConfig(int32_t* ga, int32_t* gat, int32_t* bp, int32_t* bd) const;
     int32_t hotPrefix(int32_t precision, int32_t* primal, int32_t* dual) const;
+    int32_t longTiles(int32_t* chunks, int32_t* groups) const;
 
     std::string last_error;
 

@@ -444,6 +444,13 @@ class PdlpSolver:
         _capi.check(self._lib.pdlpx_get_hot_prefix(self._h, int(precision), C.byref(p), C.byref(d)), self._h)
         return {"primal": p.value, "dual": d.value}
 
+    def longTiles(self) -> dict:
+        """Row chunks and column groups of the tiled long-column primal step
+        (option long_tiles); 0 chunks where the CSR launch runs."""
+        c, g = C.c_int32(), C.c_int32()
+        _capi.check(self._lib.pdlpx_get_long_tiles(self._h, C.byref(c), C.byref(g)), self._h)
+        return {"chunks": c.value, "groups": g.value}
+
     def scaling(self) -> dict:
         """Scaled-problem arrays of the last load (parity of pdlp.cpp:469-669)."""
         m, n = self._dims()
