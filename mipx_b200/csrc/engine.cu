@@ -1072,6 +1072,7 @@ static bool wantMixed(const pdlpx_options& o, int64_t m, int64_t n, int64_t nnz)
 // Build (or rebuild) the device image of the scaled LP.
 static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in, const pdlpx_options& o,
                            std::string& err) {
+    const auto tb0 = std::chrono::steady_clock::now();
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
         err = "no CUDA device visible";
@@ -1224,6 +1225,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     }
     const size_t o_st = take(sizeof(DevState)), o_dc = take(sizeof(DevConst)), o_ps = take(sizeof(PowerState));
     d.arena_bytes = off;
+    const auto tb1 = std::chrono::steady_clock::now();
     PDLPX_CK(cudaMalloc(reinterpret_cast<void**>(&d.arena), d.arena_bytes));
     PDLPX_CK(cudaMallocHost(reinterpret_cast<void**>(&d.h_st), sizeof(DevState)));
     PDLPX_CK(cudaMallocHost(reinterpret_cast<void**>(&d.h_ps), sizeof(PowerState)));
@@ -1381,6 +1383,13 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         PDLPX_CK(up(d.sig64, sc.sigma.data(), 8 * m));
         PDLPX_CK(cudaStreamSynchronize(s));
     }
+    if (o.verbose) {
+        const auto tb2 = std::chrono::steady_clock::now();
+        std::printf("PDLP device image: host build %.3fs, allocation + upload %.3fs (%.1f MB)  [B200]\n",
+                    std::chrono::duration<double>(tb1 - tb0).count(), std::chrono::duration<double>(tb2 - tb1).count(),
+                    1e-6 * static_cast<double>(d.arena_bytes));
+        std::fflush(stdout);
+    }
     return PDLPX_OK;
 }
 
@@ -1512,6 +1521,7 @@ int32_t Engine::load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const
         last_error = "null bound / objective array";
         return PDLPX_E_INVALID;
     }
+    const auto tl0 = std::chrono::steady_clock::now();
     HostLp lp;
     lp.m = m;
     lp.n = n;
@@ -1536,7 +1546,14 @@ int32_t Engine::load(int32_t m, int32_t n, int32_t nnz, const int32_t* rp, const
     warm_y_.clear();
     x_orig_.assign(static_cast<size_t>(n), 0.0);
     y_orig_.assign(static_cast<size_t>(m), 0.0);
+    const auto tl1 = std::chrono::steady_clock::now();
     rescale();
+    if (opt_.verbose) {
+        const auto tl2 = std::chrono::steady_clock::now();
+        std::printf("PDLP load: CSR check and copy %.3fs, scaling %.3fs  [B200]\n",
+                    std::chrono::duration<double>(tl1 - tl0).count(), std::chrono::duration<double>(tl2 - tl1).count());
+        std::fflush(stdout);
+    }
     return PDLPX_OK;
 }
 
