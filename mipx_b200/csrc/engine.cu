@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <limits>
 #include <random>
 
@@ -839,6 +840,23 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
 // the other side's gathers had survives the renumbering.
 constexpr int32_t kSellWindow = 4096;
 
+// f(begin, end) over contiguous blocks of [0, count) on up to 16 host threads
+// (one below 1M entries of `work`); the blocks write disjoint output.
+template <class F>
+static void hostBlocks(size_t work, int64_t count, F&& f) {
+    const int nt = work < (size_t(1) << 20)
+                       ? 1
+                       : static_cast<int>(std::min<int64_t>(
+                             count, std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
+    if (nt <= 1) {
+        f(int64_t{0}, count);
+        return;
+    }
+    std::vector<std::thread> ts;
+    for (int t = 0; t < nt; ++t) ts.emplace_back([&, t] { f(count * t / nt, count * (t + 1) / nt); });
+    for (auto& th : ts) th.join();
+}
+
 // Device numbering of one matrix side's rows.  Rows far longer than the rest
 // (more entries than max(64, 8 x the mean)) come first, longest first; the
 // other rows follow -- sorted by length (longest first, stable) inside windows
@@ -869,10 +887,13 @@ static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int
     if (!sht.empty())
         sell = sell_opt > 0 || (sell_opt < 0 && static_cast<double>(zs) <= 64.0 * static_cast<double>(sht.size()));
     if (sell) {
-        for (size_t w0 = 0; w0 < sht.size(); w0 += kSellWindow) {
-            const size_t w1 = std::min(sht.size(), w0 + kSellWindow);
-            std::stable_sort(sht.begin() + w0, sht.begin() + w1, [&](int32_t x, int32_t y) { return len(x) > len(y); });
-        }
+        const int64_t windows = (static_cast<int64_t>(sht.size()) + kSellWindow - 1) / kSellWindow;
+        hostBlocks(sht.size() * 16, windows, [&](int64_t w0, int64_t w1) {
+            for (int64_t w = w0; w < w1; ++w) {
+                const size_t b = static_cast<size_t>(w) * kSellWindow, e = std::min(sht.size(), b + kSellWindow);
+                std::stable_sort(sht.begin() + b, sht.begin() + e, [&](int32_t x, int32_t y) { return len(x) > len(y); });
+            }
+        });
     }
     std::stable_sort(lng.begin(), lng.end(), [&](int32_t x, int32_t y) { return len(x) > len(y); });
     bool identity = true;
@@ -907,15 +928,18 @@ static bool buildSell(const Csr& a, int32_t r0, SellHost& h) {
     }
     h.idx.assign(static_cast<size_t>(e), 0);
     h.val.assign(static_cast<size_t>(e), 0.0);
-    for (int64_t r = 0; r < rows; ++r) {
-        const int64_t first = h.hdr[static_cast<size_t>(r / kSlice)].x + (r % kSlice);
-        const int32_t b = a.ptr[r0 + r], cnt = a.ptr[r0 + r + 1] - b;
-        for (int32_t k = 0; k < cnt; ++k) {
-            const size_t at = static_cast<size_t>(first + static_cast<int64_t>(k) * kSlice);
-            h.idx[at] = a.idx[b + k];
-            h.val[at] = a.val[b + k];
+    // slices own disjoint entry ranges: fill them in parallel blocks of slices
+    hostBlocks(static_cast<size_t>(e), slices, [&](int64_t s0, int64_t s1) {
+        for (int64_t r = s0 * kSlice; r < std::min<int64_t>(rows, s1 * kSlice); ++r) {
+            const int64_t first = h.hdr[static_cast<size_t>(r / kSlice)].x + (r % kSlice);
+            const int32_t b = a.ptr[r0 + r], cnt = a.ptr[r0 + r + 1] - b;
+            for (int32_t k = 0; k < cnt; ++k) {
+                const size_t at = static_cast<size_t>(first + static_cast<int64_t>(k) * kSlice);
+                h.idx[at] = a.idx[b + k];
+                h.val[at] = a.val[b + k];
+            }
         }
-    }
+    });
     return true;
 }
 
@@ -1004,27 +1028,31 @@ static void permuteScaled(const ScaledLp& sc, const std::vector<int32_t>& ro, co
     out.obj_scale = sc.obj_scale;
     out.con_scale = sc.con_scale;
     out.precond_pw = sc.precond_pw;
-    auto permuteCsr = [](const Csr& a, int32_t rows, int32_t cols, const std::function<int32_t(int32_t)>& old,
+    // new row r is old row ord[r] with its indices renumbered; rows are copied
+    // in parallel blocks once the pointers are known
+    auto permuteCsr = [](const Csr& a, int32_t rows, int32_t cols, const std::vector<int32_t>& ord,
                          const std::vector<int32_t>& idxPos, Csr& b) {
+        auto old = [&](int32_t r) { return ord.empty() ? r : ord[r]; };
         b.rows = rows;
         b.cols = cols;
-        b.ptr.assign(1, 0);
-        b.ptr.reserve(rows + 1);
-        b.idx.clear();
-        b.val.clear();
-        b.idx.reserve(a.idx.size());
-        b.val.reserve(a.val.size());
-        for (int32_t r = 0; r < rows; ++r) {
-            const int32_t o = old(r);
-            for (int32_t k = a.ptr[o]; k < a.ptr[o + 1]; ++k) {
-                b.idx.push_back(idxPos[a.idx[k]]);
-                b.val.push_back(a.val[k]);
+        b.ptr.resize(static_cast<size_t>(rows) + 1);
+        b.ptr[0] = 0;
+        for (int32_t r = 0; r < rows; ++r) b.ptr[r + 1] = b.ptr[r] + (a.ptr[old(r) + 1] - a.ptr[old(r)]);
+        b.idx.resize(a.idx.size());
+        b.val.resize(a.val.size());
+        hostBlocks(a.idx.size(), rows, [&](int64_t r0, int64_t r1) {
+            for (int64_t r = r0; r < r1; ++r) {
+                const int32_t o = old(static_cast<int32_t>(r));
+                int32_t p = b.ptr[r];
+                for (int32_t k = a.ptr[o]; k < a.ptr[o + 1]; ++k, ++p) {
+                    b.idx[p] = idxPos[a.idx[k]];
+                    b.val[p] = a.val[k];
+                }
             }
-            b.ptr.push_back(static_cast<int32_t>(b.idx.size()));
-        }
+        });
     };
-    permuteCsr(sc.a, m, n, oldRow, cpos, out.a);
-    permuteCsr(sc.at, n, m, oldCol, rpos, out.at);
+    permuteCsr(sc.a, m, n, ro, cpos, out.a);
+    permuteCsr(sc.at, n, m, co, rpos, out.at);
     auto cols = [&](const std::vector<double>& v, std::vector<double>& w) {
         w.resize(n);
         for (int32_t j = 0; j < n; ++j) w[j] = v[oldCol(j)];
@@ -1106,9 +1134,11 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     const ScaledLp& sc = perm ? permuted : sc_in;
     if (ro.empty()) d.rpos.clear();
     if (co.empty()) d.cpos.clear();
+    const auto tbp = std::chrono::steady_clock::now();
     SellHost hsP, hsD;
     if (sellP && !buildSell(sc.at, d.nlP, hsP)) sellP = false;
     if (sellD && !buildSell(sc.a, d.nlD, hsD)) sellD = false;
+    const auto tbs = std::chrono::steady_clock::now();
     d.m = sc.a.rows;
     d.n = sc.a.cols;
     d.nnz = sc.a.nnz();
@@ -1135,6 +1165,7 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         d.lt_G = ltH.G;
         d.lt_maxcols = ltH.maxcols;
     }
+    const auto tbt = std::chrono::steady_clock::now();
     const int32_t msD = d.m - d.nlD, msP = d.n - d.nlP;  // short rows
     d.gA = o.spmv_group_a > 0 ? o.spmv_group_a : pickGroup(nnz - zlD, msD);
     d.gAT = o.spmv_group_at > 0 ? o.spmv_group_at : pickGroup(nnz - zlP, msP);
@@ -1385,8 +1416,12 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     }
     if (o.verbose) {
         const auto tb2 = std::chrono::steady_clock::now();
-        std::printf("PDLP device image: host build %.3fs, allocation + upload %.3fs (%.1f MB)  [B200]\n",
-                    std::chrono::duration<double>(tb1 - tb0).count(), std::chrono::duration<double>(tb2 - tb1).count(),
+        auto sec = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double>(b - a).count();
+        };
+        std::printf("PDLP device image: host build %.3fs (order + permute %.3fs, sliced ELL %.3fs, long tiles %.3fs), "
+                    "allocation + upload %.3fs (%.1f MB)  [B200]\n",
+                    sec(tb0, tb1), sec(tb0, tbp), sec(tbp, tbs), sec(tbs, tbt), sec(tb1, tb2),
                     1e-6 * static_cast<double>(d.arena_bytes));
         std::fflush(stdout);
     }

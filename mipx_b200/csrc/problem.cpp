@@ -1,7 +1,9 @@
 #include "problem.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <numeric>
 #include <thread>
 
@@ -163,6 +165,8 @@ void pockChambolle(const ScaledLp& s, std::vector<double>& sigma, std::vector<do
 
 void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const RuizFn& ruiz) {
     const int32_t m = lp.m, n = lp.n;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     s.obj_sign = lp.maximize ? -1.0 : 1.0;
     s.c.resize(static_cast<size_t>(n));
     for (int32_t j = 0; j < n; ++j) s.c[j] = s.obj_sign * lp.obj[j];
@@ -194,6 +198,7 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
         a.val = lp.a.val;
     }
 
+    const auto t1 = clk::now();
     // Ruiz: alternate row and column infinity-norm equilibration, scale 1/sqrt(max).
     if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0 && !(ruiz && ruiz(a, s.row_scale, s.col_scale, o.ruiz_iterations))) {
         std::vector<double> cmax(static_cast<size_t>(n));
@@ -228,7 +233,9 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
         if (fin(s.rl[i])) s.rl[i] *= s.row_scale[i];
         if (fin(s.ru[i])) s.ru[i] *= s.row_scale[i];
     }
+    const auto t2 = clk::now();
     transposeCsr(a, s.at);
+    const auto t3 = clk::now();
 
     if (o.do_pock_chambolle_scaling && m > 0 && n > 0) {
         pockChambolle(s, s.sigma, s.tau);
@@ -236,6 +243,7 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
         s.sigma.assign(static_cast<size_t>(m), 1.0);
         s.tau.assign(static_cast<size_t>(n), 1.0);
     }
+    const auto t4 = clk::now();
 
     s.obj_scale = 1.0;
     s.con_scale = 1.0;
@@ -273,6 +281,12 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
             s.row_type[i] = kRowRanged;
     }
     s.precond_pw = o.primal_weight;
+    if (o.verbose) {
+        auto sec = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+        std::printf("PDLP scaling: copy %.3fs, Ruiz %.3fs, transpose %.3fs, Pock-Chambolle %.3fs, rest %.3fs\n",
+                    sec(t0, t1), sec(t1, t2), sec(t2, t3), sec(t3, t4), sec(t4, clk::now()));
+        std::fflush(stdout);
+    }
 }
 
 void terminationNorms(const HostLp& lp, int32_t norm, double& c_norm, double& b_norm) {

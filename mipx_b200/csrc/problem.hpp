@@ -67,8 +67,9 @@ using RuizFn = std::function<bool(Csr& a, std::vector<double>& row_scale, std::v
 void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const RuizFn& ruiz = {});
 
 // Ruiz passes on `device` (scaling.cu); bit-identical to the host loop.
+// verbose prints the time of its phases.
 bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& col_scale, int passes, int device,
-                  std::string& err);
+                  std::string& err, bool verbose = false);
 
 // The Ruiz hook the options ask for: the device for scale_on_device = 1, or for
 // -1 (auto) from 200k nonzeros; none (host loop) otherwise.  When the device

@@ -13,7 +13,9 @@
 // Pock-Chambolle, bound/objective rescaling, the transpose) stays on the host.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -66,7 +68,9 @@ __global__ void __launch_bounds__(kThreads) ruizCols(int n, int64_t nnz, const i
 }  // namespace
 
 bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& col_scale, int passes, int device,
-                  std::string& err) {
+                  std::string& err, bool verbose) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     const int m = a.rows, n = a.cols;
     const int64_t nnz = a.nnz();
     if (m <= 0 || n <= 0 || nnz <= 0 || passes <= 0) return true;
@@ -111,6 +115,7 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
         (e = cudaMemcpyAsync(rs, row_scale.data(), 8 * static_cast<size_t>(m), h2d, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(cs, col_scale.data(), 8 * static_cast<size_t>(n), h2d, s)) != cudaSuccess)
         return fail(e, "upload");
+    const auto t1 = clk::now();
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const int grow = static_cast<int>((static_cast<int64_t>(m) + kThreads / 32 - 1) / (kThreads / 32));
@@ -122,6 +127,8 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
         ruizCols<<<gent, kThreads, 0, s>>>(n, nnz, idx, val, cm, cs);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "launch");
+    if (verbose && (e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e, "synchronize");
+    const auto t2 = clk::now();
     // read back into new arrays: the caller's stay untouched unless everything succeeded
     std::vector<double> v2(static_cast<size_t>(nnz)), r2(static_cast<size_t>(m)), c2(static_cast<size_t>(n));
     if ((e = cudaMemcpyAsync(v2.data(), val, 8 * static_cast<size_t>(nnz), d2h, s)) != cudaSuccess ||
@@ -136,15 +143,22 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
     a.val.swap(v2);
     row_scale.swap(r2);
     col_scale.swap(c2);
+    if (verbose) {
+        auto sec = [](clk::time_point x, clk::time_point y) { return std::chrono::duration<double>(y - x).count(); };
+        std::printf("PDLP device Ruiz: set-up + upload %.3fs, %d passes %.3fs, read back %.3fs\n", sec(t0, t1), passes,
+                    sec(t1, t2), sec(t2, clk::now()));
+        std::fflush(stdout);
+    }
     return true;
 }
 
 RuizFn ruizFor(const pdlpx_options& o, int64_t nnz, std::string* fallback_note) {
     if (!(o.scale_on_device > 0 || (o.scale_on_device < 0 && nnz >= 200000))) return {};
     const int device = o.device;
-    return [device, fallback_note](Csr& a, std::vector<double>& rs, std::vector<double>& cs, int passes) {
+    const bool verbose = o.verbose != 0;
+    return [device, verbose, fallback_note](Csr& a, std::vector<double>& rs, std::vector<double>& cs, int passes) {
         std::string err;
-        const bool ok = ruizOnDevice(a, rs, cs, passes, device, err);
+        const bool ok = ruizOnDevice(a, rs, cs, passes, device, err, verbose);
         if (!ok && fallback_note != nullptr) *fallback_note = "device Ruiz scaling fell back to the host: " + err;
         return ok;
     };
