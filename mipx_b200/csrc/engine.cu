@@ -283,8 +283,8 @@ __global__ void __launch_bounds__(kTileBlock, 1) primalLongTiles(IterArgs<float>
     }
 }
 
-__global__ void __launch_bounds__(kBlock) primalLongFinish(IterArgs<float> p, LongTileArgs t, int koff) {
-    const int j = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+// Long column j: the sum of its chunk partials in chunk order, then its primal step.
+__device__ __forceinline__ void longFinishColumn(const IterArgs<float>& p, const LongTileArgs& t, int j, int koff) {
     if (j >= t.nl) return;
     const ColPack<float> q = p.cp[j];
     const double xc = p.xc[j];
@@ -298,6 +298,28 @@ __global__ void __launch_bounds__(kBlock) primalLongFinish(IterArgs<float> p, Lo
     const int k = p.st->inner + koff;
     const double lam = static_cast<double>(k) / static_cast<double>(k + 1);
     primalUpdate<float>(p, j, q, xc, xi, s, step, pw, lam, last);
+}
+
+__global__ void __launch_bounds__(kBlock) primalLongFinish(IterArgs<float> p, LongTileArgs t, int koff) {
+    longFinishColumn(p, t, static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x), koff);
+}
+
+// The finish of the long columns and the sliced-ELL step of the short ones in
+// one launch: blocks [0, finish_blocks) finish long columns (first, so they
+// overlap the short columns instead of trailing them), the rest run
+// primalSellStep's work.  Same per-thread work as the two launches.
+template <int U, bool ST>
+__global__ void __launch_bounds__(kBlock, sellMinBlocks<float, true>())
+    primalSellFinish(IterArgs<float> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
+                     const float* __restrict__ val, int koff, int begin, int end, LongTileArgs t, int finish_blocks) {
+    const int b = static_cast<int>(blockIdx.x);
+    if (b < finish_blocks) {
+        longFinishColumn(p, t, b * kBlock + static_cast<int>(threadIdx.x), koff);
+        return;
+    }
+    const int r = (b - finish_blocks) * kBlock + static_cast<int>(threadIdx.x);
+    if (begin + r >= end) return;
+    primalSellFrom<U, float, ST, false, true>(p, idx, val, begin + r, hdr[r / kSlice], koff);
 }
 
 // Sliced-ELL shapes of the single-LP engine: kNumShapes + k for k < kEngSell,
@@ -674,8 +696,15 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
         if (d.lt_C > 0) {
             const LongTileArgs t = d.tiles();
             primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R, d.lt_maxcols), s>>>(ia, t, k);
+            ++n;
+            if (d.n > d.nlP && isSell(d.shapeP) && hotPrimal<T>(d) == 0) {
+                const int fb = sellGrid(d.nlP);
+                PDLPX_ENG_SELL_SWITCH(d.shapeP, (primalSellFinish<UU, SS><<<fb + sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
+                                                   ia, d.sp_hdr, d.sp_idx, d.sp_v32, k, d.nlP, d.n, t, fb)));
+                return n + 1;
+            }
             primalLongFinish<<<sellGrid(d.nlP), kBlock, 0, s>>>(ia, t, k);
-            n += 2;
+            ++n;
             if (d.n > d.nlP) {
                 launchPrimalShort<T>(d, ia, d.shapeP, k, s);
                 ++n;
