@@ -167,10 +167,17 @@ def barrier(pg):
         torch.cuda.synchronize()
 
 
-def rank_share(count: int, rank: int, world: int) -> range:
-    """The contiguous share of `count` independent items that rank `rank` of
-    `world` works on (sizes differ by at most one)."""
-    return range(count * rank // world, count * (rank + 1) // world)
+def rank_lps(sizes, rank: int, world: int) -> list[int]:
+    """The batch LPs (indices into `sizes`, (m, n) pairs) that rank `rank` of
+    `world` solves: the engine's longest-processing-time sharding
+    (pdlpx_shard_lps) on the per-iteration work m + n + 8 n of each LP (the
+    generator draws 4-12 nonzeros per column), so the ranks' shares of work,
+    not of LP counts, are balanced."""
+    if world <= 1:
+        return list(range(len(sizes)))
+    from mipx_b200.pdlp import shard_lps
+    owner = shard_lps([m + 9 * n for m, n in sizes], world)
+    return [k for k in range(len(sizes)) if owner[k] == rank]
 
 
 class ClockSampler:
@@ -504,7 +511,7 @@ def batch_line(rank, world, local, count: int) -> dict:
     from mipx_b200.pdlp import PdlpOptions, PdlpSolver, Precision, Status, batch_solve
     tol = dict(primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL, device=local)
     sizes = G.batch_sizes(count, seed=5)
-    lps = [G.random_lp(sizes[k][0], sizes[k][1], 4, 12, 1000 + k)[0] for k in rank_share(count, rank, world)]
+    lps = [G.random_lp(sizes[k][0], sizes[k][1], 4, 12, 1000 + k)[0] for k in rank_lps(sizes, rank, world)]
     batch_solve(lps[:4], PdlpOptions(verbose=False, max_iter=400, **tol))  # warm-up (module load)
     t0 = time.perf_counter()
     out = batch_solve(lps, PdlpOptions(verbose=False, **tol))

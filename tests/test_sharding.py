@@ -52,11 +52,16 @@ def test_shard_edge_cases():
         shard_lps([1, 2], 0)
 
 
-def test_bench_rank_share_covers_every_lp_once():
+def test_bench_rank_lps_balances_work_and_covers_every_lp_once():
+    """bench.py's batch line under torchrun: every LP on exactly one rank, and the
+    ranks' shares of work (m + 9 n) within 1 % of each other on the 512-LP
+    workload (its lognormal sizes make equal LP counts uneven in work)."""
     sys.path.insert(0, str(ROOT))
     import bench
-    for count in (0, 1, 7, 512):
-        for world in (1, 2, 3, 8):
-            shares = [list(bench.rank_share(count, r, world)) for r in range(world)]
-            assert sorted(k for s in shares for k in s) == list(range(count))
-            assert max(map(len, shares)) - min(map(len, shares)) <= 1
+    from mipx_b200 import generators as G
+    sizes = G.batch_sizes(512, seed=5)
+    for world in (1, 2, 4, 8):
+        shares = [bench.rank_lps(sizes, r, world) for r in range(world)]
+        assert sorted(k for s in shares for k in s) == list(range(len(sizes)))
+        work = [sum(sizes[k][0] + 9 * sizes[k][1] for k in s) for s in shares]
+        assert max(work) <= 1.01 * min(work), work
