@@ -166,6 +166,12 @@ typedef struct pdlpx_options {
                                          a graph of per-class launches: 1 on, 0 (default) off.  Packs
                                          with CSR tiles or 16-entry rounds, and the request server's
                                          packs, keep the graph.  Identical results either way */
+    int32_t sell_window;              /* single-LP engine, sliced-ELL sides: the short rows are renumbered
+                                         longest first inside windows of this many rows; 0 (default): one
+                                         window, the whole side.  A window keeps each row within that many
+                                         places of its original position (for LPs whose numbering gives
+                                         the gathers locality) */
+    int32_t reserved[1];
 } pdlpx_options;
 
 /* Image of mipx::LpResult (lp_solver.h:11-16) plus engine diagnostics. */

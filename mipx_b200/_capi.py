@@ -42,7 +42,7 @@ class Options(C.Structure):
         ("spmv_group_at", i32), ("autotune", i32), ("shape_primal", i32), ("shape_dual", i32), ("batch_pack_mb", i32),
         ("batch_compact", i32), ("batch_sell", i32), ("scale_on_device", i32), ("sell", i32),
         ("reference_fixed_columns", i32), ("hot_cache", i32),
-        ("long_tiles", i32), ("batch_persistent", i32),
+        ("long_tiles", i32), ("batch_persistent", i32), ("sell_window", i32), ("reserved", i32 * 1),
     ]
 
 

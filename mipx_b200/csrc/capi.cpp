@@ -107,6 +107,7 @@ void pdlpx_options_default(pdlpx_options* o) {
     o->hot_cache = 0;
     o->long_tiles = -1;
     o->batch_persistent = 0;
+    o->sell_window = 0;
 }
 
 const char* pdlpx_error_string(int32_t code) {

@@ -905,13 +905,6 @@ bool timeUp(std::chrono::steady_clock::time_point t0, double lim) {
 
 }  // namespace
 
-// Rows per window inside which a sliced-ELL side's short rows are sorted by
-// length: slices of 32 rows then hold rows of nearly equal length (on the
-// 500k x 2M power-law LP 5% padding, against 100% for 256-row windows), while
-// every row stays within 4096 places of where it was, so whatever locality
-// the other side's gathers had survives the renumbering.
-constexpr int32_t kSellWindow = 4096;
-
 // f(begin, end) over contiguous blocks of [0, count) on up to 16 host threads
 // (one below 1M entries of `work`); the blocks write disjoint output.
 template <class F>
@@ -932,12 +925,21 @@ static void hostBlocks(size_t work, int64_t count, F&& f) {
 // Device numbering of one matrix side's rows.  Rows far longer than the rest
 // (more entries than max(64, 8 x the mean)) come first, longest first; the
 // other rows follow -- sorted by length (longest first, stable) inside windows
-// of kSellWindow rows when the side is stored as sliced ELL, else in their
-// original order.  `sell_opt` is the option (-1 automatic: sliced ELL when the
+// of `window` rows (option sell_window; by default the whole side) when the
+// side is stored as sliced ELL, else in their original order.  Sorting puts
+// rows of nearly equal length into each 32-row slice (on the 500k x 2M
+// power-law LP 5 % padding), hands the block scheduler the heaviest slices
+// first, and, over the whole side, puts the most-gathered rows of a power-law
+// LP next to each other in the vector the other side gathers.  Measured on that
+// LP (B200, live step times, primal / dual): windows of 4,096 rows 115.0 /
+// 78.7 us, whole-side order for the columns 94.4 / 75.0, for the rows 116.2 /
+// 71.8, for both 96.5 / 68.4 (solve 12.61 -> 10.54 s).  A window keeps every
+// row within `window` places of where it was, for LPs whose original numbering
+// gives the other side's gathers locality.  `sell_opt` is the option (-1 automatic: sliced ELL when the
 // short rows' mean length is at most 64; 1 whenever there are short rows;
 // 0 never); `sell` receives the decision.  Returns the number of long rows;
 // `order` stays empty for the identity.
-static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int32_t>& order) {
+static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int32_t>& order, int64_t window) {
     order.clear();
     sell = false;
     const int32_t rows = a.rows;
@@ -959,10 +961,10 @@ static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int
     if (!sht.empty())
         sell = sell_opt > 0 || (sell_opt < 0 && static_cast<double>(zs) <= 64.0 * static_cast<double>(sht.size()));
     if (sell) {
-        const int64_t windows = (static_cast<int64_t>(sht.size()) + kSellWindow - 1) / kSellWindow;
+        const int64_t windows = (static_cast<int64_t>(sht.size()) + window - 1) / window;
         hostBlocks(sht.size() * 16, windows, [&](int64_t w0, int64_t w1) {
             for (int64_t w = w0; w < w1; ++w) {
-                const size_t b = static_cast<size_t>(w) * kSellWindow, e = std::min(sht.size(), b + kSellWindow);
+                const size_t b = static_cast<size_t>(w) * window, e = std::min(sht.size(), b + static_cast<size_t>(window));
                 std::stable_sort(sht.begin() + b, sht.begin() + e, [&](int32_t x, int32_t y) { return len(x) > len(y); });
             }
         });
@@ -1198,8 +1200,9 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
                           : o.shape_primal > kNumShapes                                           ? 1
                                                                                                    : o.sell;
     bool sellD = false, sellP = false;
-    d.nlD = sideOrder(sc_in.a, sellD_opt, sellD, ro);
-    d.nlP = sideOrder(sc_in.at, sellP_opt, sellP, co);
+    const int64_t window = o.sell_window > 0 ? o.sell_window : std::numeric_limits<int32_t>::max();
+    d.nlD = sideOrder(sc_in.a, sellD_opt, sellD, ro, window);
+    d.nlP = sideOrder(sc_in.at, sellP_opt, sellP, co, window);
     const bool perm = !ro.empty() || !co.empty();
     ScaledLp permuted;
     if (perm) permuteScaled(sc_in, ro, co, permuted, d.rpos, d.cpos);

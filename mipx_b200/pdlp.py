@@ -138,10 +138,11 @@ class PdlpOptions:
     hot_cache: int = 0
     long_tiles: int = -1
     batch_persistent: bool = False
+    sell_window: int = 0
 
     def to_c(self) -> _capi.Options:
-        # every field of pdlpx_options is set here, so no library call is
-        # needed to build the struct
+        # every field of pdlpx_options but `reserved` (zero) is set here, so
+        # no library call is needed to build the struct
         o = _capi.Options()
         for f in fields(self):
             if f.name == "stop_flag":
