@@ -15,8 +15,8 @@
 // 32-row slices, entries column-major inside a slice and padded to the
 // slice's longest row, so a warp's load of the k-th entries of its 32 rows is
 // one coalesced 128-byte (FP32) request and every thread owns one row; the
-// rows of each 256-row tile are renumbered longest first (stable) so a slice's
-// rows have similar lengths.  The renumbering is a relabelling of the LP's
+// rows of each LP are renumbered longest first (stable) so a slice's rows have
+// similar lengths and the heaviest tiles come first.  The renumbering is a relabelling of the LP's
 // variables and constraints, undone when the results are read back.  Long
 // rows keep CSR with a G-lane group per row.  The FP64 check pass and the
 // power iteration read CSR.
@@ -550,18 +550,17 @@ struct SideOrder {
 };
 
 // Renumbering of `rows` CSR rows padded to `padded`: identity for CSR sides;
-// for sliced-ELL sides, rows sorted by length (longest first, stable) inside
-// each tile of `tile` rows, then the slice lengths.
-void orderSide(const std::vector<int32_t>& ptr, int32_t rows, int64_t padded, int tile, bool sell, SideOrder& so) {
+// for sliced-ELL sides, rows sorted by length over the whole LP (longest
+// first, stable), then the slice lengths.  (Sorting inside each 256-row tile
+// only measured 2.91 s against 2.84 s for the 512-LP workload on B200: the
+// whole-LP order puts the heaviest tiles first.)
+void orderSide(const std::vector<int32_t>& ptr, int32_t rows, int64_t padded, bool sell, SideOrder& so) {
     so.order.resize(rows);
     std::iota(so.order.begin(), so.order.end(), 0);
     if (sell) {
-        for (int32_t t0 = 0; t0 < rows; t0 += tile) {
-            const int32_t t1 = std::min<int32_t>(rows, t0 + tile);
-            std::stable_sort(so.order.begin() + t0, so.order.begin() + t1, [&](int32_t a, int32_t b) {
-                return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
-            });
-        }
+        std::stable_sort(so.order.begin(), so.order.end(), [&](int32_t a, int32_t b) {
+            return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
+        });
         const int64_t slices = padded / kSlice;
         so.slice_len.assign(slices, 0);
         so.entries = 0;
@@ -1716,8 +1715,8 @@ int32_t prepareItem(const pdlpx_lp& in, const pdlpx_options& o, Item& it) {
     it.nrt = static_cast<int>((static_cast<int64_t>(lp.m) + td - 1) / td);
     it.np = static_cast<int64_t>(it.nct) * tp;
     it.mp = static_cast<int64_t>(it.nrt) * td;
-    orderSide(it.sc.at.ptr, lp.n, it.np, tp, isSell(it.shapeP), it.cols);
-    orderSide(it.sc.a.ptr, lp.m, it.mp, td, isSell(it.shapeD), it.rows);
+    orderSide(it.sc.at.ptr, lp.n, it.np, isSell(it.shapeP), it.cols);
+    orderSide(it.sc.a.ptr, lp.m, it.mp, isSell(it.shapeD), it.rows);
     it.bytes = itemBytes(it, mixed);
     return PDLPX_OK;
 }
