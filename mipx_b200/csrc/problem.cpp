@@ -193,9 +193,15 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
             a.ptr[i + 1] = static_cast<int32_t>(a.idx.size());
         }
     } else {
+        // the copy of a large matrix on host threads (blocks of entries)
         a.ptr = lp.a.ptr;
-        a.idx = lp.a.idx;
-        a.val = lp.a.val;
+        a.idx.resize(lp.a.idx.size());
+        a.val.resize(lp.a.val.size());
+        const int64_t z = static_cast<int64_t>(lp.a.idx.size());
+        forBlocks(hostThreads(static_cast<size_t>(z)), z, [&](int, int64_t k0, int64_t k1) {
+            std::copy(lp.a.idx.begin() + k0, lp.a.idx.begin() + k1, a.idx.begin() + k0);
+            std::copy(lp.a.val.begin() + k0, lp.a.val.begin() + k1, a.val.begin() + k0);
+        });
     }
 
     const auto t1 = clk::now();
