@@ -156,8 +156,13 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<T>())
     dualSellStep(IterArgs<T> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                  const T* __restrict__ val, int koff, int begin, int end) {
     const int r = static_cast<int>(blockIdx.x) * kBlock + static_cast<int>(threadIdx.x);
+    const int2 h = hdr[min(r, end - begin - 1) / kSlice];
+    // the primal step before this one writes the x_refl gathered here and
+    // reads the y written here
+    pdlWait();
+    pdlTrigger();
     if (begin + r >= end) return;
-    dualSellFrom<U, T, ST>(p, idx, val, begin + r, hdr[r / kSlice], koff);
+    dualSellFrom<U, T, ST>(p, idx, val, begin + r, h, koff);
 }
 
 // ---- sliced-ELL steps with the hot prefix of the gathered vector in shared memory
@@ -250,6 +255,9 @@ __global__ void __launch_bounds__(kTileBlock, 1) primalLongTiles(IterArgs<float>
     const int j0 = t.gb[g], ncol = t.gb[g + 1] - j0;
     const int* __restrict__ off = t.off + static_cast<size_t>(c) * t.nl + j0;
     for (int q = static_cast<int>(threadIdx.x); q <= ncol; q += kTileBlock) so[q] = __ldg(off + q);
+    // the dual step before this one writes the y copied here
+    pdlWait();
+    pdlTrigger();
     const int r0 = c * t.R;
     fillHot(ys, p.yg + r0, min(t.R, p.m - r0));  // ends with the block barrier
     const int lane = static_cast<int>(threadIdx.x) % kTileLanes;
@@ -313,7 +321,11 @@ __global__ void __launch_bounds__(kBlock, sellMinBlocks<float, true>())
     primalSellFinish(IterArgs<float> p, const int2* __restrict__ hdr, const int* __restrict__ idx,
                      const float* __restrict__ val, int koff, int begin, int end, LongTileArgs t, int finish_blocks) {
     const int b = static_cast<int>(blockIdx.x);
+    // the tile launch before this one writes the partials the finish blocks
+    // read; the short columns read only what earlier kernels wrote
+    pdlTrigger();
     if (b < finish_blocks) {
+        pdlWait();
         longFinishColumn(p, t, b * kBlock + static_cast<int>(threadIdx.x), koff);
         return;
     }
@@ -633,6 +645,26 @@ const double* sellVals<double>(const DeviceLp& d, bool primal) {
 
 static int sellGrid(int64_t rows) { return static_cast<int>(std::max<int64_t>(1, (rows + kBlock - 1) / kBlock)); }
 
+// A launch with programmatic stream serialization: the kernel may begin while
+// the one before it on the stream finishes (it calls pdlWait before reading
+// what that kernel writes).  Inside a stream capture the edge becomes a
+// programmatic dependency of the graph.
+template <class... KArgs, class... Args>
+static cudaError_t launchPdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Shared memory per block of a hot kernel running `minb` blocks per SM: the
 // prefix's share of the SM, within the device limits (1 KB of each block's
 // share is the runtime's).  Shared memory is carved out of the SM's L1, which
@@ -716,8 +748,8 @@ void launchDualShort(const DeviceLp& d, const IterArgs<T>& ia, int shape, int k,
                                       <<<sellGrid(d.m - d.nlD), kBlock, bytes, s>>>(
                                           ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m, H)));
     } else if (isSell(shape)) {
-        PDLPX_ENG_SELL_SWITCH(shape, (dualSellStep<UU, T, SS><<<sellGrid(d.m - d.nlD), kBlock, 0, s>>>(
-                                         ia, d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
+        PDLPX_ENG_SELL_SWITCH(shape, (launchPdl(dualSellStep<UU, T, SS>, sellGrid(d.m - d.nlD), kBlock, 0, s, ia,
+                                                d.sd_hdr, d.sd_idx, sellVals<T>(d, false), k, d.nlD, d.m)));
     } else {
         PDLPX_SHAPE_SWITCH(shape, (dualStep<GG, RR, UU, T><<<gridForShape(d.m - d.nlD, shape), kBlock, 0, s>>>(
                                       ia, k, d.nlD, d.m)));
@@ -731,12 +763,12 @@ int launchPrimal(const DeviceLp& d, const IterArgs<T>& ia, int k, cudaStream_t s
     if constexpr (sizeof(T) == 4) {
         if (d.lt_C > 0) {
             const LongTileArgs t = d.tiles();
-            primalLongTiles<<<d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R, d.lt_maxcols), s>>>(ia, t, k);
+            launchPdl(primalLongTiles, d.lt_C * d.lt_G, kTileBlock, tileSmemBytes(d.lt_R, d.lt_maxcols), s, ia, t, k);
             ++n;
             if (d.n > d.nlP && isSell(d.shapeP) && hotPrimal<T>(d) == 0) {
                 const int fb = sellGrid(d.nlP);
-                PDLPX_ENG_SELL_SWITCH(d.shapeP, (primalSellFinish<UU, SS><<<fb + sellGrid(d.n - d.nlP), kBlock, 0, s>>>(
-                                                   ia, d.sp_hdr, d.sp_idx, d.sp_v32, k, d.nlP, d.n, t, fb)));
+                PDLPX_ENG_SELL_SWITCH(d.shapeP, (launchPdl(primalSellFinish<UU, SS>, fb + sellGrid(d.n - d.nlP), kBlock, 0,
+                                                           s, ia, d.sp_hdr, d.sp_idx, d.sp_v32, k, d.nlP, d.n, t, fb)));
                 return n + 1;
             }
             primalLongFinish<<<sellGrid(d.nlP), kBlock, 0, s>>>(ia, t, k);

@@ -589,6 +589,16 @@ __global__ void __launch_bounds__(kBlock) dualStep(IterArgs<T> p, int koff, int 
                          koff);
 }
 
+// ---- programmatic dependent launch ------------------------------------------
+// Step kernels launched with programmatic stream serialization may start while
+// the kernel before them finishes its last wave.  pdlWait() returns once every
+// grid this one depends on has completed and its writes are visible; code
+// before it may read only data that no kernel still running writes.
+// pdlTrigger() lets the next such kernel be scheduled once every block of this
+// one has called it.  Both are no-ops for a kernel launched the usual way.
+__device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- sliced ELL (SELL-32) step ----------------------------------------------
 // A matrix side stored as 32-row slices: entry k of the slice's row `lane` sits
 // at hdr.x + k * 32 + lane, hdr.y is the slice's longest row, and shorter rows
