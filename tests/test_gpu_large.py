@@ -164,3 +164,22 @@ def test_powerlaw_full_size_certificate():
     assert np.all(x >= lp.col_lower - 1e-9) and np.all(x <= lp.col_upper + 1e-9)
     rp, gap = _duality_certificate(lp, x, y)
     assert rp <= 1e-6 and gap <= 2e-6, (rp, gap, r.objective)
+
+
+def test_sell_window_changes_only_the_numbering():
+    """sell_window limits the length sort of the sliced-ELL rows to windows;
+    the numbering is undone on read back, so both orders reach the same optimum
+    (to 1e-6 relative) with x and y in the caller's numbering."""
+    lp, _ = G.powerlaw_lp(20000, 80000, 2, 2000, 10.0, 0.01, 1e3, 5)
+    out = []
+    for w in (0, 4096):
+        s = PdlpSolver()
+        s.setOptions(PdlpOptions(verbose=False, primal_tol=TOL, dual_tol=TOL, optimality_tol=TOL,
+                                 max_solve_seconds=120, sell_window=w))
+        s.load(lp)
+        r = s.solve()
+        assert r.status == Status.Optimal, (w, r)
+        x = s.getPrimalValues()
+        assert _feasibility(lp, x) <= 2 * TOL
+        out.append(r.objective)
+    assert GC.rel_err(out[0], out[1]) <= GC.OBJ_TOL, out
