@@ -992,7 +992,16 @@ static int32_t sideOrder(const Csr& a, int sell_opt, bool& sell, std::vector<int
     auto len = [&](int32_t x) { return a.ptr[x + 1] - a.ptr[x]; };
     if (!sht.empty())
         sell = sell_opt > 0 || (sell_opt < 0 && static_cast<double>(zs) <= 64.0 * static_cast<double>(sht.size()));
-    if (sell) {
+    if (sell && static_cast<int64_t>(sht.size()) <= window) {
+        // one window: a stable counting sort by length (short rows have at
+        // most thr entries), the same order as the stable comparison sort
+        std::vector<int64_t> start(static_cast<size_t>(thr) + 2, 0);
+        for (int32_t x : sht) ++start[static_cast<size_t>(thr - len(x)) + 1];
+        for (size_t q = 1; q < start.size(); ++q) start[q] += start[q - 1];
+        std::vector<int32_t> out(sht.size());
+        for (int32_t x : sht) out[static_cast<size_t>(start[static_cast<size_t>(thr - len(x))]++)] = x;
+        sht.swap(out);
+    } else if (sell) {
         const int64_t windows = (static_cast<int64_t>(sht.size()) + window - 1) / window;
         hostBlocks(sht.size() * 16, windows, [&](int64_t w0, int64_t w1) {
             for (int64_t w = w0; w < w1; ++w) {
