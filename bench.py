@@ -88,7 +88,9 @@ def parse():
     p.add_argument("--batch-lps", type=int, default=512)
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serving-requests", type=int, default=512)
-    p.add_argument("--serving-rates", default="20,200,2000", help="arrival rates (requests/s) of the serving line")
+    p.add_argument("--serving-rates", default="5,20,200,2000",
+                   help="arrival rates (requests/s) of the serving line; rates below the server's capacity "
+                        "(~14 node LPs/s) send at most 128 requests")
     p.add_argument("--verbose", action="store_true")
     p.add_argument("--profile-large", type=int, default=0, metavar="M",
                    help="profiling run: one solve of an M x 4M power-law LP, no JSON line")
@@ -581,13 +583,16 @@ def serving_line(local, requests: int, rates) -> dict:
     out["single_lp_fp64_lps_per_sec"] = 4 / single
     out["single_lp_fp64_seconds_per_lp"] = single / 4
     for rate in rates:
-        arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, requests))
+        # below capacity a stream of 128 requests shows the unqueued latency
+        # without stretching the run (512 requests at 5/s would take 100 s)
+        count = requests if rate >= 20 else min(requests, 128)
+        arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, count))
         with Server(PdlpOptions(**tol), max_packs=4, max_pack_lps=32, batch_window_ms=50) as srv:
             tb = srv.submit(base)
             srv.wait(tb)
             start = time.perf_counter()
             tickets = []
-            for k, nd in enumerate(nodes):
+            for k, nd in enumerate(nodes[:count]):
                 d = start + arrivals[k] - time.perf_counter()
                 if d > 0:
                     time.sleep(d)
@@ -595,9 +600,10 @@ def serving_line(local, requests: int, rates) -> dict:
             res = [srv.wait(t)[0] for t in tickets]
             end = time.perf_counter()
             st = srv.stats()
-        lps = requests / (end - start)
+        lps = count / (end - start)
         out[f"rate_{int(rate)}"] = {
-            "offered_req_per_sec": rate, "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "offered_req_per_sec": rate, "requests": count, "p50_latency_s": st["p50_latency_s"],
+            "p99_latency_s": st["p99_latency_s"],
             "lps_per_sec": lps, "optimal": sum(1 for r in res if r.status == Status.Optimal),
             "iterations_median": float(np.median([r.iterations for r in res])),
             "speedup_vs_single_lp_fp64": lps / out["single_lp_fp64_lps_per_sec"]}
