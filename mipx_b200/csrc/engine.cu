@@ -954,6 +954,15 @@ static void hostBlocks(size_t work, int64_t count, F&& f) {
     for (auto& th : ts) th.join();
 }
 
+// out = the FP32 roundings of v, on host threads for large arrays.
+static void toFloat(const std::vector<double>& v, std::vector<float>& out) {
+    out.resize(v.size());
+    const int64_t n = static_cast<int64_t>(v.size());
+    hostBlocks(v.size(), n, [&](int64_t b, int64_t e) {
+        for (int64_t k = b; k < e; ++k) out[static_cast<size_t>(k)] = static_cast<float>(v[static_cast<size_t>(k)]);
+    });
+}
+
 // Device numbering of one matrix side's rows.  Rows far longer than the rest
 // (more entries than max(64, 8 x the mean)) come first, longest first; the
 // other rows follow -- sorted by length (longest first, stable) inside windows
@@ -1472,10 +1481,10 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
     PDLPX_CK(up(d.at_v64, sc.at.val.data(), 8 * nnz));
     std::vector<float> f32;
     if (mixed) {
-        f32.assign(sc.a.val.begin(), sc.a.val.end());
+        toFloat(sc.a.val, f32);
         PDLPX_CK(up(d.a_v32, f32.data(), 4 * nnz));
         PDLPX_CK(cudaStreamSynchronize(s));
-        f32.assign(sc.at.val.begin(), sc.at.val.end());
+        toFloat(sc.at.val, f32);
         PDLPX_CK(up(d.at_v32, f32.data(), 4 * nnz));
         std::vector<ColPack<float>> cp;
         std::vector<RowPack<float>> rp;
@@ -1492,7 +1501,8 @@ static int32_t buildDevice(std::unique_ptr<DeviceLp>& dp, const ScaledLp& sc_in,
         if ((e = up(idx, h.idx.data(), 4 * h.idx.size())) != cudaSuccess) return e;
         if ((e = up(v64, h.val.data(), 8 * h.val.size())) != cudaSuccess) return e;
         if (v32 != nullptr) {
-            std::vector<float> f(h.val.begin(), h.val.end());
+            std::vector<float> f;
+            toFloat(h.val, f);
             if ((e = up(v32, f.data(), 4 * f.size())) != cudaSuccess) return e;
             if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
         }
