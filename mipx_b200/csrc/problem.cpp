@@ -206,7 +206,22 @@ void buildScaled(const HostLp& lp, const pdlpx_options& o, ScaledLp& s, const Ru
 
     const auto t1 = clk::now();
     // Ruiz: alternate row and column infinity-norm equilibration, scale 1/sqrt(max).
-    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0 && !(ruiz && ruiz(a, s.row_scale, s.col_scale, o.ruiz_iterations))) {
+    bool ruiz_done = false;
+    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0 && ruiz) {
+        ruiz_done = ruiz(a, s.row_scale, s.col_scale, o.ruiz_iterations);
+        if (!ruiz_done) {
+            // the device path may have written part of its result before it
+            // failed: the host loop starts again from the unscaled values
+            const double tol = o.matrix_zero_tol;
+            size_t q = 0;
+            for (int32_t i = 0; i < m; ++i)
+                for (int32_t k = lp.a.ptr[i]; k < lp.a.ptr[i + 1]; ++k)
+                    if (!(tol > 0.0) || std::abs(lp.a.val[k]) >= tol) a.val[q++] = lp.a.val[k];
+            std::fill(s.row_scale.begin(), s.row_scale.end(), 1.0);
+            std::fill(s.col_scale.begin(), s.col_scale.end(), 1.0);
+        }
+    }
+    if (o.do_ruiz_scaling && m > 0 && n > 0 && a.nnz() > 0 && !ruiz_done) {
         std::vector<double> cmax(static_cast<size_t>(n));
         for (int32_t pass = 0; pass < o.ruiz_iterations; ++pass) {
             for (int32_t i = 0; i < m; ++i) {

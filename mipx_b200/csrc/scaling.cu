@@ -129,20 +129,18 @@ bool ruizOnDevice(Csr& a, std::vector<double>& row_scale, std::vector<double>& c
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "launch");
     if (verbose && (e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e, "synchronize");
     const auto t2 = clk::now();
-    // read back into new arrays: the caller's stay untouched unless everything succeeded
-    std::vector<double> v2(static_cast<size_t>(nnz)), r2(static_cast<size_t>(m)), c2(static_cast<size_t>(n));
-    if ((e = cudaMemcpyAsync(v2.data(), val, 8 * static_cast<size_t>(nnz), d2h, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(r2.data(), rs, 8 * static_cast<size_t>(m), d2h, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(c2.data(), cs, 8 * static_cast<size_t>(n), d2h, s)) != cudaSuccess)
+    // read back into the caller's arrays (already touched memory: no page
+    // faults during the copy); a failure from here on leaves them partly
+    // written, and the caller restarts from the unscaled values
+    if ((e = cudaMemcpyAsync(a.val.data(), val, 8 * static_cast<size_t>(nnz), d2h, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(row_scale.data(), rs, 8 * static_cast<size_t>(m), d2h, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(col_scale.data(), cs, 8 * static_cast<size_t>(n), d2h, s)) != cudaSuccess)
         return fail(e, "read back");
     cudaFreeAsync(d, s);
     d = nullptr;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e, "synchronize");
     cudaStreamDestroy(s);
     cudaSetDevice(prev);
-    a.val.swap(v2);
-    row_scale.swap(r2);
-    col_scale.swap(c2);
     if (verbose) {
         auto sec = [](clk::time_point x, clk::time_point y) { return std::chrono::duration<double>(y - x).count(); };
         std::printf("PDLP device Ruiz: set-up + upload %.3fs, %d passes %.3fs, read back %.3fs\n", sec(t0, t1), passes,
