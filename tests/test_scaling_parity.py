@@ -16,6 +16,9 @@ CASES = [
     ("medium_nopc", F.medium_lp, {"do_pock_chambolle_scaling": False}),
     ("medium_norescale", F.medium_lp, {"do_bound_obj_rescaling": False}),
     ("filter", F.filter_lp, {"matrix_zero_tol": 1e-10}),
+    # the device Ruiz passes asked for: on a GPU they run there; without one the
+    # attempt fails and the host loop restarts from the filtered, unscaled copy
+    ("filter_device", F.filter_lp, {"matrix_zero_tol": 1e-10, "scale_on_device": 1}),
     ("maximize", F.maximize_lp, {}),
     ("ranged", F.ranged_lp, {"ruiz_iterations": 3}),
     ("rand", lambda: G.random_lp(300, 700, 4, 12, 9)[0], {}),
