@@ -344,6 +344,20 @@ int32_t pdlpx_batch_solve_devices(int32_t count, const pdlpx_lp* lps, const pdlp
                                   const int32_t* devices, int32_t ndev, pdlpx_result* results,
                                   double* const* x_out, double* const* y_out);
 
+/* The grid barrier of the persistent batch cycle (option batch_persistent) run
+ * on its own: `rounds` barriers over `blocks` cooperative blocks of one warp on
+ * `device`.  No counterpart in the reference.  Each block waits on the
+ * barrier's generation word for at most 2^22 polls of a 64 ns sleep (about
+ * 0.3-1 s); a block that runs out sets the error word and returns, and so does
+ * every other block at its next barrier.  stall != 0 preloads the arrival
+ * count so that no barrier completes: every block runs out.  Returns PDLPX_OK
+ * when every barrier completed, PDLPX_E_TIMEOUT when one ran out (the status
+ * pdlpx_batch_solve returns then), PDLPX_E_INVALID when the blocks do not fit
+ * one cooperative wave; *barrier_error receives the error word and *seconds
+ * (may be NULL) the launch's device time. */
+int32_t pdlpx_grid_barrier_check(int32_t device, int32_t blocks, int32_t rounds, int32_t stall,
+                                 int32_t* barrier_error, double* seconds);
+
 /* ---- request server: LP solves as they arrive, continuously batched ----
  * No counterpart in the reference (the MIP search there calls PdlpSolver::solve
  * once per LP).  Submitted LPs are copied and scaled by a pool of host threads,

@@ -122,6 +122,7 @@ SIGNATURES = [
     ("pdlpx_get_hot_prefix", i32, [C.c_void_p, i32, P_i32, P_i32]),
     ("pdlpx_get_long_tiles", i32, [C.c_void_p, P_i32, P_i32]),
     ("pdlpx_shard_lps", i32, [i32, C.POINTER(C.c_int64), i32, P_i32]),
+    ("pdlpx_grid_barrier_check", i32, [i32, i32, i32, i32, P_i32, P_f64]),
     ("pdlpx_batch_solve_devices", i32, [i32, C.POINTER(Lp), C.POINTER(Options), P_i32, i32, C.POINTER(Result),
                                         C.POINTER(P_f64), C.POINTER(P_f64)]),
     ("pdlpx_batch_solve", i32, [i32, C.POINTER(Lp), C.POINTER(Options), C.POINTER(Result),

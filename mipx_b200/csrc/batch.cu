@@ -303,6 +303,15 @@ __global__ void __launch_bounds__(kBlock, PDLPX_SELL_MIN_BLOCKS) packCycleSell(P
     }
 }
 
+// The grid barrier on its own: `rounds` barriers over a cooperative grid, with
+// the words laid out as in PersistArgs (bar[0] arrivals, bar[1] generation,
+// bar[2] the error word).
+__global__ void barrierRounds(unsigned* bar, int rounds) {
+    int* err = reinterpret_cast<int*>(bar + 2);
+    for (int r = 0; r < rounds; ++r)
+        if (!gridBarrier(bar, err)) return;
+}
+
 // ---- FP64 check pass, one partial per tile -----------------------------------
 template <int G, bool IND>
 __global__ void __launch_bounds__(kBlock) packCheckRows(PackArgs a, int tile0, int list0) {
@@ -2047,6 +2056,70 @@ int32_t batchSolveDevices(int32_t count, const pdlpx_lp* lps, const pdlpx_option
         }
     }
     return rc;
+}
+
+// Runs the persistent cycle's grid barrier alone (pdlpx_grid_barrier_check).
+// With `stall` the arrival word starts far above any grid size, so no arrival
+// completes a barrier: every block polls up to its limit, sets the error word
+// and returns, and the call reports PDLPX_E_TIMEOUT with the context intact.
+int32_t gridBarrierCheck(int32_t device, int32_t blocks, int32_t rounds, int32_t stall, int32_t* barrier_error,
+                         double* seconds, std::string& err) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        err = "grid barrier check: no device " + std::to_string(device);
+        return PDLPX_E_NO_DEVICE;
+    }
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, barrierRounds, 32, 0);
+    if (!coop || blocks > per_sm * sms) {
+        cudaGetLastError();
+        cudaSetDevice(prev);
+        err = "grid barrier check: " + std::to_string(blocks) + " blocks do not fit one cooperative wave (" +
+              std::to_string(per_sm * sms) + ")";
+        return PDLPX_E_INVALID;
+    }
+    const unsigned preset[4] = {stall ? (1u << 30) : 0u, 0u, 0u, 0u};
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    unsigned* d = nullptr;
+    int h_err = 0;
+    float ms = 0.0f;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev1);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d), sizeof(preset));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, preset, sizeof(preset), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ev0, s);
+    if (e == cudaSuccess) {
+        int r = rounds;
+        void* kargs[] = {&d, &r};
+        e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&barrierRounds), dim3(blocks), dim3(32), kargs,
+                                        0, s);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev1, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d + 2, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev0, ev1);
+    if (e != cudaSuccess) err = std::string("grid barrier check: ") + cudaGetErrorString(e);
+    if (s) cudaStreamSynchronize(s);
+    if (d) cudaFree(d);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (s) cudaStreamDestroy(s);
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return PDLPX_E_CUDA;
+    *barrier_error = h_err;
+    if (seconds) *seconds = ms / 1000.0;
+    if (h_err != 0) {
+        err = "grid barrier check: a grid barrier ran out of polls";
+        return PDLPX_E_TIMEOUT;
+    }
+    return PDLPX_OK;
 }
 
 }  // namespace pdlpx

@@ -431,6 +431,18 @@ int32_t pdlpx_batch_solve_devices(int32_t count, const pdlpx_lp* lps, const pdlp
     }
 }
 
+int32_t pdlpx_grid_barrier_check(int32_t device, int32_t blocks, int32_t rounds, int32_t stall,
+                                 int32_t* barrier_error, double* seconds) {
+    if (barrier_error == nullptr || blocks < 1 || rounds < 1) return PDLPX_E_INVALID;
+    try {
+        return pdlpx::gridBarrierCheck(device, blocks, rounds, stall, barrier_error, seconds, g_last_error);
+    } catch (const std::bad_alloc&) {
+        return PDLPX_E_NOMEM;
+    } catch (...) {
+        return PDLPX_E_INVALID;
+    }
+}
+
 int32_t pdlpx_csr_spmv(int32_t rows, int32_t cols, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx,
                        const double* val, const double* x, double* y, int32_t precision, int32_t group) {
     try {

@@ -118,6 +118,10 @@ int32_t batchSolveDevices(int32_t count, const pdlpx_lp* lps, const pdlpx_option
                           int32_t ndev, pdlpx_result* results, double* const* x_out, double* const* y_out,
                           std::string& err);
 
+// The persistent batch cycle's grid barrier run on its own (batch.cu).
+int32_t gridBarrierCheck(int32_t device, int32_t blocks, int32_t rounds, int32_t stall, int32_t* barrier_error,
+                         double* seconds, std::string& err);
+
 // Message returned by pdlpx_last_error(NULL) on this thread (calls without a handle).
 void setGlobalError(const std::string& msg);
 

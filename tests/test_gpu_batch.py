@@ -246,3 +246,24 @@ def test_persistent_cycle_gives_identical_results():
             np.testing.assert_array_equal(y, v)
         # the persistent launch replaces the per-class step launches of every cycle
         assert pers[0][0].kernel_launches < graph[0][0].kernel_launches
+
+
+def test_grid_barrier_wait_is_bounded():
+    """The persistent cycle's grid barrier waits a bounded time: with the arrival
+    count preloaded so that no barrier completes (a flag nothing sets), every
+    block runs out of polls, the call returns PDLPX_E_TIMEOUT with the error word
+    set, and the context stays usable for the next launch."""
+    import ctypes as C
+
+    from mipx_b200 import _capi
+    lib = _capi.load()
+    err, sec = C.c_int32(-1), C.c_double(-1.0)
+    assert lib.pdlpx_grid_barrier_check(0, 148, 1000, 0, C.byref(err), C.byref(sec)) == 0, lib.pdlpx_last_error(None)
+    assert err.value == 0 and 0.0 < sec.value < 5.0
+    err, sec = C.c_int32(-1), C.c_double(-1.0)
+    assert lib.pdlpx_grid_barrier_check(0, 4, 3, 1, C.byref(err), C.byref(sec)) == 6  # PDLPX_E_TIMEOUT
+    assert err.value == 1 and 0.0 < sec.value < 30.0
+    assert b"ran out" in lib.pdlpx_last_error(None)
+    err = C.c_int32(-1)
+    assert lib.pdlpx_grid_barrier_check(0, 148, 10, 0, C.byref(err), None) == 0
+    assert err.value == 0
