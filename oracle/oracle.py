@@ -31,7 +31,7 @@ _libs: dict = {}
 def reference_dir() -> Path | None:
     """The mipx source tree the reference libraries are compiled from:
     $MIPX_REFERENCE_DIR, else the checkout this build recipe reads
-    (/root/reference); None where neither exists (the GPU box, which uses the
+    (/root/reference); None where neither exists (a machine that only runs the
     libraries built beforehand)."""
     for cand in (os.environ.get("MIPX_REFERENCE_DIR"), "/root/reference"):
         if cand and (Path(cand) / "src" / "lp" / "pdlp.cpp").exists():
