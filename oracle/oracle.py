@@ -30,7 +30,7 @@ _libs: dict = {}
 
 def reference_dir() -> Path | None:
     """The mipx source tree the reference libraries are compiled from:
-    $MIPX_REFERENCE_DIR, else the checkout this build recipe reads
+    $MIPX_REFERENCE_DIR, else the checkout the oracle's Makefile recipe reads
     (/root/reference); None where neither exists (a machine that only runs the
     libraries built beforehand)."""
     for cand in (os.environ.get("MIPX_REFERENCE_DIR"), "/root/reference"):

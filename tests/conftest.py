@@ -16,7 +16,7 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session", autouse=True)
 def _built_libraries():
-    """Engine and oracle libraries (built here when missing; the GPU box gets them prebuilt)."""
+    """Engine and oracle libraries (built here when missing; a machine without the sources gets them prebuilt)."""
     from mipx_b200 import build as engine_build
     engine_build.build()
     from oracle import oracle
